@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LBM step on the 256^3 gravity-down scene.
+
+Workload (one "step" = one worker tick of src/worker.js:96-100: Sim.step,
+absorbDeadCells, RigidSphere.step): 256x256x256 grid, FP32, walls on every
+face, liquid below a seeded +-0.5-cell sinusoidal interface at y = 96, tau 0.6,
+tauPhi 0.8, sigma 1e-3, W 4, rhoL/rhoG = 10, g = -1e-5, a density-2 sphere of
+radius 24 at (128, 200, 128).  Synthetic data; the state (5.3 GB) is far larger
+than L2, so no flush is needed between steps.
+
+Metric: MLUPS counting every cell of the grid each step (test/bench.mjs:28-29).
+  value  -- K device-resident steps (lbm_run_coupled), CUDA events on the
+            library's stream, max over ranks, all ranks' cells summed.
+  e2e    -- the public Python API as src/worker.js drives it: per step
+            sim.step / absorbDeadCells / RigidSphere.step (sphere state and plan
+            up, impulses down), and the RG8 volume read back every 2 steps.
+
+`python bench.py --impl reference` times the CPU restatement of the reference's
+step (oracle/, OpenMP over the host's cores) on the same scene.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "claude-vibe-code-raytracing_b200")
+for _p in (ROOT, PKG, os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "D3Q27+D3Q7 MLUPS (all cells per step), 256^3 plain FP32"
+UNIT = "MLUPS"
+BYTES_PER_CELL = {"f32": 313, "f16": 177, "bf16": 177, "f64": 626}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f64"])
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--rows", type=int, default=0)
+    ap.add_argument("--zchunk", type=int, default=0)
+    return ap.parse_args()
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def max_over_ranks(v, ws, local):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return float("nan")
+        sm = [num(r[1]) for r in rows]
+        mx = max(num(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(size, storage):
+    """DRAM bytes per fused-kernel launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get(f"{storage}_{size}")
+    except Exception:
+        return None
+
+
+def cpu_baseline(size, steps, threads=None):
+    """The oracle (CPU restatement of src/sim.js + src/solid.js) on the same scene,
+    OpenMP over the host's cores; `steps` timed steps after one warm-up."""
+    import scenes
+    from oracle import oracle
+    threads = threads or os.cpu_count()
+    sim, sol = scenes.cfg2(oracle.OracleSim, oracle.OracleSphere, n=size)
+    sim.set_threads(threads)
+    scenes.substep(sim, sol)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        scenes.substep(sim, sol)
+    dt = (time.perf_counter() - t0) / steps
+    n = size ** 3
+    return {"value": n / dt * 1e-6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} timed steps (+1 warm-up) of the {size}^3 scene, "
+                      f"{dt * 1e3:.0f} ms/step, oracle/lbm_oracle.c with OpenMP"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    size = args.size
+    budget_s = 150.0
+    import scenes
+    from oracle import oracle
+    threads = os.cpu_count()
+    sim, sol = scenes.cfg2(oracle.OracleSim, oracle.OracleSphere, n=size)
+    sim.set_threads(threads)
+    for _ in range(max(1, min(args.warmup, 2))):
+        scenes.substep(sim, sol)
+    t0 = time.perf_counter()
+    done = 0
+    while done < args.steps:
+        scenes.substep(sim, sol)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = (time.perf_counter() - t0) / done
+    v = size ** 3 / dt * 1e-6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": done, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 math, f32 storage",
+        "data": "synthetic",
+        "config": {"workload": f"gravity-down pool {size}^3, sphere r={24 * size // 256}",
+                   "grid": [size] * 3, "storage": "f32", "l2": "state > L2, no flush"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{done} of {args.steps} steps of the {size}^3 scene "
+                                   f"(bounded to ~{budget_s:.0f} s), CPU restatement of the "
+                                   "reference with OpenMP; the reference JS needs Node, absent here"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import torch
+
+    import scenes
+    from b200lbm import RigidSphere, Sim
+    from b200lbm._capi import LbmSphere, check, lib
+
+    dev = local
+    torch.cuda.set_device(dev)
+    size = args.size
+    L = lib()
+
+    sim, sol = scenes.cfg2(lambda *a: Sim(*a, storage=args.storage, device=dev), RigidSphere, n=size)
+    h = sim.handle
+    if args.rows:
+        check(h, L.lbm_set_fused_config(h, args.rows, args.zchunk or 32))
+    sim._sync()
+    sph = (LbmSphere * 1)()
+    sol.to_c(sph[0])
+    stream = torch.cuda.ExternalStream(L.lbm_stream(h), device=dev)
+
+    # warm-up through the device loop
+    check(h, L.lbm_run_coupled(h, sph, 1, args.warmup, 0, None))
+
+    # ---------------- timed region: K device-resident steps
+    n_cells = size ** 3
+    interior = (size - 2) ** 3
+    clocks = Clocks(dev)
+    c0 = C.c_int64()
+    check(h, L.lbm_launch_count(h, C.byref(c0)))
+    check(h, L.lbm_fused_timing(h, 1))
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    check(h, L.lbm_run_coupled(h, sph, 1, args.steps, 0, None))
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    fused_ms = C.c_double()
+    fused_n = C.c_int64()
+    check(h, L.lbm_fused_timing_query(h, C.byref(fused_ms), C.byref(fused_n)))
+    check(h, L.lbm_fused_timing(h, 0))
+    c1 = C.c_int64()
+    check(h, L.lbm_launch_count(h, C.byref(c1)))
+    ms_max = max_over_ranks(ms, ws, local)
+    value = ws * n_cells * args.steps / (ms_max * 1e-3) * 1e-6
+    sol.from_c(sph[0])
+
+    # roofline of the fused kernel
+    peak, peak_kind = measured_peak()
+    per_launch_ms = fused_ms.value / max(1, fused_n.value)
+    bpc = BYTES_PER_CELL[args.storage]
+    achieved = bpc * interior / (per_launch_ms * 1e-3) / 1e9
+    traffic = ncu_traffic(size, args.storage)
+
+    # ---------------- e2e through the public API (worker.js cadence)
+    e2e_steps = min(args.e2e_steps, args.steps)
+    frame = np.empty(n_cells * 2, dtype=np.uint8)
+    substeps = 2
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    x0 = (C.c_uint64(), C.c_uint64())
+    check(h, L.lbm_transfer_bytes(h, C.byref(x0[0]), C.byref(x0[1])))
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        sim.step(sol)
+        sol.absorbDeadCells(sim)
+        sol.step(1.0, sim.gravity)
+        if (s + 1) % substeps == 0:
+            sim.packVolume(frame)
+    sim.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, ws, local)
+    e2e_value = ws * n_cells * e2e_steps / e2e_s * 1e-6
+    x1 = (C.c_uint64(), C.c_uint64())
+    check(h, L.lbm_transfer_bytes(h, C.byref(x1[0]), C.byref(x1[1])))
+    h2d = (x1[0].value - x0[0].value) / e2e_steps
+    d2h = (x1[1].value - x0[1].value) / e2e_steps
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(size, args.cpu_steps)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+            "config": {"workload": f"gravity-down pool {size}^3 with a density-2 sphere r={24 * size // 256}",
+                       "grid": [size] * 3, "storage": args.storage, "parallelism": f"replicas x{ws}",
+                       "l2": "state 5.3 GB > 126 MB L2, no flush needed",
+                       "fused_rows": args.rows or 8, "zchunk": args.zchunk or 32},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind,
+                         "kernel": "k_fused_step", "kernel_ms": per_launch_ms,
+                         "bytes_per_cell": bpc, "cells_per_launch": interior},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                    "path": "Sim.step + absorbDeadCells + RigidSphere.step, packVolume every 2 steps"},
+            "gpu_launches": int(c1.value - c0.value),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "sphere": {"cx": sol.cx, "cy": sol.cy, "cz": sol.cz},
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,318 @@
+"""Sim -- the reference's `class Sim` (src/sim.js:29-601) backed by the
+sm_100a CUDA library through its C ABI.
+
+Same constructor, methods, fields and parameter properties as the reference, so
+its driver loop (src/worker.js:94-115) and test scripts read unchanged:
+
+    sim = Sim(40, 28, 40); sim.initFlat(14); sim.tau = 0.7
+    solid = RigidSphere(40, 28, 40, cx=20, cy=6, cz=20, r=4, density=1.6)
+    sim.step(solid); solid.absorbDeadCells(sim); solid.step(1.0, sim.gravity)
+    sim.phi[sim.idx(6, 6, 6)]
+
+Field arrays (f, h, rho, phi, ux, ...) are host mirrors in the reference
+layout.  Reading one downloads it if the device has moved on since the last
+read; writing elements marks it dirty and it is uploaded before the next
+device call -- the JS code's direct typed-array access (src/worker.js:58-69)
+keeps working.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import FIELDS, LbmImpulse, LbmParams, check, lib
+from .solid import impulse_array, spheres_of, to_c_array
+
+_PARAM_NAMES = ("tau", "tauPhi", "sigma", "gravity", "rhoL", "rhoG", "W", "mobility")
+# upload order: phi before h (h may be stored relative to phi), tags last
+_UPLOAD_ORDER = ("phi", "rho", "ux", "uy", "uz", "f", "f2", "h", "h2", "usx", "usy", "usz",
+                 "gx", "gy", "gz", "lap", "bodyFx", "bodyFy", "bodyFz", "tag", "tagPrev",
+                 "phiPrev")
+
+
+class TrackedArray(np.ndarray):
+    """numpy array that tells its Sim when elements are written, and refreshes
+    itself from the device when read after the device state moved on."""
+
+    def __array_finalize__(self, obj):
+        self._sim = getattr(obj, "_sim", None)
+        self._field = getattr(obj, "_field", None)
+
+    def _fresh(self):
+        sim = self._sim
+        if sim is not None and self._field is not None:
+            sim._refresh(self._field)
+
+    def __getitem__(self, key):
+        self._fresh()
+        return super().__getitem__(key)
+
+    def __setitem__(self, key, value):
+        self._fresh()
+        super().__setitem__(key, value)
+        if self._sim is not None and self._field is not None:
+            self._sim._dirty.add(self._field)
+
+    def __array_wrap__(self, arr, context=None, return_scalar=False):
+        # results of arithmetic on a field are plain arrays, not field mirrors
+        arr = np.asarray(arr).view(np.ndarray)
+        return arr[()] if return_scalar else arr
+
+    def fill(self, value):
+        super().fill(value)
+        if self._sim is not None and self._field is not None:
+            self._sim._dirty.add(self._field)
+
+    def set(self, src, offset=0):  # TypedArray.prototype.set
+        self[offset:offset + len(src)] = np.asarray(src)
+
+
+def _np_dtype(field):
+    return np.uint8 if field in ("tag", "tagPrev") else np.float32
+
+
+class Sim:
+    """class Sim (src/sim.js:29-601) on the GPU."""
+
+    def __init__(self, nx, ny, nz, storage="f32", device=0):
+        h = C.c_void_p()
+        rc = lib().lbm_create(nx, ny, nz, _capi.STORAGE[storage], device, C.byref(h))
+        if rc != _capi.OK:
+            raise _capi.LbmError(rc, f"lbm_create({nx},{ny},{nz},{storage}) failed")
+        object.__setattr__(self, "_h", h)
+        object.__setattr__(self, "nx", nx)
+        object.__setattr__(self, "ny", ny)
+        object.__setattr__(self, "nz", nz)
+        object.__setattr__(self, "n", nx * ny * nz)
+        object.__setattr__(self, "storage", storage)
+        # src/sim.js:88-95
+        object.__setattr__(self, "_params", dict(tau=0.6, tauPhi=0.7, sigma=0.012, gravity=0.0010,
+                                                 rhoL=1.0, rhoG=0.05, W=4.0, mobility=0.02))
+        object.__setattr__(self, "_params_dirty", True)
+        object.__setattr__(self, "_mirror", {})
+        object.__setattr__(self, "_mirror_version", {})
+        object.__setattr__(self, "_version", 0)
+        object.__setattr__(self, "_dirty", set())
+        # lattice offsets (src/sim.js:71-85), read-only views for callers
+        nxny = nx * ny
+        dirs = [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1),
+                (1, 1, 0), (-1, -1, 0), (1, -1, 0), (-1, 1, 0), (1, 0, 1), (-1, 0, -1), (1, 0, -1),
+                (-1, 0, 1), (0, 1, 1), (0, -1, -1), (0, 1, -1), (0, -1, 1), (1, 1, 1), (-1, -1, -1),
+                (1, 1, -1), (-1, -1, 1), (1, -1, 1), (-1, 1, -1), (-1, 1, 1), (1, -1, -1)]
+        off27 = np.array([-(ez * nxny + ey * nx + ex) for ex, ey, ez in dirs], dtype=np.int32)
+        object.__setattr__(self, "neighOffset27", off27)
+        object.__setattr__(self, "fOffset27", off27 * 27 + np.arange(27, dtype=np.int32))
+        object.__setattr__(self, "neighOffset7", off27[:7].copy())
+        object.__setattr__(self, "hOffset7", off27[:7] * 7 + np.arange(7, dtype=np.int32))
+
+    # ------------------------------------------------------------ lifetime
+    def close(self):
+        h = self.__dict__.get("_h")
+        if h:
+            lib().lbm_destroy(h)
+            self.__dict__["_h"] = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ------------------------------------------------------------ params
+    def __getattr__(self, name):
+        d = self.__dict__
+        if name in _PARAM_NAMES:
+            return d["_params"][name]
+        if name in FIELDS:
+            self._refresh(name)
+            return d["_mirror"][name]
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name in _PARAM_NAMES:
+            self._params[name] = float(value)
+            self.__dict__["_params_dirty"] = True
+        elif name in FIELDS:
+            arr = getattr(self, name)
+            arr[...] = value
+        else:
+            object.__setattr__(self, name, value)
+
+    # ------------------------------------------------------------ mirrors
+    def _count(self, field):
+        if field in ("f", "f2"):
+            return self.n * 27
+        if field in ("h", "h2"):
+            return self.n * 7
+        return self.n
+
+    def _refresh(self, field):
+        d = self.__dict__
+        mirror = d["_mirror"]
+        if field in mirror and (d["_mirror_version"][field] == d["_version"] or field in d["_dirty"]):
+            return
+        arr = mirror.get(field)
+        if arr is None:
+            base = np.empty(self._count(field), dtype=_np_dtype(field))
+            arr = base.view(TrackedArray)
+            arr._sim = self
+            arr._field = field
+            mirror[field] = arr
+        buf = np.asarray(arr).view(np.ndarray)
+        check(self._h, lib().lbm_download_field(self._h, FIELDS[field], buf.ctypes.data_as(C.c_void_p),
+                                                buf.size))
+        d["_mirror_version"][field] = d["_version"]
+
+    def _sync(self):
+        """Push parameter changes and host-side field writes to the device."""
+        d = self.__dict__
+        if d["_params_dirty"]:
+            p = LbmParams(**{k: d["_params"][k] for k in _PARAM_NAMES})
+            check(self._h, lib().lbm_set_params(self._h, C.byref(p)))
+            d["_params_dirty"] = False
+        if d["_dirty"]:
+            uploaded = set(d["_dirty"])
+            for field in _UPLOAD_ORDER:
+                if field in uploaded:
+                    buf = np.ascontiguousarray(np.asarray(d["_mirror"][field]).view(np.ndarray))
+                    check(self._h, lib().lbm_upload_field(self._h, FIELDS[field],
+                                                          buf.ctypes.data_as(C.c_void_p), buf.size))
+            d["_dirty"].clear()
+            old = d["_version"]
+            d["_version"] = old + 1
+            # mirrors that matched the device still do; the uploaded ones now match
+            for f in d["_mirror"]:
+                if d["_mirror_version"][f] == old or f in uploaded:
+                    d["_mirror_version"][f] = d["_version"]
+            if "phiPrev" in uploaded:
+                # phiPrev writes stay host-side until the next retag overwrites it
+                d["_mirror_version"]["phiPrev"] = d["_version"]
+
+    def _moved(self):
+        self.__dict__["_version"] += 1
+
+    # ------------------------------------------------------------ reference API
+    def idx(self, x, y, z):
+        return ((z * self.ny) + y) * self.nx + x
+
+    def rhoFromPhi(self, p):
+        return self.rhoG + p * (self.rhoL - self.rhoG)
+
+    def initFlat(self, waterlineY):
+        """src/sim.js:112-134 (tanh profile, wall tags, f = w, h = w*phi, then seedHydrostatic)."""
+        self.__dict__["_dirty"].clear()
+        self._sync()
+        check(self._h, lib().lbm_init_flat(self._h, float(waterlineY)))
+        self._moved()
+
+    def seedHydrostatic(self):
+        """src/sim.js:144-173"""
+        self._sync()
+        check(self._h, lib().lbm_seed_hydrostatic(self._h))
+        self._moved()
+
+    def computePhiGradients(self):
+        self._sync()
+        check(self._h, lib().lbm_compute_phi_gradients(self._h))
+        self._moved()
+
+    def retagCells(self, solid):
+        sp = spheres_of(solid)
+        self._sync()
+        arr = to_c_array(sp)
+        check(self._h, lib().lbm_retag_cells(self._h, arr, len(sp)))
+        self._moved()
+
+    def handleFreshCells(self, solid=None):
+        self._sync()
+        check(self._h, lib().lbm_handle_fresh_cells(self._h))
+        self._moved()
+
+    def collidePhase(self):
+        self._sync()
+        check(self._h, lib().lbm_collide_phase(self._h))
+        self._moved()
+
+    def streamPhase(self):
+        self._sync()
+        check(self._h, lib().lbm_stream_phase(self._h))
+        self._moved()
+
+    def collideHydro(self):
+        self._sync()
+        check(self._h, lib().lbm_collide_hydro(self._h))
+        self._moved()
+
+    def streamHydroAndMacro(self, solid):
+        sp = spheres_of(solid)
+        self._sync()
+        arr = to_c_array(sp)
+        out = impulse_array(len(sp))
+        check(self._h, lib().lbm_stream_hydro_and_macro(self._h, arr, len(sp), out))
+        self._moved()
+        for i, b in enumerate(sp):
+            b.add_impulse(out[i])
+
+    def step(self, solid):
+        """src/sim.js:202-210, as one fused device step."""
+        sp = spheres_of(solid)
+        self._sync()
+        arr = to_c_array(sp)
+        out = impulse_array(len(sp))
+        check(self._h, lib().lbm_step(self._h, arr, len(sp), out))
+        self._moved()
+        for i, b in enumerate(sp):
+            b.add_impulse(out[i])
+
+    def _absorb_dead(self, spheres):
+        """RigidSphere.absorbDeadCells(sim) (src/solid.js:87-101) on the device."""
+        if not spheres:
+            return
+        self._sync()
+        arr = to_c_array(spheres)
+        out = impulse_array(len(spheres))
+        check(self._h, lib().lbm_absorb_dead_cells(self._h, arr, len(spheres), out))
+        for i, b in enumerate(spheres):
+            b.add_impulse(out[i])
+
+    def packVolume(self, out=None, solidContains=None):
+        """src/sim.js:586-600 (second argument ignored, as in the reference)."""
+        self._sync()
+        if out is None:
+            out = np.empty(self.n * 2, dtype=np.uint8)
+        buf = np.asarray(out).view(np.ndarray)
+        if buf.dtype != np.uint8 or buf.size < self.n * 2 or not buf.flags.c_contiguous:
+            raise ValueError("packVolume needs a contiguous uint8 buffer of 2*n bytes")
+        check(self._h, lib().lbm_pack_volume(self._h, buf.ctypes.data_as(C.c_void_p)))
+        return out
+
+    # ------------------------------------------------------------ extras
+    def synchronize(self):
+        check(self._h, lib().lbm_synchronize(self._h))
+
+    def last_sets(self):
+        """(fresh, dead) cell index arrays found at the last retag, scan order."""
+        nf, nd = C.c_int(), C.c_int()
+        check(self._h, lib().lbm_last_sets(self._h, C.byref(nf), C.byref(nd)))
+        fr = np.zeros(max(1, nf.value), dtype=np.int32)
+        de = np.zeros(max(1, nd.value), dtype=np.int32)
+        check(self._h, lib().lbm_download_sets(
+            self._h, fr.ctypes.data_as(C.POINTER(C.c_int32)), nf.value,
+            de.ctypes.data_as(C.POINTER(C.c_int32)), nd.value))
+        return fr[:nf.value], de[:nd.value]
+
+    def launch_count(self):
+        v = C.c_int64()
+        check(self._h, lib().lbm_launch_count(self._h, C.byref(v)))
+        return v.value
+
+    def device_bytes(self):
+        v = C.c_size_t()
+        check(self._h, lib().lbm_device_bytes(self._h, C.byref(v)))
+        return v.value

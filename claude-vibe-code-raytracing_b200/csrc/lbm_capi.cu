@@ -1,0 +1,1030 @@
+// C ABI of the B200-native LBM step (declarations and reference citations in
+// include/lbm_b200.h).  Host orchestration only: allocation, field transfers,
+// the sphere bounding boxes, and the launch sequence of every entry point.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "lbm_kernels.cuh"
+#include "lbm_state.h"
+
+using namespace lbm;
+
+namespace {
+
+int fail(lbm_sim *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(lbm_sim *h, const char *what, cudaError_t e) {
+  cudaGetLastError();  // clear a sticky-free error so the handle stays usable
+  return fail(h, e == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                            \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_fail(h, #call, e_); \
+  } while (0)
+
+#define CKL(what)                                           \
+  do {                                                      \
+    cudaError_t e_ = cudaGetLastError();                    \
+    if (e_ != cudaSuccess) return cuda_fail(h, what, e_);   \
+  } while (0)
+
+OpsBase *ops_for(int storage) {
+  switch (storage) {
+    case LBM_STORE_F32: return make_ops_f32();
+    case LBM_STORE_F16: return make_ops_f16();
+    case LBM_STORE_BF16: return make_ops_bf16();
+    case LBM_STORE_F64: return make_ops_f64();
+  }
+  return nullptr;
+}
+
+size_t pop_bytes_of(int storage) {
+  return storage == LBM_STORE_F64 ? 8 : storage == LBM_STORE_F32 ? 4 : 2;
+}
+size_t mac_bytes_of(int storage) { return storage == LBM_STORE_F64 ? 8 : 4; }
+
+long long pitch_of(long long n) { return (n + 127) / 128 * 128; }
+
+int dalloc(lbm_sim *h, void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_fail(h, "cudaMalloc", e);
+  }
+  h->deviceBytes += bytes;
+  return LBM_OK;
+}
+
+#define DALLOC(ptr, bytes)                                        \
+  do {                                                            \
+    int rc_ = dalloc(h, (void **)&(ptr), (size_t)(bytes));        \
+    if (rc_ != LBM_OK) return rc_;                                \
+  } while (0)
+
+// Every host<->device copy of the ABI goes through here and is counted
+// (lbm_transfer_bytes), so callers can report the bytes a step moves.
+cudaError_t copy_async(lbm_sim *h, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind,
+                       cudaStream_t s) {
+  if (kind == cudaMemcpyHostToDevice) h->h2dBytes += bytes;
+  if (kind == cudaMemcpyDeviceToHost) h->d2hBytes += bytes;
+  return cudaMemcpyAsync(dst, src, bytes, kind, s);
+}
+
+int ensure_staging(lbm_sim *h, size_t bytes) {
+  if (h->stagingBytes >= bytes) return LBM_OK;
+  if (h->staging) {
+    cudaFree(h->staging);
+    h->deviceBytes -= h->stagingBytes;
+    h->staging = nullptr;
+    h->stagingBytes = 0;
+  }
+  DALLOC(h->staging, bytes);
+  h->stagingBytes = bytes;
+  return LBM_OK;
+}
+
+int ensure_scalar(lbm_sim *h, void **arr) {
+  if (*arr) return LBM_OK;
+  size_t bytes = (size_t)h->n * h->ops->macro_bytes();
+  DALLOC(*arr, bytes);
+  CK(cudaMemsetAsync(*arr, 0, bytes, h->stream));
+  return LBM_OK;
+}
+
+int ensure_phase_scratch(lbm_sim *h) {
+  for (int a = 0; a < 4; a++) {
+    int rc = ensure_scalar(h, &h->grad[a]);
+    if (rc) return rc;
+  }
+  for (int a = 0; a < 3; a++) {
+    int rc = ensure_scalar(h, &h->us[a]);
+    if (rc) return rc;
+  }
+  return LBM_OK;
+}
+
+Box interior(const lbm_sim *h) {
+  Box b;
+  b.lo[0] = b.lo[1] = b.lo[2] = 1;
+  b.hi[0] = h->nx - 2;
+  b.hi[1] = h->ny - 2;
+  b.hi[2] = h->nz - 2;
+  return b;
+}
+
+Box spheres_box(const lbm_sim *h, const lbm_sphere *sp, int ns) {
+  Box u{{1, 1, 1}, {0, 0, 0}};
+  for (int b = 0; b < ns; b++)
+    u = box_union(u, sphere_box(sp[b].cx, sp[b].cy, sp[b].cz, sp[b].r, h->nx, h->ny, h->nz));
+  return u;
+}
+
+int check_spheres(lbm_sim *h, const lbm_sphere *sp, int ns) {
+  if (ns < 0 || ns > LBM_MAX_SPHERES) return fail(h, LBM_ERR_ARG, "nspheres out of range");
+  if (ns > 0 && !sp) return fail(h, LBM_ERR_ARG, "spheres is NULL");
+  return LBM_OK;
+}
+
+int upload_plan(lbm_sim *h) {
+  // pageable source: the copy is staged before cudaMemcpyAsync returns, so the
+  // host plan can be rewritten for the next call right away
+  CK(copy_async(h, h->dPlan, &h->hPlan, sizeof(Plan), cudaMemcpyHostToDevice, h->stream));
+  return LBM_OK;
+}
+
+// Fill the plan's solid set; when `targets` is true also lay out and clear the
+// per-sphere impulse arrays.
+int set_solids(lbm_sim *h, const lbm_sphere *sp, int ns, bool targets) {
+  SolidSet &ss = h->hPlan.ss;
+  memset(&ss, 0, sizeof(ss));
+  ss.nsph = ns;
+  long long off = 0;
+  int maxChunks = 1;
+  long long offs[LBM_MAX_SPHERES] = {0};
+  for (int b = 0; b < ns; b++) {
+    SphereDesc &d = ss.sph[b];
+    d.cx = sp[b].cx;
+    d.cy = sp[b].cy;
+    d.cz = sp[b].cz;
+    d.r = sp[b].r;
+    d.vx = sp[b].vx;
+    d.vy = sp[b].vy;
+    d.vz = sp[b].vz;
+    d.wx = sp[b].wx;
+    d.wy = sp[b].wy;
+    d.wz = sp[b].wz;
+    if (!targets) continue;
+    Box bx = box_grow(sphere_box(d.cx, d.cy, d.cz, d.r, h->nx, h->ny, h->nz), 1, h->nx, h->ny, h->nz);
+    ImpulseTarget &t = ss.imp[b];
+    long long cells = 0;
+    if (box_empty(bx)) {
+      t.lo[0] = t.lo[1] = t.lo[2] = 0;
+      t.dim[0] = t.dim[1] = t.dim[2] = 0;
+    } else {
+      for (int a = 0; a < 3; a++) {
+        t.lo[a] = bx.lo[a];
+        t.dim[a] = bx.hi[a] - bx.lo[a] + 1;
+      }
+      cells = box_cells(bx);
+    }
+    offs[b] = off;
+    off += cells;
+    maxChunks = std::max(maxChunks, (int)((cells + RED_CHUNK - 1) / RED_CHUNK));
+  }
+  h->hPlan.impDoubles = off * 6;
+  h->hPlan.redChunks = maxChunks;
+  if (!targets) return LBM_OK;
+  long long need = std::max(1LL, off * 6);
+  if (need > h->impCap) {
+    if (h->impAcc) {
+      cudaFree(h->impAcc);
+      h->deviceBytes -= h->impCap * sizeof(double);
+      h->impAcc = nullptr;
+    }
+    long long cap = need + need / 2;
+    DALLOC(h->impAcc, cap * sizeof(double));
+    h->impCap = cap;
+  }
+  long long pneed = (long long)std::max(ns, 1) * maxChunks * 6;
+  if (pneed > h->partialsCap) {
+    if (h->partials) {
+      cudaFree(h->partials);
+      h->deviceBytes -= h->partialsCap * sizeof(double);
+      h->partials = nullptr;
+    }
+    DALLOC(h->partials, pneed * sizeof(double));
+    h->partialsCap = pneed;
+  }
+  h->partialsChunks = maxChunks;
+  for (int b = 0; b < ns; b++) ss.imp[b].acc = h->impAcc + offs[b] * 6;
+  if (off > 0) CK(cudaMemsetAsync(h->impAcc, 0, off * 6 * sizeof(double), h->stream));
+  return LBM_OK;
+}
+
+int reduce_impulses(lbm_sim *h, double *d_out) {
+  int ns = h->hPlan.ss.nsph;
+  if (ns == 0) return LBM_OK;
+  dim3 g1(h->partialsChunks, ns);
+  k_impulse_reduce1<<<g1, 256, 0, h->stream>>>(&h->dPlan->ss, h->partials, h->partialsChunks);
+  k_impulse_reduce2<<<ns, 32, 0, h->stream>>>(&h->dPlan->ss, h->partials, h->partialsChunks, d_out);
+  h->launches += 2;
+  CKL("impulse reduction");
+  return LBM_OK;
+}
+
+int ensure_counts(lbm_sim *h, long long nch) {
+  if (nch <= h->countsCap) return LBM_OK;
+  if (h->counts) {
+    cudaFree(h->counts);
+    h->deviceBytes -= h->countsCap * sizeof(int2);
+    h->counts = nullptr;
+  }
+  DALLOC(h->counts, nch * sizeof(int2));
+  h->countsCap = nch;
+  return LBM_OK;
+}
+
+// Launch the fresh / dead compaction over the plan's box U (already on the
+// device); maxChunks bounds the plan's chunk count.
+int launch_compaction(lbm_sim *h, long long maxChunks) {
+  if (maxChunks <= 0) {
+    CK(cudaMemsetAsync(h->totals, 0, 2 * sizeof(int), h->stream));
+    h->listsValid = true;
+    return LBM_OK;
+  }
+  int rc = ensure_counts(h, maxChunks);
+  if (rc) return rc;
+  k_compact_count<<<(unsigned)maxChunks, COMPACT_THREADS, 0, h->stream>>>(h->tag, h->tagPrev, h->nx,
+                                                                            h->ny, h->dPlan, h->counts);
+  k_compact_scan<<<1, 1024, 0, h->stream>>>(h->counts, h->dPlan, h->totals);
+  k_compact_emit<<<(unsigned)maxChunks, COMPACT_THREADS, 0, h->stream>>>(
+      h->tag, h->tagPrev, h->nx, h->ny, h->dPlan, h->counts, h->fresh, h->dead, (int)h->listCap);
+  h->launches += 3;
+  CKL("fresh/dead compaction");
+  h->listsValid = true;
+  return LBM_OK;
+}
+
+// The fused step kernel, bracketed by CUDA events when timing is on.
+void launch_fused(lbm_sim *h) {
+  if (h->timing) {
+    if (h->evUsed == h->evStart.size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      h->evStart.push_back(a);
+      h->evStop.push_back(b);
+    }
+    cudaEventRecord(h->evStart[h->evUsed], h->stream);
+    h->ops->fused_step(h, h->cfg);
+    cudaEventRecord(h->evStop[h->evUsed], h->stream);
+    h->evUsed++;
+  } else {
+    h->ops->fused_step(h, h->cfg);
+  }
+}
+
+void set_box(lbm_sim *h, const Box &bx) {
+  h->hPlan.U = bx;
+  h->hPlan.ucells = box_cells(bx);
+  h->hPlan.nchunks = (int)((h->hPlan.ucells + COMPACT_CHUNK - 1) / COMPACT_CHUNK);
+}
+
+// fresh / dead lists over a box, scan order
+int compact_sets(lbm_sim *h, const Box &bx) {
+  set_box(h, bx);
+  int rc = upload_plan(h);
+  if (rc) return rc;
+  return launch_compaction(h, h->hPlan.nchunks);
+}
+
+void shift_boxes(lbm_sim *h, const Box &now) {
+  h->boxLastLast = h->boxLast;
+  h->boxLast = now;
+}
+
+int fetch_out(lbm_sim *h, const double *d_src, int ns, lbm_impulse *out) {
+  if (!out || ns == 0) return LBM_OK;
+  CK(copy_async(h, h->hOut, d_src, (size_t)ns * 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int b = 0; b < ns; b++) {
+    out[b].Fx = h->hOut[6 * b + 0];
+    out[b].Fy = h->hOut[6 * b + 1];
+    out[b].Fz = h->hOut[6 * b + 2];
+    out[b].Tx = h->hOut[6 * b + 3];
+    out[b].Ty = h->hOut[6 * b + 4];
+    out[b].Tz = h->hOut[6 * b + 5];
+  }
+  return LBM_OK;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    cudaGetDevice(&now);
+    if (prev >= 0 && now != prev) cudaSetDevice(prev);
+  }
+};
+
+__global__ void k_f32_to_real_d(double *dst, const float *src, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (double)src[i];
+}
+__global__ void k_real_d_to_f32(float *dst, const double *src, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (float)src[i];
+}
+
+// float32 host -> device scalar array of the handle's macro type
+int put_scalar(lbm_sim *h, void *dst, const float *host) {
+  size_t n = (size_t)h->n;
+  if (h->ops->macro_bytes() == 4) {
+    CK(copy_async(h, dst, host, n * 4, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    int rc = ensure_staging(h, n * 4);
+    if (rc) return rc;
+    CK(copy_async(h, h->staging, host, n * 4, cudaMemcpyHostToDevice, h->stream));
+    k_f32_to_real_d<<<nblocks(n, 256), 256, 0, h->stream>>>((double *)dst, (const float *)h->staging, n);
+    h->launches++;
+    CKL("convert");
+  }
+  return LBM_OK;
+}
+
+int get_scalar(lbm_sim *h, const void *src, float *host) {
+  size_t n = (size_t)h->n;
+  if (h->ops->macro_bytes() == 4) {
+    CK(copy_async(h, host, src, n * 4, cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    int rc = ensure_staging(h, n * 4);
+    if (rc) return rc;
+    k_real_d_to_f32<<<nblocks(n, 256), 256, 0, h->stream>>>((float *)h->staging, (const double *)src, n);
+    h->launches++;
+    CKL("convert");
+    CK(copy_async(h, host, h->staging, n * 4, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+void free_all(lbm_sim *h) {
+  void *ptrs[] = {h->F[0], h->F[1], h->H[0], h->H[1], h->tag, h->tagPrev, h->grad[0], h->grad[1],
+                  h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
+                  h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
+                  h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (int c = 0; c < 2; c++)
+    for (int a = 0; a < 5; a++)
+      if (h->mac[c][a]) cudaFree(h->mac[c][a]);
+  for (cudaEvent_t e : h->evStart) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->evStop) cudaEventDestroy(e);
+  if (h->hOut) cudaFreeHost(h->hOut);
+  if (h->hTotals) cudaFreeHost(h->hTotals);
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+size_t lbm_footprint_bytes(int nx, int ny, int nz, int storage) {
+  if (nx < 3 || ny < 3 || nz < 3 || storage < 0 || storage > 3) return 0;
+  long long n = (long long)nx * ny * nz;
+  long long pitch = pitch_of(n);
+  size_t pb = pop_bytes_of(storage), mb = mac_bytes_of(storage);
+  size_t bytes = 2 * (size_t)(27 + 7) * pitch * pb;  // F, H ping-pong
+  bytes += 2 * 5 * (size_t)n * mb;                     // macros ping-pong
+  bytes += 2 * (size_t)n;                              // tag, tagPrev
+  bytes += 2 * (size_t)n * sizeof(int);                // fresh / dead lists
+  return bytes;
+}
+
+int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
+  if (!out) return LBM_ERR_ARG;
+  *out = nullptr;
+  if (nx < 3 || ny < 3 || nz < 3) return LBM_ERR_ARG;
+  if ((long long)nx * ny * nz >= (1LL << 31)) return LBM_ERR_ARG;
+  OpsBase *ops = ops_for(storage);
+  if (!ops) return LBM_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LBM_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return LBM_ERR_ARG;
+  DeviceGuard g(device);
+  lbm_sim *h = new lbm_sim();
+  h->nx = nx;
+  h->ny = ny;
+  h->nz = nz;
+  h->storage = storage;
+  h->device = device;
+  h->ops = ops;
+  h->n = (long long)nx * ny * nz;
+  h->pitch = pitch_of(h->n);
+  h->params = lbm_params{0.6, 0.7, 0.012, 0.0010, 1.0, 0.05, 4.0, 0.02};  // src/sim.js:88-95
+  int rc = LBM_OK;
+  auto body = [&]() -> int {
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    size_t pb = ops->pop_bytes(), mb = ops->macro_bytes();
+    for (int c = 0; c < 2; c++) {
+      DALLOC(h->F[c], 27 * h->pitch * pb);
+      DALLOC(h->H[c], 7 * h->pitch * pb);
+      CK(cudaMemsetAsync(h->F[c], 0, 27 * h->pitch * pb, h->stream));
+      CK(cudaMemsetAsync(h->H[c], 0, 7 * h->pitch * pb, h->stream));
+      for (int a = 0; a < 5; a++) {
+        DALLOC(h->mac[c][a], h->n * mb);
+        CK(cudaMemsetAsync(h->mac[c][a], 0, h->n * mb, h->stream));
+      }
+    }
+    DALLOC(h->tag, h->n);
+    DALLOC(h->tagPrev, h->n);
+    CK(cudaMemsetAsync(h->tag, 0, h->n, h->stream));
+    CK(cudaMemsetAsync(h->tagPrev, 0, h->n, h->stream));
+    h->listCap = h->n;
+    DALLOC(h->fresh, h->listCap * sizeof(int));
+    DALLOC(h->dead, h->listCap * sizeof(int));
+    DALLOC(h->totals, 2 * sizeof(int));
+    CK(cudaMemsetAsync(h->totals, 0, 2 * sizeof(int), h->stream));
+    DALLOC(h->dOut, 2 * LBM_MAX_SPHERES * 6 * sizeof(double));
+    DALLOC(h->dSph, LBM_MAX_SPHERES * sizeof(lbm_sphere));
+    DALLOC(h->dPlan, sizeof(Plan));
+    CK(cudaMemsetAsync(h->dPlan, 0, sizeof(Plan), h->stream));
+    DALLOC(h->dPhiCol, (size_t)ny * sizeof(double));
+    CK(cudaMallocHost((void **)&h->hOut, 2 * LBM_MAX_SPHERES * 6 * sizeof(double)));
+    CK(cudaMallocHost((void **)&h->hTotals, 2 * sizeof(int)));
+    CK(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+  };
+  rc = body();
+  if (rc != LBM_OK) {
+    free_all(h);
+    delete h;
+    return rc;
+  }
+  // A fresh Sim has every cell FLUID (zeroed Uint8Array); the first retag
+  // covers the whole grid so the walls get their tags.
+  h->fullRetagSteps = 2;
+  *out = h;
+  return LBM_OK;
+}
+
+int lbm_destroy(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return LBM_OK;
+}
+
+const char *lbm_last_error(const lbm_sim *h) { return h ? h->err.c_str() : "null handle"; }
+
+int lbm_get_dims(const lbm_sim *h, int *nx, int *ny, int *nz, int *storage) {
+  if (!h) return LBM_ERR_ARG;
+  if (nx) *nx = h->nx;
+  if (ny) *ny = h->ny;
+  if (nz) *nz = h->nz;
+  if (storage) *storage = h->storage;
+  return LBM_OK;
+}
+
+int lbm_device_bytes(const lbm_sim *h, size_t *bytes) {
+  if (!h || !bytes) return LBM_ERR_ARG;
+  *bytes = h->deviceBytes;
+  return LBM_OK;
+}
+
+int lbm_set_params(lbm_sim *h, const lbm_params *p) {
+  if (!h || !p) return fail(h, LBM_ERR_ARG, "null");
+  h->params = *p;
+  return LBM_OK;
+}
+
+int lbm_get_params(const lbm_sim *h, lbm_params *p) {
+  if (!h || !p) return LBM_ERR_ARG;
+  *p = h->params;
+  return LBM_OK;
+}
+
+static size_t field_count(const lbm_sim *h, int field) {
+  if (field == LBM_FIELD_F || field == LBM_FIELD_F2) return (size_t)h->n * 27;
+  if (field == LBM_FIELD_H || field == LBM_FIELD_H2) return (size_t)h->n * 7;
+  return (size_t)h->n;
+}
+
+static int pops_transfer(lbm_sim *h, int field, const float *up, float *down) {
+  bool isH = field == LBM_FIELD_H || field == LBM_FIELD_H2;
+  bool second = field == LBM_FIELD_F2 || field == LBM_FIELD_H2;
+  int Q = isH ? 7 : 27;
+  long long chunk = std::min<long long>(h->n, 1 << 20);
+  int rc = ensure_staging(h, (size_t)chunk * Q * sizeof(float));
+  if (rc) return rc;
+  for (long long c0 = 0; c0 < h->n; c0 += chunk) {
+    long long cells = std::min(chunk, h->n - c0);
+    if (up) {
+      CK(copy_async(h, h->staging, up + c0 * Q, cells * Q * sizeof(float), cudaMemcpyHostToDevice,
+                         h->stream));
+      h->ops->upload_pops(h, isH, second ? 2 : 0, (const float *)h->staging, c0, cells);
+      CKL("upload populations");
+      CK(cudaStreamSynchronize(h->stream));
+    } else {
+      h->ops->download_pops(h, isH, second ? 2 : 1, (float *)h->staging, c0, cells);
+      CKL("download populations");
+      CK(copy_async(h, down + c0 * Q, h->staging, cells * Q * sizeof(float), cudaMemcpyDeviceToHost,
+                         h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+    }
+  }
+  return LBM_OK;
+}
+
+int lbm_upload_field(lbm_sim *h, int field, const void *host, size_t count) {
+  if (!h || !host) return fail(h, LBM_ERR_ARG, "null");
+  if (field < 0 || field >= LBM_FIELD_COUNT) return fail(h, LBM_ERR_ARG, "unknown field");
+  if (count != field_count(h, field)) return fail(h, LBM_ERR_ARG, "element count mismatch");
+  DeviceGuard g(h->device);
+  const float *src = (const float *)host;
+  size_t n = (size_t)h->n;
+  switch (field) {
+    case LBM_FIELD_F:
+    case LBM_FIELD_F2:
+    case LBM_FIELD_H:
+    case LBM_FIELD_H2:
+      return pops_transfer(h, field, src, nullptr);
+    case LBM_FIELD_TAG:
+    case LBM_FIELD_TAG_PREV:
+      CK(copy_async(h, field == LBM_FIELD_TAG ? h->tag : h->tagPrev, host, n, cudaMemcpyHostToDevice,
+                         h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      h->fullRetagSteps = 2;
+      h->listsValid = false;
+      return LBM_OK;
+    case LBM_FIELD_PHI_PREV:
+      // phiPrev is overwritten from phi by the next retagCells before anything
+      // reads it (src/sim.js:216-217); a write to it has no effect on the run.
+      return LBM_OK;
+    case LBM_FIELD_PHI: {
+      size_t mb = h->ops->macro_bytes();
+      void *old = nullptr;
+      bool off = !h->ops->phases_supported();
+      if (off) {
+        CK(cudaMalloc(&old, n * mb));
+      }
+      for (int c = 0; c < 2; c++) {
+        if (off) CK(copy_async(h, old, h->mac[c][0], n * mb, cudaMemcpyDeviceToDevice, h->stream));
+        int rc = put_scalar(h, h->mac[c][0], src);
+        if (rc) {
+          if (old) cudaFree(old);
+          return rc;
+        }
+        if (off) h->ops->reencode_h(h, c, old);
+      }
+      cudaError_t e = cudaStreamSynchronize(h->stream);
+      if (old) cudaFree(old);
+      if (e != cudaSuccess) return cuda_fail(h, "upload phi", e);
+      return LBM_OK;
+    }
+    case LBM_FIELD_RHO:
+    case LBM_FIELD_UX:
+    case LBM_FIELD_UY:
+    case LBM_FIELD_UZ: {
+      int a = field - LBM_FIELD_RHO + 1;
+      for (int c = 0; c < 2; c++) {
+        int rc = put_scalar(h, h->mac[c][a], src);
+        if (rc) return rc;
+      }
+      CK(cudaStreamSynchronize(h->stream));
+      return LBM_OK;
+    }
+    default: {
+      void **arr = nullptr;
+      if (field >= LBM_FIELD_USX && field <= LBM_FIELD_USZ) arr = &h->us[field - LBM_FIELD_USX];
+      else if (field >= LBM_FIELD_GX && field <= LBM_FIELD_LAP) arr = &h->grad[field - LBM_FIELD_GX];
+      else arr = &h->bf[field - LBM_FIELD_BODY_FX];
+      int rc = ensure_scalar(h, arr);
+      if (rc) return rc;
+      rc = put_scalar(h, *arr, src);
+      if (rc) return rc;
+      if (field >= LBM_FIELD_BODY_FX) {
+        for (int a = 0; a < 3; a++) {
+          rc = ensure_scalar(h, &h->bf[a]);
+          if (rc) return rc;
+        }
+        h->bfActive = true;
+      }
+      CK(cudaStreamSynchronize(h->stream));
+      return LBM_OK;
+    }
+  }
+}
+
+int lbm_download_field(lbm_sim *h, int field, void *host, size_t count) {
+  if (!h || !host) return fail(h, LBM_ERR_ARG, "null");
+  if (field < 0 || field >= LBM_FIELD_COUNT) return fail(h, LBM_ERR_ARG, "unknown field");
+  if (count != field_count(h, field)) return fail(h, LBM_ERR_ARG, "element count mismatch");
+  DeviceGuard g(h->device);
+  float *dst = (float *)host;
+  size_t n = (size_t)h->n;
+  switch (field) {
+    case LBM_FIELD_F:
+    case LBM_FIELD_F2:
+    case LBM_FIELD_H:
+    case LBM_FIELD_H2:
+      return pops_transfer(h, field, nullptr, dst);
+    case LBM_FIELD_TAG:
+    case LBM_FIELD_TAG_PREV:
+      CK(copy_async(h, host, field == LBM_FIELD_TAG ? h->tag : h->tagPrev, n, cudaMemcpyDeviceToHost,
+                         h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      return LBM_OK;
+    case LBM_FIELD_PHI_PREV:
+      return get_scalar(h, h->mac[1 - h->cur][0], dst);
+    case LBM_FIELD_PHI:
+    case LBM_FIELD_RHO:
+    case LBM_FIELD_UX:
+    case LBM_FIELD_UY:
+    case LBM_FIELD_UZ:
+      return get_scalar(h, h->mac[h->cur][field - LBM_FIELD_PHI], dst);
+    default: {
+      void *arr = nullptr;
+      if (field >= LBM_FIELD_USX && field <= LBM_FIELD_USZ) arr = h->us[field - LBM_FIELD_USX];
+      else if (field >= LBM_FIELD_GX && field <= LBM_FIELD_LAP) arr = h->grad[field - LBM_FIELD_GX];
+      else arr = h->bf[field - LBM_FIELD_BODY_FX];
+      if (!arr) {
+        memset(dst, 0, n * sizeof(float));
+        return LBM_OK;
+      }
+      return get_scalar(h, arr, dst);
+    }
+  }
+}
+
+int lbm_init_flat(lbm_sim *h, double waterlineY) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  std::vector<double> col(h->ny);
+  for (int y = 0; y < h->ny; y++) col[y] = 0.5 * (1 + tanh(2 * ((double)y - waterlineY) / h->params.W));
+  CK(copy_async(h, h->dPhiCol, col.data(), h->ny * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  h->ops->init_flat(h, h->dPhiCol);
+  CKL("init_flat");
+  h->ops->seed_hydrostatic(h);
+  CKL("seed_hydrostatic");
+  CK(cudaStreamSynchronize(h->stream));
+  h->boxLast = h->boxLastLast = Box{{1, 1, 1}, {0, 0, 0}};
+  h->fullRetagSteps = 0;
+  h->listsValid = false;
+  return LBM_OK;
+}
+
+int lbm_seed_hydrostatic(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  h->ops->seed_hydrostatic(h);
+  CKL("seed_hydrostatic");
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+static int need_phases(lbm_sim *h) {
+  if (!h->ops->phases_supported())
+    return fail(h, LBM_ERR_UNSUPPORTED,
+                "phase-by-phase entry points need FP32 or FP64 storage; FP16/BF16 run lbm_step only");
+  return ensure_phase_scratch(h);
+}
+
+int lbm_retag_cells(lbm_sim *h, const lbm_sphere *sp, int ns) {
+  if (!h) return LBM_ERR_ARG;
+  int rc = check_spheres(h, sp, ns);
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if ((rc = need_phases(h))) return rc;
+  if ((rc = set_solids(h, sp, ns, false))) return rc;
+  if ((rc = upload_plan(h))) return rc;
+  h->ops->retag_full(h);
+  CKL("retag");
+  shift_boxes(h, spheres_box(h, sp, ns));
+  h->lastRetagBox = interior(h);
+  h->fullRetagSteps = h->fullRetagSteps > 0 ? h->fullRetagSteps - 1 : 0;
+  h->listsValid = false;
+  return LBM_OK;
+}
+
+int lbm_handle_fresh_cells(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  if ((rc = compact_sets(h, h->lastRetagBox))) return rc;
+  h->ops->fresh_fill(h);
+  CKL("fresh cells");
+  return LBM_OK;
+}
+
+int lbm_compute_phi_gradients(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  h->ops->gradients(h);
+  CKL("gradients");
+  return LBM_OK;
+}
+
+int lbm_collide_phase(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  h->ops->collide_phase(h);
+  CKL("collidePhase");
+  return LBM_OK;
+}
+
+int lbm_stream_phase(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  h->ops->stream_phase(h);
+  CKL("streamPhase");
+  return LBM_OK;
+}
+
+int lbm_collide_hydro(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  h->ops->collide_hydro(h);
+  CKL("collideHydro");
+  return LBM_OK;
+}
+
+int lbm_stream_hydro_and_macro(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
+  if (!h) return LBM_ERR_ARG;
+  int rc = check_spheres(h, sp, ns);
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if ((rc = need_phases(h))) return rc;
+  if ((rc = set_solids(h, sp, ns, true))) return rc;
+  if ((rc = upload_plan(h))) return rc;
+  h->ops->stream_hydro_macro(h);
+  CKL("streamHydroAndMacro");
+  if (h->bfActive) {  // bodyF.fill(0) (src/sim.js:581)
+    for (int a = 0; a < 3; a++) CK(cudaMemsetAsync(h->bf[a], 0, h->n * h->ops->macro_bytes(), h->stream));
+    h->bfActive = false;
+  }
+  if ((rc = reduce_impulses(h, h->dOut))) return rc;
+  return fetch_out(h, h->dOut, ns, out);
+}
+
+int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
+  if (!h) return LBM_ERR_ARG;
+  int rc = check_spheres(h, sp, ns);
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if (h->bfActive) {
+    // A pending external body force is consumed by the phase-by-phase path,
+    // which reads it (src/sim.js:434-436, 558-560).
+    if ((rc = lbm_retag_cells(h, sp, ns))) return rc;
+    if ((rc = lbm_handle_fresh_cells(h))) return rc;
+    if ((rc = lbm_compute_phi_gradients(h))) return rc;
+    if ((rc = lbm_collide_phase(h))) return rc;
+    if ((rc = lbm_stream_phase(h))) return rc;
+    if ((rc = lbm_collide_hydro(h))) return rc;
+    return lbm_stream_hydro_and_macro(h, sp, ns, out);
+  }
+  if ((rc = set_solids(h, sp, ns, true))) return rc;
+  Box now = spheres_box(h, sp, ns);
+  Box U;
+  if (h->fullRetagSteps > 0) {
+    U = Box{{0, 0, 0}, {h->nx - 1, h->ny - 1, h->nz - 1}};
+    h->fullRetagSteps--;
+  } else {
+    U = box_union(box_union(now, h->boxLast), h->boxLastLast);
+  }
+  set_box(h, U);
+  h->hPlan.boxLast = h->boxLast;
+  h->hPlan.boxLastLast = h->boxLastLast;
+  if ((rc = upload_plan(h))) return rc;
+  h->ops->retag_box(h, h->hPlan.ucells);
+  CKL("retag box");
+  h->lastRetagBox = U;
+  if ((rc = launch_compaction(h, h->hPlan.nchunks))) return rc;
+  h->ops->fresh_fill(h);
+  CKL("fresh cells");
+  launch_fused(h);
+  CKL("fused step");
+  if ((rc = reduce_impulses(h, h->dOut))) return rc;
+  h->cur = 1 - h->cur;
+  shift_boxes(h, now);
+  return fetch_out(h, h->dOut, ns, out);
+}
+
+int lbm_absorb_dead_cells(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
+  if (!h) return LBM_ERR_ARG;
+  int rc = check_spheres(h, sp, ns);
+  if (rc) return rc;
+  if (ns == 0) return LBM_OK;
+  DeviceGuard g(h->device);
+  if (!h->listsValid && (rc = compact_sets(h, h->lastRetagBox))) return rc;
+  if ((rc = set_solids(h, sp, ns, false))) return rc;
+  if ((rc = upload_plan(h))) return rc;
+  double *d = h->dOut + LBM_MAX_SPHERES * 6;
+  h->ops->absorb_dead(h, d);
+  CKL("absorbDeadCells");
+  return fetch_out(h, d, ns, out);
+}
+
+int lbm_pack_volume_device(lbm_sim *h, void *dev_out) {
+  if (!h || !dev_out) return fail(h, LBM_ERR_ARG, "null");
+  DeviceGuard g(h->device);
+  h->ops->pack(h, (uint8_t *)dev_out);
+  CKL("packVolume");
+  return LBM_OK;
+}
+
+int lbm_pack_volume(lbm_sim *h, uint8_t *host_out) {
+  if (!h || !host_out) return fail(h, LBM_ERR_ARG, "null");
+  DeviceGuard g(h->device);
+  int rc = ensure_staging(h, (size_t)h->n * 2);
+  if (rc) return rc;
+  h->ops->pack(h, (uint8_t *)h->staging);
+  CKL("packVolume");
+  CK(copy_async(h, host_out, h->staging, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_every, uint8_t *frames) {
+  if (!h || nsteps < 0) return LBM_ERR_ARG;
+  int rc = check_spheres(h, sp, ns);
+  if (rc) return rc;
+  if (h->bfActive) return fail(h, LBM_ERR_STATE, "a pending body force needs lbm_step");
+  DeviceGuard g(h->device);
+  // capacity bounds for the device-computed plan
+  double rmax = 0;
+  for (int b = 0; b < ns; b++) rmax = std::max(rmax, sp[b].r);
+  long long side = 2 * (long long)ceil(rmax) + 7;
+  long long slotCells = std::min(h->n, side * side * side);
+  long long uside = 2 * (long long)ceil(rmax) + 12;
+  long long maxU = (h->fullRetagSteps > 0 || ns > 1) ? h->n : std::min(h->n, uside * uside * uside);
+  if (ns == 0) maxU = (h->fullRetagSteps > 0) ? h->n : box_cells(box_union(h->boxLast, h->boxLastLast));
+  long long maxChunks = (maxU + COMPACT_CHUNK - 1) / COMPACT_CHUNK;
+  int redChunks = (int)((slotCells + RED_CHUNK - 1) / RED_CHUNK);
+  long long need = std::max(1LL, (long long)ns * slotCells * 6);
+  if (need > h->impCap) {
+    if (h->impAcc) {
+      cudaFree(h->impAcc);
+      h->deviceBytes -= h->impCap * sizeof(double);
+      h->impAcc = nullptr;
+    }
+    DALLOC(h->impAcc, need * sizeof(double));
+    h->impCap = need;
+  }
+  long long pneed = (long long)std::max(ns, 1) * redChunks * 6;
+  if (pneed > h->partialsCap) {
+    if (h->partials) {
+      cudaFree(h->partials);
+      h->deviceBytes -= h->partialsCap * sizeof(double);
+      h->partials = nullptr;
+    }
+    DALLOC(h->partials, pneed * sizeof(double));
+    h->partialsCap = pneed;
+  }
+  h->partialsChunks = redChunks;
+  if ((rc = ensure_counts(h, std::max(1LL, maxChunks)))) return rc;
+  if (frame_every > 0 && frames && (rc = ensure_staging(h, (size_t)h->n * 2))) return rc;
+  // seed the device plan's history from the host's
+  memset(&h->hPlan, 0, sizeof(Plan));
+  h->hPlan.boxLast = h->boxLast;
+  h->hPlan.boxLastLast = h->boxLastLast;
+  h->hPlan.fullRetag = h->fullRetagSteps;
+  h->hPlan.ss.nsph = ns;
+  if ((rc = upload_plan(h))) return rc;
+  if (ns > 0)
+    CK(copy_async(h, h->dSph, sp, ns * sizeof(lbm_sphere), cudaMemcpyHostToDevice, h->stream));
+  double *dFluid = h->dOut, *dDead = h->dOut + LBM_MAX_SPHERES * 6;
+  const unsigned zeroBlocks = 148 * 4;
+  long long frame = 0;
+  for (int s = 0; s < nsteps; s++) {
+    k_plan<<<1, 1, 0, h->stream>>>(h->dPlan, h->dSph, ns, h->nx, h->ny, h->nz, h->impAcc, slotCells, maxU);
+    h->launches++;
+    h->ops->retag_box(h, maxU);
+    if ((rc = launch_compaction(h, maxChunks))) return rc;
+    h->ops->fresh_fill(h);
+    if (ns > 0) {
+      k_zero_targets<<<zeroBlocks, 256, 0, h->stream>>>(h->dPlan, h->impAcc);
+      h->launches++;
+    }
+    launch_fused(h);
+    if (ns > 0) {
+      dim3 g1(redChunks, ns);
+      k_impulse_reduce1<<<g1, 256, 0, h->stream>>>(&h->dPlan->ss, h->partials, redChunks);
+      k_impulse_reduce2<<<ns, 32, 0, h->stream>>>(&h->dPlan->ss, h->partials, redChunks, dFluid);
+      h->ops->absorb_dead(h, dDead);
+      h->ops->sphere_step_device(h, h->dSph, ns, h->params.gravity, dFluid, dDead);
+      h->launches += 2;
+    }
+    CKL("coupled step");
+    h->cur = 1 - h->cur;
+    if (frame_every > 0 && frames && (s + 1) % frame_every == 0) {
+      h->ops->pack(h, (uint8_t *)h->staging);
+      CKL("packVolume");
+      CK(copy_async(h, frames + frame * 2 * h->n, h->staging, (size_t)h->n * 2,
+                         cudaMemcpyDeviceToHost, h->stream));
+      frame++;
+    }
+  }
+  CK(copy_async(h, &h->hPlan, h->dPlan, sizeof(Plan), cudaMemcpyDeviceToHost, h->stream));
+  if (ns > 0)
+    CK(copy_async(h, sp, h->dSph, ns * sizeof(lbm_sphere), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->boxLast = h->hPlan.boxLast;
+  h->boxLastLast = h->hPlan.boxLastLast;
+  h->fullRetagSteps = h->hPlan.fullRetag;
+  h->lastRetagBox = h->hPlan.U;
+  h->listsValid = true;
+  if (h->hPlan.overflow) return fail(h, LBM_ERR_CAPACITY, "sphere moved beyond the planned retag box");
+  return LBM_OK;
+}
+
+int lbm_synchronize(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+void *lbm_stream(lbm_sim *h) { return h ? (void *)h->stream : nullptr; }
+
+int lbm_last_sets(lbm_sim *h, int *n_fresh, int *n_dead) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  CK(copy_async(h, h->hTotals, h->totals, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (n_fresh) *n_fresh = h->hTotals[0];
+  if (n_dead) *n_dead = h->hTotals[1];
+  return LBM_OK;
+}
+
+int lbm_download_sets(lbm_sim *h, int32_t *fresh, int cap_fresh, int32_t *dead, int cap_dead) {
+  if (!h) return LBM_ERR_ARG;
+  int nf = 0, nd = 0;
+  int rc = lbm_last_sets(h, &nf, &nd);
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if (fresh && cap_fresh > 0 && nf > 0)
+    CK(copy_async(h, fresh, h->fresh, std::min(nf, cap_fresh) * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (dead && cap_dead > 0 && nd > 0)
+    CK(copy_async(h, dead, h->dead, std::min(nd, cap_dead) * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+int lbm_launch_count(const lbm_sim *h, int64_t *count) {
+  if (!h || !count) return LBM_ERR_ARG;
+  *count = h->launches;
+  return LBM_OK;
+}
+
+int lbm_transfer_bytes(const lbm_sim *h, uint64_t *h2d, uint64_t *d2h) {
+  if (!h) return LBM_ERR_ARG;
+  if (h2d) *h2d = h->h2dBytes;
+  if (d2h) *d2h = h->d2hBytes;
+  return LBM_OK;
+}
+
+int lbm_fused_timing(lbm_sim *h, int enable) {
+  if (!h) return LBM_ERR_ARG;
+  h->timing = enable != 0;
+  if (enable) h->evUsed = 0;
+  return LBM_OK;
+}
+
+int lbm_fused_timing_query(lbm_sim *h, double *total_ms, int64_t *launches) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  CK(cudaStreamSynchronize(h->stream));
+  double tot = 0;
+  for (size_t i = 0; i < h->evUsed; i++) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->evStart[i], h->evStop[i]));
+    tot += ms;
+  }
+  if (total_ms) *total_ms = tot;
+  if (launches) *launches = (int64_t)h->evUsed;
+  return LBM_OK;
+}
+
+int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
+  if (!h) return LBM_ERR_ARG;
+  if (!(rows == 2 || rows == 4 || rows == 8 || rows == 16) || zchunk < 1)
+    return fail(h, LBM_ERR_ARG, "rows must be 2, 4, 8 or 16 and zchunk >= 1");
+  if (h->ops->fused_smem(rows) > 227 * 1024)
+    return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
+  h->cfg.ty = rows;
+  h->cfg.zchunk = zchunk;
+  return LBM_OK;
+}
+
+}  // extern "C"

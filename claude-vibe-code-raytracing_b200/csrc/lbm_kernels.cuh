@@ -1,0 +1,1049 @@
+// Kernel templates of the LBM step.  Included by one translation unit per
+// population storage type (lbm_inst_*.cu), which instantiates Ops<PopT>.
+//
+// Two execution forms share one device state:
+//  * phase-by-phase kernels that mirror the reference's seven Sim methods one
+//    to one (src/sim.js:176-582), for callers that invoke them individually;
+//  * the fused step: a z-marching kernel that, per cell, pulls the 27 + 7
+//    populations of its neighbours, applies each source cell's BGK collision on
+//    the fly from per-cell collision coefficients staged in shared memory,
+//    streams with halfway bounce-back / moving-wall correction, and writes the
+//    new populations and macros -- one read and one write of every state array
+//    per step.
+#pragma once
+
+#include <stdio.h>
+
+#include "lbm_core.cuh"
+
+namespace lbm {
+
+template <class PopT>
+struct Prec {
+  using Real = float;
+};
+template <>
+struct Prec<double> {
+  using Real = double;
+};
+
+inline unsigned nblocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+__device__ __forceinline__ long long cell_index(int x, int y, int z, int nx, int ny) {
+  return ((long long)z * ny + y) * nx + x;
+}
+
+// The reference's phase loops run over 1..n-2 on every axis (src/sim.js:334-338);
+// cells on the boundary are never collided or streamed, whatever their tag.
+__device__ __forceinline__ bool interior_cell(long long i, int nx, int ny, int nz) {
+  int x = (int)(i % nx);
+  long long t = i / nx;
+  int y = (int)(t % ny);
+  int z = (int)(t / ny);
+  return x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2 && z >= 1 && z <= nz - 2;
+}
+
+// Weight tables usable with a runtime index (generic kernels, host code).
+__host__ __device__ inline float w27_of(int k) {
+  int nnz = (dcomp(k, 0) != 0) + (dcomp(k, 1) != 0) + (dcomp(k, 2) != 0);
+  return (float)(nnz == 0 ? 8.0 / 27.0 : nnz == 1 ? 2.0 / 27.0 : nnz == 2 ? 1.0 / 54.0 : 1.0 / 216.0);
+}
+__host__ __device__ inline float w7_of(int k) { return (float)(k == 0 ? 0.25 : 0.125); }
+__host__ __device__ inline int opp_of(int k) { return k == 0 ? 0 : ((k & 1) ? k + 1 : k - 1); }
+
+__device__ __forceinline__ void flush_impulse(const SolidSet &ss, int owner, int x, int y, int z,
+                                              double acc[6]) {
+  if (owner < 0) return;
+  const ImpulseTarget &t = ss.imp[owner];
+  int lx = x - t.lo[0], ly = y - t.lo[1], lz = z - t.lo[2];
+  if (lx < 0 || ly < 0 || lz < 0 || lx >= t.dim[0] || ly >= t.dim[1] || lz >= t.dim[2]) return;
+  double *slot = t.acc + 6 * (((long long)lz * t.dim[1] + ly) * t.dim[0] + lx);
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    slot[j] = __dadd_rn(slot[j], acc[j]);
+    acc[j] = 0.0;
+  }
+}
+
+// =====================================================================================
+// init (src/sim.js:112-134): both ping-pong halves receive identical values so
+// that walls, which are never rewritten, read the same from either half.
+template <class PopT>
+__global__ void k_init_flat(Scene<PopT, typename Prec<PopT>::Real> s, const double *phiCol) {
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  int x = (int)(i % s.nx);
+  long long t = i / s.nx;
+  int y = (int)(t % s.ny);
+  int z = (int)(t / s.ny);
+  double pc = phiCol[y];
+  bool wall = x == 0 || x == s.nx - 1 || y == 0 || y == s.ny - 1 || z == 0 || z == s.nz - 1;
+  Real phiR = (Real)pc;
+  for (int c = 0; c < 2; c++) {
+    s.phi[c][i] = phiR;
+    s.rho[c][i] = (Real)1.0;
+    s.ux[c][i] = s.uy[c][i] = s.uz[c][i] = (Real)0;
+    for (int k = 0; k < Q27; k++) {
+      Real w = (Real)w27_of(k);
+      s.F[c][k * s.pitch + i] = Codec<PopT>::enc(w, w);
+    }
+    for (int k = 0; k < Q7; k++) {
+      Real hv = (Real)((double)w7_of(k) * pc);
+      s.H[c][k * s.pitch + i] = Codec<PopT>::enc(hv, (Real)w7_of(k) * phiR);
+    }
+  }
+  uint8_t tg = wall ? TAG_WALL : TAG_FLUID;
+  s.tag[i] = tg;
+  s.tagPrev[i] = tg;
+}
+
+// seedHydrostatic (src/sim.js:144-173): one thread per (z, x) column, y
+// ascending, FP64 arithmetic; writes rho and f into both halves.
+template <class PopT>
+__global__ void k_seed_hydrostatic(Scene<PopT, typename Prec<PopT>::Real> s, int cur, double rhoL,
+                                   double rhoG, double gravity) {
+  using Real = typename Prec<PopT>::Real;
+  long long col = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (col >= (long long)s.nx * s.nz) return;
+  int x = (int)(col % s.nx);
+  int z = (int)(col / s.nx);
+  const double dRho = rhoL - rhoG;
+  const double gOverCs2 = gravity * 3.0;
+  const double uLatY = -0.5 * gravity;
+  const double uLat2 = uLatY * uLatY;
+  double pCs2 = 1.0;
+  for (int y = 0; y < s.ny; y++) {
+    long long i = cell_index(x, y, z, s.nx, s.ny);
+    double rhoPhase = rhoG + (double)s.phi[cur][i] * dRho;
+    for (int c = 0; c < 2; c++) s.rho[c][i] = (Real)pCs2;
+    for (int k = 0; k < Q27; k++) {
+      double eu = dcomp(k, 1) * uLatY;
+      double Qi = eu * (3.0 + 4.5 * eu) - 1.5 * uLat2;
+      double fk = (double)w27_of(k) * (pCs2 + rhoPhase * Qi);
+      Real w = (Real)w27_of(k);
+      PopT e = Codec<PopT>::enc((Real)fk, w);
+      s.F[0][k * s.pitch + i] = e;
+      s.F[1][k * s.pitch + i] = e;
+    }
+    pCs2 += rhoPhase * gOverCs2;
+  }
+}
+
+// =====================================================================================
+// Phase-by-phase kernels (FP32 and FP64 storage).  Reference semantics:
+// f = F[cur], f2 = F[1-cur]; h = H[cur], h2 = H[1-cur]; macros in place in
+// [cur]; phiPrev = phi[1-cur].
+
+// computePhiGradients (src/sim.js:176-199)
+template <class PopT>
+__global__ void k_gradients(Scene<PopT, typename Prec<PopT>::Real> s, int cur) {
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  int x = (int)(i % nx);
+  long long t = i / nx;
+  int y = (int)(t % ny);
+  int z = (int)(t / ny);
+  int zm = z > 0 ? z - 1 : z, zp = z < nz - 1 ? z + 1 : z;
+  int ym = y > 0 ? y - 1 : y, yp = y < ny - 1 ? y + 1 : y;
+  int xm = x > 0 ? x - 1 : x, xp = x < nx - 1 ? x + 1 : x;
+  const Real *phi = s.phi[cur];
+  Real c = phi[i];
+  Real px = phi[cell_index(xp, y, z, nx, ny)];
+  Real mx = phi[cell_index(xm, y, z, nx, ny)];
+  Real py = phi[cell_index(x, yp, z, nx, ny)];
+  Real my = phi[cell_index(x, ym, z, nx, ny)];
+  Real pz = phi[cell_index(x, y, zp, nx, ny)];
+  Real mz = phi[cell_index(x, y, zm, nx, ny)];
+  s.gx[i] = (Real)0.5 * (px - mx);
+  s.gy[i] = (Real)0.5 * (py - my);
+  s.gz[i] = (Real)0.5 * (pz - mz);
+  s.lap[i] = px + mx + py + my + pz + mz - (Real)6 * c;
+}
+
+// retagCells over the whole grid (src/sim.js:214-244): tagPrev <- tag,
+// phiPrev <- phi, classification with FP64 contains, us = float(surfaceVelocity).
+template <class PopT>
+__global__ void k_retag_full(Scene<PopT, typename Prec<PopT>::Real> s, int cur,
+                             const SolidSet *__restrict__ ssp) {
+  const SolidSet &ss = *ssp;
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  int x = (int)(i % nx);
+  long long t = i / nx;
+  int y = (int)(t % ny);
+  int z = (int)(t / ny);
+  s.tagPrev[i] = s.tag[i];
+  s.phi[1 - cur][i] = s.phi[cur][i];
+  if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
+    s.tag[i] = TAG_WALL;
+    s.usx[i] = s.usy[i] = s.usz[i] = (Real)0;
+    return;
+  }
+  int b = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z);
+  if (b >= 0) {
+    double ox, oy, oz;
+    sphere_surface_velocity(ss.sph[b], x, y, z, ox, oy, oz);
+    s.tag[i] = TAG_SOLID;
+    s.usx[i] = (Real)(float)ox;
+    s.usy[i] = (Real)(float)oy;
+    s.usz[i] = (Real)(float)oz;
+  } else {
+    s.tag[i] = TAG_FLUID;
+    s.usx[i] = s.usy[i] = s.usz[i] = (Real)0;
+  }
+}
+
+// collidePhase (src/sim.js:324-364)
+template <class PopT>
+__global__ void k_collide_phase(Scene<PopT, typename Prec<PopT>::Real> s, int cur, StepConst k) {
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n || s.tag[i] != TAG_FLUID || !interior_cell(i, s.nx, s.ny, s.nz)) return;
+  const Real invTau = (Real)k.invTauPhi;
+  const Real sharpC = (Real)k.sharpC;
+  const Real sharpFac = (Real)4.0;
+  Real p = s.phi[cur][i];
+  Real uxi = s.ux[cur][i], uyi = s.uy[cur][i], uzi = s.uz[cur][i];
+  Real ggx = s.gx[i], ggy = s.gy[i], ggz = s.gz[i];
+  Real gmag = sqrt(ggx * ggx + ggy * ggy + ggz * ggz) + (Real)1e-12;
+  Real sharpen = sharpC * p * ((Real)1 - p);
+  Real Sx = sharpen * sharpFac * ggx / gmag;
+  Real Sy = sharpen * sharpFac * ggy / gmag;
+  Real Sz = sharpen * sharpFac * ggz / gmag;
+  const PopT *h = s.H[cur];
+  PopT *h2 = s.H[1 - cur];
+  for (int q = 0; q < Q7; q++) {
+    Real wk = (Real)w7_of(q);
+    Real ex = (Real)dcomp(q, 0), ey = (Real)dcomp(q, 1), ez = (Real)dcomp(q, 2);
+    Real eu = ex * uxi + ey * uyi + ez * uzi;
+    Real heq = wk * p * ((Real)1 + (Real)4 * eu);
+    Real Fk = wk * (ex * Sx + ey * Sy + ez * Sz);
+    Real hk = Codec<PopT>::dec(h[q * s.pitch + i], (Real)0);
+    h2[q * s.pitch + i] = Codec<PopT>::enc(hk - invTau * (hk - heq) + Fk, (Real)0);
+  }
+}
+
+// streamPhase (src/sim.js:376-397): pull with plain bounce-back.
+template <class PopT>
+__global__ void k_stream_phase(Scene<PopT, typename Prec<PopT>::Real> s, int cur) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n || s.tag[i] != TAG_FLUID || !interior_cell(i, s.nx, s.ny, s.nz)) return;
+  const int nx = s.nx, ny = s.ny;
+  const PopT *h2 = s.H[1 - cur];
+  PopT *h = s.H[cur];
+  for (int q = 0; q < Q7; q++) {
+    long long src = i - (((long long)dcomp(q, 2) * ny + dcomp(q, 1)) * nx + dcomp(q, 0));
+    h[q * s.pitch + i] = s.tag[src] == TAG_FLUID ? h2[q * s.pitch + src] : h2[opp_of(q) * s.pitch + i];
+  }
+}
+
+// collideHydro (src/sim.js:406-464)
+template <class PopT>
+__global__ void k_collide_hydro(Scene<PopT, typename Prec<PopT>::Real> s, int cur, StepConst k) {
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n || s.tag[i] != TAG_FLUID || !interior_cell(i, s.nx, s.ny, s.nz)) return;
+  const Real invTau = (Real)k.invTau;
+  const Real beta = (Real)k.beta, kappa = (Real)k.kappa, dRho = (Real)k.dRho;
+  const Real A = (Real)k.A, rhoG = (Real)k.rhoG, gravity = (Real)k.gravity;
+  Real sumF = s.rho[cur][i];
+  Real p = s.phi[cur][i];
+  Real rhoPhase = rhoG + p * dRho;
+  Real mu = (Real)4 * beta * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * s.lap[i];
+  Real bx = s.bfx ? s.bfx[i] : (Real)0, by = s.bfy ? s.bfy[i] : (Real)0, bz = s.bfz ? s.bfz[i] : (Real)0;
+  Real fx = bx + mu * s.gx[i];
+  Real fy = by + mu * s.gy[i] + rhoPhase * gravity;
+  Real fz = bz + mu * s.gz[i];
+  Real uxe = s.ux[cur][i], uye = s.uy[cur][i], uze = s.uz[cur][i];
+  Real u2 = uxe * uxe + uye * uye + uze * uze;
+  Real negU2half = (Real)-1.5 * u2;
+  Real uF = uxe * fx + uye * fy + uze * fz;
+  const PopT *f = s.F[cur];
+  PopT *f2 = s.F[1 - cur];
+  for (int q = 0; q < Q27; q++) {
+    Real wk = (Real)w27_of(q);
+    Real ex = (Real)dcomp(q, 0), ey = (Real)dcomp(q, 1), ez = (Real)dcomp(q, 2);
+    Real eu = ex * uxe + ey * uye + ez * uze;
+    Real Qi = negU2half + eu * ((Real)3 + (Real)4.5 * eu);
+    Real feq = wk * (sumF + rhoPhase * Qi);
+    Real ekF = ex * fx + ey * fy + ez * fz;
+    Real Sk = A * wk * (ekF * ((Real)1 + (Real)3 * eu) - uF);
+    Real fk = Codec<PopT>::dec(f[q * s.pitch + i], (Real)0);
+    f2[q * s.pitch + i] = Codec<PopT>::enc(fk - invTau * (fk - feq) + Sk, (Real)0);
+  }
+}
+
+// streamHydroAndMacro (src/sim.js:484-582)
+template <class PopT>
+__global__ void k_stream_hydro_macro(Scene<PopT, typename Prec<PopT>::Real> s, int cur,
+                                     StepConst kc, const SolidSet *__restrict__ ssp) {
+  const SolidSet &ss = *ssp;
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n || s.tag[i] != TAG_FLUID || !interior_cell(i, s.nx, s.ny, s.nz)) return;
+  const int nx = s.nx, ny = s.ny;
+  int x = (int)(i % nx);
+  long long t = i / nx;
+  int y = (int)(t % ny);
+  int z = (int)(t / ny);
+  const Real beta = (Real)kc.beta, kappa = (Real)kc.kappa, dRho = (Real)kc.dRho;
+  const Real rhoG = (Real)kc.rhoG, gravity = (Real)kc.gravity;
+  const PopT *f2 = s.F[1 - cur];
+  PopT *f = s.F[cur];
+  Real rhoPhaseOld = rhoG + s.phi[cur][i] * dRho;
+  Real pSumF = 0, mx = 0, my = 0, mz = 0;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  int owner = -1;
+  for (int q = 0; q < Q27; q++) {
+    const int ex = dcomp(q, 0), ey = dcomp(q, 1), ez = dcomp(q, 2);
+    long long src = i - (((long long)ez * ny + ey) * nx + ex);
+    uint8_t sTag = s.tag[src];
+    Real fk;
+    if (sTag == TAG_FLUID) {
+      fk = Codec<PopT>::dec(f2[q * s.pitch + src], (Real)0);
+    } else {
+      Real fopp = Codec<PopT>::dec(f2[opp_of(q) * s.pitch + i], (Real)0);
+      Real corr = 0;
+      if (sTag == TAG_SOLID) {
+        Real eu = (Real)ex * s.usx[src] + (Real)ey * s.usy[src] + (Real)ez * s.usz[src];
+        corr = (Real)2 * (Real)w27_of(q) * rhoPhaseOld * eu * (Real)3;
+      }
+      fk = fopp + corr;
+      if (sTag == TAG_SOLID && ss.nsph > 0) {
+        int sx = x - ex, sy = y - ey, sz = z - ez;
+        int b = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, sx, sy, sz);
+        if (b >= 0) {
+          if (b != owner) {
+            flush_impulse(ss, owner, x, y, z, acc);
+            owner = b;
+          }
+          double m = __dadd_rn((double)fopp, (double)fk);
+          impulse_terms(ss.sph[b], sx, sy, sz, -m * ex, -m * ey, -m * ez, acc);
+        }
+      }
+    }
+    f[q * s.pitch + i] = Codec<PopT>::enc(fk, (Real)0);
+    pSumF += fk;
+    mx += (Real)ex * fk;
+    my += (Real)ey * fk;
+    mz += (Real)ez * fk;
+  }
+  flush_impulse(ss, owner, x, y, z, acc);
+  s.rho[cur][i] = pSumF > (Real)0.01 ? pSumF : (Real)0.01;
+  Real phiSum = 0;
+  for (int q = 0; q < Q7; q++) phiSum += Codec<PopT>::dec(s.H[cur][q * s.pitch + i], (Real)0);
+  Real p = phiSum < (Real)0 ? (Real)0 : phiSum > (Real)1 ? (Real)1 : phiSum;
+  s.phi[cur][i] = p;
+  Real rhoPhaseNew = rhoG + p * dRho;
+  Real mu = (Real)4 * beta * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * s.lap[i];
+  Real bx = s.bfx ? s.bfx[i] : (Real)0, by = s.bfy ? s.bfy[i] : (Real)0, bz = s.bfz ? s.bfz[i] : (Real)0;
+  Real fx = bx + mu * s.gx[i];
+  Real fy = by + mu * s.gy[i] + rhoPhaseNew * gravity;
+  Real fz = bz + mu * s.gz[i];
+  Real invRho = (Real)1 / rhoPhaseNew;
+  Real uxn = (mx + (Real)0.5 * fx) * invRho;
+  Real uyn = (my + (Real)0.5 * fy) * invRho;
+  Real uzn = (mz + (Real)0.5 * fz) * invRho;
+  Real u2 = uxn * uxn + uyn * uyn + uzn * uzn;
+  const Real UMAX = (Real)0.2, UMAX2 = (Real)(0.2 * 0.2);
+  if (u2 > UMAX2) {
+    Real sc = UMAX / sqrt(u2);
+    uxn *= sc;
+    uyn *= sc;
+    uzn *= sc;
+  }
+  s.ux[cur][i] = uxn;
+  s.uy[cur][i] = uyn;
+  s.uz[cur][i] = uzn;
+}
+
+// =====================================================================================
+// Sparse passes around the spheres.
+
+// retag on a box (the union of the current and the two previous sphere boxes):
+// every cell outside it keeps tag == tagPrev, so only the box changes.
+template <class PopT>
+__global__ void k_retag_box(Scene<PopT, typename Prec<PopT>::Real> s, const Plan *__restrict__ P) {
+  const SolidSet &ss = P->ss;
+  const Box bx = P->U;
+  long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int dx = bx.hi[0] - bx.lo[0] + 1, dy = bx.hi[1] - bx.lo[1] + 1, dz = bx.hi[2] - bx.lo[2] + 1;
+  if (l >= (long long)dx * dy * dz) return;
+  int x = bx.lo[0] + (int)(l % dx);
+  int y = bx.lo[1] + (int)((l / dx) % dy);
+  int z = bx.lo[2] + (int)(l / ((long long)dx * dy));
+  long long i = cell_index(x, y, z, s.nx, s.ny);
+  uint8_t old = s.tag[i];
+  s.tagPrev[i] = old;
+  if (x == 0 || x == s.nx - 1 || y == 0 || y == s.ny - 1 || z == 0 || z == s.nz - 1) {
+    s.tag[i] = TAG_WALL;
+    return;
+  }
+  s.tag[i] = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) >= 0 ? TAG_SOLID : TAG_FLUID;
+}
+
+// Count fresh (FLUID, was SOLID) and dead (SOLID, was FLUID) cells per chunk
+// of the box's linear (scan) order.
+constexpr int COMPACT_CHUNK = 2048;
+constexpr int COMPACT_THREADS = 256;
+
+__device__ __forceinline__ void box_cell(const Box &bx, long long l, int &x, int &y, int &z) {
+  int dx = bx.hi[0] - bx.lo[0] + 1, dy = bx.hi[1] - bx.lo[1] + 1;
+  x = bx.lo[0] + (int)(l % dx);
+  y = bx.lo[1] + (int)((l / dx) % dy);
+  z = bx.lo[2] + (int)(l / ((long long)dx * dy));
+}
+
+static __global__ void k_compact_count(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
+                                       const Plan *__restrict__ P, int2 *counts) {
+  __shared__ int sf[COMPACT_THREADS / 32], sd[COMPACT_THREADS / 32];
+  const Box bx = P->U;
+  const long long total = P->ucells;
+  if ((int)blockIdx.x >= P->nchunks) return;
+  long long base = (long long)blockIdx.x * COMPACT_CHUNK;
+  int nf = 0, nd = 0;
+  for (int j = threadIdx.x; j < COMPACT_CHUNK; j += blockDim.x) {
+    long long l = base + j;
+    if (l >= total) break;
+    int x, y, z;
+    box_cell(bx, l, x, y, z);
+    long long i = cell_index(x, y, z, nx, ny);
+    uint8_t t = tag[i], p = tagPrev[i];
+    nf += (t == TAG_FLUID && p == TAG_SOLID);
+    nd += (t == TAG_SOLID && p == TAG_FLUID);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    nf += __shfl_xor_sync(0xffffffffu, nf, o);
+    nd += __shfl_xor_sync(0xffffffffu, nd, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sf[threadIdx.x >> 5] = nf;
+    sd[threadIdx.x >> 5] = nd;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int a = 0, b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      a += sf[w];
+      b += sd[w];
+    }
+    counts[blockIdx.x] = make_int2(a, b);
+  }
+}
+
+// Exclusive scan of the per-chunk counts (single CTA, sequential per thread).
+static __global__ void k_compact_scan(int2 *counts, const Plan *__restrict__ P, int *totals) {
+  __shared__ int2 part[1024];
+  const int nchunks = P->nchunks;
+  int per = (nchunks + blockDim.x - 1) / blockDim.x;
+  int b0 = threadIdx.x * per, b1 = min(b0 + per, nchunks);
+  int2 sum = make_int2(0, 0);
+  for (int b = b0; b < b1; b++) {
+    sum.x += counts[b].x;
+    sum.y += counts[b].y;
+  }
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int2 run = make_int2(0, 0);
+    for (int t = 0; t < (int)blockDim.x; t++) {
+      int2 v = part[t];
+      part[t] = run;
+      run.x += v.x;
+      run.y += v.y;
+    }
+    totals[0] = run.x;
+    totals[1] = run.y;
+  }
+  __syncthreads();
+  int2 run = part[threadIdx.x];
+  for (int b = b0; b < b1; b++) {
+    int2 v = counts[b];
+    counts[b] = run;
+    run.x += v.x;
+    run.y += v.y;
+  }
+}
+
+// Emit the fresh / dead cell indices in scan order.
+static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
+                                      const Plan *__restrict__ P, const int2 *offsets, int *fresh,
+                                      int *dead, int cap) {
+  __shared__ int wf[COMPACT_THREADS / 32], wd[COMPACT_THREADS / 32];
+  __shared__ int runF, runD;
+  const Box bx = P->U;
+  const long long total = P->ucells;
+  if ((int)blockIdx.x >= P->nchunks) return;
+  long long base = (long long)blockIdx.x * COMPACT_CHUNK;
+  if (threadIdx.x == 0) {
+    runF = offsets[blockIdx.x].x;
+    runD = offsets[blockIdx.x].y;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j0 = 0; j0 < COMPACT_CHUNK; j0 += blockDim.x) {
+    long long l = base + j0 + threadIdx.x;
+    bool isF = false, isD = false;
+    long long i = 0;
+    if (l < total && j0 + (int)threadIdx.x < COMPACT_CHUNK) {
+      int x, y, z;
+      box_cell(bx, l, x, y, z);
+      i = cell_index(x, y, z, nx, ny);
+      uint8_t t = tag[i], p = tagPrev[i];
+      isF = (t == TAG_FLUID && p == TAG_SOLID);
+      isD = (t == TAG_SOLID && p == TAG_FLUID);
+    }
+    unsigned bf = __ballot_sync(0xffffffffu, isF), bd = __ballot_sync(0xffffffffu, isD);
+    if (lane == 0) {
+      wf[warp] = __popc(bf);
+      wd[warp] = __popc(bd);
+    }
+    __syncthreads();
+    int offF = runF, offD = runD;
+    for (int w = 0; w < warp; w++) {
+      offF += wf[w];
+      offD += wd[w];
+    }
+    unsigned below = (1u << lane) - 1u;
+    if (isF) {
+      int pos = offF + __popc(bf & below);
+      if (pos < cap) fresh[pos] = (int)i;
+    }
+    if (isD) {
+      int pos = offD + __popc(bd & below);
+      if (pos < cap) dead[pos] = (int)i;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int a = 0, b = 0;
+      for (int w = 0; w < nw; w++) {
+        a += wf[w];
+        b += wd[w];
+      }
+      runF += a;
+      runD += b;
+    }
+    __syncthreads();
+  }
+}
+
+// handleFreshCells (src/sim.js:257-310) over the scan-ordered fresh list, one
+// thread, FP64 arithmetic, in place -- later fresh cells see the values written
+// for earlier ones exactly as in the reference's single sweep.
+template <class PopT>
+__global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *fresh,
+                             const int *totals, int cap, double rhoL, double rhoG) {
+  using Real = typename Prec<PopT>::Real;
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int nf = totals[0];
+  if (nf > cap) nf = cap;
+  const int nx = s.nx, ny = s.ny;
+  for (int q = 0; q < nf; q++) {
+    long long i = fresh[q];
+    double psum = 0, rsum = 0, vxs = 0, vys = 0, vzs = 0;
+    int pcnt = 0;
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          if (!dx && !dy && !dz) continue;
+          long long j = i + ((long long)dz * ny + dy) * nx + dx;
+          if (s.tag[j] == TAG_FLUID) {
+            psum += (double)s.phi[cur][j];
+            rsum += (double)s.rho[cur][j];
+            vxs += (double)s.ux[cur][j];
+            vys += (double)s.uy[cur][j];
+            vzs += (double)s.uz[cur][j];
+            pcnt++;
+          }
+        }
+    double p = pcnt > 0 ? psum / pcnt : (double)s.phi[cur][i];
+    double r = pcnt > 0 ? rsum / pcnt : 1.0;
+    double vx = pcnt > 0 ? vxs / pcnt : 0;
+    double vy = pcnt > 0 ? vys / pcnt : 0;
+    double vz = pcnt > 0 ? vzs / pcnt : 0;
+    Real pR = (Real)p;
+    s.phi[cur][i] = pR;
+    s.phi[1 - cur][i] = pR;  // phiPrev[i] = p
+    s.rho[cur][i] = (Real)r;
+    s.ux[cur][i] = (Real)vx;
+    s.uy[cur][i] = (Real)vy;
+    s.uz[cur][i] = (Real)vz;
+    double rhoPhase = rhoG + p * (rhoL - rhoG);
+    double u2 = vx * vx + vy * vy + vz * vz;
+    for (int k = 0; k < Q27; k++) {
+      double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
+      double Qi = eu * (3.0 + 4.5 * eu) - 1.5 * u2;
+      double fk = (double)w27_of(k) * (r + rhoPhase * Qi);
+      s.F[cur][k * s.pitch + i] = Codec<PopT>::enc((Real)fk, (Real)w27_of(k));
+    }
+    for (int k = 0; k < Q7; k++) {
+      double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
+      double hk = (double)w7_of(k) * p * (1 + 4.0 * eu);
+      s.H[cur][k * s.pitch + i] = Codec<PopT>::enc((Real)hk, (Real)w7_of(k) * pR);
+    }
+  }
+}
+
+// absorbDeadCells (src/solid.js:87-101): scan-ordered dead list, FP64, one
+// thread per sphere; impulse rho(phi)*u to the owning sphere.
+template <class PopT>
+__global__ void k_absorb_dead(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *dead,
+                              const int *totals, int cap, double rhoL, double rhoG,
+                              const SolidSet *__restrict__ ssp, double *out) {
+  const SolidSet &ss = *ssp;
+  int b = threadIdx.x;
+  if (blockIdx.x != 0 || b >= ss.nsph) return;
+  int nd = totals[1];
+  if (nd > cap) nd = cap;
+  const double dRho = rhoL - rhoG;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int q = 0; q < nd; q++) {
+    long long i = dead[q];
+    int x = (int)(i % s.nx);
+    long long t = i / s.nx;
+    int y = (int)(t % s.ny);
+    int z = (int)(t / s.ny);
+    if (owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) != b) continue;
+    double rhoPhase = __dadd_rn(rhoG, __dmul_rn((double)s.phi[cur][i], dRho));
+    impulse_terms(ss.sph[b], x, y, z, __dmul_rn(rhoPhase, (double)s.ux[cur][i]),
+                  __dmul_rn(rhoPhase, (double)s.uy[cur][i]), __dmul_rn(rhoPhase, (double)s.uz[cur][i]),
+                  acc);
+  }
+  for (int j = 0; j < 6; j++) out[6 * b + j] = acc[j];
+}
+
+// Deterministic two-level reduction of the per-cell impulse arrays:
+// level 1 sums fixed chunks of 1024 cells, level 2 sums the chunk partials in
+// index order.  Independent of how the stream kernel was tiled.
+constexpr int RED_CHUNK = 1024;
+
+static __global__ void k_impulse_reduce1(const SolidSet *__restrict__ ssp, double *partials, int maxChunks) {
+  const SolidSet &ss = *ssp;
+  int b = blockIdx.y;
+  if (b >= ss.nsph) return;
+  const ImpulseTarget &t = ss.imp[b];
+  long long cells = (long long)t.dim[0] * t.dim[1] * t.dim[2];
+  long long c0 = (long long)blockIdx.x * RED_CHUNK;
+  __shared__ double sh[6][256];
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  if (c0 < cells) {
+    for (int j = threadIdx.x; j < RED_CHUNK; j += blockDim.x) {
+      long long c = c0 + j;
+      if (c >= cells) break;
+      const double *p = t.acc + 6 * c;
+      for (int q = 0; q < 6; q++) a[q] = __dadd_rn(a[q], p[q]);
+    }
+  }
+  for (int q = 0; q < 6; q++) sh[q][threadIdx.x] = a[q];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int q = 0; q < 6; q++) sh[q][threadIdx.x] = __dadd_rn(sh[q][threadIdx.x], sh[q][threadIdx.x + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 6; q++) partials[((long long)b * maxChunks + blockIdx.x) * 6 + q] = sh[q][0];
+}
+
+static __global__ void k_impulse_reduce2(const SolidSet *__restrict__ ssp, const double *partials, int maxChunks,
+                                         double *out) {
+  const SolidSet &ss = *ssp;
+  int b = blockIdx.x;
+  if (b >= ss.nsph) return;
+  const ImpulseTarget &t = ss.imp[b];
+  long long cells = (long long)t.dim[0] * t.dim[1] * t.dim[2];
+  int nch = (int)((cells + RED_CHUNK - 1) / RED_CHUNK);
+  if (threadIdx.x < 6) {
+    double a = 0;
+    for (int c = 0; c < nch; c++) a = __dadd_rn(a, partials[((long long)b * maxChunks + c) * 6 + threadIdx.x]);
+    out[6 * b + threadIdx.x] = a;
+  }
+}
+
+// Clear the per-cell impulse slots the plan uses.
+static __global__ void k_zero_targets(const Plan *__restrict__ P, double *base) {
+  long long n = P->impDoubles;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    base[i] = 0.0;
+}
+
+// Device-side plan for the device-resident loop: sphere descriptors from the
+// device sphere state, the retag box (current and two previous sphere boxes),
+// compaction chunking, and impulse slots of slotCells cells per sphere.
+static __global__ void k_plan(Plan *P, const lbm_sphere *sph, int nsph, int nx, int ny, int nz,
+                              double *impBase, long long slotCells, long long maxUCells) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  SolidSet &ss = P->ss;
+  ss.nsph = nsph;
+  Box now{{1, 1, 1}, {0, 0, 0}};
+  int redChunks = 1;
+  for (int b = 0; b < nsph; b++) {
+    SphereDesc &d = ss.sph[b];
+    d.cx = sph[b].cx;
+    d.cy = sph[b].cy;
+    d.cz = sph[b].cz;
+    d.r = sph[b].r;
+    d.vx = sph[b].vx;
+    d.vy = sph[b].vy;
+    d.vz = sph[b].vz;
+    d.wx = sph[b].wx;
+    d.wy = sph[b].wy;
+    d.wz = sph[b].wz;
+    Box sb = sphere_box(d.cx, d.cy, d.cz, d.r, nx, ny, nz);
+    now = box_union(now, sb);
+    Box tb = box_grow(sb, 1, nx, ny, nz);
+    ImpulseTarget &t = ss.imp[b];
+    t.acc = impBase + (long long)b * slotCells * 6;
+    long long cells = box_cells(tb);
+    if (cells > slotCells) {
+      P->overflow = 1;
+      cells = 0;
+      tb = Box{{1, 1, 1}, {0, 0, 0}};
+    }
+    for (int a = 0; a < 3; a++) {
+      t.lo[a] = box_empty(tb) ? 0 : tb.lo[a];
+      t.dim[a] = box_empty(tb) ? 0 : tb.hi[a] - tb.lo[a] + 1;
+    }
+    int rc = (int)((cells + RED_CHUNK - 1) / RED_CHUNK);
+    redChunks = rc > redChunks ? rc : redChunks;
+  }
+  Box U;
+  if (P->fullRetag > 0) {
+    U = Box{{0, 0, 0}, {nx - 1, ny - 1, nz - 1}};
+    P->fullRetag--;
+  } else {
+    U = box_union(box_union(now, P->boxLast), P->boxLastLast);
+  }
+  long long uc = box_cells(U);
+  if (uc > maxUCells) {
+    P->overflow = 1;
+    uc = 0;
+    U = Box{{1, 1, 1}, {0, 0, 0}};
+  }
+  P->U = U;
+  P->ucells = uc;
+  P->nchunks = (int)((uc + COMPACT_CHUNK - 1) / COMPACT_CHUNK);
+  P->redChunks = redChunks;
+  P->impDoubles = (long long)nsph * slotCells * 6;
+  P->boxLastLast = P->boxLast;
+  P->boxLast = now;
+}
+
+// packVolume (src/sim.js:586-600)
+template <class PopT>
+__global__ void k_pack(Scene<PopT, typename Prec<PopT>::Real> s, int cur, uint8_t *out) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  float p = (float)s.phi[cur][i];
+  if (p < 0.f) p = 0.f;
+  else if (p > 1.f) p = 1.f;
+  double v = (double)p * 255.0;
+  int r = (v == v) ? (int)v : 0;
+  uchar2 o;
+  o.x = (uint8_t)r;
+  o.y = s.tag[i] == TAG_SOLID ? 255 : 0;
+  reinterpret_cast<uchar2 *>(out)[i] = o;
+}
+
+// =====================================================================================
+// The fused step.
+//
+// A CTA owns a 32 x TY column of cells and marches it through a range of z
+// planes.  For every plane it first stages, for the plane ahead (z+1) and its
+// one-cell in-plane halo, the per-cell collision coefficients in shared memory
+// (a ring of three planes), then every thread handles its cell in plane z:
+//
+//   for each of the 27 directions k with source s = i - e_k:
+//     s fluid:  f'_k(i) = (1 - w) f_k(s) + w_k (C0 + e.V + (e.u)(e.Q))   [coefficients of s]
+//     s solid/wall: halfway bounce-back of the cell's own collided f_opp(k)
+//                   (+ Ladd moving-wall term and FP64 momentum exchange)
+//
+// which is algebraically the reference's collideHydro (src/sim.js:450-460)
+// applied at the source followed by streamHydroAndMacro's pull
+// (src/sim.js:509-543), with
+//   C0 = w sumF - 1.5 w rho_phase u^2 - A u.F,  V = 3 w rho_phase u + A F,
+//   Q  = 4.5 w rho_phase u + 3 A F             (w = 1/tau, A = 3(1 - w/2)).
+// The D3Q7 phase lattice is treated the same way with
+//   h'_k(i) = (1 - wp) h_k(s) + w7_k (D0 + e.Dv),  D0 = wp phi,
+//   Dv = 4 wp phi u + S (the sharpening source, src/sim.js:346-357).
+// Then the macros of the cell follow (src/sim.js:545-576).
+
+template <class Real>
+struct alignas(4 * sizeof(Real)) V4 {
+  Real x, y, z, w;
+};
+
+template <class PopT>
+struct FusedArgs {
+  Scene<PopT, typename Prec<PopT>::Real> s;
+  int cur;
+  int zchunk;
+  // collision constants (Real precision)
+  double om, omP, A, beta4, kappa, rhoG, dRho, gravity, sharpC4;
+  const SolidSet *ss;
+};
+
+template <class PopT, int TY>
+struct FusedSmem {
+  using Real = typename Prec<PopT>::Real;
+  static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;
+  static constexpr size_t bytes = 3 * 4 * NC * sizeof(V4<Real>) + 3 * NC;
+};
+
+template <class PopT, int TY>
+__global__ void __launch_bounds__(32 * TY) k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
+  using Real = typename Prec<PopT>::Real;
+  using C = Codec<PopT>;
+  using SM = FusedSmem<PopT, TY>;
+  constexpr int RX = SM::RX, NC = SM::NC;
+  extern __shared__ __align__(32) unsigned char smem_raw[];
+  V4<Real> *ring = reinterpret_cast<V4<Real> *>(smem_raw);  // [3][4][NC]
+  uint8_t *stag = smem_raw + 3 * 4 * NC * sizeof(V4<Real>);  // [3][NC]
+
+  const auto &s = a.s;
+  const SolidSet &ss = *a.ss;
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  const long long nxny = (long long)nx * ny;
+  const long long pitch = s.pitch;
+  const int cur = a.cur, nxt = 1 - cur;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * 32 + tx;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TY;
+  const int zb = 1 + blockIdx.z * a.zchunk;
+  const int ze = min(zb + a.zchunk, nz - 1);
+  if (zb >= ze) return;
+  const int x = x0 + tx, y = y0 + ty;
+  const int own = (ty + 1) * RX + (tx + 1);
+
+  const Real om = (Real)a.om, omP = (Real)a.omP, A = (Real)a.A;
+  const Real beta4 = (Real)a.beta4, kappa = (Real)a.kappa, rhoG = (Real)a.rhoG;
+  const Real dRho = (Real)a.dRho, grav = (Real)a.gravity, sharpC4 = (Real)a.sharpC4;
+  const Real *__restrict__ phiC = s.phi[cur];
+
+  // Stage the collision coefficients of plane zp (own cell first, then halo).
+  // Returns the own cell's gradient and laplacian (used by its macro update).
+  auto fill = [&](int zp, Real &ogx, Real &ogy, Real &ogz, Real &olap) {
+    const int slot = zp % 3;
+    V4<Real> *R = ring + slot * 4 * NC;
+    uint8_t *T = stag + slot * NC;
+    const int nHalo = NC - 32 * TY;
+    for (int j = -1; j < nHalo; j += (j < 0 ? 1 + tid : 32 * TY)) {
+      int lc, gx_, gy_;
+      if (j < 0) {
+        lc = own;
+        gx_ = x;
+        gy_ = y;
+      } else {
+        // halo cell j: top row, bottom row, then the left and right columns
+        int lx, ly;
+        if (j < RX) {
+          lx = j;
+          ly = 0;
+        } else if (j < 2 * RX) {
+          lx = j - RX;
+          ly = TY + 1;
+        } else {
+          int r = j - 2 * RX;
+          lx = (r & 1) ? RX - 1 : 0;
+          ly = 1 + (r >> 1);
+        }
+        lc = ly * RX + lx;
+        gx_ = x0 - 1 + lx;
+        gy_ = y0 - 1 + ly;
+      }
+      uint8_t tg = TAG_WALL;
+      long long ci = 0;
+      bool inside = gx_ >= 0 && gx_ < nx && gy_ >= 0 && gy_ < ny && zp >= 0 && zp < nz;
+      if (inside) {
+        ci = zp * nxny + (long long)gy_ * nx + gx_;
+        tg = s.tag[ci];
+        // boundary cells never act as fluid (they are walls after any retag)
+        bool inner = gx_ >= 1 && gx_ <= nx - 2 && gy_ >= 1 && gy_ <= ny - 2 && zp >= 1 && zp <= nz - 2;
+        if (!inner && tg == TAG_FLUID) tg = TAG_WALL;
+      }
+      T[lc] = tg;
+      if (tg == TAG_FLUID) {
+        Real p = phiC[ci];
+        Real pxp = phiC[ci + 1], pxm = phiC[ci - 1];
+        Real pyp = phiC[ci + nx], pym = phiC[ci - nx];
+        Real pzp = phiC[ci + nxny], pzm = phiC[ci - nxny];
+        Real gxv = (Real)0.5 * (pxp - pxm);
+        Real gyv = (Real)0.5 * (pyp - pym);
+        Real gzv = (Real)0.5 * (pzp - pzm);
+        Real lap = pxp + pxm + pyp + pym + pzp + pzm - (Real)6 * p;
+        Real rhoPh = rhoG + p * dRho;
+        Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lap;
+        Real Fx = mu * gxv, Fy = mu * gyv + rhoPh * grav, Fz = mu * gzv;
+        Real sumF = s.rho[cur][ci];
+        Real ux = s.ux[cur][ci], uy = s.uy[cur][ci], uz = s.uz[cur][ci];
+        Real u2 = ux * ux + uy * uy + uz * uz;
+        Real uF = ux * Fx + uy * Fy + uz * Fz;
+        Real orh = om * rhoPh;
+        V4<Real> g0, g1, g2, g3;
+        g0.x = om * sumF - (Real)1.5 * orh * u2 - A * uF;
+        g0.y = (Real)3 * orh * ux + A * Fx;
+        g0.z = (Real)3 * orh * uy + A * Fy;
+        g0.w = (Real)3 * orh * uz + A * Fz;
+        g1.x = ux;
+        g1.y = uy;
+        g1.z = uz;
+        g1.w = p;
+        g2.x = (Real)4.5 * orh * ux + (Real)3 * A * Fx;
+        g2.y = (Real)4.5 * orh * uy + (Real)3 * A * Fy;
+        g2.z = (Real)4.5 * orh * uz + (Real)3 * A * Fz;
+        g2.w = omP * p;
+        Real gmag = sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + (Real)1e-12;
+        Real sh = sharpC4 * p * ((Real)1 - p) / gmag;
+        Real fp = (Real)4 * omP * p;
+        g3.x = fp * ux + sh * gxv;
+        g3.y = fp * uy + sh * gyv;
+        g3.z = fp * uz + sh * gzv;
+        g3.w = rhoPh;
+        R[0 * NC + lc] = g0;
+        R[1 * NC + lc] = g1;
+        R[2 * NC + lc] = g2;
+        R[3 * NC + lc] = g3;
+        if (j < 0) {
+          ogx = gxv;
+          ogy = gyv;
+          ogz = gzv;
+          olap = lap;
+        }
+      }
+    }
+  };
+
+  Real gxC = 0, gyC = 0, gzC = 0, lapC = 0, gxN = 0, gyN = 0, gzN = 0, lapN = 0;
+  fill(zb - 1, gxN, gyN, gzN, lapN);
+  fill(zb, gxC, gyC, gzC, lapC);
+
+  const bool colActive = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
+
+  for (int z = zb; z < ze; z++) {
+    fill(z + 1, gxN, gyN, gzN, lapN);
+    __syncthreads();
+    const int sC = z % 3;
+    const uint8_t tagI = colActive ? stag[sC * NC + own] : TAG_WALL;
+    const long long i = z * nxny + (long long)y * nx + x;
+    if (tagI == TAG_SOLID) {
+      // Solid cells are not updated; carry their state into the next half so
+      // both halves hold the reference's stale values.
+#pragma unroll 1
+      for (int k = 0; k < Q27; k++) s.F[nxt][k * pitch + i] = s.F[cur][k * pitch + i];
+#pragma unroll 1
+      for (int k = 0; k < Q7; k++) s.H[nxt][k * pitch + i] = s.H[cur][k * pitch + i];
+      s.phi[nxt][i] = s.phi[cur][i];
+      s.rho[nxt][i] = s.rho[cur][i];
+      s.ux[nxt][i] = s.ux[cur][i];
+      s.uy[nxt][i] = s.uy[cur][i];
+      s.uz[nxt][i] = s.uz[cur][i];
+    } else if (tagI == TAG_FLUID) {
+      const V4<Real> *R0 = ring;
+      const V4<Real> ownG1 = ring[(sC * 4 + 1) * NC + own];
+      const V4<Real> ownG3 = ring[(sC * 4 + 3) * NC + own];
+      const Real rhoPhOld = ownG3.w;
+      const PopT *__restrict__ Fc = s.F[cur];
+      const PopT *__restrict__ Hc = s.H[cur];
+      PopT *__restrict__ Fn = s.F[nxt];
+      PopT *__restrict__ Hn = s.H[nxt];
+      Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
+      Real hn[Q7];
+      double acc[6] = {0, 0, 0, 0, 0, 0};
+      int owner = -1;
+      static_for<0, Q27>([&](auto KK) {
+        constexpr int k = decltype(KK)::value;
+        using D = D27<k>;
+        constexpr int ex = D::ex, ey = D::ey, ez = D::ez;
+        const int sp = (z - ez + 3) % 3;
+        const int sc = own - ey * RX - ex;
+        const uint8_t ts = stag[sp * NC + sc];
+        const bool fl = ts == TAG_FLUID;
+        const long long off = ((long long)(-ez) * ny + (-ey)) * nx + (-ex);
+        const PopT *pf = fl ? (Fc + k * pitch + (i + off)) : (Fc + D::opp * pitch + i);
+        const int pc = fl ? (sp * 4) * NC + sc : (sC * 4) * NC + own;
+        const V4<Real> G0 = R0[pc], G1 = R0[pc + NC], G2 = R0[pc + 2 * NC];
+        const Real v = C::dec(*pf, (Real)D::w);
+        const Real sg = fl ? (Real)1 : (Real)-1;
+        const Real ev = (Real)ex * G0.y + (Real)ey * G0.z + (Real)ez * G0.w;
+        const Real eu = (Real)ex * G1.x + (Real)ey * G1.y + (Real)ez * G1.z;
+        const Real eq = (Real)ex * G2.x + (Real)ey * G2.y + (Real)ez * G2.z;
+        Real fk = ((Real)1 - om) * v + (Real)D::w * (G0.x + sg * ev + eu * eq);
+        if (ts == TAG_SOLID) {
+          const int sx = x - ex, sy = y - ey, sz = z - ez;
+          const int b = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, sx, sy, sz);
+          Real corr = 0;
+          if (b >= 0) {
+            double ox, oy, oz;
+            sphere_surface_velocity(ss.sph[b], sx, sy, sz, ox, oy, oz);
+            const Real eus = (Real)ex * (Real)(float)ox + (Real)ey * (Real)(float)oy +
+                             (Real)ez * (Real)(float)oz;
+            corr = (Real)2 * (Real)D::w * rhoPhOld * eus * (Real)3;
+            const Real fopp = fk;
+            fk = fopp + corr;
+            if (b != owner) {
+              flush_impulse(ss, owner, x, y, z, acc);
+              owner = b;
+            }
+            const double m = __dadd_rn((double)fopp, (double)fk);
+            impulse_terms(ss.sph[b], sx, sy, sz, -m * ex, -m * ey, -m * ez, acc);
+          }
+        }
+        Fn[k * pitch + i] = C::enc(fk, (Real)D::w);
+        rhoA += fk;
+        if (ex) mx += (Real)ex * fk;
+        if (ey) my += (Real)ey * fk;
+        if (ez) mz += (Real)ez * fk;
+        if constexpr (k < Q7) {
+          using E = D7<k>;
+          const PopT *ph = fl ? (Hc + k * pitch + (i + off)) : (Hc + E::opp * pitch + i);
+          const V4<Real> G3 = R0[pc + 3 * NC];
+          const Real phiRef = fl ? G1.w : ownG1.w;
+          const Real hv = C::dec(*ph, (Real)E::w * phiRef);
+          const Real ed = (Real)ex * G3.x + (Real)ey * G3.y + (Real)ez * G3.z;
+          const Real hk = ((Real)1 - omP) * hv + (Real)E::w * (G2.w + sg * ed);
+          hn[k] = hk;
+          hsum += hk;
+        }
+      });
+      flush_impulse(ss, owner, x, y, z, acc);
+      const Real rhoN = rhoA > (Real)0.01 ? rhoA : (Real)0.01;
+      const Real p = hsum < (Real)0 ? (Real)0 : hsum > (Real)1 ? (Real)1 : hsum;
+      static_for<0, Q7>([&](auto KK) {
+        constexpr int k = decltype(KK)::value;
+        Hn[k * pitch + i] = C::enc(hn[k], (Real)D7<k>::w * p);
+      });
+      const Real rhoPhN = rhoG + p * dRho;
+      const Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lapC;
+      const Real Fx = mu * gxC, Fy = mu * gyC + rhoPhN * grav, Fz = mu * gzC;
+      const Real inv = (Real)1 / rhoPhN;
+      Real uxn = (mx + (Real)0.5 * Fx) * inv;
+      Real uyn = (my + (Real)0.5 * Fy) * inv;
+      Real uzn = (mz + (Real)0.5 * Fz) * inv;
+      const Real u2 = uxn * uxn + uyn * uyn + uzn * uzn;
+      if (u2 > (Real)(0.2 * 0.2)) {
+        const Real sc = (Real)0.2 / sqrt(u2);
+        uxn *= sc;
+        uyn *= sc;
+        uzn *= sc;
+      }
+      s.rho[nxt][i] = rhoN;
+      s.phi[nxt][i] = p;
+      s.ux[nxt][i] = uxn;
+      s.uy[nxt][i] = uyn;
+      s.uz[nxt][i] = uzn;
+    }
+    __syncthreads();
+    gxC = gxN;
+    gyC = gyN;
+    gzC = gzN;
+    lapC = lapN;
+  }
+}
+
+}  // namespace lbm

@@ -1,0 +1,325 @@
+// Typed kernel launchers: Ops<PopT> implements OpsBase for one population
+// storage type.  Included once per storage type by lbm_inst_*.cu.
+#pragma once
+
+#include "lbm_kernels.cuh"
+#include "lbm_state.h"
+
+namespace lbm {
+
+// ---------------------------------------------------------------- transfers
+template <class PopT>
+__global__ void k_aos_to_soa(Scene<PopT, typename Prec<PopT>::Real> s, int isH, int half, int cur,
+                             const float *aos, long long c0, long long cells) {
+  using Real = typename Prec<PopT>::Real;
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  long long i = c0 + c;
+  const int Q = isH ? Q7 : Q27;
+  for (int hf = 0; hf < 2; hf++) {
+    int dst = hf == 0 ? cur : 1 - cur;
+    if (half == 1 && dst != cur) continue;
+    if (half == 2 && dst == cur) continue;
+    PopT *P = isH ? s.H[dst] : s.F[dst];
+    for (int k = 0; k < Q; k++) {
+      Real v = (Real)aos[c * Q + k];
+      Real ref = isH ? (Real)w7_of(k) * s.phi[dst][i] : (Real)w27_of(k);
+      P[k * s.pitch + i] = Codec<PopT>::enc(v, ref);
+    }
+  }
+}
+
+template <class PopT>
+__global__ void k_soa_to_aos(Scene<PopT, typename Prec<PopT>::Real> s, int isH, int src, float *aos,
+                             long long c0, long long cells) {
+  using Real = typename Prec<PopT>::Real;
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= cells) return;
+  long long i = c0 + c;
+  const int Q = isH ? Q7 : Q27;
+  const PopT *P = isH ? s.H[src] : s.F[src];
+  for (int k = 0; k < Q; k++) {
+    Real ref = isH ? (Real)w7_of(k) * s.phi[src][i] : (Real)w27_of(k);
+    aos[c * Q + k] = (float)Codec<PopT>::dec(P[k * s.pitch + i], ref);
+  }
+}
+
+template <class PopT>
+__global__ void k_reencode_h(Scene<PopT, typename Prec<PopT>::Real> s, int half,
+                             const typename Prec<PopT>::Real *oldPhi) {
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  Real po = oldPhi[i], pn = s.phi[half][i];
+  for (int k = 0; k < Q7; k++) {
+    Real w = (Real)w7_of(k);
+    Real v = Codec<PopT>::dec(s.H[half][k * s.pitch + i], w * po);
+    s.H[half][k * s.pitch + i] = Codec<PopT>::enc(v, w * pn);
+  }
+}
+
+// RigidSphere.step(1.0, gravity) (src/solid.js:104-210) on the device, one
+// thread per sphere, FP64 round-to-nearest intrinsics in the reference's
+// evaluation order.  The momentum-exchange and dead-cell impulses of the step
+// are added first, as RigidSphere.applyImpulseAtCell would have.
+__device__ __forceinline__ double js_max0(double v) {
+  if (v != v) return v;
+  if (v == 0) return signbit(v) ? 0.0 : v;
+  return v > 0 ? v : 0.0;
+}
+__device__ __forceinline__ double js_min0(double v) {
+  if (v != v) return v;
+  if (v == 0) return signbit(v) ? v : 0.0;
+  return v < 0 ? v : 0.0;
+}
+
+static __global__ void k_sphere_step(lbm_sphere *sph, int nsph, double gravity, const double *fluid,
+                              const double *dead, int nx, int ny, int nz) {
+  int b = threadIdx.x;
+  if (blockIdx.x != 0 || b >= nsph) return;
+  lbm_sphere s = sph[b];
+  const double dt = 1.0;
+  double *F[6] = {&s.Fx, &s.Fy, &s.Fz, &s.Tx, &s.Ty, &s.Tz};
+  for (int j = 0; j < 6; j++) {
+    if (fluid) *F[j] = __dadd_rn(*F[j], fluid[6 * b + j]);
+    if (dead) *F[j] = __dadd_rn(*F[j], dead[6 * b + j]);
+  }
+  s.Fy = __dadd_rn(s.Fy, __dmul_rn(s.mass, gravity));
+  if (s.dragging) {
+    double k = __dmul_rn(0.004, s.mass);
+    double cD = __dmul_rn(2.0, __dsqrt_rn(__dmul_rn(k, s.mass)));
+    s.Fx = __dadd_rn(s.Fx, __dsub_rn(__dmul_rn(k, __dsub_rn(s.dragTargetX, s.cx)), __dmul_rn(cD, s.vx)));
+    s.Fy = __dadd_rn(s.Fy, __dsub_rn(__dmul_rn(k, __dsub_rn(s.dragTargetY, s.cy)), __dmul_rn(cD, s.vy)));
+    s.Fz = __dadd_rn(s.Fz, __dsub_rn(__dmul_rn(k, __dsub_rn(s.dragTargetZ, s.cz)), __dmul_rn(cD, s.vz)));
+  }
+  double gsel = (gravity == 0 || gravity != gravity) ? 0.001 : gravity;
+  double accCap = __dmul_rn(3.5, fabs(gsel));
+  {
+    double ax = __ddiv_rn(s.Fx, s.mass);
+    double ay = __ddiv_rn(s.Fy, s.mass);
+    double az = __ddiv_rn(s.Fz, s.mass);
+    double a2 = __dadd_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)), __dmul_rn(az, az));
+    double c2 = __dmul_rn(accCap, accCap);
+    double sc = a2 > c2 ? __ddiv_rn(accCap, __dsqrt_rn(a2)) : 1.0;
+    s.vx = __dadd_rn(s.vx, __dmul_rn(__dmul_rn(dt, ax), sc));
+    s.vy = __dadd_rn(s.vy, __dmul_rn(__dmul_rn(dt, ay), sc));
+    s.vz = __dadd_rn(s.vz, __dmul_rn(__dmul_rn(dt, az), sc));
+  }
+  s.wx = __dadd_rn(s.wx, __ddiv_rn(__dmul_rn(dt, s.Tx), s.I));
+  s.wy = __dadd_rn(s.wy, __ddiv_rn(__dmul_rn(dt, s.Ty), s.I));
+  s.wz = __dadd_rn(s.wz, __ddiv_rn(__dmul_rn(dt, s.Tz), s.I));
+  const double BODY_UMAX = 0.08;
+  double sp2 = __dadd_rn(__dadd_rn(__dmul_rn(s.vx, s.vx), __dmul_rn(s.vy, s.vy)), __dmul_rn(s.vz, s.vz));
+  if (sp2 > __dmul_rn(BODY_UMAX, BODY_UMAX)) {
+    double sc = __ddiv_rn(BODY_UMAX, __dsqrt_rn(sp2));
+    s.vx = __dmul_rn(s.vx, sc);
+    s.vy = __dmul_rn(s.vy, sc);
+    s.vz = __dmul_rn(s.vz, sc);
+  }
+  s.vx = __dmul_rn(s.vx, 0.98);
+  s.vy = __dmul_rn(s.vy, 0.98);
+  s.vz = __dmul_rn(s.vz, 0.98);
+  s.wx = __dmul_rn(s.wx, 0.95);
+  s.wy = __dmul_rn(s.wy, 0.95);
+  s.wz = __dmul_rn(s.wz, 0.95);
+  const double SNAP = 0.0001;
+  if (fabs(s.vx) < SNAP) s.vx = 0;
+  if (fabs(s.vy) < SNAP) s.vy = 0;
+  if (fabs(s.vz) < SNAP) s.vz = 0;
+  if (fabs(s.wx) < SNAP) s.wx = 0;
+  if (fabs(s.wy) < SNAP) s.wy = 0;
+  if (fabs(s.wz) < SNAP) s.wz = 0;
+  s.cx = __dadd_rn(s.cx, __dmul_rn(dt, s.vx));
+  s.cy = __dadd_rn(s.cy, __dmul_rn(dt, s.vy));
+  s.cz = __dadd_rn(s.cz, __dmul_rn(dt, s.vz));
+  double m = __dadd_rn(s.r, 1.5);
+  double limX = __dsub_rn((double)(nx - 1), m), limY = __dsub_rn((double)(ny - 1), m);
+  double limZ = __dsub_rn((double)(nz - 1), m);
+  if (s.cx < m) { s.cx = m; s.vx = js_max0(s.vx); }
+  if (s.cx > limX) { s.cx = limX; s.vx = js_min0(s.vx); }
+  if (s.cy < m) { s.cy = m; s.vy = js_max0(s.vy); }
+  if (s.cy > limY) { s.cy = limY; s.vy = js_min0(s.vy); }
+  if (s.cz < m) { s.cz = m; s.vz = js_max0(s.vz); }
+  if (s.cz > limZ) { s.cz = limZ; s.vz = js_min0(s.vz); }
+  s.Fx = s.Fy = s.Fz = 0;
+  s.Tx = s.Ty = s.Tz = 0;
+  sph[b] = s;
+}
+
+// ---------------------------------------------------------------- launcher
+
+template <class PopT>
+class Ops final : public OpsBase {
+ public:
+  using Real = typename Prec<PopT>::Real;
+  using SceneT = Scene<PopT, Real>;
+
+  size_t pop_bytes() const override { return sizeof(PopT); }
+  size_t macro_bytes() const override { return sizeof(Real); }
+  bool phases_supported() const override { return !Codec<PopT>::offset; }
+
+  static SceneT scene(lbm_sim *h) {
+    SceneT s;
+    s.nx = h->nx;
+    s.ny = h->ny;
+    s.nz = h->nz;
+    s.n = h->n;
+    s.pitch = h->pitch;
+    for (int c = 0; c < 2; c++) {
+      s.F[c] = (PopT *)h->F[c];
+      s.H[c] = (PopT *)h->H[c];
+      s.phi[c] = (Real *)h->mac[c][0];
+      s.rho[c] = (Real *)h->mac[c][1];
+      s.ux[c] = (Real *)h->mac[c][2];
+      s.uy[c] = (Real *)h->mac[c][3];
+      s.uz[c] = (Real *)h->mac[c][4];
+    }
+    s.tag = h->tag;
+    s.tagPrev = h->tagPrev;
+    s.gx = (Real *)h->grad[0];
+    s.gy = (Real *)h->grad[1];
+    s.gz = (Real *)h->grad[2];
+    s.lap = (Real *)h->grad[3];
+    s.usx = (Real *)h->us[0];
+    s.usy = (Real *)h->us[1];
+    s.usz = (Real *)h->us[2];
+    bool bfa = h->bfActive;
+    s.bfx = bfa ? (Real *)h->bf[0] : nullptr;
+    s.bfy = bfa ? (Real *)h->bf[1] : nullptr;
+    s.bfz = bfa ? (Real *)h->bf[2] : nullptr;
+    return s;
+  }
+
+  void init_flat(lbm_sim *h, const double *d_phiCol) override {
+    k_init_flat<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), d_phiCol);
+    h->launches++;
+  }
+  void seed_hydrostatic(lbm_sim *h) override {
+    long long cols = (long long)h->nx * h->nz;
+    k_seed_hydrostatic<PopT><<<nblocks(cols, 128), 128, 0, h->stream>>>(
+        scene(h), h->cur, h->params.rhoL, h->params.rhoG, h->params.gravity);
+    h->launches++;
+  }
+  void gradients(lbm_sim *h) override {
+    k_gradients<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur);
+    h->launches++;
+  }
+  void retag_full(lbm_sim *h) override {
+    k_retag_full<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur, &h->dPlan->ss);
+    h->launches++;
+  }
+  void collide_phase(lbm_sim *h) override {
+    k_collide_phase<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur,
+                                                                       make_const(h->params));
+    h->launches++;
+  }
+  void stream_phase(lbm_sim *h) override {
+    k_stream_phase<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur);
+    h->launches++;
+  }
+  void collide_hydro(lbm_sim *h) override {
+    k_collide_hydro<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur,
+                                                                       make_const(h->params));
+    h->launches++;
+  }
+  void stream_hydro_macro(lbm_sim *h) override {
+    k_stream_hydro_macro<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(
+        scene(h), h->cur, make_const(h->params), &h->dPlan->ss);
+    h->launches++;
+  }
+  void retag_box(lbm_sim *h, long long maxCells) override {
+    if (maxCells <= 0) return;
+    k_retag_box<PopT><<<nblocks(maxCells, 256), 256, 0, h->stream>>>(scene(h), h->dPlan);
+    h->launches++;
+  }
+  void fresh_fill(lbm_sim *h) override {
+    k_fresh_fill<PopT><<<1, 32, 0, h->stream>>>(scene(h), h->cur, h->fresh, h->totals,
+                                                 (int)h->listCap, h->params.rhoL, h->params.rhoG);
+    h->launches++;
+  }
+  void absorb_dead(lbm_sim *h, double *d_out) override {
+    k_absorb_dead<PopT><<<1, 32, 0, h->stream>>>(scene(h), h->cur, h->dead, h->totals,
+                                                  (int)h->listCap, h->params.rhoL, h->params.rhoG,
+                                                  &h->dPlan->ss, d_out);
+    h->launches++;
+  }
+
+  template <int TY>
+  void launch_fused(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
+    constexpr size_t smem = FusedSmem<PopT, TY>::bytes;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_fused_step<PopT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr = true;
+    }
+    dim3 block(32, TY);
+    dim3 grid((h->nx + 31) / 32, (h->ny + TY - 1) / TY, (h->nz - 2 + zchunk - 1) / zchunk);
+    k_fused_step<PopT, TY><<<grid, block, smem, h->stream>>>(a);
+    h->launches++;
+  }
+
+  void fused_step(lbm_sim *h, const FusedCfg &cfg) override {
+    FusedArgs<PopT> a;
+    a.s = scene(h);
+    a.cur = h->cur;
+    a.zchunk = cfg.zchunk;
+    StepConst k = make_const(h->params);
+    a.om = k.invTau;
+    a.omP = k.invTauPhi;
+    a.A = k.A;
+    a.beta4 = 4 * k.beta;
+    a.kappa = k.kappa;
+    a.rhoG = k.rhoG;
+    a.dRho = k.dRho;
+    a.gravity = k.gravity;
+    a.sharpC4 = 4 * k.sharpC;
+    a.ss = &h->dPlan->ss;
+    switch (cfg.ty) {
+      case 2: launch_fused<2>(h, a, cfg.zchunk); break;
+      case 4: launch_fused<4>(h, a, cfg.zchunk); break;
+      case 16: launch_fused<16>(h, a, cfg.zchunk); break;
+      default: launch_fused<8>(h, a, cfg.zchunk); break;
+    }
+  }
+
+  size_t fused_smem(int ty) const override {
+    switch (ty) {
+      case 2: return FusedSmem<PopT, 2>::bytes;
+      case 4: return FusedSmem<PopT, 4>::bytes;
+      case 16: return FusedSmem<PopT, 16>::bytes;
+      default: return FusedSmem<PopT, 8>::bytes;
+    }
+  }
+
+  void pack(lbm_sim *h, uint8_t *d_out) override {
+    k_pack<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur, d_out);
+    h->launches++;
+  }
+  void upload_pops(lbm_sim *h, bool isH, int half, const float *d_aos, long long c0,
+                   long long cells) override {
+    k_aos_to_soa<PopT><<<nblocks(cells, 256), 256, 0, h->stream>>>(scene(h), isH ? 1 : 0, half,
+                                                                     h->cur, d_aos, c0, cells);
+    h->launches++;
+  }
+  void download_pops(lbm_sim *h, bool isH, int half, float *d_aos, long long c0,
+                     long long cells) override {
+    int src = half == 2 ? 1 - h->cur : h->cur;
+    k_soa_to_aos<PopT><<<nblocks(cells, 256), 256, 0, h->stream>>>(scene(h), isH ? 1 : 0, src,
+                                                                     d_aos, c0, cells);
+    h->launches++;
+  }
+  void reencode_h(lbm_sim *h, int half, const void *d_oldPhi) override {
+    if (!Codec<PopT>::offset) return;
+    k_reencode_h<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), half,
+                                                                    (const Real *)d_oldPhi);
+    h->launches++;
+  }
+  void sphere_step_device(lbm_sim *h, lbm_sphere *d_sph, int nsph, double gravity,
+                          const double *d_fluid, const double *d_dead) override {
+    k_sphere_step<<<1, 32, 0, h->stream>>>(d_sph, nsph, gravity, d_fluid, d_dead, h->nx, h->ny, h->nz);
+    h->launches++;
+  }
+};
+
+}  // namespace lbm

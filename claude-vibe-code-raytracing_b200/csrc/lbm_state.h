@@ -1,0 +1,122 @@
+// Host-side state of one scene handle and the per-storage-type kernel
+// launcher interface.  Shared by the C ABI (lbm_capi.cu) and the typed
+// launchers (lbm_inst_*.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "lbm_b200.h"
+#include "lbm_core.cuh"
+
+struct lbm_sim;
+
+namespace lbm {
+
+// Launch configuration of the fused step kernel.
+struct FusedCfg {
+  int ty = 8;       // CTA rows (CTA = 32 x ty threads)
+  int zchunk = 32;  // z planes marched per CTA
+};
+
+class OpsBase {
+ public:
+  virtual ~OpsBase() {}
+  virtual size_t pop_bytes() const = 0;    // bytes per stored population
+  virtual size_t macro_bytes() const = 0;  // bytes per macro value
+  virtual bool phases_supported() const = 0;
+  virtual void init_flat(lbm_sim *h, const double *d_phiCol) = 0;
+  virtual void seed_hydrostatic(lbm_sim *h) = 0;
+  virtual void gradients(lbm_sim *h) = 0;
+  // Kernels of a step read the sphere set and boxes from h->dPlan.
+  virtual void retag_full(lbm_sim *h) = 0;
+  virtual void collide_phase(lbm_sim *h) = 0;
+  virtual void stream_phase(lbm_sim *h) = 0;
+  virtual void collide_hydro(lbm_sim *h) = 0;
+  virtual void stream_hydro_macro(lbm_sim *h) = 0;
+  virtual void retag_box(lbm_sim *h, long long maxCells) = 0;
+  virtual void fresh_fill(lbm_sim *h) = 0;
+  virtual void absorb_dead(lbm_sim *h, double *d_out) = 0;
+  virtual void fused_step(lbm_sim *h, const FusedCfg &cfg) = 0;
+  virtual void pack(lbm_sim *h, uint8_t *d_out) = 0;
+  // Reference-layout float32 <-> device storage for population fields.
+  // half: 0 = both halves (current state), 1 = [cur], 2 = [1-cur].
+  virtual void upload_pops(lbm_sim *h, bool isH, int half, const float *d_aos, long long c0,
+                           long long cells) = 0;
+  virtual void download_pops(lbm_sim *h, bool isH, int half, float *d_aos, long long c0,
+                             long long cells) = 0;
+  // Re-express h offsets after phi changed from d_oldPhi (both halves).
+  virtual void reencode_h(lbm_sim *h, int half, const void *d_oldPhi) = 0;
+  virtual void sphere_step_device(lbm_sim *h, lbm_sphere *d_sph, int nsph, double gravity,
+                                  const double *d_fluid, const double *d_dead) = 0;
+  // Fused-step kernel geometry (for the bench and the autotuner).
+  virtual size_t fused_smem(int ty) const = 0;
+};
+
+OpsBase *make_ops_f32();
+OpsBase *make_ops_f16();
+OpsBase *make_ops_bf16();
+OpsBase *make_ops_f64();
+
+}  // namespace lbm
+
+struct lbm_sim {
+  int nx = 0, ny = 0, nz = 0, storage = 0, device = 0;
+  long long n = 0, pitch = 0;
+  cudaStream_t stream = nullptr;
+  lbm_params params{};
+  int cur = 0;
+  lbm::OpsBase *ops = nullptr;
+  lbm::FusedCfg cfg;
+
+  // device memory
+  void *F[2] = {nullptr, nullptr};
+  void *H[2] = {nullptr, nullptr};
+  void *mac[2][5] = {{nullptr}};  // phi, rho, ux, uy, uz
+  uint8_t *tag = nullptr, *tagPrev = nullptr;
+  void *grad[4] = {nullptr};  // gx gy gz lap (phase-by-phase scratch)
+  void *us[3] = {nullptr};
+  void *bf[3] = {nullptr};
+  bool bfActive = false;
+
+  int *fresh = nullptr, *dead = nullptr;  // scan-ordered lists
+  long long listCap = 0;
+  int2 *counts = nullptr;
+  long long countsCap = 0;
+  int *totals = nullptr;  // device [2]: n_fresh, n_dead
+  bool listsValid = false;
+
+  double *impAcc = nullptr;  // per-cell impulse slots of every sphere
+  long long impCap = 0;      // doubles
+  double *partials = nullptr;
+  long long partialsCap = 0;  // doubles
+  int partialsChunks = 0;
+  double *dOut = nullptr;      // device [2][MAX][6]: fluid impulses, dead impulses
+  double *hOut = nullptr;      // pinned host mirror
+  lbm_sphere *dSph = nullptr;  // device sphere array for the coupled loop
+  lbm::Plan hPlan{};           // host copy of the step plan
+  lbm::Plan *dPlan = nullptr;  // device step plan read by the kernels
+  void *staging = nullptr;
+  size_t stagingBytes = 0;
+  double *dPhiCol = nullptr;
+  int *hTotals = nullptr;  // pinned
+
+  lbm::Box boxLast{{1, 1, 1}, {0, 0, 0}};
+  lbm::Box boxLastLast{{1, 1, 1}, {0, 0, 0}};
+  lbm::Box lastRetagBox{{1, 1, 1}, {0, 0, 0}};
+  int fullRetagSteps = 0;
+  int nsphLast = 0;
+
+  size_t deviceBytes = 0;
+  long long launches = 0;
+  unsigned long long h2dBytes = 0, d2hBytes = 0;
+  std::string err;
+
+  // CUDA-event timing of the fused kernel (lbm_fused_timing)
+  bool timing = false;
+  std::vector<cudaEvent_t> evStart, evStop;
+  size_t evUsed = 0;
+};

@@ -1,0 +1,191 @@
+/*
+ * lbm_b200.h -- C ABI of the B200-native LBM step.
+ *
+ * Drop-in for the reference's `Sim` (src/sim.js:29-601) and the per-cell /
+ * per-link work of `RigidSphere` (src/solid.js:50-101).  A Node N-API addon,
+ * a ctypes module or a C program binds these symbols; every entry point takes
+ * plain pointers and sizes and returns an int status (0 = ok, negative = error,
+ * message via lbm_last_error).  A handle owns one CUDA stream and all device
+ * state of one scene; it is not thread-safe (one owner thread, like the
+ * reference's single Web Worker, src/worker.js:1-6).
+ *
+ * Layout seen through this ABI is the reference's: cell i = (z*ny + y)*nx + x,
+ * populations array-of-structures f[i*27 + k], h[i*7 + k] (src/sim.js:35-38,
+ * 98).  On the device the populations live structure-of-arrays.
+ *
+ * The sphere is passed as a descriptor (cx..wz); the device evaluates
+ * RigidSphere.contains / surfaceVelocity in FP64 and returns the summed
+ * momentum-exchange force and torque that RigidSphere.applyImpulseAtCell would
+ * have accumulated (src/solid.js:70-80).  Several spheres form a composite
+ * solid: the first sphere that contains a cell owns it.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define LBM_OK 0
+#define LBM_ERR_ARG (-1)          /* bad argument (null, size, range)          */
+#define LBM_ERR_OOM (-2)          /* device allocation refused                 */
+#define LBM_ERR_CUDA (-3)         /* CUDA runtime error                        */
+#define LBM_ERR_TIMEOUT (-4)      /* bounded device wait ran out               */
+#define LBM_ERR_NAN (-5)          /* NaN/Inf watchdog tripped                  */
+#define LBM_ERR_STATE (-6)        /* call not valid in the current state       */
+#define LBM_ERR_UNSUPPORTED (-7)  /* option not built / not supported          */
+#define LBM_ERR_CAPACITY (-8)     /* a fixed-size device list overflowed       */
+
+/* ---- population storage forms -------------------------------------------- */
+#define LBM_STORE_F32 0  /* plain FP32 drop-in                                    */
+#define LBM_STORE_F16 1  /* FP16 offsets f-w_k, h-w_k*phi; FP32 arithmetic         */
+#define LBM_STORE_BF16 2 /* BF16 offsets f-w_k, h-w_k*phi; FP32 arithmetic         */
+#define LBM_STORE_F64 3  /* FP64 storage and arithmetic (GPU error reference)     */
+
+/* ---- fields (lbm_upload_field / lbm_download_field) ----------------------- */
+/* Element type is float32 for every field except TAG/TAG_PREV (uint8).       */
+#define LBM_FIELD_F 0        /* n*27, AoS, current populations  (sim.f)       */
+#define LBM_FIELD_F2 1       /* n*27, AoS, post-collision       (sim.f2)      */
+#define LBM_FIELD_H 2        /* n*7                              (sim.h)      */
+#define LBM_FIELD_H2 3       /* n*7                              (sim.h2)     */
+#define LBM_FIELD_RHO 4      /* sum f, the pressure proxy        (sim.rho)    */
+#define LBM_FIELD_UX 5
+#define LBM_FIELD_UY 6
+#define LBM_FIELD_UZ 7
+#define LBM_FIELD_PHI 8
+#define LBM_FIELD_PHI_PREV 9
+#define LBM_FIELD_TAG 10     /* uint8: 0 FLUID, 1 SOLID, 2 WALL (src/lattices.js:102-104) */
+#define LBM_FIELD_TAG_PREV 11
+#define LBM_FIELD_USX 12     /* solid surface velocity at SOLID cells          */
+#define LBM_FIELD_USY 13
+#define LBM_FIELD_USZ 14
+#define LBM_FIELD_GX 15      /* grad phi / lap phi scratch (sim.gx..sim.lap)   */
+#define LBM_FIELD_GY 16
+#define LBM_FIELD_GZ 17
+#define LBM_FIELD_LAP 18
+#define LBM_FIELD_BODY_FX 19 /* per-cell external force, consumed and zeroed by
+                                the next hydro stream (src/sim.js:61-64, 581) */
+#define LBM_FIELD_BODY_FY 20
+#define LBM_FIELD_BODY_FZ 21
+#define LBM_FIELD_COUNT 22
+
+typedef struct lbm_sim lbm_sim;
+
+/* Physics parameters (src/sim.js:88-95); plain doubles like the JS fields. */
+typedef struct {
+  double tau, tauPhi, sigma, gravity, rhoL, rhoG, W, mobility;
+} lbm_params;
+
+/* RigidSphere state (src/solid.js:9-44).  The per-cell kernels read only
+ * cx..wz; the device-resident integrator (lbm_run_coupled) reads and writes
+ * all of it, with RigidSphere.step's FP64 arithmetic (src/solid.js:104-210). */
+typedef struct {
+  double cx, cy, cz, r;
+  double vx, vy, vz, wx, wy, wz;
+  double density, mass, I;
+  double dragTargetX, dragTargetY, dragTargetZ;
+  double Fx, Fy, Fz, Tx, Ty, Tz;
+  int32_t dragging;
+  int32_t reserved;
+} lbm_sphere;
+
+/* Summed momentum exchange for one sphere. */
+typedef struct {
+  double Fx, Fy, Fz, Tx, Ty, Tz;
+} lbm_impulse;
+
+#define LBM_MAX_SPHERES 8
+
+/* ---- lifetime ------------------------------------------------------------- */
+/* new Sim(nx, ny, nz) (src/sim.js:30-96).  device: CUDA ordinal.  Every field
+ * starts zeroed, params take the reference defaults. */
+int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out);
+int lbm_destroy(lbm_sim *sim);
+const char *lbm_last_error(const lbm_sim *sim);
+int lbm_get_dims(const lbm_sim *sim, int *nx, int *ny, int *nz, int *storage);
+/* Bytes of device memory this handle holds. */
+int lbm_device_bytes(const lbm_sim *sim, size_t *bytes);
+/* Bytes a handle of this size would hold (admission control). */
+size_t lbm_footprint_bytes(int nx, int ny, int nz, int storage);
+
+/* Plain property writes sim.tau = ... (src/sim.js:88-95, src/worker.js:139-145). */
+int lbm_set_params(lbm_sim *sim, const lbm_params *p);
+int lbm_get_params(const lbm_sim *sim, lbm_params *p);
+
+/* ---- field transfer (reference layout, synchronous) ------------------------ */
+int lbm_upload_field(lbm_sim *sim, int field, const void *host, size_t count);
+int lbm_download_field(lbm_sim *sim, int field, void *host, size_t count);
+
+/* ---- init (src/sim.js:112-173) --------------------------------------------- */
+int lbm_init_flat(lbm_sim *sim, double waterlineY);
+int lbm_seed_hydrostatic(lbm_sim *sim);
+
+/* ---- the seven phases, callable one by one (src/sim.js:176-582) ------------- */
+/* spheres may be NULL with nspheres 0 (the reference's solid === null). */
+int lbm_retag_cells(lbm_sim *sim, const lbm_sphere *spheres, int nspheres);
+int lbm_handle_fresh_cells(lbm_sim *sim);
+int lbm_compute_phi_gradients(lbm_sim *sim);
+int lbm_collide_phase(lbm_sim *sim);
+int lbm_stream_phase(lbm_sim *sim);
+int lbm_collide_hydro(lbm_sim *sim);
+/* out: one lbm_impulse per sphere (may be NULL). */
+int lbm_stream_hydro_and_macro(lbm_sim *sim, const lbm_sphere *spheres, int nspheres,
+                               lbm_impulse *out);
+
+/* ---- Sim.step (src/sim.js:202-210), fused ---------------------------------- */
+/* retag + fresh cells on the spheres' bounding boxes, then one fused
+ * gradient + collide + pull-stream + bounce-back + macro pass per step. */
+int lbm_step(lbm_sim *sim, const lbm_sphere *spheres, int nspheres, lbm_impulse *out);
+
+/* RigidSphere.absorbDeadCells(sim) (src/solid.js:87-101): impulse rho(phi)*u
+ * of every cell that turned FLUID -> SOLID at the last retag, summed in scan
+ * order in FP64 per owning sphere. */
+int lbm_absorb_dead_cells(lbm_sim *sim, const lbm_sphere *spheres, int nspheres,
+                          lbm_impulse *out);
+
+/* Sim.packVolume(out) (src/sim.js:586-600): 2*n bytes, R = (clamp01(phi)*255)|0,
+ * G = 255 on SOLID cells. */
+int lbm_pack_volume(lbm_sim *sim, uint8_t *host_out);
+/* Same, into device memory, asynchronous on the handle's stream. */
+int lbm_pack_volume_device(lbm_sim *sim, void *device_out);
+
+/* ---- device-resident coupled loop ------------------------------------------ */
+/* nsteps x (sim.step, absorbDeadCells, RigidSphere.step(1, gravity)) entirely
+ * on the device (src/worker.js:96-100); spheres in/out on the host.  When
+ * frame_every > 0 and frames is non-NULL, the RG8 volume after every
+ * frame_every-th step is copied to frames (2*n bytes per frame). */
+int lbm_run_coupled(lbm_sim *sim, lbm_sphere *spheres, int nspheres, int nsteps,
+                    int frame_every, uint8_t *frames);
+
+/* Wait for all work queued on the handle's stream. */
+int lbm_synchronize(lbm_sim *sim);
+/* CUDA stream of the handle (cudaStream_t), for callers that enqueue around it. */
+void *lbm_stream(lbm_sim *sim);
+
+/* ---- introspection used by tests and the bench ------------------------------ */
+/* Sizes of the fresh (SOLID->FLUID) and dead (FLUID->SOLID) sets found at the
+ * last retag, and the number of SOLID-source links seen by the last stream. */
+int lbm_last_sets(lbm_sim *sim, int *n_fresh, int *n_dead);
+/* Copy the last fresh / dead cell index lists (ascending scan order). */
+int lbm_download_sets(lbm_sim *sim, int32_t *fresh, int cap_fresh, int32_t *dead,
+                      int cap_dead);
+/* Number of kernels this handle has launched since creation. */
+int lbm_launch_count(const lbm_sim *sim, int64_t *count);
+/* Host->device and device->host bytes this handle has copied since creation. */
+int lbm_transfer_bytes(const lbm_sim *sim, uint64_t *h2d, uint64_t *d2h);
+/* Time the fused step kernel with CUDA events on the handle's stream.
+ * enable = 1 starts recording (and clears the totals), 0 stops; the query
+ * synchronises the stream and returns the summed kernel time and launch count. */
+int lbm_fused_timing(lbm_sim *sim, int enable);
+int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
+/* Fused-kernel launch shape: rows per CTA (2, 4, 8 or 16) and z planes per CTA. */
+int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
