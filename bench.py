@@ -257,7 +257,12 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    check(h, L.lbm_run_coupled(h, sph, 1, args.steps, 0, None))
+    rc = L.lbm_run_coupled(h, sph, 1, args.steps, 0, None)
+    if L.lbm_checked_build():
+        rec = (C.c_int64 * 4)()
+        L.lbm_fault_record(h, rec)
+        print("fault record", list(rec), file=sys.stderr, flush=True)
+    check(h, rc)
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
@@ -316,7 +321,7 @@ def main():
             "config": {"workload": f"gravity-down pool {size}^3 with a density-2 sphere r={24 * size // 256}",
                        "grid": [size] * 3, "storage": args.storage, "parallelism": f"replicas x{ws}",
                        "l2": "state 5.3 GB > 126 MB L2, no flush needed",
-                       "fused_rows": args.rows or 8, "zchunk": args.zchunk or 32},
+                       "fused_rows": args.rows or 4, "zchunk": args.zchunk or 32},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,

@@ -10,7 +10,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblbm_b200.so")
+# LBM_B200_CHECKED=1 selects the bounds-checked build (csrc/Makefile target `checked`)
+LIB_PATH = os.path.join(_HERE, "liblbm_b200_checked.so" if os.environ.get("LBM_B200_CHECKED") == "1"
+                        else "liblbm_b200.so")
 
 OK = 0
 ERR_ARG = -1
@@ -70,6 +72,7 @@ _SIGS = [
     ("lbm_get_params", C.c_int, [C.c_void_p, C.POINTER(LbmParams)]),
     ("lbm_upload_field", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     ("lbm_download_field", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    ("lbm_download_field_f64", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_size_t]),
     ("lbm_init_flat", C.c_int, [C.c_void_p, C.c_double]),
     ("lbm_seed_hydrostatic", C.c_int, [C.c_void_p]),
     ("lbm_retag_cells", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int]),
@@ -93,6 +96,8 @@ _SIGS = [
     ("lbm_download_sets", C.c_int,
      [C.c_void_p, C.POINTER(C.c_int32), C.c_int, C.POINTER(C.c_int32), C.c_int]),
     ("lbm_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    ("lbm_checked_build", C.c_int, []),
+    ("lbm_fault_record", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("lbm_transfer_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("lbm_fused_timing", C.c_int, [C.c_void_p, C.c_int]),
     ("lbm_fused_timing_query", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

@@ -293,6 +293,14 @@ class Sim:
         return out
 
     # ------------------------------------------------------------ extras
+    def field64(self, name):
+        """A field as a float64 copy (exact for the FP64 storage form)."""
+        self._sync()
+        out = np.empty(self._count(name), dtype=np.float64)
+        check(self._h, lib().lbm_download_field_f64(self._h, FIELDS[name],
+                                                    out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        return out
+
     def synchronize(self):
         check(self._h, lib().lbm_synchronize(self._h))
 

@@ -54,7 +54,6 @@ size_t pop_bytes_of(int storage) {
 }
 size_t mac_bytes_of(int storage) { return storage == LBM_STORE_F64 ? 8 : 4; }
 
-long long pitch_of(long long n) { return (n + 127) / 128 * 128; }
 
 int dalloc(lbm_sim *h, void **p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
@@ -363,6 +362,23 @@ int get_scalar(lbm_sim *h, const void *src, float *host) {
   return LBM_OK;
 }
 
+// device scalar array of the handle's macro type -> double host array
+int get_scalar64(lbm_sim *h, const void *src, double *host) {
+  size_t n = (size_t)h->n;
+  if (h->ops->macro_bytes() == 8) {
+    CK(copy_async(h, host, src, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    int rc = ensure_staging(h, n * 8);
+    if (rc) return rc;
+    k_f32_to_real_d<<<nblocks(n, 256), 256, 0, h->stream>>>((double *)h->staging, (const float *)src, n);
+    h->launches++;
+    CKL("convert");
+    CK(copy_async(h, host, h->staging, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
 void free_all(lbm_sim *h) {
   void *ptrs[] = {h->F[0], h->F[1], h->H[0], h->H[1], h->tag, h->tagPrev, h->grad[0], h->grad[1],
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
@@ -388,9 +404,8 @@ extern "C" {
 size_t lbm_footprint_bytes(int nx, int ny, int nz, int storage) {
   if (nx < 3 || ny < 3 || nz < 3 || storage < 0 || storage > 3) return 0;
   long long n = (long long)nx * ny * nz;
-  long long pitch = pitch_of(n);
   size_t pb = pop_bytes_of(storage), mb = mac_bytes_of(storage);
-  size_t bytes = 2 * (size_t)(27 + 7) * pitch * pb;  // F, H ping-pong
+  size_t bytes = 2 * (size_t)pop_elems(n, 27 + 7) * pb;  // F, H ping-pong
   bytes += 2 * 5 * (size_t)n * mb;                     // macros ping-pong
   bytes += 2 * (size_t)n;                              // tag, tagPrev
   bytes += 2 * (size_t)n * sizeof(int);                // fresh / dead lists
@@ -419,17 +434,17 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
   h->device = device;
   h->ops = ops;
   h->n = (long long)nx * ny * nz;
-  h->pitch = pitch_of(h->n);
+  h->fusedOK = pop_elems(h->n, 27) < (1LL << 31) - 1;
   h->params = lbm_params{0.6, 0.7, 0.012, 0.0010, 1.0, 0.05, 4.0, 0.02};  // src/sim.js:88-95
   int rc = LBM_OK;
   auto body = [&]() -> int {
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     size_t pb = ops->pop_bytes(), mb = ops->macro_bytes();
     for (int c = 0; c < 2; c++) {
-      DALLOC(h->F[c], 27 * h->pitch * pb);
-      DALLOC(h->H[c], 7 * h->pitch * pb);
-      CK(cudaMemsetAsync(h->F[c], 0, 27 * h->pitch * pb, h->stream));
-      CK(cudaMemsetAsync(h->H[c], 0, 7 * h->pitch * pb, h->stream));
+      DALLOC(h->F[c], pop_elems(h->n, 27) * pb);
+      DALLOC(h->H[c], pop_elems(h->n, 7) * pb);
+      CK(cudaMemsetAsync(h->F[c], 0, pop_elems(h->n, 27) * pb, h->stream));
+      CK(cudaMemsetAsync(h->H[c], 0, pop_elems(h->n, 7) * pb, h->stream));
       for (int a = 0; a < 5; a++) {
         DALLOC(h->mac[c][a], h->n * mb);
         CK(cudaMemsetAsync(h->mac[c][a], 0, h->n * mb, h->stream));
@@ -643,7 +658,8 @@ int lbm_download_field(lbm_sim *h, int field, void *host, size_t count) {
     case LBM_FIELD_UX:
     case LBM_FIELD_UY:
     case LBM_FIELD_UZ:
-      return get_scalar(h, h->mac[h->cur][field - LBM_FIELD_PHI], dst);
+      // macro slots: 0 phi, 1 rho, 2 ux, 3 uy, 4 uz
+      return get_scalar(h, h->mac[h->cur][field == LBM_FIELD_PHI ? 0 : field - LBM_FIELD_RHO + 1], dst);
     default: {
       void *arr = nullptr;
       if (field >= LBM_FIELD_USX && field <= LBM_FIELD_USZ) arr = h->us[field - LBM_FIELD_USX];
@@ -656,6 +672,45 @@ int lbm_download_field(lbm_sim *h, int field, void *host, size_t count) {
       return get_scalar(h, arr, dst);
     }
   }
+}
+
+int lbm_download_field_f64(lbm_sim *h, int field, double *host, size_t count) {
+  if (!h || !host) return fail(h, LBM_ERR_ARG, "null");
+  if (field < 0 || field >= LBM_FIELD_COUNT) return fail(h, LBM_ERR_ARG, "unknown field");
+  if (field == LBM_FIELD_TAG || field == LBM_FIELD_TAG_PREV)
+    return fail(h, LBM_ERR_ARG, "tags are uint8; use lbm_download_field");
+  if (count != field_count(h, field)) return fail(h, LBM_ERR_ARG, "element count mismatch");
+  DeviceGuard g(h->device);
+  size_t n = (size_t)h->n;
+  if (field <= LBM_FIELD_H2) {
+    bool isH = field == LBM_FIELD_H || field == LBM_FIELD_H2;
+    bool second = field == LBM_FIELD_F2 || field == LBM_FIELD_H2;
+    int Q = isH ? 7 : 27;
+    long long chunk = std::min<long long>(h->n, 1 << 19);
+    int rc = ensure_staging(h, (size_t)chunk * Q * sizeof(double));
+    if (rc) return rc;
+    for (long long c0 = 0; c0 < h->n; c0 += chunk) {
+      long long cells = std::min(chunk, h->n - c0);
+      h->ops->download_pops64(h, isH, second ? 2 : 1, (double *)h->staging, c0, cells);
+      CKL("download populations");
+      CK(copy_async(h, host + c0 * Q, h->staging, cells * Q * sizeof(double), cudaMemcpyDeviceToHost,
+                    h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+    }
+    return LBM_OK;
+  }
+  const void *arr = nullptr;
+  if (field == LBM_FIELD_PHI_PREV) arr = h->mac[1 - h->cur][0];
+  else if (field >= LBM_FIELD_RHO && field <= LBM_FIELD_PHI)
+    arr = h->mac[h->cur][field == LBM_FIELD_PHI ? 0 : field - LBM_FIELD_RHO + 1];
+  else if (field >= LBM_FIELD_USX && field <= LBM_FIELD_USZ) arr = h->us[field - LBM_FIELD_USX];
+  else if (field >= LBM_FIELD_GX && field <= LBM_FIELD_LAP) arr = h->grad[field - LBM_FIELD_GX];
+  else arr = h->bf[field - LBM_FIELD_BODY_FX];
+  if (!arr) {
+    memset(host, 0, n * sizeof(double));
+    return LBM_OK;
+  }
+  return get_scalar64(h, arr, host);
 }
 
 int lbm_init_flat(lbm_sim *h, double waterlineY) {
@@ -782,9 +837,10 @@ int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
   DeviceGuard g(h->device);
-  if (h->bfActive) {
+  if (h->bfActive || !h->fusedOK) {
     // A pending external body force is consumed by the phase-by-phase path,
-    // which reads it (src/sim.js:434-436, 558-560).
+    // which reads it (src/sim.js:434-436, 558-560); grids too large for the
+    // fused kernel's 32-bit indexing take the same path.
     if ((rc = lbm_retag_cells(h, sp, ns))) return rc;
     if ((rc = lbm_handle_fresh_cells(h))) return rc;
     if ((rc = lbm_compute_phi_gradients(h))) return rc;
@@ -860,6 +916,7 @@ int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_ev
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
   if (h->bfActive) return fail(h, LBM_ERR_STATE, "a pending body force needs lbm_step");
+  if (!h->fusedOK) return fail(h, LBM_ERR_UNSUPPORTED, "grid too large for the fused kernel");
   DeviceGuard g(h->device);
   // capacity bounds for the device-computed plan
   double rmax = 0;
@@ -987,6 +1044,23 @@ int lbm_launch_count(const lbm_sim *h, int64_t *count) {
   return LBM_OK;
 }
 
+int lbm_checked_build(void) {
+#ifdef LBM_CHECKED
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+int lbm_fault_record(lbm_sim *h, int64_t out[4]) {
+  if (!h || !out) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  unsigned long long r[4] = {0, 0, 0, 0};
+  CK(h->ops->read_fault(h, r));
+  for (int j = 0; j < 4; j++) out[j] = (int64_t)r[j];
+  return LBM_OK;
+}
+
 int lbm_transfer_bytes(const lbm_sim *h, uint64_t *h2d, uint64_t *d2h) {
   if (!h) return LBM_ERR_ARG;
   if (h2d) *h2d = h->h2dBytes;
@@ -1018,8 +1092,8 @@ int lbm_fused_timing_query(lbm_sim *h, double *total_ms, int64_t *launches) {
 
 int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
   if (!h) return LBM_ERR_ARG;
-  if (!(rows == 2 || rows == 4 || rows == 8 || rows == 16) || zchunk < 1)
-    return fail(h, LBM_ERR_ARG, "rows must be 2, 4, 8 or 16 and zchunk >= 1");
+  if (!(rows == 2 || rows == 4 || rows == 8) || zchunk < 1)
+    return fail(h, LBM_ERR_ARG, "rows must be 2, 4 or 8 and zchunk >= 1");
   if (h->ops->fused_smem(rows) > 227 * 1024)
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;

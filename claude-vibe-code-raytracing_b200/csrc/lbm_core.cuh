@@ -114,6 +114,17 @@ struct Codec<__nv_bfloat16> {
   }
 };
 
+// ---------------------------------------------------------------- population layout
+// Populations are stored in blocks of 8 consecutive cells (flat cell order),
+// direction-major inside a block: element (k, i) of a Q-direction lattice is at
+// ((i >> 3) * Q + k) * 8 + (i & 7).  A warp touching 32 consecutive cells reads
+// whole 32-byte sectors, and the offset between directions is a constant.
+template <int Q>
+__host__ __device__ __forceinline__ long long pidx(int k, long long i) {
+  return ((i >> 3) * Q + k) * 8 + (i & 7);
+}
+__host__ __device__ inline long long pop_elems(long long n, int Q) { return (n + 7) / 8 * 8 * Q; }
+
 // ---------------------------------------------------------------- scene view
 // Device pointers of one scene.  Index c in [0,1] selects a ping-pong half:
 // populations and macros are double-buffered so the fused step can read the
@@ -122,8 +133,7 @@ struct Codec<__nv_bfloat16> {
 template <class PopT, class Real>
 struct Scene {
   int nx, ny, nz;
-  long long n;     // cells
-  long long pitch; // elements between direction planes of F/H
+  long long n;  // cells
   PopT *F[2];
   PopT *H[2];
   Real *phi[2], *rho[2], *ux[2], *uy[2], *uz[2];

@@ -1,0 +1,497 @@
+// The fused LBM step kernel (one launch per step over the whole grid).
+//
+// A CTA owns a 32 x TY column of cells and marches it up a range of z planes,
+// with TY "cell" warps (one cell per thread) and two "halo" warps.  For each
+// plane z:
+//   1. plane z+1 is collided: every cell thread loads its cell's 27 + 7
+//      populations, phi stencil, rho and u, evaluates the reference's BGK
+//      collisions (collideHydro src/sim.js:406-464, collidePhase
+//      src/sim.js:324-364) in registers and writes the post-collision values
+//      into a shared-memory ring; meanwhile the halo warps collide the
+//      one-cell in-plane halo, only for the directions that point into the
+//      tile (halo warp A: the rows above and below, halo warp B: the side
+//      columns and corners);
+//   2. after a barrier the cell threads pull plane z from the ring
+//      (streamPhase src/sim.js:376-397, streamHydroAndMacro src/sim.js:509-543):
+//      fluid sources give their post-collision value, wall and solid sources
+//      bounce back the cell's own value, SOLID sources add the Ladd
+//      moving-wall term and FP64 momentum exchange; then the macros
+//      (src/sim.js:545-576), and the new populations and macros are written
+//      once.
+//
+// The collision is evaluated in the equivalent form
+//   f*_k = (1 - w) f_k + w_k (C0 + e.V + (e.u)(e.Q)),
+//   C0 = w sumF - 1.5 w rho_phase u^2 - A u.F,  V = 3 w rho_phase u + A F,
+//   Q  = 4.5 w rho_phase u + 3 A F   (w = 1/tau, A = 3(1 - w/2)),
+//   h*_k = (1 - wp) h_k + w7_k (wp phi + e.(4 wp phi u + S)),
+// which expands to the reference's feq / Guo source / sharpening terms.
+//
+// Ring layout: directions grouped by e_z.  Values pulled from plane z+1
+// (e_z = -1) are read in the iteration they are written, but a plane's own
+// e_z = -1 values are needed for bounce-back, so that group keeps 2 planes;
+// e_z = 0 keeps 2 planes; e_z = +1 keeps 3.
+//
+// Per cell and step the kernel reads the 34 populations, phi, rho, u and the
+// tag once and writes 34 populations and 5 macros once (313 B at FP32).
+#pragma once
+
+#include "lbm_kernels.cuh"
+
+namespace lbm {
+
+template <class PopT>
+struct FusedArgs {
+  Scene<PopT, typename Prec<PopT>::Real> s;
+  int cur;
+  int zchunk;
+  double om, omP, A, beta4, kappa, rhoG, dRho, gravity, sharpC4;
+  const SolidSet *ss;
+};
+
+// slot of direction k within its e_z group (0..8 for D3Q27)
+constexpr int slot27(int k) {
+  int s = 0;
+  for (int j = 0; j < k; j++)
+    if (kDir[j][2] == kDir[k][2]) s++;
+  return s;
+}
+// the same, indexable at run time
+static __constant__ signed char c_slot27[27] = {0, 1, 2, 3, 4, 0, 0, 5, 6, 7, 8, 1, 1, 2,
+                                                 2, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 8, 8};
+// ring plane offsets (in planes of NC values)
+constexpr int RING_F_M = 0, RING_F_Z = 18, RING_F_P = 36;  // 2x9, 2x9, 3x9
+constexpr int RING_H_M = 63, RING_H_Z = 65, RING_H_P = 75;  // 2x1, 2x5, 3x1
+constexpr int RING_PLANES = 78;
+
+template <class PopT, int TY>
+struct FusedSmem {
+  using Real = typename Prec<PopT>::Real;
+  static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;
+  static constexpr size_t bytes = (size_t)RING_PLANES * NC * sizeof(Real) + 3 * NC;
+  static constexpr int warps = TY + 2;  // TY cell warps, 2 halo warps
+  static constexpr int threads = 32 * warps;
+};
+
+// CTAs per SM the register budget is sized for
+template <int TY>
+struct FusedOcc {
+  static constexpr int blocks = TY >= 8 ? 2 : (TY >= 4 ? 3 : 5);
+};
+
+// Directions a halo cell must collide: those pointing into the tile.
+// SX / SY = +-1 select e_x / e_y equal to that value, 0 means any.
+template <int SX, int SY, int K>
+constexpr bool halo_dir() {
+  return (SX == 0 || kDir[K][0] == SX) && (SY == 0 || kDir[K][1] == SY);
+}
+
+template <int V>
+using IC = std::integral_constant<int, V>;
+
+// ---------------------------------------------------------------- checked build
+// Built with -DLBM_CHECKED, every global and shared access of the fused kernel
+// is bounds-checked; the first violation is recorded (location code, index,
+// block, thread) in lbm_fault_word and the access is skipped instead of
+// faulting.  Without the macro the helpers are plain loads and stores.
+static __device__ unsigned long long lbm_fault_word[4];
+
+__device__ __forceinline__ bool lbm_ok(bool ok, int code, long long idx) {
+#ifdef LBM_CHECKED
+  if (!ok) {
+    if (atomicCAS(&lbm_fault_word[0], 0ull, (unsigned long long)code) == 0ull) {
+      lbm_fault_word[1] = (unsigned long long)idx;
+      lbm_fault_word[2] = blockIdx.x | ((unsigned long long)blockIdx.y << 20) |
+                          ((unsigned long long)blockIdx.z << 40);
+      lbm_fault_word[3] = threadIdx.x | (threadIdx.y << 8);
+    }
+  }
+  return ok;
+#else
+  (void)code;
+  (void)idx;
+  return true;
+#endif
+}
+
+template <class T>
+__device__ __forceinline__ T ldg_at(const T *p, long long idx, long long lim, int code) {
+  if (!lbm_ok(idx >= 0 && idx < lim, code, idx)) return T();
+  return __ldg(p + idx);
+}
+template <class T>
+__device__ __forceinline__ void st_at(T *p, long long idx, long long lim, int code, T v) {
+  if (lbm_ok(idx >= 0 && idx < lim, code, idx)) p[idx] = v;
+}
+__device__ __forceinline__ int sm_at(int idx, int lim, int code) {
+  return lbm_ok(idx >= 0 && idx < lim, code, idx) ? idx : 0;
+}
+
+// Everything the collision of one cell reads from global memory.
+template <class PopT>
+struct CellLoad {
+  using Real = typename Prec<PopT>::Real;
+  PopT fv[Q27];
+  PopT hv[Q7];
+  Real p, pxp, pxm, pyp, pym, pzp, pzm, sumF, ux, uy, uz;
+  uint8_t tg;
+};
+
+template <class PopT, int TY>
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
+    k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
+  using Real = typename Prec<PopT>::Real;
+  using C = Codec<PopT>;
+  using SM = FusedSmem<PopT, TY>;
+  using LD = CellLoad<PopT>;
+  constexpr int RX = SM::RX, NC = SM::NC;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real *ring = reinterpret_cast<Real *>(smem_raw);                        // [78][NC]
+  uint8_t *stag = smem_raw + (size_t)RING_PLANES * NC * sizeof(Real);    // [3][NC]
+
+  const auto &s = a.s;
+  const SolidSet &ss = *a.ss;
+  const int cur = a.cur, nxt = 1 - cur;
+  const PopT *__restrict__ Fc = s.F[cur];
+  const PopT *__restrict__ Hc = s.H[cur];
+  PopT *__restrict__ Fn = s.F[nxt];
+  PopT *__restrict__ Hn = s.H[nxt];
+  const Real *__restrict__ phiC = s.phi[cur];
+  const Real *__restrict__ rhoC = s.rho[cur];
+  const Real *__restrict__ uxC = s.ux[cur];
+  const Real *__restrict__ uyC = s.uy[cur];
+  const Real *__restrict__ uzC = s.uz[cur];
+  const uint8_t *__restrict__ tagA = s.tag;
+  const int nx = s.nx, ny = s.ny, nz = s.nz, nxny = nx * ny;
+  const long long nCell = s.n, nF = pop_elems(s.n, Q27), nH = pop_elems(s.n, Q7);
+  constexpr int RING = RING_PLANES * NC, TAGS = 3 * NC;
+  const Real om = (Real)a.om, omP = (Real)a.omP, A = (Real)a.A;
+  const Real beta4 = (Real)a.beta4, kappa = (Real)a.kappa, rhoG = (Real)a.rhoG;
+  const Real dRho = (Real)a.dRho, grav = (Real)a.gravity, sharpC4 = (Real)a.sharpC4;
+
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const bool haloA = ty == TY, haloB = ty == TY + 1, haloWarp = ty >= TY;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TY;
+  const int zb = 1 + blockIdx.z * a.zchunk;
+  const int ze = min(zb + a.zchunk, nz - 1);
+  if (zb >= ze) return;
+  const int x = x0 + tx, y = y0 + ty;
+  const int own = (ty + 1) * RX + (tx + 1);
+
+  // Side lane of halo warp B: 0..TY-1 left column, TY..2TY-1 right column,
+  // then the four corners (0,0) (33,0) (0,TY+1) (33,TY+1); others idle.
+  int sideLx = 0, sideLy = 0, sideSx = 2, sideSy = 2;
+  const bool sideAct = tx < 2 * TY + 4;
+  if (tx < TY) {
+    sideLx = 0, sideLy = tx + 1, sideSx = 1, sideSy = 0;
+  } else if (tx < 2 * TY) {
+    sideLx = RX - 1, sideLy = tx - TY + 1, sideSx = -1, sideSy = 0;
+  } else if (sideAct) {
+    const int c = tx - 2 * TY;
+    sideLx = (c & 1) ? RX - 1 : 0;
+    sideLy = (c & 2) ? TY + 1 : 0;
+    sideSx = (c & 1) ? -1 : 1;
+    sideSy = (c & 2) ? -1 : 1;
+  }
+
+  // Directions a pass needs: MODE 0 all (a tile cell); MODE 1 the compile-time
+  // halo side (SX, SY); MODE 2 the run-time side (sx, sy), none when inactive.
+  auto needs = [&](auto MODEc, auto SXc, auto SYc, auto KK, int sx, int sy,
+                   bool active) __attribute__((always_inline)) -> bool {
+    constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
+    constexpr int k = decltype(KK)::value;
+    if constexpr (MODE == 0) return true;
+    else if constexpr (MODE == 1) return halo_dir<SX, SY, k>();
+    else return active && (sx == 0 || D27<k>::ex == sx) && (sy == 0 || D27<k>::ey == sy);
+  };
+
+  // Load phase: every load comes from a valid, clamped address and none waits
+  // on the tag, so a pass costs one memory latency.
+  auto load = [&](auto MODEc, auto SXc, auto SYc, int sx, int sy, bool active, int q, int gx_, int gy_,
+                  LD &L) __attribute__((always_inline)) {
+    constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
+    const bool inside = gx_ >= 0 && gx_ < nx && gy_ >= 0 && gy_ < ny && q >= 0 && q < nz;
+    const int ci = inside ? q * nxny + gy_ * nx + gx_ : 0;
+    const int bF = (ci >> 3) * (8 * Q27) + (ci & 7);
+    const int bH = (ci >> 3) * (8 * Q7) + (ci & 7);
+    static_for<0, Q27>([&](auto KK) {
+      constexpr int k = decltype(KK)::value;
+      if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
+        const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
+        L.fv[k] = nd ? ldg_at(Fc, bF + 8 * k, nF, 3) : PopT();
+        if constexpr (k < Q7) L.hv[k] = nd ? ldg_at(Hc, bH + 8 * k, nH, 4) : PopT();
+      }
+    });
+    uint8_t tg = ldg_at(tagA, ci, nCell, 1);
+    const int last = (int)nCell - 1;
+    L.p = ldg_at(phiC, ci, nCell, 5);
+    L.pxp = ldg_at(phiC, min(ci + 1, last), nCell, 5);
+    L.pxm = ldg_at(phiC, max(ci - 1, 0), nCell, 5);
+    L.pyp = ldg_at(phiC, min(ci + nx, last), nCell, 5);
+    L.pym = ldg_at(phiC, max(ci - nx, 0), nCell, 5);
+    L.pzp = ldg_at(phiC, min(ci + nxny, last), nCell, 5);
+    L.pzm = ldg_at(phiC, max(ci - nxny, 0), nCell, 5);
+    L.sumF = ldg_at(rhoC, ci, nCell, 6);
+    L.ux = ldg_at(uxC, ci, nCell, 6);
+    L.uy = ldg_at(uyC, ci, nCell, 6);
+    L.uz = ldg_at(uzC, ci, nCell, 6);
+    // boundary cells never act as fluid (they are walls after any retag)
+    const bool inner = gx_ >= 1 && gx_ <= nx - 2 && gy_ >= 1 && gy_ <= ny - 2 && q >= 1 && q <= nz - 2;
+    if (!inside || (!inner && tg == TAG_FLUID)) tg = TAG_WALL;
+    L.tg = tg;
+  };
+
+  // Compute phase: collision into ring cell lc of plane q and the cell's tag.
+  // Values computed for non-fluid cells land in ring slots that are never
+  // read as sources.  Returns gradient, laplacian and phi of the cell.
+  auto compute = [&](auto MODEc, auto SXc, auto SYc, int sx, int sy, bool active, int q, int lc,
+                     const LD &L, Real &ogx, Real &ogy, Real &ogz, Real &olap,
+                     Real &ophi) __attribute__((always_inline)) {
+    constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
+    const int fbM = (RING_F_M + (q & 1) * 9) * NC + lc, fbZ = (RING_F_Z + (q & 1) * 9) * NC + lc;
+    const int fbP = (RING_F_P + (q % 3) * 9) * NC + lc;
+    const int hbM = (RING_H_M + (q & 1)) * NC + lc, hbZ = (RING_H_Z + (q & 1) * 5) * NC + lc;
+    const int hbP = (RING_H_P + (q % 3)) * NC + lc;
+    if (MODE != 2 || active) stag[sm_at((q % 3) * NC + lc, TAGS, 2)] = L.tg;
+    const Real p = L.p, ux = L.ux, uy = L.uy, uz = L.uz;
+    const Real gxv = (Real)0.5 * (L.pxp - L.pxm);
+    const Real gyv = (Real)0.5 * (L.pyp - L.pym);
+    const Real gzv = (Real)0.5 * (L.pzp - L.pzm);
+    const Real lap = L.pxp + L.pxm + L.pyp + L.pym + L.pzp + L.pzm - (Real)6 * p;
+    const Real rhoPh = rhoG + p * dRho;
+    const Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lap;
+    const Real Fx = mu * gxv, Fy = mu * gyv + rhoPh * grav, Fz = mu * gzv;
+    const Real u2 = ux * ux + uy * uy + uz * uz;
+    const Real uF = ux * Fx + uy * Fy + uz * Fz;
+    const Real orh = om * rhoPh;
+    const Real C0 = om * L.sumF - (Real)1.5 * orh * u2 - A * uF;
+    const Real orh3 = (Real)3 * orh;
+    const Real Vx = orh3 * ux + A * Fx, Vy = orh3 * uy + A * Fy, Vz = orh3 * uz + A * Fz;
+    const Real A3 = (Real)3 * A, orh45 = (Real)4.5 * orh;
+    const Real Qx = orh45 * ux + A3 * Fx, Qy = orh45 * uy + A3 * Fy, Qz = orh45 * uz + A3 * Fz;
+    const Real gmag = sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + (Real)1e-12;
+    const Real sh = sharpC4 * p * ((Real)1 - p) / gmag;
+    const Real fp = (Real)4 * omP * p;
+    const Real D0 = omP * p;
+    const Real Dx = fp * ux + sh * gxv, Dy = fp * uy + sh * gyv, Dz = fp * uz + sh * gzv;
+    const Real om1 = (Real)1 - om, omP1 = (Real)1 - omP;
+    static_for<0, Q27>([&](auto KK) {
+      constexpr int k = decltype(KK)::value;
+      using D = D27<k>;
+      constexpr int ex = D::ex, ey = D::ey, ez = D::ez;
+      if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
+        const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
+        Real ev = 0, eu = 0, eq = 0;
+        if constexpr (ex != 0) {
+          ev += (Real)ex * Vx;
+          eu += (Real)ex * ux;
+          eq += (Real)ex * Qx;
+        }
+        if constexpr (ey != 0) {
+          ev += (Real)ey * Vy;
+          eu += (Real)ey * uy;
+          eq += (Real)ey * Qy;
+        }
+        if constexpr (ez != 0) {
+          ev += (Real)ez * Vz;
+          eu += (Real)ez * uz;
+          eq += (Real)ez * Qz;
+        }
+        const Real fk = om1 * C::dec(L.fv[k], (Real)D::w) + (Real)D::w * (C0 + ev + eu * eq);
+        const int fb = ez < 0 ? fbM : (ez == 0 ? fbZ : fbP);
+        if (nd) ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
+        if constexpr (k < Q7) {
+          using E = D7<k>;
+          Real ed = 0;
+          if constexpr (ex != 0) ed += (Real)ex * Dx;
+          if constexpr (ey != 0) ed += (Real)ey * Dy;
+          if constexpr (ez != 0) ed += (Real)ez * Dz;
+          Real href = 0;
+          if constexpr (C::offset) href = (Real)E::w * p;
+          const Real hk = omP1 * C::dec(L.hv[k], href) + (Real)E::w * (D0 + ed);
+          const int hb = ez < 0 ? hbM : (ez == 0 ? hbZ : hbP);
+          if (nd) ring[sm_at(hb + (ez == 0 ? k : 0) * NC, RING, 8)] = hk;
+        }
+      }
+    });
+    ogx = gxv;
+    ogy = gyv;
+    ogz = gzv;
+    olap = lap;
+    ophi = p;
+  };
+
+  // Collide plane q: cell warps their own cells; halo warp A the rows above
+  // and below the tile (both rows loaded before either is computed); halo
+  // warp B the side columns and corners.
+  // (lambdas are forced inline: an outlined closure would live in local memory)
+  auto collide_plane = [&](int q, Real &ogx, Real &ogy, Real &ogz, Real &olap,
+                           Real &ophi) __attribute__((always_inline)) {
+    if (!haloWarp) {
+      LD L;
+      load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
+      compute(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, L, ogx, ogy, ogz, olap, ophi);
+    } else if (haloA) {
+      Real d0, d1, d2, d3, d4;
+      LD top, bot;
+      load(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, x, y0 - 1, top);
+      load(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, x, y0 + TY, bot);
+      compute(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, tx + 1, top, d0, d1, d2, d3, d4);
+      compute(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, (TY + 1) * RX + tx + 1, bot, d0, d1, d2, d3,
+              d4);
+    } else {
+      Real d0, d1, d2, d3, d4;
+      LD L;
+      load(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, x0 - 1 + sideLx, y0 - 1 + sideLy, L);
+      compute(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, sideLy * RX + sideLx, L, d0, d1,
+              d2, d3, d4);
+    }
+  };
+
+  Real gxC = 0, gyC = 0, gzC = 0, lapC = 0, phC = 0;
+  Real gxN = 0, gyN = 0, gzN = 0, lapN = 0, phN = 0;
+  collide_plane(zb - 1, gxN, gyN, gzN, lapN, phN);
+  collide_plane(zb, gxC, gyC, gzC, lapC, phC);
+
+  const bool colActive = !haloWarp && x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
+
+  for (int z = zb; z < ze; z++) {
+    collide_plane(z + 1, gxN, gyN, gzN, lapN, phN);
+    __syncthreads();
+    const int sC = z % 3;
+    const uint8_t tagI = colActive ? stag[sm_at(sC * NC + own, TAGS, 9)] : TAG_WALL;
+    const int i = z * nxny + y * nx + x;
+    const int bF = (i >> 3) * (8 * Q27) + (i & 7);
+    const int bH = (i >> 3) * (8 * Q7) + (i & 7);
+    if (tagI == TAG_SOLID) {
+      // Solid cells are not updated; carry their state into the next half so
+      // both halves hold the reference's stale values.
+#pragma unroll 1
+      for (int k = 0; k < Q27; k++) st_at(Fn, bF + 8 * k, nF, 10, ldg_at(Fc, bF + 8 * k, nF, 10));
+#pragma unroll 1
+      for (int k = 0; k < Q7; k++) st_at(Hn, bH + 8 * k, nH, 11, ldg_at(Hc, bH + 8 * k, nH, 11));
+      st_at(s.phi[nxt], i, nCell, 12, ldg_at(phiC, i, nCell, 12));
+      st_at(s.rho[nxt], i, nCell, 12, ldg_at(rhoC, i, nCell, 12));
+      st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
+      st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
+      st_at(s.uz[nxt], i, nCell, 12, ldg_at(uzC, i, nCell, 12));
+    } else if (tagI == TAG_FLUID) {
+      // ring bases: group e_z sources come from plane z - e_z; the cell's own
+      // (bounce-back) values are in plane z
+      const int sbFM = (RING_F_M + ((z + 1) & 1) * 9) * NC + own;
+      const int sbFZ = (RING_F_Z + (z & 1) * 9) * NC + own;
+      const int sbFP = (RING_F_P + ((z + 2) % 3) * 9) * NC + own;
+      const int obFM = (RING_F_M + (z & 1) * 9) * NC + own;
+      const int obFP = (RING_F_P + (z % 3) * 9) * NC + own;
+      const int sbHM = (RING_H_M + ((z + 1) & 1)) * NC + own;
+      const int sbHZ = (RING_H_Z + (z & 1) * 5) * NC + own;
+      const int sbHP = (RING_H_P + ((z + 2) % 3)) * NC + own;
+      const int obHM = (RING_H_M + (z & 1)) * NC + own;
+      const int obHP = (RING_H_P + (z % 3)) * NC + own;
+      const int tbM = ((z + 1) % 3) * NC + own, tbZ = sC * NC + own, tbP = ((z + 2) % 3) * NC + own;
+      const Real rhoPhOld = rhoG + phC * dRho;
+      Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
+      Real hn[Q7];
+      uint32_t solidM = 0;
+      static_for<0, Q27>([&](auto KK) {
+        constexpr int k = decltype(KK)::value;
+        using D = D27<k>;
+        constexpr int ex = D::ex, ey = D::ey, ez = D::ez, o = D::opp;
+        constexpr int oz = D27<o>::ez;
+        constexpr int so = -ey * RX - ex;  // source offset in the ring plane
+        const int tb = ez < 0 ? tbM : (ez == 0 ? tbZ : tbP);
+        const int sbF = ez < 0 ? sbFM : (ez == 0 ? sbFZ : sbFP);
+        const int obF = oz < 0 ? obFM : (oz == 0 ? sbFZ : obFP);
+        const uint8_t ts = stag[sm_at(tb + so, TAGS, 13)];
+        const bool fl = ts == TAG_FLUID;
+        // fluid source: its post-collision value; otherwise halfway bounce-back
+        // of the cell's own opposite value (moving-wall term added below)
+        const Real fk = ring[sm_at(fl ? sbF + slot27(k) * NC + so : obF + slot27(o) * NC, RING, 14)];
+        solidM |= (uint32_t)(ts == TAG_SOLID) << k;
+        st_at(Fn, bF + 8 * k, nF, 15, C::enc(fk, (Real)D::w));
+        rhoA += fk;
+        if constexpr (ex != 0) mx += (Real)ex * fk;
+        if constexpr (ey != 0) my += (Real)ey * fk;
+        if constexpr (ez != 0) mz += (Real)ez * fk;
+        if constexpr (k < Q7) {
+          constexpr int hs = (ez == 0 ? k : 0), hso = (oz == 0 ? o : 0);
+          const int sbH = ez < 0 ? sbHM : (ez == 0 ? sbHZ : sbHP);
+          const int obH = oz < 0 ? obHM : (oz == 0 ? sbHZ : obHP);
+          const Real hk = ring[sm_at(fl ? sbH + hs * NC + so : obH + hso * NC, RING, 16)];
+          hn[k] = hk;
+          hsum += hk;
+        }
+      });
+      // Links to SOLID sources (rare): Ladd moving-wall term
+      // 2 w_k rho_phase(phi_old) (e_k . u_s) / cs^2 and the FP64 momentum
+      // exchange -(f_opp + f_k) e_k at the solid cell (src/sim.js:517-536).
+      if (solidM) {
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        int owner = -1;
+        for (uint32_t m = solidM; m; m &= m - 1) {
+          const int k = __ffs(m) - 1;
+          const int ex = dcomp(k, 0), ey = dcomp(k, 1), ez = dcomp(k, 2);
+          const int o = opp_of(k), oz = -ez;
+          const int sx = x - ex, sy = y - ey, sz = z - ez;
+          const int b = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, sx, sy, sz);
+          if (b < 0) continue;
+          double ox, oy, oz_;
+          sphere_surface_velocity(ss.sph[b], sx, sy, sz, ox, oy, oz_);
+          // surface velocity rounded as the reference stores it (Float32Array us)
+          const Real eus = (Real)ex * (Real)ox + (Real)ey * (Real)oy + (Real)ez * (Real)oz_;
+          const Real w = (Real)w27_of(k);
+          const Real corr = (Real)2 * w * rhoPhOld * eus * (Real)3;
+          const int obF = oz < 0 ? obFM : (oz == 0 ? sbFZ : obFP);
+          const Real fopp = ring[sm_at(obF + c_slot27[o] * NC, RING, 19)];
+          const Real fk = fopp + corr;
+          st_at(Fn, bF + 8 * k, nF, 15, C::enc(fk, w));
+          rhoA += corr;
+          mx += (Real)ex * corr;
+          my += (Real)ey * corr;
+          mz += (Real)ez * corr;
+          if (b != owner) {
+            flush_impulse(ss, owner, x, y, z, acc);
+            owner = b;
+          }
+          const double mom = __dadd_rn((double)fopp, (double)fk);
+          impulse_terms(ss.sph[b], sx, sy, sz, -mom * ex, -mom * ey, -mom * ez, acc);
+        }
+        flush_impulse(ss, owner, x, y, z, acc);
+      }
+
+      // macros (src/sim.js:545-576)
+      const Real rhoN = rhoA > (Real)0.01 ? rhoA : (Real)0.01;
+      const Real p = hsum < (Real)0 ? (Real)0 : hsum > (Real)1 ? (Real)1 : hsum;
+      static_for<0, Q7>([&](auto KK) {
+        constexpr int k = decltype(KK)::value;
+        st_at(Hn, bH + 8 * k, nH, 17, C::enc(hn[k], (Real)D7<k>::w * p));
+      });
+      const Real rhoPhN = rhoG + p * dRho;
+      const Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lapC;
+      const Real Fx = mu * gxC, Fy = mu * gyC + rhoPhN * grav, Fz = mu * gzC;
+      const Real inv = (Real)1 / rhoPhN;
+      Real uxn = (mx + (Real)0.5 * Fx) * inv;
+      Real uyn = (my + (Real)0.5 * Fy) * inv;
+      Real uzn = (mz + (Real)0.5 * Fz) * inv;
+      const Real u2 = uxn * uxn + uyn * uyn + uzn * uzn;
+      if (u2 > (Real)(0.2 * 0.2)) {
+        const Real sc = (Real)0.2 / sqrt(u2);
+        uxn *= sc;
+        uyn *= sc;
+        uzn *= sc;
+      }
+      st_at(s.rho[nxt], i, nCell, 18, rhoN);
+      st_at(s.phi[nxt], i, nCell, 18, p);
+      st_at(s.ux[nxt], i, nCell, 18, uxn);
+      st_at(s.uy[nxt], i, nCell, 18, uyn);
+      st_at(s.uz[nxt], i, nCell, 18, uzn);
+    }
+    __syncthreads();
+    gxC = gxN;
+    gyC = gyN;
+    gzC = gzN;
+    lapC = lapN;
+    phC = phN;
+  }
+}
+
+}  // namespace lbm

@@ -86,11 +86,11 @@ __global__ void k_init_flat(Scene<PopT, typename Prec<PopT>::Real> s, const doub
     s.ux[c][i] = s.uy[c][i] = s.uz[c][i] = (Real)0;
     for (int k = 0; k < Q27; k++) {
       Real w = (Real)w27_of(k);
-      s.F[c][k * s.pitch + i] = Codec<PopT>::enc(w, w);
+      s.F[c][pidx<27>(k, i)] = Codec<PopT>::enc(w, w);
     }
     for (int k = 0; k < Q7; k++) {
       Real hv = (Real)((double)w7_of(k) * pc);
-      s.H[c][k * s.pitch + i] = Codec<PopT>::enc(hv, (Real)w7_of(k) * phiR);
+      s.H[c][pidx<7>(k, i)] = Codec<PopT>::enc(hv, (Real)w7_of(k) * phiR);
     }
   }
   uint8_t tg = wall ? TAG_WALL : TAG_FLUID;
@@ -123,8 +123,8 @@ __global__ void k_seed_hydrostatic(Scene<PopT, typename Prec<PopT>::Real> s, int
       double fk = (double)w27_of(k) * (pCs2 + rhoPhase * Qi);
       Real w = (Real)w27_of(k);
       PopT e = Codec<PopT>::enc((Real)fk, w);
-      s.F[0][k * s.pitch + i] = e;
-      s.F[1][k * s.pitch + i] = e;
+      s.F[0][pidx<27>(k, i)] = e;
+      s.F[1][pidx<27>(k, i)] = e;
     }
     pCs2 += rhoPhase * gOverCs2;
   }
@@ -189,9 +189,10 @@ __global__ void k_retag_full(Scene<PopT, typename Prec<PopT>::Real> s, int cur,
     double ox, oy, oz;
     sphere_surface_velocity(ss.sph[b], x, y, z, ox, oy, oz);
     s.tag[i] = TAG_SOLID;
-    s.usx[i] = (Real)(float)ox;
-    s.usy[i] = (Real)(float)oy;
-    s.usz[i] = (Real)(float)oz;
+    // stored like the reference's Float32Array us (double in the FP64 form)
+    s.usx[i] = (Real)ox;
+    s.usy[i] = (Real)oy;
+    s.usz[i] = (Real)oz;
   } else {
     s.tag[i] = TAG_FLUID;
     s.usx[i] = s.usy[i] = s.usz[i] = (Real)0;
@@ -223,8 +224,8 @@ __global__ void k_collide_phase(Scene<PopT, typename Prec<PopT>::Real> s, int cu
     Real eu = ex * uxi + ey * uyi + ez * uzi;
     Real heq = wk * p * ((Real)1 + (Real)4 * eu);
     Real Fk = wk * (ex * Sx + ey * Sy + ez * Sz);
-    Real hk = Codec<PopT>::dec(h[q * s.pitch + i], (Real)0);
-    h2[q * s.pitch + i] = Codec<PopT>::enc(hk - invTau * (hk - heq) + Fk, (Real)0);
+    Real hk = Codec<PopT>::dec(h[pidx<7>(q, i)], (Real)0);
+    h2[pidx<7>(q, i)] = Codec<PopT>::enc(hk - invTau * (hk - heq) + Fk, (Real)0);
   }
 }
 
@@ -238,7 +239,7 @@ __global__ void k_stream_phase(Scene<PopT, typename Prec<PopT>::Real> s, int cur
   PopT *h = s.H[cur];
   for (int q = 0; q < Q7; q++) {
     long long src = i - (((long long)dcomp(q, 2) * ny + dcomp(q, 1)) * nx + dcomp(q, 0));
-    h[q * s.pitch + i] = s.tag[src] == TAG_FLUID ? h2[q * s.pitch + src] : h2[opp_of(q) * s.pitch + i];
+    h[pidx<7>(q, i)] = s.tag[src] == TAG_FLUID ? h2[pidx<7>(q, src)] : h2[pidx<7>(opp_of(q), i)];
   }
 }
 
@@ -273,8 +274,8 @@ __global__ void k_collide_hydro(Scene<PopT, typename Prec<PopT>::Real> s, int cu
     Real feq = wk * (sumF + rhoPhase * Qi);
     Real ekF = ex * fx + ey * fy + ez * fz;
     Real Sk = A * wk * (ekF * ((Real)1 + (Real)3 * eu) - uF);
-    Real fk = Codec<PopT>::dec(f[q * s.pitch + i], (Real)0);
-    f2[q * s.pitch + i] = Codec<PopT>::enc(fk - invTau * (fk - feq) + Sk, (Real)0);
+    Real fk = Codec<PopT>::dec(f[pidx<27>(q, i)], (Real)0);
+    f2[pidx<27>(q, i)] = Codec<PopT>::enc(fk - invTau * (fk - feq) + Sk, (Real)0);
   }
 }
 
@@ -305,9 +306,9 @@ __global__ void k_stream_hydro_macro(Scene<PopT, typename Prec<PopT>::Real> s, i
     uint8_t sTag = s.tag[src];
     Real fk;
     if (sTag == TAG_FLUID) {
-      fk = Codec<PopT>::dec(f2[q * s.pitch + src], (Real)0);
+      fk = Codec<PopT>::dec(f2[pidx<27>(q, src)], (Real)0);
     } else {
-      Real fopp = Codec<PopT>::dec(f2[opp_of(q) * s.pitch + i], (Real)0);
+      Real fopp = Codec<PopT>::dec(f2[pidx<27>(opp_of(q), i)], (Real)0);
       Real corr = 0;
       if (sTag == TAG_SOLID) {
         Real eu = (Real)ex * s.usx[src] + (Real)ey * s.usy[src] + (Real)ez * s.usz[src];
@@ -327,7 +328,7 @@ __global__ void k_stream_hydro_macro(Scene<PopT, typename Prec<PopT>::Real> s, i
         }
       }
     }
-    f[q * s.pitch + i] = Codec<PopT>::enc(fk, (Real)0);
+    f[pidx<27>(q, i)] = Codec<PopT>::enc(fk, (Real)0);
     pSumF += fk;
     mx += (Real)ex * fk;
     my += (Real)ey * fk;
@@ -336,7 +337,7 @@ __global__ void k_stream_hydro_macro(Scene<PopT, typename Prec<PopT>::Real> s, i
   flush_impulse(ss, owner, x, y, z, acc);
   s.rho[cur][i] = pSumF > (Real)0.01 ? pSumF : (Real)0.01;
   Real phiSum = 0;
-  for (int q = 0; q < Q7; q++) phiSum += Codec<PopT>::dec(s.H[cur][q * s.pitch + i], (Real)0);
+  for (int q = 0; q < Q7; q++) phiSum += Codec<PopT>::dec(s.H[cur][pidx<7>(q, i)], (Real)0);
   Real p = phiSum < (Real)0 ? (Real)0 : phiSum > (Real)1 ? (Real)1 : phiSum;
   s.phi[cur][i] = p;
   Real rhoPhaseNew = rhoG + p * dRho;
@@ -579,12 +580,12 @@ __global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, 
       double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
       double Qi = eu * (3.0 + 4.5 * eu) - 1.5 * u2;
       double fk = (double)w27_of(k) * (r + rhoPhase * Qi);
-      s.F[cur][k * s.pitch + i] = Codec<PopT>::enc((Real)fk, (Real)w27_of(k));
+      s.F[cur][pidx<27>(k, i)] = Codec<PopT>::enc((Real)fk, (Real)w27_of(k));
     }
     for (int k = 0; k < Q7; k++) {
       double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
       double hk = (double)w7_of(k) * p * (1 + 4.0 * eu);
-      s.H[cur][k * s.pitch + i] = Codec<PopT>::enc((Real)hk, (Real)w7_of(k) * pR);
+      s.H[cur][pidx<7>(k, i)] = Codec<PopT>::enc((Real)hk, (Real)w7_of(k) * pR);
     }
   }
 }
@@ -740,310 +741,15 @@ template <class PopT>
 __global__ void k_pack(Scene<PopT, typename Prec<PopT>::Real> s, int cur, uint8_t *out) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= s.n) return;
-  float p = (float)s.phi[cur][i];
-  if (p < 0.f) p = 0.f;
-  else if (p > 1.f) p = 1.f;
-  double v = (double)p * 255.0;
+  double p = (double)s.phi[cur][i];
+  if (p < 0.0) p = 0.0;
+  else if (p > 1.0) p = 1.0;
+  double v = p * 255.0;
   int r = (v == v) ? (int)v : 0;
   uchar2 o;
   o.x = (uint8_t)r;
   o.y = s.tag[i] == TAG_SOLID ? 255 : 0;
   reinterpret_cast<uchar2 *>(out)[i] = o;
-}
-
-// =====================================================================================
-// The fused step.
-//
-// A CTA owns a 32 x TY column of cells and marches it through a range of z
-// planes.  For every plane it first stages, for the plane ahead (z+1) and its
-// one-cell in-plane halo, the per-cell collision coefficients in shared memory
-// (a ring of three planes), then every thread handles its cell in plane z:
-//
-//   for each of the 27 directions k with source s = i - e_k:
-//     s fluid:  f'_k(i) = (1 - w) f_k(s) + w_k (C0 + e.V + (e.u)(e.Q))   [coefficients of s]
-//     s solid/wall: halfway bounce-back of the cell's own collided f_opp(k)
-//                   (+ Ladd moving-wall term and FP64 momentum exchange)
-//
-// which is algebraically the reference's collideHydro (src/sim.js:450-460)
-// applied at the source followed by streamHydroAndMacro's pull
-// (src/sim.js:509-543), with
-//   C0 = w sumF - 1.5 w rho_phase u^2 - A u.F,  V = 3 w rho_phase u + A F,
-//   Q  = 4.5 w rho_phase u + 3 A F             (w = 1/tau, A = 3(1 - w/2)).
-// The D3Q7 phase lattice is treated the same way with
-//   h'_k(i) = (1 - wp) h_k(s) + w7_k (D0 + e.Dv),  D0 = wp phi,
-//   Dv = 4 wp phi u + S (the sharpening source, src/sim.js:346-357).
-// Then the macros of the cell follow (src/sim.js:545-576).
-
-template <class Real>
-struct alignas(4 * sizeof(Real)) V4 {
-  Real x, y, z, w;
-};
-
-template <class PopT>
-struct FusedArgs {
-  Scene<PopT, typename Prec<PopT>::Real> s;
-  int cur;
-  int zchunk;
-  // collision constants (Real precision)
-  double om, omP, A, beta4, kappa, rhoG, dRho, gravity, sharpC4;
-  const SolidSet *ss;
-};
-
-template <class PopT, int TY>
-struct FusedSmem {
-  using Real = typename Prec<PopT>::Real;
-  static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;
-  static constexpr size_t bytes = 3 * 4 * NC * sizeof(V4<Real>) + 3 * NC;
-};
-
-template <class PopT, int TY>
-__global__ void __launch_bounds__(32 * TY) k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
-  using Real = typename Prec<PopT>::Real;
-  using C = Codec<PopT>;
-  using SM = FusedSmem<PopT, TY>;
-  constexpr int RX = SM::RX, NC = SM::NC;
-  extern __shared__ __align__(32) unsigned char smem_raw[];
-  V4<Real> *ring = reinterpret_cast<V4<Real> *>(smem_raw);  // [3][4][NC]
-  uint8_t *stag = smem_raw + 3 * 4 * NC * sizeof(V4<Real>);  // [3][NC]
-
-  const auto &s = a.s;
-  const SolidSet &ss = *a.ss;
-  const int nx = s.nx, ny = s.ny, nz = s.nz;
-  const long long nxny = (long long)nx * ny;
-  const long long pitch = s.pitch;
-  const int cur = a.cur, nxt = 1 - cur;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * 32 + tx;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TY;
-  const int zb = 1 + blockIdx.z * a.zchunk;
-  const int ze = min(zb + a.zchunk, nz - 1);
-  if (zb >= ze) return;
-  const int x = x0 + tx, y = y0 + ty;
-  const int own = (ty + 1) * RX + (tx + 1);
-
-  const Real om = (Real)a.om, omP = (Real)a.omP, A = (Real)a.A;
-  const Real beta4 = (Real)a.beta4, kappa = (Real)a.kappa, rhoG = (Real)a.rhoG;
-  const Real dRho = (Real)a.dRho, grav = (Real)a.gravity, sharpC4 = (Real)a.sharpC4;
-  const Real *__restrict__ phiC = s.phi[cur];
-
-  // Stage the collision coefficients of plane zp (own cell first, then halo).
-  // Returns the own cell's gradient and laplacian (used by its macro update).
-  auto fill = [&](int zp, Real &ogx, Real &ogy, Real &ogz, Real &olap) {
-    const int slot = zp % 3;
-    V4<Real> *R = ring + slot * 4 * NC;
-    uint8_t *T = stag + slot * NC;
-    const int nHalo = NC - 32 * TY;
-    for (int j = -1; j < nHalo; j += (j < 0 ? 1 + tid : 32 * TY)) {
-      int lc, gx_, gy_;
-      if (j < 0) {
-        lc = own;
-        gx_ = x;
-        gy_ = y;
-      } else {
-        // halo cell j: top row, bottom row, then the left and right columns
-        int lx, ly;
-        if (j < RX) {
-          lx = j;
-          ly = 0;
-        } else if (j < 2 * RX) {
-          lx = j - RX;
-          ly = TY + 1;
-        } else {
-          int r = j - 2 * RX;
-          lx = (r & 1) ? RX - 1 : 0;
-          ly = 1 + (r >> 1);
-        }
-        lc = ly * RX + lx;
-        gx_ = x0 - 1 + lx;
-        gy_ = y0 - 1 + ly;
-      }
-      uint8_t tg = TAG_WALL;
-      long long ci = 0;
-      bool inside = gx_ >= 0 && gx_ < nx && gy_ >= 0 && gy_ < ny && zp >= 0 && zp < nz;
-      if (inside) {
-        ci = zp * nxny + (long long)gy_ * nx + gx_;
-        tg = s.tag[ci];
-        // boundary cells never act as fluid (they are walls after any retag)
-        bool inner = gx_ >= 1 && gx_ <= nx - 2 && gy_ >= 1 && gy_ <= ny - 2 && zp >= 1 && zp <= nz - 2;
-        if (!inner && tg == TAG_FLUID) tg = TAG_WALL;
-      }
-      T[lc] = tg;
-      if (tg == TAG_FLUID) {
-        Real p = phiC[ci];
-        Real pxp = phiC[ci + 1], pxm = phiC[ci - 1];
-        Real pyp = phiC[ci + nx], pym = phiC[ci - nx];
-        Real pzp = phiC[ci + nxny], pzm = phiC[ci - nxny];
-        Real gxv = (Real)0.5 * (pxp - pxm);
-        Real gyv = (Real)0.5 * (pyp - pym);
-        Real gzv = (Real)0.5 * (pzp - pzm);
-        Real lap = pxp + pxm + pyp + pym + pzp + pzm - (Real)6 * p;
-        Real rhoPh = rhoG + p * dRho;
-        Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lap;
-        Real Fx = mu * gxv, Fy = mu * gyv + rhoPh * grav, Fz = mu * gzv;
-        Real sumF = s.rho[cur][ci];
-        Real ux = s.ux[cur][ci], uy = s.uy[cur][ci], uz = s.uz[cur][ci];
-        Real u2 = ux * ux + uy * uy + uz * uz;
-        Real uF = ux * Fx + uy * Fy + uz * Fz;
-        Real orh = om * rhoPh;
-        V4<Real> g0, g1, g2, g3;
-        g0.x = om * sumF - (Real)1.5 * orh * u2 - A * uF;
-        g0.y = (Real)3 * orh * ux + A * Fx;
-        g0.z = (Real)3 * orh * uy + A * Fy;
-        g0.w = (Real)3 * orh * uz + A * Fz;
-        g1.x = ux;
-        g1.y = uy;
-        g1.z = uz;
-        g1.w = p;
-        g2.x = (Real)4.5 * orh * ux + (Real)3 * A * Fx;
-        g2.y = (Real)4.5 * orh * uy + (Real)3 * A * Fy;
-        g2.z = (Real)4.5 * orh * uz + (Real)3 * A * Fz;
-        g2.w = omP * p;
-        Real gmag = sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + (Real)1e-12;
-        Real sh = sharpC4 * p * ((Real)1 - p) / gmag;
-        Real fp = (Real)4 * omP * p;
-        g3.x = fp * ux + sh * gxv;
-        g3.y = fp * uy + sh * gyv;
-        g3.z = fp * uz + sh * gzv;
-        g3.w = rhoPh;
-        R[0 * NC + lc] = g0;
-        R[1 * NC + lc] = g1;
-        R[2 * NC + lc] = g2;
-        R[3 * NC + lc] = g3;
-        if (j < 0) {
-          ogx = gxv;
-          ogy = gyv;
-          ogz = gzv;
-          olap = lap;
-        }
-      }
-    }
-  };
-
-  Real gxC = 0, gyC = 0, gzC = 0, lapC = 0, gxN = 0, gyN = 0, gzN = 0, lapN = 0;
-  fill(zb - 1, gxN, gyN, gzN, lapN);
-  fill(zb, gxC, gyC, gzC, lapC);
-
-  const bool colActive = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
-
-  for (int z = zb; z < ze; z++) {
-    fill(z + 1, gxN, gyN, gzN, lapN);
-    __syncthreads();
-    const int sC = z % 3;
-    const uint8_t tagI = colActive ? stag[sC * NC + own] : TAG_WALL;
-    const long long i = z * nxny + (long long)y * nx + x;
-    if (tagI == TAG_SOLID) {
-      // Solid cells are not updated; carry their state into the next half so
-      // both halves hold the reference's stale values.
-#pragma unroll 1
-      for (int k = 0; k < Q27; k++) s.F[nxt][k * pitch + i] = s.F[cur][k * pitch + i];
-#pragma unroll 1
-      for (int k = 0; k < Q7; k++) s.H[nxt][k * pitch + i] = s.H[cur][k * pitch + i];
-      s.phi[nxt][i] = s.phi[cur][i];
-      s.rho[nxt][i] = s.rho[cur][i];
-      s.ux[nxt][i] = s.ux[cur][i];
-      s.uy[nxt][i] = s.uy[cur][i];
-      s.uz[nxt][i] = s.uz[cur][i];
-    } else if (tagI == TAG_FLUID) {
-      const V4<Real> *R0 = ring;
-      const V4<Real> ownG1 = ring[(sC * 4 + 1) * NC + own];
-      const V4<Real> ownG3 = ring[(sC * 4 + 3) * NC + own];
-      const Real rhoPhOld = ownG3.w;
-      const PopT *__restrict__ Fc = s.F[cur];
-      const PopT *__restrict__ Hc = s.H[cur];
-      PopT *__restrict__ Fn = s.F[nxt];
-      PopT *__restrict__ Hn = s.H[nxt];
-      Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
-      Real hn[Q7];
-      double acc[6] = {0, 0, 0, 0, 0, 0};
-      int owner = -1;
-      static_for<0, Q27>([&](auto KK) {
-        constexpr int k = decltype(KK)::value;
-        using D = D27<k>;
-        constexpr int ex = D::ex, ey = D::ey, ez = D::ez;
-        const int sp = (z - ez + 3) % 3;
-        const int sc = own - ey * RX - ex;
-        const uint8_t ts = stag[sp * NC + sc];
-        const bool fl = ts == TAG_FLUID;
-        const long long off = ((long long)(-ez) * ny + (-ey)) * nx + (-ex);
-        const PopT *pf = fl ? (Fc + k * pitch + (i + off)) : (Fc + D::opp * pitch + i);
-        const int pc = fl ? (sp * 4) * NC + sc : (sC * 4) * NC + own;
-        const V4<Real> G0 = R0[pc], G1 = R0[pc + NC], G2 = R0[pc + 2 * NC];
-        const Real v = C::dec(*pf, (Real)D::w);
-        const Real sg = fl ? (Real)1 : (Real)-1;
-        const Real ev = (Real)ex * G0.y + (Real)ey * G0.z + (Real)ez * G0.w;
-        const Real eu = (Real)ex * G1.x + (Real)ey * G1.y + (Real)ez * G1.z;
-        const Real eq = (Real)ex * G2.x + (Real)ey * G2.y + (Real)ez * G2.z;
-        Real fk = ((Real)1 - om) * v + (Real)D::w * (G0.x + sg * ev + eu * eq);
-        if (ts == TAG_SOLID) {
-          const int sx = x - ex, sy = y - ey, sz = z - ez;
-          const int b = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, sx, sy, sz);
-          Real corr = 0;
-          if (b >= 0) {
-            double ox, oy, oz;
-            sphere_surface_velocity(ss.sph[b], sx, sy, sz, ox, oy, oz);
-            const Real eus = (Real)ex * (Real)(float)ox + (Real)ey * (Real)(float)oy +
-                             (Real)ez * (Real)(float)oz;
-            corr = (Real)2 * (Real)D::w * rhoPhOld * eus * (Real)3;
-            const Real fopp = fk;
-            fk = fopp + corr;
-            if (b != owner) {
-              flush_impulse(ss, owner, x, y, z, acc);
-              owner = b;
-            }
-            const double m = __dadd_rn((double)fopp, (double)fk);
-            impulse_terms(ss.sph[b], sx, sy, sz, -m * ex, -m * ey, -m * ez, acc);
-          }
-        }
-        Fn[k * pitch + i] = C::enc(fk, (Real)D::w);
-        rhoA += fk;
-        if (ex) mx += (Real)ex * fk;
-        if (ey) my += (Real)ey * fk;
-        if (ez) mz += (Real)ez * fk;
-        if constexpr (k < Q7) {
-          using E = D7<k>;
-          const PopT *ph = fl ? (Hc + k * pitch + (i + off)) : (Hc + E::opp * pitch + i);
-          const V4<Real> G3 = R0[pc + 3 * NC];
-          const Real phiRef = fl ? G1.w : ownG1.w;
-          const Real hv = C::dec(*ph, (Real)E::w * phiRef);
-          const Real ed = (Real)ex * G3.x + (Real)ey * G3.y + (Real)ez * G3.z;
-          const Real hk = ((Real)1 - omP) * hv + (Real)E::w * (G2.w + sg * ed);
-          hn[k] = hk;
-          hsum += hk;
-        }
-      });
-      flush_impulse(ss, owner, x, y, z, acc);
-      const Real rhoN = rhoA > (Real)0.01 ? rhoA : (Real)0.01;
-      const Real p = hsum < (Real)0 ? (Real)0 : hsum > (Real)1 ? (Real)1 : hsum;
-      static_for<0, Q7>([&](auto KK) {
-        constexpr int k = decltype(KK)::value;
-        Hn[k * pitch + i] = C::enc(hn[k], (Real)D7<k>::w * p);
-      });
-      const Real rhoPhN = rhoG + p * dRho;
-      const Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lapC;
-      const Real Fx = mu * gxC, Fy = mu * gyC + rhoPhN * grav, Fz = mu * gzC;
-      const Real inv = (Real)1 / rhoPhN;
-      Real uxn = (mx + (Real)0.5 * Fx) * inv;
-      Real uyn = (my + (Real)0.5 * Fy) * inv;
-      Real uzn = (mz + (Real)0.5 * Fz) * inv;
-      const Real u2 = uxn * uxn + uyn * uyn + uzn * uzn;
-      if (u2 > (Real)(0.2 * 0.2)) {
-        const Real sc = (Real)0.2 / sqrt(u2);
-        uxn *= sc;
-        uyn *= sc;
-        uzn *= sc;
-      }
-      s.rho[nxt][i] = rhoN;
-      s.phi[nxt][i] = p;
-      s.ux[nxt][i] = uxn;
-      s.uy[nxt][i] = uyn;
-      s.uz[nxt][i] = uzn;
-    }
-    __syncthreads();
-    gxC = gxN;
-    gyC = gyN;
-    gzC = gzN;
-    lapC = lapN;
-  }
 }
 
 }  // namespace lbm

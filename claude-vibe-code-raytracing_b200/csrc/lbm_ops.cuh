@@ -2,6 +2,7 @@
 // storage type.  Included once per storage type by lbm_inst_*.cu.
 #pragma once
 
+#include "lbm_fused.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_state.h"
 
@@ -24,13 +25,13 @@ __global__ void k_aos_to_soa(Scene<PopT, typename Prec<PopT>::Real> s, int isH, 
     for (int k = 0; k < Q; k++) {
       Real v = (Real)aos[c * Q + k];
       Real ref = isH ? (Real)w7_of(k) * s.phi[dst][i] : (Real)w27_of(k);
-      P[k * s.pitch + i] = Codec<PopT>::enc(v, ref);
+      P[isH ? pidx<7>(k, i) : pidx<27>(k, i)] = Codec<PopT>::enc(v, ref);
     }
   }
 }
 
-template <class PopT>
-__global__ void k_soa_to_aos(Scene<PopT, typename Prec<PopT>::Real> s, int isH, int src, float *aos,
+template <class PopT, class OutT>
+__global__ void k_soa_to_aos(Scene<PopT, typename Prec<PopT>::Real> s, int isH, int src, OutT *aos,
                              long long c0, long long cells) {
   using Real = typename Prec<PopT>::Real;
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -40,7 +41,7 @@ __global__ void k_soa_to_aos(Scene<PopT, typename Prec<PopT>::Real> s, int isH, 
   const PopT *P = isH ? s.H[src] : s.F[src];
   for (int k = 0; k < Q; k++) {
     Real ref = isH ? (Real)w7_of(k) * s.phi[src][i] : (Real)w27_of(k);
-    aos[c * Q + k] = (float)Codec<PopT>::dec(P[k * s.pitch + i], ref);
+    aos[c * Q + k] = (OutT)Codec<PopT>::dec(P[isH ? pidx<7>(k, i) : pidx<27>(k, i)], ref);
   }
 }
 
@@ -53,8 +54,8 @@ __global__ void k_reencode_h(Scene<PopT, typename Prec<PopT>::Real> s, int half,
   Real po = oldPhi[i], pn = s.phi[half][i];
   for (int k = 0; k < Q7; k++) {
     Real w = (Real)w7_of(k);
-    Real v = Codec<PopT>::dec(s.H[half][k * s.pitch + i], w * po);
-    s.H[half][k * s.pitch + i] = Codec<PopT>::enc(v, w * pn);
+    Real v = Codec<PopT>::dec(s.H[half][pidx<7>(k, i)], w * po);
+    s.H[half][pidx<7>(k, i)] = Codec<PopT>::enc(v, w * pn);
   }
 }
 
@@ -164,7 +165,6 @@ class Ops final : public OpsBase {
     s.ny = h->ny;
     s.nz = h->nz;
     s.n = h->n;
-    s.pitch = h->pitch;
     for (int c = 0; c < 2; c++) {
       s.F[c] = (PopT *)h->F[c];
       s.H[c] = (PopT *)h->H[c];
@@ -253,7 +253,7 @@ class Ops final : public OpsBase {
                            (int)smem);
       attr = true;
     }
-    dim3 block(32, TY);
+    dim3 block(32, FusedSmem<PopT, TY>::warps);  // TY cell warps and two halo warps
     dim3 grid((h->nx + 31) / 32, (h->ny + TY - 1) / TY, (h->nz - 2 + zchunk - 1) / zchunk);
     k_fused_step<PopT, TY><<<grid, block, smem, h->stream>>>(a);
     h->launches++;
@@ -278,16 +278,24 @@ class Ops final : public OpsBase {
     switch (cfg.ty) {
       case 2: launch_fused<2>(h, a, cfg.zchunk); break;
       case 4: launch_fused<4>(h, a, cfg.zchunk); break;
-      case 16: launch_fused<16>(h, a, cfg.zchunk); break;
       default: launch_fused<8>(h, a, cfg.zchunk); break;
     }
+  }
+
+  cudaError_t read_fault(lbm_sim *h, unsigned long long out[4]) override {
+    cudaError_t e = cudaMemcpyFromSymbolAsync(out, lbm_fault_word, 4 * sizeof(unsigned long long), 0,
+                                              cudaMemcpyDeviceToHost, h->stream);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return e;
+    static const unsigned long long zero[4] = {0, 0, 0, 0};
+    return cudaMemcpyToSymbol(lbm_fault_word, zero, sizeof(zero));
   }
 
   size_t fused_smem(int ty) const override {
     switch (ty) {
       case 2: return FusedSmem<PopT, 2>::bytes;
       case 4: return FusedSmem<PopT, 4>::bytes;
-      case 16: return FusedSmem<PopT, 16>::bytes;
       default: return FusedSmem<PopT, 8>::bytes;
     }
   }
@@ -305,8 +313,15 @@ class Ops final : public OpsBase {
   void download_pops(lbm_sim *h, bool isH, int half, float *d_aos, long long c0,
                      long long cells) override {
     int src = half == 2 ? 1 - h->cur : h->cur;
-    k_soa_to_aos<PopT><<<nblocks(cells, 256), 256, 0, h->stream>>>(scene(h), isH ? 1 : 0, src,
-                                                                     d_aos, c0, cells);
+    k_soa_to_aos<PopT, float><<<nblocks(cells, 256), 256, 0, h->stream>>>(scene(h), isH ? 1 : 0, src,
+                                                                            d_aos, c0, cells);
+    h->launches++;
+  }
+  void download_pops64(lbm_sim *h, bool isH, int half, double *d_aos, long long c0,
+                       long long cells) override {
+    int src = half == 2 ? 1 - h->cur : h->cur;
+    k_soa_to_aos<PopT, double><<<nblocks(cells, 256), 256, 0, h->stream>>>(scene(h), isH ? 1 : 0, src,
+                                                                             d_aos, c0, cells);
     h->launches++;
   }
   void reencode_h(lbm_sim *h, int half, const void *d_oldPhi) override {

@@ -18,7 +18,7 @@ namespace lbm {
 
 // Launch configuration of the fused step kernel.
 struct FusedCfg {
-  int ty = 8;       // CTA rows (CTA = 32 x ty threads)
+  int ty = 4;       // cell rows per CTA (CTA = 32 x (ty + 2) threads)
   int zchunk = 32;  // z planes marched per CTA
 };
 
@@ -48,12 +48,16 @@ class OpsBase {
                            long long cells) = 0;
   virtual void download_pops(lbm_sim *h, bool isH, int half, float *d_aos, long long c0,
                              long long cells) = 0;
+  virtual void download_pops64(lbm_sim *h, bool isH, int half, double *d_aos, long long c0,
+                               long long cells) = 0;
   // Re-express h offsets after phi changed from d_oldPhi (both halves).
   virtual void reencode_h(lbm_sim *h, int half, const void *d_oldPhi) = 0;
   virtual void sphere_step_device(lbm_sim *h, lbm_sphere *d_sph, int nsph, double gravity,
                                   const double *d_fluid, const double *d_dead) = 0;
   // Fused-step kernel geometry (for the bench and the autotuner).
   virtual size_t fused_smem(int ty) const = 0;
+  // Fault record of the bounds-checked build (all zero otherwise); cleared on read.
+  virtual cudaError_t read_fault(lbm_sim *h, unsigned long long out[4]) = 0;
 };
 
 OpsBase *make_ops_f32();
@@ -65,12 +69,13 @@ OpsBase *make_ops_f64();
 
 struct lbm_sim {
   int nx = 0, ny = 0, nz = 0, storage = 0, device = 0;
-  long long n = 0, pitch = 0;
+  long long n = 0;
   cudaStream_t stream = nullptr;
   lbm_params params{};
   int cur = 0;
   lbm::OpsBase *ops = nullptr;
   lbm::FusedCfg cfg;
+  bool fusedOK = true;  // the fused kernel's 32-bit indexing covers this grid
 
   // device memory
   void *F[2] = {nullptr, nullptr};

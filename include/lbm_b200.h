@@ -119,6 +119,8 @@ int lbm_get_params(const lbm_sim *sim, lbm_params *p);
 /* ---- field transfer (reference layout, synchronous) ------------------------ */
 int lbm_upload_field(lbm_sim *sim, int field, const void *host, size_t count);
 int lbm_download_field(lbm_sim *sim, int field, void *host, size_t count);
+/* Same, as double (exact for the FP64 storage form); not for the tag fields. */
+int lbm_download_field_f64(lbm_sim *sim, int field, double *host, size_t count);
 
 /* ---- init (src/sim.js:112-173) --------------------------------------------- */
 int lbm_init_flat(lbm_sim *sim, double waterlineY);
@@ -175,6 +177,12 @@ int lbm_download_sets(lbm_sim *sim, int32_t *fresh, int cap_fresh, int32_t *dead
                       int cap_dead);
 /* Number of kernels this handle has launched since creation. */
 int lbm_launch_count(const lbm_sim *sim, int64_t *count);
+/* 1 when the library was built with bounds checks in the fused kernel
+ * (make checked).  lbm_fault_record returns and clears the first recorded
+ * violation: {location code, index, block (x | y<<20 | z<<40), thread
+ * (x | y<<8)}, all zero when none. */
+int lbm_checked_build(void);
+int lbm_fault_record(lbm_sim *sim, int64_t out[4]);
 /* Host->device and device->host bytes this handle has copied since creation. */
 int lbm_transfer_bytes(const lbm_sim *sim, uint64_t *h2d, uint64_t *d2h);
 /* Time the fused step kernel with CUDA events on the handle's stream.

@@ -74,6 +74,8 @@ void or_tables(int8_t ex27[27], int8_t ey27[27], int8_t ez27[27], float w27[27],
 #define CS2_7 0.25
 #define INV_CS2_7 4.0
 
+int or_store_bytes(void) { return (int)sizeof(or_real); }
+
 /* ---------------------------------------------------------------- create */
 /* src/sim.js:30-96 */
 or_sim *or_sim_create(int nx, int ny, int nz) {
@@ -84,15 +86,15 @@ or_sim *or_sim_create(int nx, int ny, int nz) {
   s->nz = nz;
   int n = nx * ny * nz;
   s->n = n;
-  s->f = (float *)calloc((size_t)n * 27, sizeof(float));
-  s->f2 = (float *)calloc((size_t)n * 27, sizeof(float));
-  s->h = (float *)calloc((size_t)n * 7, sizeof(float));
-  s->h2 = (float *)calloc((size_t)n * 7, sizeof(float));
-  float **scalars[] = {&s->rho, &s->ux, &s->uy, &s->uz, &s->phi, &s->phiPrev,
+  s->f = (or_real *)calloc((size_t)n * 27, sizeof(or_real));
+  s->f2 = (or_real *)calloc((size_t)n * 27, sizeof(or_real));
+  s->h = (or_real *)calloc((size_t)n * 7, sizeof(or_real));
+  s->h2 = (or_real *)calloc((size_t)n * 7, sizeof(or_real));
+  or_real **scalars[] = {&s->rho, &s->ux, &s->uy, &s->uz, &s->phi, &s->phiPrev,
                        &s->usx, &s->usy, &s->usz, &s->gx, &s->gy, &s->gz,
                        &s->lap, &s->bodyFx, &s->bodyFy, &s->bodyFz};
   for (size_t a = 0; a < sizeof(scalars) / sizeof(scalars[0]); a++)
-    *scalars[a] = (float *)calloc((size_t)n, sizeof(float));
+    *scalars[a] = (or_real *)calloc((size_t)n, sizeof(or_real));
   s->tag = (uint8_t *)calloc((size_t)n, 1);
   s->tagPrev = (uint8_t *)calloc((size_t)n, 1);
   int nxny = nx * ny;
@@ -120,7 +122,7 @@ or_sim *or_sim_create(int nx, int ny, int nz) {
 
 void or_sim_destroy(or_sim *s) {
   if (!s) return;
-  float *arrs[] = {s->f, s->f2, s->h, s->h2, s->rho, s->ux, s->uy, s->uz, s->phi,
+  or_real *arrs[] = {s->f, s->f2, s->h, s->h2, s->rho, s->ux, s->uy, s->uz, s->phi,
                    s->phiPrev, s->usx, s->usy, s->usz, s->gx, s->gy, s->gz, s->lap,
                    s->bodyFx, s->bodyFy, s->bodyFz};
   for (size_t a = 0; a < sizeof(arrs) / sizeof(arrs[0]); a++) free(arrs[a]);
@@ -148,15 +150,15 @@ void or_init_flat(or_sim *s, double waterlineY) {
       double phiCol = 0.5 * (1 + tanh(2 * ((double)y - waterlineY) / W));
       for (int x = 0; x < nx; x++) {
         int i = IDX(s, x, y, z);
-        s->phi[i] = (float)phiCol;
-        s->phiPrev[i] = (float)phiCol;
-        s->rho[i] = 1.0f;
-        s->ux[i] = s->uy[i] = s->uz[i] = 0.0f;
+        s->phi[i] = (or_real)phiCol;
+        s->phiPrev[i] = (or_real)phiCol;
+        s->rho[i] = 1.0;
+        s->ux[i] = s->uy[i] = s->uz[i] = 0.0;
         int onWall = x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
         s->tag[i] = onWall ? OR_TAG_WALL : OR_TAG_FLUID;
         s->tagPrev[i] = s->tag[i];
         for (int k = 0; k < 27; k++) s->f[(size_t)i * 27 + k] = W27[k];
-        for (int k = 0; k < 7; k++) s->h[(size_t)i * 7 + k] = (float)((double)W7[k] * phiCol);
+        for (int k = 0; k < 7; k++) s->h[(size_t)i * 7 + k] = (or_real)((double)W7[k] * phiCol);
       }
     }
   }
@@ -176,13 +178,13 @@ void or_seed_hydrostatic(or_sim *s) {
       double pCs2 = 1.0;
       for (int y = 0; y < ny; y++) {
         int i = IDX(s, x, y, z);
-        s->rho[i] = (float)pCs2;
+        s->rho[i] = (or_real)pCs2;
         size_t i27 = (size_t)i * 27;
         double rhoPhase = s->rhoG + (double)s->phi[i] * dRho;
         for (int k = 0; k < 27; k++) {
           double eu = EY27[k] * uLatY;
           double Qi = eu * (INV_CS2_27 + INV_2CS4_27 * eu) - 1.5 * uLat2;
-          s->f[i27 + k] = (float)((double)W27[k] * (pCs2 + rhoPhase * Qi));
+          s->f[i27 + k] = (or_real)((double)W27[k] * (pCs2 + rhoPhase * Qi));
         }
         pCs2 += rhoPhase * gOverCs2;
       }
@@ -194,7 +196,7 @@ void or_seed_hydrostatic(or_sim *s) {
 /* src/sim.js:176-199: central differences with index clamping at the edges. */
 void or_compute_phi_gradients(or_sim *s) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
-  const float *phi = s->phi;
+  const or_real *phi = s->phi;
 #pragma omp parallel for schedule(static) if (s->omp > 0)
   for (int z = 0; z < nz; z++) {
     int zm = z > 0 ? z - 1 : z, zp = z < nz - 1 ? z + 1 : z;
@@ -210,10 +212,10 @@ void or_compute_phi_gradients(or_sim *s) {
         double my = phi[((z * ny) + ym) * nx + x];
         double pz = phi[((zp * ny) + y) * nx + x];
         double mz = phi[((zm * ny) + y) * nx + x];
-        s->gx[i] = (float)(0.5 * (px - mx));
-        s->gy[i] = (float)(0.5 * (py - my));
-        s->gz[i] = (float)(0.5 * (pz - mz));
-        s->lap[i] = (float)(px + mx + py + my + pz + mz - 6 * c);
+        s->gx[i] = (or_real)(0.5 * (px - mx));
+        s->gy[i] = (or_real)(0.5 * (py - my));
+        s->gz[i] = (or_real)(0.5 * (pz - mz));
+        s->lap[i] = (or_real)(px + mx + py + my + pz + mz - 6 * c);
       }
     }
   }
@@ -232,7 +234,7 @@ static int owner_of(const or_sphere *solids, int nsolids, int x, int y, int z) {
 void or_retag_cells(or_sim *s, const or_sphere *solids, int nsolids) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   memcpy(s->tagPrev, s->tag, (size_t)s->n);
-  memcpy(s->phiPrev, s->phi, (size_t)s->n * sizeof(float));
+  memcpy(s->phiPrev, s->phi, (size_t)s->n * sizeof(or_real));
   double tmp[3];
   for (int z = 0; z < nz; z++) {
     int zOnWall = z == 0 || z == nz - 1;
@@ -242,19 +244,19 @@ void or_retag_cells(or_sim *s, const or_sphere *solids, int nsolids) {
         int i = IDX(s, x, y, z);
         if (zOnWall || yOnWall || x == 0 || x == nx - 1) {
           s->tag[i] = OR_TAG_WALL;
-          s->usx[i] = s->usy[i] = s->usz[i] = 0.0f;
+          s->usx[i] = s->usy[i] = s->usz[i] = 0.0;
           continue;
         }
         int b = solids ? owner_of(solids, nsolids, x, y, z) : -1;
         if (b >= 0) {
           s->tag[i] = OR_TAG_SOLID;
           or_sphere_surface_velocity(&solids[b], x, y, z, tmp);
-          s->usx[i] = (float)tmp[0];
-          s->usy[i] = (float)tmp[1];
-          s->usz[i] = (float)tmp[2];
+          s->usx[i] = (or_real)tmp[0];
+          s->usy[i] = (or_real)tmp[1];
+          s->usz[i] = (or_real)tmp[2];
         } else {
           s->tag[i] = OR_TAG_FLUID;
-          s->usx[i] = s->usy[i] = s->usz[i] = 0.0f;
+          s->usx[i] = s->usy[i] = s->usz[i] = 0.0;
         }
       }
     }
@@ -291,22 +293,22 @@ void or_handle_fresh_cells(or_sim *s) {
         double vx = pcnt > 0 ? vxs / pcnt : 0;
         double vy = pcnt > 0 ? vys / pcnt : 0;
         double vz = pcnt > 0 ? vzs / pcnt : 0;
-        s->phi[i] = (float)p;
-        s->phiPrev[i] = (float)p;
-        s->rho[i] = (float)r;
-        s->ux[i] = (float)vx;
-        s->uy[i] = (float)vy;
-        s->uz[i] = (float)vz;
+        s->phi[i] = (or_real)p;
+        s->phiPrev[i] = (or_real)p;
+        s->rho[i] = (or_real)r;
+        s->ux[i] = (or_real)vx;
+        s->uy[i] = (or_real)vy;
+        s->uz[i] = (or_real)vz;
         double rhoPhase = s->rhoG + p * (s->rhoL - s->rhoG);
         double u2 = vx * vx + vy * vy + vz * vz;
         for (int k = 0; k < 27; k++) {
           double eu = EX27[k] * vx + EY27[k] * vy + EZ27[k] * vz;
           double Qi = eu * (INV_CS2_27 + INV_2CS4_27 * eu) - 1.5 * u2;
-          s->f[(size_t)i * 27 + k] = (float)((double)W27[k] * (r + rhoPhase * Qi));
+          s->f[(size_t)i * 27 + k] = (or_real)((double)W27[k] * (r + rhoPhase * Qi));
         }
         for (int k = 0; k < 7; k++) {
           double eu = EX7[k] * vx + EY7[k] * vy + EZ7[k] * vz;
-          s->h[(size_t)i * 7 + k] = (float)((double)W7[k] * p * (1 + INV_CS2_7 * eu));
+          s->h[(size_t)i * 7 + k] = (or_real)((double)W7[k] * p * (1 + INV_CS2_7 * eu));
         }
       }
     }
@@ -343,7 +345,7 @@ void or_collide_phase(or_sim *s) {
           double heq = wk * p * (1 + INV_CS2_7 * eu);
           double Fk = wk * (EX7[k] * Sx + EY7[k] * Sy + EZ7[k] * Sz);
           double hk = s->h[i7 + k];
-          s->h2[i7 + k] = (float)(hk - invTau * (hk - heq) + Fk);
+          s->h2[i7 + k] = (or_real)(hk - invTau * (hk - heq) + Fk);
         }
       }
     }
@@ -407,7 +409,7 @@ void or_collide_hydro(or_sim *s) {
           double ekF = EX27[k] * fx + EY27[k] * fy + EZ27[k] * fz;
           double Sk = A * wk * (ekF * (1 + INV_CS2_27 * eu) - uF);
           double fk = s->f[i27 + k];
-          s->f2[i27 + k] = (float)(fk - invTau * (fk - feq) + Sk);
+          s->f2[i27 + k] = (or_real)(fk - invTau * (fk - feq) + Sk);
         }
       }
     }
@@ -457,17 +459,17 @@ void or_stream_hydro_and_macro(or_sim *s, or_sphere *solids, int nsolids) {
               if (b >= 0) or_sphere_apply_impulse(&solids[b], sx, sy, sz, -m * ekx, -m * eky, -m * ekz);
             }
           }
-          s->f[i27 + k] = (float)fk;
+          s->f[i27 + k] = (or_real)fk;
           pSumF += fk;
           mx += ekx * fk;
           my += eky * fk;
           mz += ekz * fk;
         }
-        s->rho[i] = (float)(pSumF > 0.01 ? pSumF : 0.01);
+        s->rho[i] = (or_real)(pSumF > 0.01 ? pSumF : 0.01);
         double phiSum = 0;
         for (int k = 0; k < 7; k++) phiSum += s->h[(size_t)i * 7 + k];
         double p = phiSum < 0 ? 0 : phiSum > 1 ? 1 : phiSum;
-        s->phi[i] = (float)p;
+        s->phi[i] = (or_real)p;
         double rhoPhaseNew = rhoG + p * dRho;
         double mu = 4 * beta * p * (p - 1) * (2 * p - 1) - kappa * (double)s->lap[i];
         double fx = (double)s->bodyFx[i] + mu * (double)s->gx[i];
@@ -485,15 +487,15 @@ void or_stream_hydro_and_macro(or_sim *s, or_sphere *solids, int nsolids) {
           uyn *= sc;
           uzn *= sc;
         }
-        s->ux[i] = (float)uxn;
-        s->uy[i] = (float)uyn;
-        s->uz[i] = (float)uzn;
+        s->ux[i] = (or_real)uxn;
+        s->uy[i] = (or_real)uyn;
+        s->uz[i] = (or_real)uzn;
       }
     }
   }
-  memset(s->bodyFx, 0, (size_t)s->n * sizeof(float));
-  memset(s->bodyFy, 0, (size_t)s->n * sizeof(float));
-  memset(s->bodyFz, 0, (size_t)s->n * sizeof(float));
+  memset(s->bodyFx, 0, (size_t)s->n * sizeof(or_real));
+  memset(s->bodyFy, 0, (size_t)s->n * sizeof(or_real));
+  memset(s->bodyFz, 0, (size_t)s->n * sizeof(or_real));
 }
 
 /* src/sim.js:202-210 */

@@ -35,6 +35,15 @@
 extern "C" {
 #endif
 
+/* Element type of the Float32Array fields.  The default build stores float32
+ * like the reference; building with -DOR_STORE_DOUBLE keeps every field in
+ * double, giving an FP64 reference for the GPU's FP64 storage form. */
+#ifdef OR_STORE_DOUBLE
+typedef double or_real;
+#else
+typedef float or_real;
+#endif
+
 #define OR_Q27 27
 #define OR_Q7 7
 #define OR_TAG_FLUID 0
@@ -58,17 +67,20 @@ typedef struct {
  * cell i = (z*ny + y)*nx + x, populations AoS f[i*27 + k], h[i*7 + k]. */
 typedef struct {
   int nx, ny, nz, n;
-  float *f, *f2, *h, *h2;
-  float *rho, *ux, *uy, *uz, *phi, *phiPrev;
+  or_real *f, *f2, *h, *h2;
+  or_real *rho, *ux, *uy, *uz, *phi, *phiPrev;
   uint8_t *tag, *tagPrev;
-  float *usx, *usy, *usz;
-  float *gx, *gy, *gz, *lap;
-  float *bodyFx, *bodyFy, *bodyFz;
+  or_real *usx, *usy, *usz;
+  or_real *gx, *gy, *gz, *lap;
+  or_real *bodyFx, *bodyFy, *bodyFz;
   int32_t neighOffset27[OR_Q27], fOffset27[OR_Q27];
   int32_t neighOffset7[OR_Q7], hOffset7[OR_Q7];
   double tau, tauPhi, sigma, gravity, rhoL, rhoG, W, mobility;
   int omp; /* >0: parallelise the order-free phases with OpenMP (timing only) */
 } or_sim;
+
+/* sizeof(or_real) of this build */
+int or_store_bytes(void);
 
 /* Lattice tables (src/lattices.js:31-104). */
 void or_tables(int8_t ex27[27], int8_t ey27[27], int8_t ez27[27], float w27[27],

@@ -1,7 +1,7 @@
 """Python view of the C oracle -- TEST INFRASTRUCTURE ONLY.
 
-Wraps oracle/_build/liblbm_oracle.so (built by oracle/Makefile) with the
-reference's own names, so parity tests read like the reference's test/ scripts:
+Wraps the oracle libraries built by oracle/Makefile with the reference's own
+names, so parity tests read like the reference's test/ scripts:
 
     sim = OracleSim(40, 28, 40); sim.initFlat(14); sim.tau = 0.7
     ball = OracleSphere(40, 28, 40, cx=20, cy=6, cz=20, r=4, density=1.6)
@@ -10,6 +10,9 @@ reference's own names, so parity tests read like the reference's test/ scripts:
 Class Sim follows src/sim.js:29-601, RigidSphere follows src/solid.js:8-211.
 Field arrays are zero-copy numpy views of the oracle's own memory, in the
 reference layout (cell i = (z*ny + y)*nx + x; f[i*27 + k], h[i*7 + k]).
+store='f32' (default) keeps fields in float32 exactly as the reference's
+Float32Arrays; store='f64' keeps them in double (reference for the GPU's FP64
+storage form).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module.
@@ -23,8 +26,9 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "_build", "liblbm_oracle.so")
-_lib = None
+_LIB_PATHS = {"f32": os.path.join(_HERE, "_build", "liblbm_oracle.so"),
+              "f64": os.path.join(_HERE, "_build", "liblbm_oracle_f64.so")}
+_libs = {}
 
 
 class _Sphere(C.Structure):
@@ -42,26 +46,33 @@ class _Sphere(C.Structure):
     ]
 
 
-_FP = C.POINTER(C.c_float)
 _U8 = C.POINTER(C.c_uint8)
 
 
-class _Sim(C.Structure):
-    _fields_ = [
-        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("n", C.c_int),
-        ("f", _FP), ("f2", _FP), ("h", _FP), ("h2", _FP),
-        ("rho", _FP), ("ux", _FP), ("uy", _FP), ("uz", _FP), ("phi", _FP), ("phiPrev", _FP),
-        ("tag", _U8), ("tagPrev", _U8),
-        ("usx", _FP), ("usy", _FP), ("usz", _FP),
-        ("gx", _FP), ("gy", _FP), ("gz", _FP), ("lap", _FP),
-        ("bodyFx", _FP), ("bodyFy", _FP), ("bodyFz", _FP),
-        ("neighOffset27", C.c_int32 * 27), ("fOffset27", C.c_int32 * 27),
-        ("neighOffset7", C.c_int32 * 7), ("hOffset7", C.c_int32 * 7),
-        ("tau", C.c_double), ("tauPhi", C.c_double), ("sigma", C.c_double),
-        ("gravity", C.c_double), ("rhoL", C.c_double), ("rhoG", C.c_double),
-        ("W", C.c_double), ("mobility", C.c_double),
-        ("omp", C.c_int),
-    ]
+def _sim_struct(real):
+    FP = C.POINTER(real)
+
+    class _Sim(C.Structure):
+        _fields_ = [
+            ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("n", C.c_int),
+            ("f", FP), ("f2", FP), ("h", FP), ("h2", FP),
+            ("rho", FP), ("ux", FP), ("uy", FP), ("uz", FP), ("phi", FP), ("phiPrev", FP),
+            ("tag", _U8), ("tagPrev", _U8),
+            ("usx", FP), ("usy", FP), ("usz", FP),
+            ("gx", FP), ("gy", FP), ("gz", FP), ("lap", FP),
+            ("bodyFx", FP), ("bodyFy", FP), ("bodyFz", FP),
+            ("neighOffset27", C.c_int32 * 27), ("fOffset27", C.c_int32 * 27),
+            ("neighOffset7", C.c_int32 * 7), ("hOffset7", C.c_int32 * 7),
+            ("tau", C.c_double), ("tauPhi", C.c_double), ("sigma", C.c_double),
+            ("gravity", C.c_double), ("rhoL", C.c_double), ("rhoG", C.c_double),
+            ("W", C.c_double), ("mobility", C.c_double),
+            ("omp", C.c_int),
+        ]
+    return _Sim
+
+
+_SIM_STRUCT = {"f32": _sim_struct(C.c_float), "f64": _sim_struct(C.c_double)}
+_DTYPE = {"f32": np.float32, "f64": np.float64}
 
 
 def build():
@@ -69,14 +80,17 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+def lib(store="f32"):
+    L = _libs.get(store)
+    if L is None:
+        path = _LIB_PATHS[store]
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(_LIB_PATH)
-        SP = C.POINTER(_Sim)
+        L = C.CDLL(path)
+        SP = C.POINTER(_SIM_STRUCT[store])
         BP = C.POINTER(_Sphere)
+        L.or_store_bytes.restype = C.c_int
+        assert L.or_store_bytes() == (8 if store == "f64" else 4)
         L.or_sim_create.restype = SP
         L.or_sim_create.argtypes = [C.c_int, C.c_int, C.c_int]
         L.or_sim_destroy.argtypes = [SP]
@@ -94,11 +108,12 @@ def lib():
         L.or_sphere_contains.argtypes = [BP, C.c_int, C.c_int, C.c_int]
         L.or_sphere_contains.restype = C.c_int
         L.or_sphere_surface_velocity.argtypes = [BP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
-        L.or_sphere_apply_impulse.argtypes = [BP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.or_sphere_apply_impulse.argtypes = [BP, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                              C.c_double]
         L.or_absorb_dead_cells.argtypes = [BP, C.c_int, SP]
         L.or_sphere_step.argtypes = [BP, C.c_double, C.c_double]
-        _lib = L
-    return _lib
+        _libs[store] = L
+    return L
 
 
 _SPHERE_FIELDS = {name for name, _ in _Sphere._fields_}
@@ -153,7 +168,7 @@ class OracleSphere:
         lib().or_sphere_apply_impulse(C.byref(self._s), x, y, z, px, py, pz)
 
     def absorbDeadCells(self, sim):
-        lib().or_absorb_dead_cells(C.byref(self._s), 1, sim._p)
+        sim._L.or_absorb_dead_cells(C.byref(self._s), 1, sim._p)
 
     def step(self, dt, gravity):
         lib().or_sphere_step(C.byref(self._s), dt, gravity)
@@ -173,7 +188,7 @@ class OracleSpheres:
         self.count = len(spheres)
 
     def absorbDeadCells(self, sim):
-        lib().or_absorb_dead_cells(self.arr, self.count, sim._p)
+        sim._L.or_absorb_dead_cells(self.arr, self.count, sim._p)
 
     def step(self, dt, gravity):
         for b in range(self.count):
@@ -201,9 +216,12 @@ def _solid_args(solid):
 class OracleSim:
     """class Sim (src/sim.js:29-601) backed by the C oracle."""
 
-    def __init__(self, nx, ny, nz):
-        p = lib().or_sim_create(nx, ny, nz)
+    def __init__(self, nx, ny, nz, store="f32"):
+        L = lib(store)
+        p = L.or_sim_create(nx, ny, nz)
+        object.__setattr__(self, "_L", L)
         object.__setattr__(self, "_p", p)
+        object.__setattr__(self, "store", store)
         object.__setattr__(self, "nx", nx)
         object.__setattr__(self, "ny", ny)
         object.__setattr__(self, "nz", nz)
@@ -223,8 +241,9 @@ class OracleSim:
 
     def __del__(self):
         p = self.__dict__.get("_p")
-        if p and _lib is not None:
-            _lib.or_sim_destroy(p)
+        L = self.__dict__.get("_L")
+        if p and L is not None:
+            L.or_sim_destroy(p)
             self.__dict__["_p"] = None
 
     def __getattr__(self, name):
@@ -242,7 +261,7 @@ class OracleSim:
             object.__setattr__(self, name, value)
 
     def set_threads(self, nthreads):
-        lib().or_sim_set_omp(self._p, int(nthreads))
+        self._L.or_sim_set_omp(self._p, int(nthreads))
 
     def idx(self, x, y, z):
         return ((z * self.ny) + y) * self.nx + x
@@ -251,42 +270,42 @@ class OracleSim:
         return self.rhoG + p * (self.rhoL - self.rhoG)
 
     def initFlat(self, waterlineY):
-        lib().or_init_flat(self._p, waterlineY)
+        self._L.or_init_flat(self._p, waterlineY)
 
     def seedHydrostatic(self):
-        lib().or_seed_hydrostatic(self._p)
+        self._L.or_seed_hydrostatic(self._p)
 
     def computePhiGradients(self):
-        lib().or_compute_phi_gradients(self._p)
+        self._L.or_compute_phi_gradients(self._p)
 
     def step(self, solid):
-        lib().or_step(self._p, *_solid_args(solid))
+        self._L.or_step(self._p, *_solid_args(solid))
 
     def retagCells(self, solid):
-        lib().or_retag_cells(self._p, *_solid_args(solid))
+        self._L.or_retag_cells(self._p, *_solid_args(solid))
 
     def handleFreshCells(self, solid=None):
-        lib().or_handle_fresh_cells(self._p)
+        self._L.or_handle_fresh_cells(self._p)
 
     def collidePhase(self):
-        lib().or_collide_phase(self._p)
+        self._L.or_collide_phase(self._p)
 
     def streamPhase(self):
-        lib().or_stream_phase(self._p)
+        self._L.or_stream_phase(self._p)
 
     def collideHydro(self):
-        lib().or_collide_hydro(self._p)
+        self._L.or_collide_hydro(self._p)
 
     def streamHydroAndMacro(self, solid):
-        lib().or_stream_hydro_and_macro(self._p, *_solid_args(solid))
+        self._L.or_stream_hydro_and_macro(self._p, *_solid_args(solid))
 
     def packVolume(self, out=None, solidContains=None):
         if out is None:
             out = np.zeros(self.n * 2, dtype=np.uint8)
         assert out.dtype == np.uint8 and out.size >= self.n * 2 and out.flags.c_contiguous
-        lib().or_pack_volume(self._p, out.ctypes.data_as(_U8))
+        self._L.or_pack_volume(self._p, out.ctypes.data_as(_U8))
         return out
 
     def worker_substep(self, solid):
         """sim.step(solid); solid.absorbDeadCells(sim); solid.step(1.0, g) (src/worker.js:96-100)."""
-        lib().or_worker_substep(self._p, *_solid_args(solid))
+        self._L.or_worker_substep(self._p, *_solid_args(solid))

@@ -6,9 +6,17 @@ computes in FP32, so fields agree to FP32 rounding, not bit for bit):
   * tags, fresh-cell and dead-cell sets: bit-exact, given the same sphere state;
   * RG8 packing of identical inputs: bit-exact;
   * phi, rho: rel-L2 <= TOL_REL, Linf <= TOL_INF after the run;
-  * u: rel-L2 <= TOL_REL_U, Linf / max|u_ref| <= TOL_INF_U;
+  * u: rel-L2 <= TOL_REL_U, Linf / max|u_ref| <= TOL_INF_U.  u is a small
+    difference of O(w_k) populations (sum e_k f_k); FP32 evaluation leaves an
+    absolute error of ~1e-7, which is ~1e-3..1e-2 of |u| in the gravity-down
+    scenes where |u| ~ 1e-5..1e-4;
   * sphere centre drift <= TOL_POS cells.
+The FP64 storage form against the oracle's FP64 build (every field kept in
+double) agrees to ~1e-12: only the association of the collision algebra and
+of the impulse sums differ.
 """
+import functools
+
 import numpy as np
 import pytest
 
@@ -19,9 +27,10 @@ pytestmark = pytest.mark.gpu
 
 TOL_REL = 2e-5
 TOL_INF = 2e-4
-TOL_REL_U = 2e-3
+TOL_REL_U = 1e-2
 TOL_INF_U = 2e-2
 TOL_POS = 1e-5
+TOL64 = 1e-10
 
 
 @pytest.fixture(scope="module")
@@ -74,6 +83,29 @@ def test_fused_step_matches_oracle(name, gpu, oracle_mod):
     if osol is not None:
         for k in ("cx", "cy", "cz"):
             assert abs(getattr(gsol, k) - getattr(osol, k)) <= TOL_POS, k
+
+
+@pytest.mark.parametrize("name", ["smoke", "cfg1", "drop"])
+def test_fp64_storage_matches_fp64_oracle(name, gpu, oracle_mod):
+    """The fused step in the FP64 storage form against the oracle with every
+    field kept in double: agreement to ~1e-12 pins the fused kernel's algebra
+    (collision at the source, bounce-back, moving wall, macros) to the
+    reference's formulas independently of float32 rounding."""
+    b = scenes.SCENES[name]
+    o, osol = b(functools.partial(oracle_mod.OracleSim, store="f64"), oracle_mod.OracleSphere)
+    g, gsol = b(functools.partial(gpu.Sim, storage="f64"), gpu.RigidSphere)
+    for s in range(60):
+        substep(o, osol)
+        substep(g, gsol)
+    for fld in ("phi", "rho", "ux", "uy", "uz", "f", "h"):
+        ref = np.asarray(getattr(o, fld), np.float64)
+        got = g.field64(fld)
+        scale = max(np.abs(ref).max(), 1e-30)
+        err = np.abs(got - ref).max() / scale
+        assert err <= TOL64, (name, fld, err)
+    assert np.array_equal(np.asarray(g.tag), np.asarray(o.tag))
+    for k in ("cx", "cy", "cz", "vx", "vy", "vz"):
+        assert abs(getattr(gsol, k) - getattr(osol, k)) <= TOL64, (name, k)
 
 
 def test_phase_by_phase_matches_oracle(gpu, oracle_mod):
