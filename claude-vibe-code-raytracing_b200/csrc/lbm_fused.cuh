@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
   const Real dRho = (Real)a.dRho, grav = (Real)a.gravity, sharpC4 = (Real)a.sharpC4;
 
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const bool haloA = ty == TY, haloB = ty == TY + 1, haloWarp = ty >= TY;
+  const bool haloA = ty == TY, haloWarp = ty >= TY;
   const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TY;
   const int zb = 1 + blockIdx.z * a.zchunk;
   const int ze = min(zb + a.zchunk, nz - 1);

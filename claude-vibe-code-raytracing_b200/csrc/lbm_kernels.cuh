@@ -590,32 +590,49 @@ __global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, 
   }
 }
 
-// absorbDeadCells (src/solid.js:87-101): scan-ordered dead list, FP64, one
-// thread per sphere; impulse rho(phi)*u to the owning sphere.
-template <class PopT>
-__global__ void k_absorb_dead(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *dead,
-                              const int *totals, int cap, double rhoL, double rhoG,
-                              const SolidSet *__restrict__ ssp, double *out) {
+// absorbDeadCells (src/solid.js:87-101): impulse rho(phi)*u of every cell on
+// the scan-ordered dead list, in FP64, to the sphere owning the cell.  One CTA
+// per sphere; thread t sums the contiguous t-th share of the list in scan
+// order, then a fixed shared-memory tree adds the shares -- deterministic,
+// and independent of how many dead cells there are per step.
+constexpr int DEAD_THREADS = 256;
+
+// (static: Real = float is instantiated by several translation units)
+template <class Real>
+static __global__ void __launch_bounds__(DEAD_THREADS)
+    k_absorb_dead(const Real *__restrict__ phi, const Real *__restrict__ ux,
+                  const Real *__restrict__ uy, const Real *__restrict__ uz, int nx, int ny,
+                  const int *__restrict__ dead, const int *__restrict__ totals, int cap, double rhoL,
+                  double rhoG, const SolidSet *__restrict__ ssp, double *out) {
+  __shared__ double sh[6][DEAD_THREADS];
   const SolidSet &ss = *ssp;
-  int b = threadIdx.x;
-  if (blockIdx.x != 0 || b >= ss.nsph) return;
+  const int b = blockIdx.x;
+  if (b >= ss.nsph) return;
   int nd = totals[1];
   if (nd > cap) nd = cap;
   const double dRho = rhoL - rhoG;
+  const int per = (nd + DEAD_THREADS - 1) / DEAD_THREADS;
+  const int q0 = threadIdx.x * per, q1 = min(q0 + per, nd);
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int q = 0; q < nd; q++) {
-    long long i = dead[q];
-    int x = (int)(i % s.nx);
-    long long t = i / s.nx;
-    int y = (int)(t % s.ny);
-    int z = (int)(t / s.ny);
+  for (int q = q0; q < q1; q++) {
+    const long long i = dead[q];
+    const int x = (int)(i % nx);
+    const long long t = i / nx;
+    const int y = (int)(t % ny);
+    const int z = (int)(t / ny);
     if (owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) != b) continue;
-    double rhoPhase = __dadd_rn(rhoG, __dmul_rn((double)s.phi[cur][i], dRho));
-    impulse_terms(ss.sph[b], x, y, z, __dmul_rn(rhoPhase, (double)s.ux[cur][i]),
-                  __dmul_rn(rhoPhase, (double)s.uy[cur][i]), __dmul_rn(rhoPhase, (double)s.uz[cur][i]),
-                  acc);
+    const double rhoPhase = __dadd_rn(rhoG, __dmul_rn((double)phi[i], dRho));
+    impulse_terms(ss.sph[b], x, y, z, __dmul_rn(rhoPhase, (double)ux[i]),
+                  __dmul_rn(rhoPhase, (double)uy[i]), __dmul_rn(rhoPhase, (double)uz[i]), acc);
   }
-  for (int j = 0; j < 6; j++) out[6 * b + j] = acc[j];
+  for (int j = 0; j < 6; j++) sh[j][threadIdx.x] = acc[j];
+  __syncthreads();
+  for (int st = DEAD_THREADS / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int j = 0; j < 6; j++) sh[j][threadIdx.x] = __dadd_rn(sh[j][threadIdx.x], sh[j][threadIdx.x + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) out[6 * b + threadIdx.x] = sh[threadIdx.x][0];
 }
 
 // Deterministic two-level reduction of the per-cell impulse arrays:

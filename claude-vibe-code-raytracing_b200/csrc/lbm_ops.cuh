@@ -238,9 +238,11 @@ class Ops final : public OpsBase {
     h->launches++;
   }
   void absorb_dead(lbm_sim *h, double *d_out) override {
-    k_absorb_dead<PopT><<<1, 32, 0, h->stream>>>(scene(h), h->cur, h->dead, h->totals,
-                                                  (int)h->listCap, h->params.rhoL, h->params.rhoG,
-                                                  &h->dPlan->ss, d_out);
+    const int ns = h->hPlan.ss.nsph > 0 ? h->hPlan.ss.nsph : 1;
+    k_absorb_dead<Real><<<ns, DEAD_THREADS, 0, h->stream>>>(
+        (const Real *)h->mac[h->cur][0], (const Real *)h->mac[h->cur][2], (const Real *)h->mac[h->cur][3],
+        (const Real *)h->mac[h->cur][4], h->nx, h->ny, h->dead, h->totals, (int)h->listCap,
+        h->params.rhoL, h->params.rhoG, &h->dPlan->ss, d_out);
     h->launches++;
   }
 

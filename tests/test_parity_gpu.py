@@ -175,6 +175,28 @@ def test_impulse_matches_oracle(gpu, oracle_mod):
         assert abs(a - b) <= 1e-4 * max(1.0, abs(b)), (k, a, b)
 
 
+def test_absorb_dead_matches_oracle(gpu, oracle_mod):
+    """absorbDeadCells (src/solid.js:87-101) over a whole sphere of dead cells
+    (the first retag after placing the sphere) on identical float32 fields: the
+    FP64 F, T agree with the oracle's scan-order sum up to summation order."""
+    (o, osol), (g, gsol) = _pair(scenes.bench, gpu, oracle_mod)
+    rng = np.random.default_rng(11)
+    fields = {"phi": rng.uniform(-0.1, 1.1, o.n), "ux": rng.normal(0, 0.02, o.n),
+              "uy": rng.normal(0, 0.02, o.n), "uz": rng.normal(0, 0.02, o.n)}
+    for sim, sol in ((o, osol), (g, gsol)):
+        sol.cx, sol.cy, sol.cz = 19.3, 13.6, 20.4
+        sol.setRadius(8.5)
+        for name, v in fields.items():
+            getattr(sim, name)[:] = v.astype(np.float32)
+        sim.retagCells(sol)
+        sol.absorbDeadCells(sim)
+    _, dead = _oracle_sets(o)
+    assert len(dead) > 2000
+    for k in ("Fx", "Fy", "Fz", "Tx", "Ty", "Tz"):
+        a, b = getattr(gsol, k), getattr(osol, k)
+        assert abs(a - b) <= 1e-12 * max(1.0, abs(b)), (k, a, b)
+
+
 def test_pack_volume_exact(gpu, oracle_mod):
     (o, osol), (g, gsol) = _pair(scenes.bench, gpu, oracle_mod)
     for sim, sol in ((o, osol), (g, gsol)):
