@@ -102,6 +102,9 @@ _SIGS = [
     ("lbm_fused_timing", C.c_int, [C.c_void_p, C.c_int]),
     ("lbm_fused_timing_query", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("lbm_set_fused_config", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("lbm_absorb_dead_cells_noalloc", C.c_int,
+     [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double] + [C.c_void_p] * 6
+     + [C.POINTER(LbmSphere), C.c_int, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]

@@ -193,6 +193,28 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
 /* Fused-kernel launch shape: rows per CTA (2, 4, 8 or 16) and z planes per CTA. */
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
 
+/* ---- allocation-free dead-cell sweep --------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory at the point of the call (an engine that owns all device memory
+ * through its own pool, a host whose allocator belongs to another runtime, a
+ * loop that must not pay cudaMalloc's synchronisation): the same sum as
+ * lbm_absorb_dead_cells, on FP32 fields the caller owns, with no handle and no
+ * allocation.  tag / tag_prev (uint8, n cells), phi, ux, uy, uz (float, n cells)
+ * and out (6*nspheres doubles: Fx Fy Fz Tx Ty Tz per sphere, overwritten) are
+ * device pointers in the reference's cell order; spheres is host memory.  The
+ * work is queued on `stream` (a cudaStream_t, NULL for the default stream).
+ * Its scratch is one fixed device array inside the library (about 8.4 MB per
+ * GPU, held until exit): the spheres' search box may hold at most 2^20 cells,
+ * larger boxes return LBM_ERR_CAPACITY.  The first call on each device sets
+ * that array up and should come before any stream capture.  Calls share the
+ * array, so calls that overlap on the GPU race.  A message for a non-zero
+ * status goes to err (errlen bytes, may be NULL). */
+int lbm_absorb_dead_cells_noalloc(int nx, int ny, int nz, double rho_liquid, double rho_gas,
+                                  const uint8_t *tag, const uint8_t *tag_prev,
+                                  const float *phi, const float *ux, const float *uy,
+                                  const float *uz, const lbm_sphere *spheres, int nspheres,
+                                  double *out, void *stream, char *err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif
