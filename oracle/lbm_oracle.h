@@ -16,10 +16,11 @@
  *
  * Pinning: the reference ships no golden vectors (its test/ scripts only
  * check finiteness, phi range and max|u|), and no JavaScript engine exists on
- * this machine.  The oracle is pinned against golden vectors produced by
- * running the reference's own sim.js / solid.js sources through the
- * JS-subset transpiler in tests/golden/ (see tests/golden/make_golden.py);
- * where that pin is absent, parity is unpinned.
+ * this machine.  tests/golden/make_golden.py runs the reference's own
+ * lattices.js / solid.js / sim.js, translated mechanically into Python by
+ * tests/golden/jsmini.py, and commits the results as tests/golden/*.npz;
+ * tests/test_golden_cpu.py requires this oracle to reproduce every field,
+ * set, sphere state and impulse of those fixtures bit for bit.
  *
  * Multi-sphere scenes (the batched workload) use a composite solid: a cell is
  * SOLID when any sphere contains it, and the first containing sphere (lowest
