@@ -249,11 +249,13 @@ class Ops final : public OpsBase {
   template <int TY>
   void launch_fused(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
     constexpr size_t smem = FusedSmem<PopT, TY>::bytes;
-    static bool attr = false;
-    if (!attr) {
+    // the shared-memory opt-in is per device
+    static unsigned long long attrSet = 0;
+    const unsigned long long bit = 1ull << (h->device & 63);
+    if (!(attrSet & bit)) {
       cudaFuncSetAttribute(k_fused_step<PopT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-      attr = true;
+      attrSet |= bit;
     }
     dim3 block(32, FusedSmem<PopT, TY>::warps);  // TY cell warps and two halo warps
     dim3 grid((h->nx + 31) / 32, (h->ny + TY - 1) / TY, (h->nz - 2 + zchunk - 1) / zchunk);

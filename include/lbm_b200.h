@@ -190,7 +190,7 @@ int lbm_transfer_bytes(const lbm_sim *sim, uint64_t *h2d, uint64_t *d2h);
  * synchronises the stream and returns the summed kernel time and launch count. */
 int lbm_fused_timing(lbm_sim *sim, int enable);
 int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
-/* Fused-kernel launch shape: rows per CTA (2, 4, 8 or 16) and z planes per CTA. */
+/* Fused-kernel launch shape: rows per CTA (2, 4 or 8) and z planes per CTA. */
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
 
 /* ---- allocation-free dead-cell sweep --------------------------------------- */

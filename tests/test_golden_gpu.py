@@ -6,8 +6,9 @@ Bars, as in test_parity_gpu.py (the plain CUDA path computes in FP32 where the
 reference computes in double and stores float32):
   * fresh / dead sets and tags: exact, given the reference's sphere state at
     the start of every step (the sphere is set from the golden trajectory);
-  * phi, rho: rel-L2 <= 2e-5, Linf <= 2e-4; u: rel-L2 <= 1e-2 and
-    Linf <= 2e-2 of max|u| (u is a small difference of O(w_k) populations);
+  * phi, rho: rel-L2 <= 2e-5, Linf <= 2e-4; u (the vector field): rel-L2
+    <= 1e-2 and Linf <= 2e-2 of max|u| (u is a small difference of O(w_k)
+    populations), or |du| <= 1e-7 where max|u| is below 5e-6;
   * sphere state after RigidSphere.step: within 1e-6 cells (cell units);
   * dead-cell impulse on identical fields: 1e-12 relative (FP64, summation
     order only); RG8 pack of identical phi: exact.
@@ -27,6 +28,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TOL_REL, TOL_INF = 2e-5, 2e-4
 TOL_REL_U, TOL_INF_U = 1e-2, 2e-2
 TOL_SPHERE = 1e-6
+U_ABS_FLOOR = 1e-7
 
 
 @pytest.fixture(scope="module")
@@ -42,14 +44,24 @@ def _load(name):
 
 
 def _check_fields(tag, got, want, stride=1):
-    """got: full GPU fields; want: golden arrays (full or strided samples)."""
-    umax = max(np.abs(want[k]).max() for k in ("ux", "uy", "uz")) or 1e-30
+    """got: full GPU fields; want: golden arrays (full or strided samples).
+
+    u is compared as one vector field (ux, uy, uz stacked): its components can
+    differ by orders of magnitude (cfg1 at step 1: |ux| ~ 6e-6, |uy| ~ 2e-4),
+    and FP32 round-off (~1e-8 per step in u) would dominate a per-component
+    relative norm of the small one.  Where max|u| itself is below
+    U_ABS_FLOOR / TOL_INF_U the bar is |du| <= U_ABS_FLOOR."""
     for k in ("phi", "rho"):
         rel, linf = field_err(got[k][::stride], want[k])
         assert rel <= TOL_REL and linf <= TOL_INF, f"{tag} {k}: rel {rel:.3e} linf {linf:.3e}"
-    for k in ("ux", "uy", "uz"):
-        rel, linf = field_err(got[k][::stride], want[k], norm=umax)
-        assert rel <= TOL_REL_U and linf <= TOL_INF_U, f"{tag} {k}: rel {rel:.3e} linf {linf:.3e}"
+    gu = np.concatenate([np.asarray(got[k][::stride], np.float64) for k in ("ux", "uy", "uz")])
+    wu = np.concatenate([np.asarray(want[k], np.float64) for k in ("ux", "uy", "uz")])
+    umax = np.abs(wu).max() or 1e-30
+    rel, linf = field_err(gu, wu, norm=umax)
+    if umax * TOL_INF_U >= U_ABS_FLOOR:
+        assert rel <= TOL_REL_U and linf <= TOL_INF_U, f"{tag} u: rel {rel:.3e} linf {linf:.3e}"
+    else:
+        assert linf * umax <= U_ABS_FLOOR, f"{tag} u: |du| {linf * umax:.3e}"
 
 
 @pytest.mark.parametrize("name", list(scenarios.PLAN))
