@@ -102,6 +102,16 @@ _SIGS = [
     ("lbm_fused_timing", C.c_int, [C.c_void_p, C.c_int]),
     ("lbm_fused_timing_query", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("lbm_set_fused_config", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("lbm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
+    ("lbm_batch_destroy", C.c_int, [C.c_void_p]),
+    ("lbm_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("lbm_batch_set_config", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("lbm_batch_run", C.c_int,
+     [C.c_void_p, C.POINTER(C.POINTER(LbmSphere)), C.POINTER(C.c_int), C.c_int, C.c_int,
+      C.POINTER(C.POINTER(C.c_uint8)), C.c_int]),
+    ("lbm_batch_time_fused", C.c_int,
+     [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    ("lbm_batch_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("lbm_absorb_dead_cells_noalloc", C.c_int,
      [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double] + [C.c_void_p] * 6
      + [C.POINTER(LbmSphere), C.c_int, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),

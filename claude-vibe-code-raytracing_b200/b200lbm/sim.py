@@ -270,6 +270,24 @@ class Sim:
         for i, b in enumerate(sp):
             b.add_impulse(out[i])
 
+    def run_coupled(self, solid, nsteps, frame_every=0):
+        """nsteps worker ticks (src/worker.js:96-100: sim.step(solid);
+        solid.absorbDeadCells(sim); solid.step(1.0, sim.gravity)) entirely on
+        the device.  The solid's state is updated in place.  Returns the RG8
+        volumes after every frame_every-th step, shape (frames, 2*n), or None."""
+        sp = spheres_of(solid)
+        self._sync()
+        arr = to_c_array(sp)
+        nfr = nsteps // frame_every if frame_every > 0 else 0
+        frames = np.empty((nfr, 2 * self.n), dtype=np.uint8) if nfr else None
+        ptr = frames.ctypes.data_as(C.POINTER(C.c_uint8)) if nfr else None
+        check(self._h, lib().lbm_run_coupled(self._h, arr, len(sp), nsteps,
+                                             frame_every if nfr else 0, ptr))
+        self._moved()
+        for i, b in enumerate(sp):
+            b.from_c(arr[i])
+        return frames
+
     def _absorb_dead(self, spheres):
         """RigidSphere.absorbDeadCells(sim) (src/solid.js:87-101) on the device."""
         if not spheres:

@@ -396,6 +396,126 @@ void free_all(lbm_sim *h) {
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
+
+// ---------------------------------------------------------------- device-resident coupled step
+// One coupled step (sim.step, absorbDeadCells, RigidSphere.step; src/worker.js:96-100)
+// entirely on the device: the plan is computed by k_plan from the device sphere
+// state, so no host round trip is needed between steps.  Split into the parts a
+// batch launches around its shared fused kernel.
+struct CoupledCtx {
+  int ns = 0;
+  long long slotCells = 0, maxU = 0, maxChunks = 0;
+  int redChunks = 0;
+};
+
+// Capacities for the device-computed plan, the plan's history and the device
+// sphere array; everything a captured step needs is allocated here.
+int coupled_prepare(lbm_sim *h, const lbm_sphere *sp, int ns, bool frames, CoupledCtx &c) {
+  int rc = check_spheres(h, sp, ns);
+  if (rc) return rc;
+  if (h->bfActive) return fail(h, LBM_ERR_STATE, "a pending body force needs lbm_step");
+  if (!h->fusedOK) return fail(h, LBM_ERR_UNSUPPORTED, "grid too large for the fused kernel");
+  double rmax = 0;
+  for (int b = 0; b < ns; b++) rmax = std::max(rmax, sp[b].r);
+  long long side = 2 * (long long)ceil(rmax) + 7;
+  c.ns = ns;
+  c.slotCells = std::min(h->n, side * side * side);
+  long long uside = 2 * (long long)ceil(rmax) + 12;
+  c.maxU = (h->fullRetagSteps > 0 || ns > 1) ? h->n : std::min(h->n, uside * uside * uside);
+  if (ns == 0) c.maxU = (h->fullRetagSteps > 0) ? h->n : box_cells(box_union(h->boxLast, h->boxLastLast));
+  c.maxChunks = (c.maxU + COMPACT_CHUNK - 1) / COMPACT_CHUNK;
+  c.redChunks = (int)((c.slotCells + RED_CHUNK - 1) / RED_CHUNK);
+  long long need = std::max(1LL, (long long)ns * c.slotCells * 6);
+  if (need > h->impCap) {
+    if (h->impAcc) {
+      cudaFree(h->impAcc);
+      h->deviceBytes -= h->impCap * sizeof(double);
+      h->impAcc = nullptr;
+    }
+    DALLOC(h->impAcc, need * sizeof(double));
+    h->impCap = need;
+  }
+  long long pneed = (long long)std::max(ns, 1) * c.redChunks * 6;
+  if (pneed > h->partialsCap) {
+    if (h->partials) {
+      cudaFree(h->partials);
+      h->deviceBytes -= h->partialsCap * sizeof(double);
+      h->partials = nullptr;
+    }
+    DALLOC(h->partials, pneed * sizeof(double));
+    h->partialsCap = pneed;
+  }
+  h->partialsChunks = c.redChunks;
+  if ((rc = ensure_counts(h, std::max(1LL, c.maxChunks)))) return rc;
+  if (frames && (rc = ensure_staging(h, (size_t)h->n * 2))) return rc;
+  // seed the device plan's history from the host's
+  memset(&h->hPlan, 0, sizeof(Plan));
+  h->hPlan.boxLast = h->boxLast;
+  h->hPlan.boxLastLast = h->boxLastLast;
+  h->hPlan.fullRetag = h->fullRetagSteps;
+  h->hPlan.ss.nsph = ns;
+  if ((rc = upload_plan(h))) return rc;
+  if (ns > 0)
+    CK(copy_async(h, h->dSph, sp, ns * sizeof(lbm_sphere), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+// plan, retag, fresh / dead compaction, fresh fill, impulse slot clearing
+int coupled_pre(lbm_sim *h, const CoupledCtx &c) {
+  k_plan<<<1, 1, 0, h->stream>>>(h->dPlan, h->dSph, c.ns, h->nx, h->ny, h->nz, h->impAcc, c.slotCells,
+                                 c.maxU);
+  h->launches++;
+  h->ops->retag_box(h, c.maxU);
+  int rc = launch_compaction(h, c.maxChunks);
+  if (rc) return rc;
+  h->ops->fresh_fill(h);
+  if (c.ns > 0) {
+    k_zero_targets<<<148 * 4, 256, 0, h->stream>>>(h->dPlan, h->impAcc);
+    h->launches++;
+  }
+  CKL("coupled step (before the fused kernel)");
+  return LBM_OK;
+}
+
+// impulse reduction, dead-cell absorption, RigidSphere.step on the device
+int coupled_post(lbm_sim *h, const CoupledCtx &c) {
+  if (c.ns > 0) {
+    double *dFluid = h->dOut, *dDead = h->dOut + LBM_MAX_SPHERES * 6;
+    dim3 g1(c.redChunks, c.ns);
+    k_impulse_reduce1<<<g1, 256, 0, h->stream>>>(&h->dPlan->ss, h->partials, c.redChunks);
+    k_impulse_reduce2<<<c.ns, 32, 0, h->stream>>>(&h->dPlan->ss, h->partials, c.redChunks, dFluid);
+    h->ops->absorb_dead(h, dDead);
+    h->ops->sphere_step_device(h, h->dSph, c.ns, h->params.gravity, dFluid, dDead);
+    h->launches += 2;
+  }
+  CKL("coupled step (after the fused kernel)");
+  return LBM_OK;
+}
+
+// RG8 volume of the current state into host memory dst (pinned when captured)
+int coupled_frame(lbm_sim *h, uint8_t *dst) {
+  h->ops->pack(h, (uint8_t *)h->staging);
+  CKL("packVolume");
+  CK(copy_async(h, dst, h->staging, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->stream));
+  return LBM_OK;
+}
+
+// sphere state and plan history back to the host
+int coupled_finish(lbm_sim *h, lbm_sphere *sp, int ns) {
+  CK(copy_async(h, &h->hPlan, h->dPlan, sizeof(Plan), cudaMemcpyDeviceToHost, h->stream));
+  if (ns > 0)
+    CK(copy_async(h, sp, h->dSph, ns * sizeof(lbm_sphere), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->boxLast = h->hPlan.boxLast;
+  h->boxLastLast = h->hPlan.boxLastLast;
+  h->fullRetagSteps = h->hPlan.fullRetag;
+  h->lastRetagBox = h->hPlan.U;
+  h->listsValid = true;
+  if (h->hPlan.overflow) return fail(h, LBM_ERR_CAPACITY, "sphere moved beyond the planned retag box");
+  return LBM_OK;
+}
+
 }  // namespace
 
 // =====================================================================================
@@ -913,96 +1033,22 @@ int lbm_pack_volume(lbm_sim *h, uint8_t *host_out) {
 
 int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_every, uint8_t *frames) {
   if (!h || nsteps < 0) return LBM_ERR_ARG;
-  int rc = check_spheres(h, sp, ns);
-  if (rc) return rc;
-  if (h->bfActive) return fail(h, LBM_ERR_STATE, "a pending body force needs lbm_step");
-  if (!h->fusedOK) return fail(h, LBM_ERR_UNSUPPORTED, "grid too large for the fused kernel");
   DeviceGuard g(h->device);
-  // capacity bounds for the device-computed plan
-  double rmax = 0;
-  for (int b = 0; b < ns; b++) rmax = std::max(rmax, sp[b].r);
-  long long side = 2 * (long long)ceil(rmax) + 7;
-  long long slotCells = std::min(h->n, side * side * side);
-  long long uside = 2 * (long long)ceil(rmax) + 12;
-  long long maxU = (h->fullRetagSteps > 0 || ns > 1) ? h->n : std::min(h->n, uside * uside * uside);
-  if (ns == 0) maxU = (h->fullRetagSteps > 0) ? h->n : box_cells(box_union(h->boxLast, h->boxLastLast));
-  long long maxChunks = (maxU + COMPACT_CHUNK - 1) / COMPACT_CHUNK;
-  int redChunks = (int)((slotCells + RED_CHUNK - 1) / RED_CHUNK);
-  long long need = std::max(1LL, (long long)ns * slotCells * 6);
-  if (need > h->impCap) {
-    if (h->impAcc) {
-      cudaFree(h->impAcc);
-      h->deviceBytes -= h->impCap * sizeof(double);
-      h->impAcc = nullptr;
-    }
-    DALLOC(h->impAcc, need * sizeof(double));
-    h->impCap = need;
-  }
-  long long pneed = (long long)std::max(ns, 1) * redChunks * 6;
-  if (pneed > h->partialsCap) {
-    if (h->partials) {
-      cudaFree(h->partials);
-      h->deviceBytes -= h->partialsCap * sizeof(double);
-      h->partials = nullptr;
-    }
-    DALLOC(h->partials, pneed * sizeof(double));
-    h->partialsCap = pneed;
-  }
-  h->partialsChunks = redChunks;
-  if ((rc = ensure_counts(h, std::max(1LL, maxChunks)))) return rc;
-  if (frame_every > 0 && frames && (rc = ensure_staging(h, (size_t)h->n * 2))) return rc;
-  // seed the device plan's history from the host's
-  memset(&h->hPlan, 0, sizeof(Plan));
-  h->hPlan.boxLast = h->boxLast;
-  h->hPlan.boxLastLast = h->boxLastLast;
-  h->hPlan.fullRetag = h->fullRetagSteps;
-  h->hPlan.ss.nsph = ns;
-  if ((rc = upload_plan(h))) return rc;
-  if (ns > 0)
-    CK(copy_async(h, h->dSph, sp, ns * sizeof(lbm_sphere), cudaMemcpyHostToDevice, h->stream));
-  double *dFluid = h->dOut, *dDead = h->dOut + LBM_MAX_SPHERES * 6;
-  const unsigned zeroBlocks = 148 * 4;
+  CoupledCtx c;
+  int rc = coupled_prepare(h, sp, ns, frame_every > 0 && frames, c);
+  if (rc) return rc;
   long long frame = 0;
   for (int s = 0; s < nsteps; s++) {
-    k_plan<<<1, 1, 0, h->stream>>>(h->dPlan, h->dSph, ns, h->nx, h->ny, h->nz, h->impAcc, slotCells, maxU);
-    h->launches++;
-    h->ops->retag_box(h, maxU);
-    if ((rc = launch_compaction(h, maxChunks))) return rc;
-    h->ops->fresh_fill(h);
-    if (ns > 0) {
-      k_zero_targets<<<zeroBlocks, 256, 0, h->stream>>>(h->dPlan, h->impAcc);
-      h->launches++;
-    }
+    if ((rc = coupled_pre(h, c))) return rc;
     launch_fused(h);
-    if (ns > 0) {
-      dim3 g1(redChunks, ns);
-      k_impulse_reduce1<<<g1, 256, 0, h->stream>>>(&h->dPlan->ss, h->partials, redChunks);
-      k_impulse_reduce2<<<ns, 32, 0, h->stream>>>(&h->dPlan->ss, h->partials, redChunks, dFluid);
-      h->ops->absorb_dead(h, dDead);
-      h->ops->sphere_step_device(h, h->dSph, ns, h->params.gravity, dFluid, dDead);
-      h->launches += 2;
-    }
-    CKL("coupled step");
+    if ((rc = coupled_post(h, c))) return rc;
     h->cur = 1 - h->cur;
     if (frame_every > 0 && frames && (s + 1) % frame_every == 0) {
-      h->ops->pack(h, (uint8_t *)h->staging);
-      CKL("packVolume");
-      CK(copy_async(h, frames + frame * 2 * h->n, h->staging, (size_t)h->n * 2,
-                         cudaMemcpyDeviceToHost, h->stream));
+      if ((rc = coupled_frame(h, frames + frame * 2 * h->n))) return rc;
       frame++;
     }
   }
-  CK(copy_async(h, &h->hPlan, h->dPlan, sizeof(Plan), cudaMemcpyDeviceToHost, h->stream));
-  if (ns > 0)
-    CK(copy_async(h, sp, h->dSph, ns * sizeof(lbm_sphere), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  h->boxLast = h->hPlan.boxLast;
-  h->boxLastLast = h->hPlan.boxLastLast;
-  h->fullRetagSteps = h->hPlan.fullRetag;
-  h->lastRetagBox = h->hPlan.U;
-  h->listsValid = true;
-  if (h->hPlan.overflow) return fail(h, LBM_ERR_CAPACITY, "sphere moved beyond the planned retag box");
-  return LBM_OK;
+  return coupled_finish(h, sp, ns);
 }
 
 int lbm_synchronize(lbm_sim *h) {
@@ -1098,6 +1144,330 @@ int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;
   h->cfg.zchunk = zchunk;
+  return LBM_OK;
+}
+
+}  // extern "C"
+
+// =====================================================================================
+// Batches of scenes stepped together (declarations in include/lbm_b200.h).
+
+struct lbm_batch {
+  std::vector<lbm_sim *> sims;
+  int device = 0, storage = 0;
+  int rows = 4, zchunk = 32;
+  std::string err;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  void *dArgs = nullptr;  // [2][n] descriptors (FusedArgs of the storage type)
+  size_t argsCap = 0;
+  int *dTileStart = nullptr;  // [n + 1]
+  int3 *dTileGrid = nullptr;  // [n]
+  int tilesCap = 0;
+  uint8_t *pinned = nullptr;  // frame ring of one chunk
+  size_t pinnedCap = 0;
+  long long launches = 0;  // batched fused launches executed
+};
+
+namespace {
+
+int bfail(lbm_batch *b, int code, const std::string &m) {
+  b->err = m;
+  return code;
+}
+int bcuda(lbm_batch *b, const char *what, cudaError_t e) {
+  cudaGetLastError();
+  return bfail(b, e == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA,
+               std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define BCK(call)                                        \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return bcuda(b, #call, e_);   \
+  } while (0)
+// a per-scene helper failed: carry its message to the batch
+#define BSIM(h, call)                                                 \
+  do {                                                                \
+    int rc_ = (call);                                                 \
+    if (rc_ != LBM_OK) return bfail(b, rc_, std::string("scene: ") + (h)->err); \
+  } while (0)
+
+// Per-scene descriptors for both ping-pong parities and the tile table.
+int batch_tables(lbm_batch *b) {
+  const int n = (int)b->sims.size();
+  OpsBase *ops = b->sims[0]->ops;
+  const size_t ab = ops->fused_args_bytes();
+  std::vector<unsigned char> args(2 * n * ab);
+  std::vector<int> start(n + 1, 0);
+  std::vector<int3> grid(n);
+  for (int s = 0; s < n; s++) {
+    lbm_sim *h = b->sims[s];
+    for (int p = 0; p < 2; p++) ops->fused_args(h, h->cur ^ p, b->zchunk, &args[(p * n + s) * ab]);
+    grid[s] = make_int3((h->nx + 31) / 32, (h->ny + b->rows - 1) / b->rows,
+                        (h->nz - 2 + b->zchunk - 1) / b->zchunk);
+    long long t = (long long)start[s] + (long long)grid[s].x * grid[s].y * grid[s].z;
+    if (t > (1LL << 30)) return bfail(b, LBM_ERR_CAPACITY, "too many tiles in one batch");
+    start[s + 1] = (int)t;
+  }
+  if (args.size() > b->argsCap) {
+    if (b->dArgs) cudaFree(b->dArgs);
+    b->dArgs = nullptr;
+    BCK(cudaMalloc(&b->dArgs, args.size()));
+    b->argsCap = args.size();
+  }
+  if (n > b->tilesCap) {
+    if (b->dTileStart) cudaFree(b->dTileStart);
+    if (b->dTileGrid) cudaFree(b->dTileGrid);
+    b->dTileStart = nullptr;
+    b->dTileGrid = nullptr;
+    BCK(cudaMalloc(&b->dTileStart, (n + 1) * sizeof(int)));
+    BCK(cudaMalloc(&b->dTileGrid, n * sizeof(int3)));
+    b->tilesCap = n;
+  }
+  BCK(cudaMemcpy(b->dArgs, args.data(), args.size(), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->dTileStart, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->dTileGrid, grid.data(), n * sizeof(int3), cudaMemcpyHostToDevice));
+  return LBM_OK;
+}
+
+int batch_tiles(const lbm_batch *b) {
+  long long t = 0;
+  for (lbm_sim *h : b->sims)
+    t += (long long)((h->nx + 31) / 32) * ((h->ny + b->rows - 1) / b->rows) *
+         ((h->nz - 2 + b->zchunk - 1) / b->zchunk);
+  return (int)t;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_batch_create(lbm_sim *const *sims, int n, lbm_batch **out) {
+  if (!sims || n < 1 || !out) return LBM_ERR_ARG;
+  *out = nullptr;
+  for (int s = 0; s < n; s++) {
+    if (!sims[s]) return LBM_ERR_ARG;
+    if (sims[s]->device != sims[0]->device || sims[s]->storage != sims[0]->storage) return LBM_ERR_ARG;
+    for (int t = 0; t < s; t++)
+      if (sims[t] == sims[s]) return LBM_ERR_ARG;
+  }
+  lbm_batch *b = new lbm_batch();
+  b->sims.assign(sims, sims + n);
+  b->device = sims[0]->device;
+  b->storage = sims[0]->storage;
+  b->rows = sims[0]->cfg.ty;
+  b->zchunk = sims[0]->cfg.zchunk;
+  DeviceGuard g(b->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  b->joins.resize(n, nullptr);
+  for (int s = 0; s < n && e == cudaSuccess; s++) e = cudaEventCreateWithFlags(&b->joins[s], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    lbm_batch_destroy(b);
+    return LBM_ERR_CUDA;
+  }
+  *out = b;
+  return LBM_OK;
+}
+
+int lbm_batch_destroy(lbm_batch *b) {
+  if (!b) return LBM_ERR_ARG;
+  DeviceGuard g(b->device);
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  for (cudaEvent_t ev : b->joins)
+    if (ev) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  if (b->dArgs) cudaFree(b->dArgs);
+  if (b->dTileStart) cudaFree(b->dTileStart);
+  if (b->dTileGrid) cudaFree(b->dTileGrid);
+  if (b->pinned) cudaFreeHost(b->pinned);
+  delete b;
+  return LBM_OK;
+}
+
+const char *lbm_batch_last_error(const lbm_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int lbm_batch_set_config(lbm_batch *b, int rows, int zchunk) {
+  if (!b) return LBM_ERR_ARG;
+  if (!(rows == 2 || rows == 4 || rows == 8) || zchunk < 1)
+    return bfail(b, LBM_ERR_ARG, "rows must be 2, 4 or 8 and zchunk >= 1");
+  b->rows = rows;
+  b->zchunk = zchunk;
+  return LBM_OK;
+}
+
+int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres, int nsteps,
+                  int frame_every, uint8_t *const *frames, int use_graph) {
+  if (!b || nsteps < 0 || !nspheres) return LBM_ERR_ARG;
+  const int n = (int)b->sims.size();
+  for (int s = 0; s < n; s++)
+    if (nspheres[s] < 0 || nspheres[s] > LBM_MAX_SPHERES || (nspheres[s] > 0 && (!spheres || !spheres[s])))
+      return bfail(b, LBM_ERR_ARG, "bad sphere arguments for scene " + std::to_string(s));
+  const bool wantFrames = frame_every > 0 && frames;
+  if (wantFrames)
+    for (int s = 0; s < n; s++)
+      if (!frames[s]) return bfail(b, LBM_ERR_ARG, "frames[" + std::to_string(s) + "] is NULL");
+  DeviceGuard g(b->device);
+  OpsBase *ops = b->sims[0]->ops;
+  std::vector<CoupledCtx> ctx(n);
+  for (int s = 0; s < n; s++)
+    BSIM(b->sims[s], coupled_prepare(b->sims[s], nspheres[s] ? spheres[s] : nullptr, nspheres[s], wantFrames,
+                                     ctx[s]));
+  int rc = batch_tables(b);
+  if (rc) return rc;
+  const int tiles = batch_tiles(b);
+  const int ctas = std::min(tiles, ops->fused_batch_ctas(b->rows, b->device));
+  const size_t ab = ops->fused_args_bytes();
+
+  // chunk of steps replayed as one graph: an even number (the ping-pong
+  // halves return to their parity) holding a whole number of frames
+  int G = 2;
+  if (wantFrames) G = frame_every % 2 == 0 ? frame_every : 2 * frame_every;
+  const bool graph = use_graph && nsteps >= G;
+  if (!graph) G = wantFrames ? frame_every : 1;
+  const int framesPerChunk = wantFrames ? G / frame_every : 0;
+  std::vector<size_t> slot(n + 1, 0);  // pinned offsets of each scene's frames in one chunk
+  for (int s = 0; s < n; s++) slot[s + 1] = slot[s] + (size_t)framesPerChunk * 2 * b->sims[s]->n;
+  if (slot[n] > b->pinnedCap) {
+    if (b->pinned) cudaFreeHost(b->pinned);
+    b->pinned = nullptr;
+    BCK(cudaMallocHost((void **)&b->pinned, slot[n]));
+    b->pinnedCap = slot[n];
+  }
+
+  // one coupled step of every scene: per-scene branches around the shared fused launch
+  auto emit_step = [&](int parity, int stepInChunk) -> int {
+    BCK(cudaEventRecord(b->fork, b->origin));
+    for (int s = 0; s < n; s++) {
+      lbm_sim *h = b->sims[s];
+      BCK(cudaStreamWaitEvent(h->stream, b->fork, 0));
+      BSIM(h, coupled_pre(h, ctx[s]));
+      BCK(cudaEventRecord(b->joins[s], h->stream));
+      BCK(cudaStreamWaitEvent(b->origin, b->joins[s], 0));
+    }
+    ops->fused_batch((const unsigned char *)b->dArgs + (size_t)parity * n * ab, b->dTileStart, b->dTileGrid,
+                     n, b->rows, ctas, b->origin);
+    BCK(cudaGetLastError());
+    BCK(cudaEventRecord(b->fork, b->origin));
+    const bool frameDue = wantFrames && (stepInChunk + 1) % frame_every == 0;
+    const int fIdx = wantFrames ? (stepInChunk + 1) / frame_every - 1 : 0;
+    for (int s = 0; s < n; s++) {
+      lbm_sim *h = b->sims[s];
+      BCK(cudaStreamWaitEvent(h->stream, b->fork, 0));
+      BSIM(h, coupled_post(h, ctx[s]));
+      h->cur = 1 - h->cur;
+      if (frameDue) BSIM(h, coupled_frame(h, b->pinned + slot[s] + (size_t)fIdx * 2 * h->n));
+      BCK(cudaEventRecord(b->joins[s], h->stream));
+      BCK(cudaStreamWaitEvent(b->origin, b->joins[s], 0));
+    }
+    return LBM_OK;
+  };
+  // frames of chunk `chunk` (count of them; fewer in a final partial chunk)
+  auto copy_frames = [&](long long chunk, int count) -> int {
+    if (!wantFrames || count <= 0) return LBM_OK;
+    BCK(cudaStreamSynchronize(b->origin));
+    for (int s = 0; s < n; s++) {
+      const size_t one = 2 * (size_t)b->sims[s]->n;
+      memcpy(frames[s] + (size_t)chunk * framesPerChunk * one, b->pinned + slot[s], (size_t)count * one);
+    }
+    return LBM_OK;
+  };
+
+  long long done = 0, chunk = 0;
+  if (graph) {
+    std::vector<long long> l0(n);
+    for (int s = 0; s < n; s++) l0[s] = b->sims[s]->launches;
+    cudaGraph_t gr = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    BCK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+    int erc = LBM_OK;
+    for (int i = 0; i < G && erc == LBM_OK; i++) erc = emit_step(i & 1, i);
+    cudaError_t ce = cudaStreamEndCapture(b->origin, &gr);
+    if (erc != LBM_OK || ce != cudaSuccess) {
+      if (gr) cudaGraphDestroy(gr);
+      cudaGetLastError();
+      for (int s = 0; s < n; s++) b->sims[s]->launches = l0[s];
+      if (erc != LBM_OK) return erc;
+      return bcuda(b, "cudaStreamEndCapture", ce);
+    }
+    ce = cudaGraphInstantiate(&ex, gr, 0);
+    cudaGraphDestroy(gr);
+    if (ce != cudaSuccess) return bcuda(b, "cudaGraphInstantiate", ce);
+    const long long chunks = nsteps / G;
+    for (; chunk < chunks; chunk++) {
+      ce = cudaGraphLaunch(ex, b->origin);
+      if (ce != cudaSuccess) {
+        cudaGraphExecDestroy(ex);
+        return bcuda(b, "cudaGraphLaunch", ce);
+      }
+      b->launches += G;
+      if ((rc = copy_frames(chunk, framesPerChunk))) {
+        cudaGraphExecDestroy(ex);
+        return rc;
+      }
+    }
+    cudaGraphExecDestroy(ex);
+    // the captured steps ran chunks times; the host flips during capture cancel (G even)
+    for (int s = 0; s < n; s++) b->sims[s]->launches = l0[s] + (b->sims[s]->launches - l0[s]) * chunks;
+    done = chunks * G;
+  }
+  // the rest eagerly, chunk by chunk so frames land in the pinned ring in order
+  while (done < nsteps) {
+    const long long len = std::min<long long>(G, nsteps - done);
+    for (long long i = 0; i < len; i++) {
+      if ((rc = emit_step((int)((done + i) & 1), (int)i))) return rc;
+      b->launches++;
+    }
+    if (wantFrames && (rc = copy_frames(chunk, (int)(len / frame_every)))) return rc;
+    done += len;
+    chunk++;
+  }
+  BCK(cudaStreamSynchronize(b->origin));
+  for (int s = 0; s < n; s++)
+    BSIM(b->sims[s], coupled_finish(b->sims[s], nspheres[s] ? spheres[s] : nullptr, nspheres[s]));
+  return LBM_OK;
+}
+
+int lbm_batch_time_fused(lbm_batch *b, int rows, int zchunk, int reps, double *ms) {
+  if (!b || !ms || reps < 1) return LBM_ERR_ARG;
+  if (!(rows == 2 || rows == 4 || rows == 8) || zchunk < 1)
+    return bfail(b, LBM_ERR_ARG, "rows must be 2, 4 or 8 and zchunk >= 1");
+  DeviceGuard g(b->device);
+  const int keepRows = b->rows, keepZ = b->zchunk;
+  b->rows = rows;
+  b->zchunk = zchunk;
+  int rc = batch_tables(b);
+  OpsBase *ops = b->sims[0]->ops;
+  const int ctas = std::min(batch_tiles(b), ops->fused_batch_ctas(rows, b->device));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (rc == LBM_OK) {
+    for (lbm_sim *h : b->sims) cudaStreamSynchronize(h->stream);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    ops->fused_batch(b->dArgs, b->dTileStart, b->dTileGrid, (int)b->sims.size(), rows, ctas, b->origin);
+    cudaEventRecord(e0, b->origin);
+    for (int r = 0; r < reps; r++)
+      ops->fused_batch(b->dArgs, b->dTileStart, b->dTileGrid, (int)b->sims.size(), rows, ctas, b->origin);
+    cudaEventRecord(e1, b->origin);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    if (e != cudaSuccess) rc = bcuda(b, "timing the batched fused kernel", e);
+    *ms = (double)t / reps;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  b->rows = keepRows;
+  b->zchunk = keepZ;
+  return rc;
+}
+
+int lbm_batch_launch_count(const lbm_batch *b, int64_t *count) {
+  if (!b || !count) return LBM_ERR_ARG;
+  *count = b->launches;
   return LBM_OK;
 }
 

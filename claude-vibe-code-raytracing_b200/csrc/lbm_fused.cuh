@@ -136,9 +136,9 @@ struct CellLoad {
   uint8_t tg;
 };
 
+// One tile (bx, by) of 32 x TY columns over z-chunk bz of one scene.
 template <class PopT, int TY>
-__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
-    k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
+__device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int by, int bz) {
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
   using SM = FusedSmem<PopT, TY>;
@@ -170,8 +170,8 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const bool haloA = ty == TY, haloWarp = ty >= TY;
-  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TY;
-  const int zb = 1 + blockIdx.z * a.zchunk;
+  const int x0 = bx * 32, y0 = by * TY;
+  const int zb = 1 + bz * a.zchunk;
   const int ze = min(zb + a.zchunk, nz - 1);
   if (zb >= ze) return;
   const int x = x0 + tx, y = y0 + ty;
@@ -491,6 +491,37 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
     gzC = gzN;
     lapC = lapN;
     phC = phN;
+  }
+}
+
+// One scene: the grid is its tiles.
+template <class PopT, int TY>
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
+    k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
+  fused_tile<PopT, TY>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Many scenes in one persistent launch: tile w of the batch belongs to the
+// scene s with tileStart[s] <= w < tileStart[s+1]; each scene's descriptor
+// gives its own grid, physics constants and state.  CTAs stride over the
+// tiles, so one launch of about one wave advances every scene by a step.
+template <class PopT, int TY>
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
+    k_fused_batch(const FusedArgs<PopT> *__restrict__ args, const int *__restrict__ tileStart,
+                  const int3 *__restrict__ tileGrid, int nscenes) {
+  const int total = tileStart[nscenes];
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    int lo = 0, hi = nscenes - 1;  // last scene whose first tile is <= w
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tileStart[mid] <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const int3 g = tileGrid[lo];
+    const int t = w - tileStart[lo];
+    const int bx = t % g.x, by = (t / g.x) % g.y, bz = t / (g.x * g.y);
+    fused_tile<PopT, TY>(args[lo], bx, by, bz);
+    __syncthreads();  // the next tile reuses shared memory
   }
 }
 

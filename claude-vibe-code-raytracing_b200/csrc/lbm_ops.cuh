@@ -2,6 +2,10 @@
 // storage type.  Included once per storage type by lbm_inst_*.cu.
 #pragma once
 
+#include <string.h>
+
+#include <algorithm>
+
 #include "lbm_fused.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_state.h"
@@ -263,11 +267,11 @@ class Ops final : public OpsBase {
     h->launches++;
   }
 
-  void fused_step(lbm_sim *h, const FusedCfg &cfg) override {
+  FusedArgs<PopT> make_args(lbm_sim *h, int cur, int zchunk) {
     FusedArgs<PopT> a;
     a.s = scene(h);
-    a.cur = h->cur;
-    a.zchunk = cfg.zchunk;
+    a.cur = cur;
+    a.zchunk = zchunk;
     StepConst k = make_const(h->params);
     a.om = k.invTau;
     a.omP = k.invTauPhi;
@@ -279,6 +283,54 @@ class Ops final : public OpsBase {
     a.gravity = k.gravity;
     a.sharpC4 = 4 * k.sharpC;
     a.ss = &h->dPlan->ss;
+    return a;
+  }
+  size_t fused_args_bytes() const override { return sizeof(FusedArgs<PopT>); }
+  void fused_args(lbm_sim *h, int cur, int zchunk, void *out) override {
+    FusedArgs<PopT> a = make_args(h, cur, zchunk);
+    memcpy(out, &a, sizeof(a));
+  }
+  template <int TY>
+  int batch_ctas(int device) {
+    constexpr size_t smem = FusedSmem<PopT, TY>::bytes;
+    static unsigned long long attrSet = 0;
+    const unsigned long long bit = 1ull << (device & 63);
+    if (!(attrSet & bit)) {
+      cudaFuncSetAttribute(k_fused_batch<PopT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attrSet |= bit;
+    }
+    int per = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_batch<PopT, TY>,
+                                                  FusedSmem<PopT, TY>::threads, smem);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return std::max(1, per) * std::max(1, sms);
+  }
+  int fused_batch_ctas(int ty, int device) override {
+    switch (ty) {
+      case 2: return batch_ctas<2>(device);
+      case 4: return batch_ctas<4>(device);
+      default: return batch_ctas<8>(device);
+    }
+  }
+  template <int TY>
+  void batch_launch(const void *d_args, const int *d_tileStart, const int3 *d_tileGrid, int n, int ctas,
+                    cudaStream_t st) {
+    dim3 block(32, FusedSmem<PopT, TY>::warps);
+    k_fused_batch<PopT, TY><<<ctas, block, FusedSmem<PopT, TY>::bytes, st>>>(
+        (const FusedArgs<PopT> *)d_args, d_tileStart, d_tileGrid, n);
+  }
+  void fused_batch(const void *d_args, const int *d_tileStart, const int3 *d_tileGrid, int nscenes, int ty,
+                   int ctas, cudaStream_t st) override {
+    switch (ty) {
+      case 2: batch_launch<2>(d_args, d_tileStart, d_tileGrid, nscenes, ctas, st); break;
+      case 4: batch_launch<4>(d_args, d_tileStart, d_tileGrid, nscenes, ctas, st); break;
+      default: batch_launch<8>(d_args, d_tileStart, d_tileGrid, nscenes, ctas, st); break;
+    }
+  }
+
+  void fused_step(lbm_sim *h, const FusedCfg &cfg) override {
+    FusedArgs<PopT> a = make_args(h, h->cur, cfg.zchunk);
     switch (cfg.ty) {
       case 2: launch_fused<2>(h, a, cfg.zchunk); break;
       case 4: launch_fused<4>(h, a, cfg.zchunk); break;

@@ -56,6 +56,14 @@ class OpsBase {
                                   const double *d_fluid, const double *d_dead) = 0;
   // Fused-step kernel geometry (for the bench and the autotuner).
   virtual size_t fused_smem(int ty) const = 0;
+  // Batched fused step: per-scene descriptors (FusedArgs of this storage type,
+  // fused_args_bytes() each) for a given ping-pong half, and one persistent
+  // launch over the tiles of every scene.
+  virtual size_t fused_args_bytes() const = 0;
+  virtual void fused_args(lbm_sim *h, int cur, int zchunk, void *out) = 0;
+  virtual int fused_batch_ctas(int ty, int device) = 0;  // resident CTAs on the device
+  virtual void fused_batch(const void *d_args, const int *d_tileStart, const int3 *d_tileGrid,
+                           int nscenes, int ty, int ctas, cudaStream_t st) = 0;
   // Fault record of the bounds-checked build (all zero otherwise); cleared on read.
   virtual cudaError_t read_fault(lbm_sim *h, unsigned long long out[4]) = 0;
 };

@@ -193,6 +193,35 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
 /* Fused-kernel launch shape: rows per CTA (2, 4 or 8) and z planes per CTA. */
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
 
+/* ---- batches: many scenes stepped together ---------------------------------- */
+/* The reference advances one scene per Web Worker (src/worker.js:94-115); a
+ * batch advances many independent scenes of any sizes with one persistent
+ * fused launch per step over the tiles of every scene (per-scene descriptors),
+ * the per-scene plan / retag / fresh-cell / impulse / RigidSphere.step kernels
+ * as parallel branches around it, and, with use_graph, the step sequence
+ * captured once as a CUDA graph and replayed.  Each scene's results are the
+ * same as lbm_run_coupled's on that scene alone.  All handles must be on one
+ * device with one storage form; a handle belongs to at most one running batch.
+ * rows / zchunk choose the fused tile shape (lbm_batch_time_fused times a
+ * shape on the batch's current state, for an autotuner). */
+typedef struct lbm_batch lbm_batch;
+int lbm_batch_create(lbm_sim *const *sims, int n, lbm_batch **out);
+int lbm_batch_destroy(lbm_batch *batch);
+const char *lbm_batch_last_error(const lbm_batch *batch);
+int lbm_batch_set_config(lbm_batch *batch, int rows, int zchunk);
+/* nsteps coupled steps of every scene (lbm_run_coupled semantics): spheres[s]
+ * holds nspheres[s] spheres of scene s (updated in place); with frame_every > 0
+ * the RG8 volume of scene s after every frame_every-th step is appended to
+ * frames[s] (2*n_s bytes per frame). */
+int lbm_batch_run(lbm_batch *batch, lbm_sphere *const *spheres, const int *nspheres, int nsteps,
+                  int frame_every, uint8_t *const *frames, int use_graph);
+/* Average time of the batched fused kernel with the given tile shape, over
+ * reps launches on the batch's current state (it rewrites the next half only;
+ * run after lbm_batch_run). */
+int lbm_batch_time_fused(lbm_batch *batch, int rows, int zchunk, int reps, double *ms);
+/* Batched fused launches executed so far. */
+int lbm_batch_launch_count(const lbm_batch *batch, int64_t *count);
+
 /* ---- allocation-free dead-cell sweep --------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory at the point of the call (an engine that owns all device memory
