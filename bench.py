@@ -55,6 +55,12 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rows", type=int, default=0)
     ap.add_argument("--zchunk", type=int, default=0)
+    ap.add_argument("--workload", default="scene", choices=["scene", "batch", "serve", "precision"],
+                    help="scene: the 256^3 line (default); batch: 64 seeded scenes stepped together; "
+                         "serve: a Poisson request stream through the continuous-batching server; "
+                         "precision: FP32/FP16/BF16 storage against an FP64 run")
+    ap.add_argument("--scenes", type=int, default=64)
+    ap.add_argument("--requests", type=int, default=24)
     return ap.parse_args()
 
 
@@ -215,11 +221,149 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, dev):
+    """64 seeded scenes of mixed sizes (FP16 storage) stepped together: one
+    persistent fused launch per step, the steps replayed as a CUDA graph, tile
+    shape from the autotuner; beside it the same scenes one after another."""
+    import torch
+
+    from b200lbm import Batch, autotune, workloads
+    torch.cuda.set_device(dev)
+    storage = "f16" if args.storage == "f32" else args.storage
+    specs = workloads.scene_specs(args.scenes, seed=0)
+    scenes = [workloads.build(sp, storage, dev) for sp in specs]
+    cells = sum(sim.n for sim, _ in scenes)
+    K = args.steps if args.steps != 2000 else 100
+    with Batch(scenes) as batch:
+        batch.run(2)
+        rows, zchunk, timings = autotune.tune(batch, [sp["dims"] for sp in specs], storage, force=True)
+        batch.run(max(2, args.warmup))
+        torch.cuda.synchronize(dev)
+        clocks = Clocks(dev)
+        clocks.start()
+        l0 = batch.launch_count()
+        t0 = time.perf_counter()
+        batch.run(K, use_graph=True)
+        dt_graph = time.perf_counter() - t0
+        clk = clocks.stop()
+        t0 = time.perf_counter()
+        batch.run(K, use_graph=False)
+        dt_eager = time.perf_counter() - t0
+        fused = batch.launch_count() - l0
+    t0 = time.perf_counter()
+    for sim, solid in scenes:
+        sim.run_coupled(solid, K)
+    dt_seq = time.perf_counter() - t0
+    for sim, _ in scenes:
+        sim.close()
+    line = {
+        "metric": f"batched MLUPS, {args.scenes} seeded scenes of mixed sizes", "value": cells * K / dt_graph / 1e6,
+        "unit": UNIT, "n_gpus": 1, "steps": K, "higher_is_better": True, "dtype": storage,
+        "data": "synthetic",
+        "config": {"workload": f"{args.scenes} scenes, edges U[32,160], pool 30-60% of ny, 1-3 spheres",
+                   "cells": cells, "storage": storage, "tile": [rows, zchunk],
+                   "timings_ms": {f"{r}x{z}": t for (r, z), t in timings.items()}},
+        "ms_per_step": dt_graph / K * 1e3,
+        "eager_mlups": cells * K / dt_eager / 1e6,
+        "sequential_mlups": cells * K / dt_seq / 1e6,
+        "batched_fused_launches": fused,
+        "timing": "wall clock around whole runs (host work included), after a synchronize",
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, dev):
+    """A seeded Poisson request stream (20/s, mixed sizes, 10% at 256^3,
+    500-5000 steps, a frame every 20 steps) through the continuous-batching
+    server (FP16 storage), and the same requests one at a time with plain
+    FP32 per-scene launches."""
+    import torch
+
+    from b200lbm import serve, workloads
+    torch.cuda.set_device(dev)
+    reqs = workloads.request_stream(args.requests, seed=0)
+    storage = "f16" if args.storage == "f32" else args.storage
+    clocks = Clocks(dev)
+    clocks.start()
+    rep = serve.Server(storage=storage, device=dev).run(reqs, realtime=True)
+    clk = clocks.stop()
+    seq = serve.sequential(reqs, storage="f32", device=dev)
+    line = {
+        "metric": "served scene-steps/s, Poisson request stream of mixed-size scenes",
+        "value": rep["scene_steps_per_s"], "unit": "scene-steps/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": storage, "data": "synthetic",
+        "config": {"workload": f"{args.requests} requests, Poisson 20/s, sizes U[32,160]^3 + 10% 256^3, "
+                               "500-5000 steps, RG8 frame every 20 steps", "storage": storage},
+        "served": rep, "sequential_plain_f32": seq,
+        "speedup_vs_sequential": rep["scene_steps_per_s"] / seq["scene_steps_per_s"],
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_precision(args, dev):
+    """The 256^3 scene in FP64 storage (the GPU error reference) and in FP32,
+    FP16 and BF16 storage from the same initial state: field errors, sphere
+    drift and the FP64 sums of mass and phase after the same steps."""
+    import torch
+
+    import scenes
+    from b200lbm import RigidSphere, Sim
+    torch.cuda.set_device(dev)
+    size = args.size
+    steps = args.steps if args.steps != 2000 else 1000
+    out = {}
+
+    def run(storage):
+        sim, sol = scenes.cfg2(lambda *a: Sim(*a, storage=storage, device=dev), RigidSphere, n=size)
+        m0 = (float(np.sum(sim.field64("rho"))), float(np.sum(sim.field64("phi"))))
+        t0 = time.perf_counter()
+        sim.run_coupled(sol, steps)
+        dt = time.perf_counter() - t0
+        f = {k: sim.field64(k) for k in ("phi", "rho", "ux", "uy", "uz")}
+        m1 = (float(np.sum(f["rho"])), float(np.sum(f["phi"])))
+        c = np.array([sol.cx, sol.cy, sol.cz])
+        sim.close()
+        return f, c, m0, m1, dt
+
+    ref, cref, m0r, m1r, _ = run("f64")
+    u_ref = np.concatenate([ref["ux"], ref["uy"], ref["uz"]])
+    for st in ("f32", "f16", "bf16"):
+        f, c, m0, m1, dt = run(st)
+        e = {}
+        for k in ("phi", "rho"):
+            d = f[k] - ref[k]
+            e[k] = {"rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref[k])), "linf": float(np.abs(d).max())}
+        u = np.concatenate([f["ux"], f["uy"], f["uz"]])
+        d = u - u_ref
+        e["u"] = {"rel_l2": float(np.linalg.norm(d) / np.linalg.norm(u_ref)),
+                  "linf_over_umax": float(np.abs(d).max() / np.abs(u_ref).max())}
+        e["sphere_drift_cells"] = float(np.abs(c - cref).max())
+        e["mass_drift"] = (m1[0] - m0[0]) / m0[0]
+        e["phase_drift"] = (m1[1] - m0[1]) / m0[1]
+        e["mlups"] = size ** 3 * steps / dt / 1e6
+        out[st] = e
+    line = {
+        "metric": f"storage-form error vs FP64 GPU run, {size}^3 gravity-down pool, {steps} steps",
+        "value": out["f16"]["phi"]["rel_l2"], "unit": "rel-L2 of phi (FP16 storage)", "n_gpus": 1,
+        "higher_is_better": False, "data": "synthetic", "steps": steps,
+        "fp64_mass_drift": (m1r[0] - m0r[0]) / m0r[0], "fp64_phase_drift": (m1r[1] - m0r[1]) / m0r[1],
+        "forms": out,
+        "timing": "mlups here is wall clock of Sim.run_coupled incl. host set-up, not the bench figure",
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.workload != "scene":
+        if rank == 0:
+            {"batch": run_batch, "serve": run_serve, "precision": run_precision}[args.workload](args, local)
         return
     import torch
 

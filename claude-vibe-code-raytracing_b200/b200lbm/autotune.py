@@ -1,0 +1,82 @@
+"""Tile-shape autotuner for batched steps.
+
+The fused kernel's tile shape -- rows per CTA (2, 4 or 8 cell warps plus two
+halo warps) and z planes per CTA -- trades halo recomputation and shared-memory
+occupancy against the number of tiles in flight; the best shape depends on the
+mix of grid sizes.  tune() times each candidate shape with
+lbm_batch_time_fused on the batch's own current state (the timed launches only
+rewrite the next ping-pong half, which the next step overwrites), keeps the
+fastest, and caches it under a coarse signature of the batch (storage form,
+number of scenes and total cells, each rounded up to a power of two), so
+batches of a similar mix reuse the choice without timing again.  The cache is
+persisted as JSON when LBM_B200_TUNE_CACHE names a file.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+CANDIDATES = [(4, 32), (4, 16), (8, 16), (8, 32), (2, 32), (4, 64)]
+
+_cache: dict = {}
+_loaded = False
+
+
+def _path():
+    return os.environ.get("LBM_B200_TUNE_CACHE")
+
+
+def _load():
+    global _loaded
+    if _loaded:
+        return
+    _loaded = True
+    p = _path()
+    if p and os.path.exists(p):
+        try:
+            with open(p) as fh:
+                _cache.update(json.load(fh))
+        except (OSError, ValueError):
+            pass
+
+
+def _save():
+    p = _path()
+    if p:
+        try:
+            with open(p, "w") as fh:
+                json.dump(_cache, fh, indent=1, sort_keys=True)
+        except OSError:
+            pass
+
+
+def signature(dims, storage):
+    total = sum(nx * ny * nz for nx, ny, nz in dims)
+    n = 2 ** math.ceil(math.log2(max(1, len(dims))))
+    c = 2 ** math.ceil(math.log2(max(1, total)))
+    return f"{storage}:n{n}:c{c}"
+
+
+def tune(batch, dims, storage, reps=3, candidates=CANDIDATES, force=False):
+    """Pick and set the fastest tile shape for `batch` (which has run at least
+    one step).  Returns (rows, zchunk, timings): timings maps each measured
+    shape to ms per launch, and is empty when the cache answered."""
+    _load()
+    key = signature(dims, storage)
+    if not force and key in _cache:
+        rows, zchunk = _cache[key]
+        batch.set_config(rows, zchunk)
+        return rows, zchunk, {}
+    timings = {}
+    for rows, zchunk in candidates:
+        timings[(rows, zchunk)] = batch.time_fused(rows, zchunk, reps=reps)
+    rows, zchunk = min(timings, key=timings.get)
+    _cache[key] = [rows, zchunk]
+    _save()
+    batch.set_config(rows, zchunk)
+    return rows, zchunk, timings
+
+
+def clear():
+    _cache.clear()

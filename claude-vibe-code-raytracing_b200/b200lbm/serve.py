@@ -1,0 +1,207 @@
+"""Serving: a continuous-batching loop for scene-simulation requests.
+
+The reference serves one interactive scene per browser tab (src/worker.js:
+a Web Worker steps its Sim and posts an RG8 volume every few steps).  Server
+runs many such scenes on one GPU at once:
+
+  * a request names a scene (grid, pool level, spheres; see workloads.py), a
+    number of steps and a frame cadence;
+  * admission: requests are taken in arrival order while their device
+    footprint (lbm_footprint_bytes plus the per-scene working buffers) fits
+    the memory budget; a request that does not fit waits until running scenes
+    finish and release theirs;
+  * each scene's lattices stay on the device from admission to completion;
+  * every tick the active scenes advance together as one Batch (one
+    persistent fused launch per step, the step sequence replayed as a CUDA
+    graph) by one frame interval, and every scene's RG8 volume is streamed
+    back to the host;
+  * between ticks finished scenes leave and newly arrived ones join, so work
+    that arrives while others run overlaps with them on the device.
+
+Each scene's results do not depend on what it was batched with: the batch
+gives every scene exactly the results of running it alone (tests/
+test_batch_gpu.py and tests/test_serve_gpu.py check this bit for bit).
+
+The report gives throughput (scene-steps/s and MLUPS over the whole run) and
+latency: time to first frame (from arrival, including the wait for admission)
+and the interval between consecutive frames of a request, as p50 / p99.
+"""
+from __future__ import annotations
+
+import collections
+import time
+
+import numpy as np
+
+from . import autotune, workloads
+from ._capi import STORAGE, lib
+from .batch import Batch
+
+# per-scene working buffers beyond lbm_footprint_bytes: compaction counts,
+# impulse slots, the frame staging buffer and the device plan (generous)
+_EXTRA_PER_CELL = 8
+_EXTRA_FIXED = 32 << 20
+
+
+def footprint(spec, storage):
+    nx, ny, nz = spec["dims"]
+    base = lib().lbm_footprint_bytes(nx, ny, nz, STORAGE[storage])
+    return int(base + _EXTRA_PER_CELL * nx * ny * nz + _EXTRA_FIXED)
+
+
+def admit(queue, used, budget, now, fp):
+    """Requests to admit now: the longest prefix of `queue` (arrival order)
+    that has arrived by `now` and fits in budget - used.  fp(req) -> bytes.
+    A request larger than the whole budget is admitted alone when nothing
+    else is running, so it is not starved forever (it may then fail to
+    allocate, which the caller reports)."""
+    out = []
+    for req in queue:
+        if req["arrival"] > now:
+            break
+        need = fp(req)
+        if used + need > budget and not (used == 0 and not out):
+            break
+        out.append(req)
+        used += need
+    return out
+
+
+def percentiles(xs, ps=(50, 99)):
+    if not xs:
+        return {f"p{p}": None for p in ps}
+    a = np.asarray(xs, dtype=np.float64)
+    return {f"p{p}": float(np.percentile(a, p)) for p in ps}
+
+
+class Server:
+    def __init__(self, storage="f16", budget_bytes=None, tick=None, use_graph=True, tune=True, device=0):
+        self.storage = storage
+        self.budget = budget_bytes if budget_bytes is not None else int(0.9 * 180e9)
+        self.tick = tick
+        self.use_graph = use_graph
+        self.tune = tune
+        self.device = device
+
+    def run(self, requests, realtime=True, on_frame=None, on_finish=None):
+        """Serve `requests` (dicts with rid, arrival, spec, steps, frame_every;
+        frame_every must be the same for all and divide every steps).
+        realtime: a request becomes visible at its arrival time (seconds after
+        the start); otherwise all are visible at once.  on_frame(rid, index,
+        volume) gets every RG8 volume; on_finish(rid, sim, solid) runs before a
+        finished scene is released.  Returns the report dict."""
+        reqs = sorted(requests, key=lambda r: (r["arrival"], r["rid"]))
+        every = {r["frame_every"] for r in reqs}
+        if len(every) != 1:
+            raise ValueError("all requests of one run share the frame cadence")
+        every = every.pop()
+        tick = self.tick or every
+        if tick % every or any(r["steps"] % tick for r in reqs):
+            raise ValueError("the tick must be a multiple of the frame cadence and divide every request")
+        queue = collections.deque(reqs)
+        active = []  # dicts: req, sim, solid, done, fp, frames, last
+        used = 0
+        batch = None
+        members = None
+        ttff, interval, done_at = [], [], {}
+        scene_steps = cell_steps = 0
+        max_active = 0
+        ticks = 0
+        t0 = time.perf_counter()
+        clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: float("inf"))
+        try:
+            while queue or active:
+                now = clock()
+                for req in admit(list(queue), used, self.budget, now,
+                                 lambda r: footprint(r["spec"], self.storage)):
+                    queue.popleft()
+                    sim, solid = workloads.build(req["spec"], self.storage, self.device)
+                    fp = footprint(req["spec"], self.storage)
+                    used += fp
+                    active.append(dict(req=req, sim=sim, solid=solid, done=0, fp=fp, frames=0, last=None))
+                if not active:
+                    # idle until the next arrival
+                    wait = queue[0]["arrival"] - (time.perf_counter() - t0)
+                    if wait > 0:
+                        time.sleep(wait)
+                    continue
+                max_active = max(max_active, len(active))
+                ids = [a["req"]["rid"] for a in active]
+                if ids != members:
+                    if batch is not None:
+                        batch.close()
+                    batch = Batch([(a["sim"], a["solid"]) for a in active])
+                    members = ids
+                    tuned = False
+                frames = batch.run(tick, frame_every=every, use_graph=self.use_graph)
+                ticks += 1
+                if self.tune and not tuned:
+                    autotune.tune(batch, [(a["sim"].nx, a["sim"].ny, a["sim"].nz) for a in active],
+                                  self.storage)
+                    tuned = True
+                t = time.perf_counter() - t0
+                for a, fr in zip(active, frames):
+                    for j in range(fr.shape[0]):
+                        if a["frames"] == 0:
+                            ttff.append(t - a["req"]["arrival"] if realtime else t)
+                        else:
+                            interval.append(t - a["last"])
+                        a["last"] = t
+                        if on_frame is not None:
+                            on_frame(a["req"]["rid"], a["frames"], fr[j])
+                        a["frames"] += 1
+                    a["done"] += tick
+                    scene_steps += tick
+                    cell_steps += tick * a["sim"].n
+                still = []
+                for a in active:
+                    if a["done"] >= a["req"]["steps"]:
+                        if on_finish is not None:
+                            on_finish(a["req"]["rid"], a["sim"], a["solid"])
+                        done_at[a["req"]["rid"]] = t
+                        used -= a["fp"]
+                        a["sim"].close()
+                    else:
+                        still.append(a)
+                if len(still) != len(active):
+                    active = still
+        finally:
+            if batch is not None:
+                batch.close()
+            for a in active:
+                a["sim"].close()
+        wall = time.perf_counter() - t0
+        return {
+            "requests": len(reqs),
+            "wall_s": wall,
+            "ticks": ticks,
+            "scene_steps": scene_steps,
+            "scene_steps_per_s": scene_steps / wall if wall > 0 else None,
+            "mlups": cell_steps / wall / 1e6 if wall > 0 else None,
+            "ttff_s": percentiles(ttff),
+            "frame_interval_s": percentiles(interval),
+            "frames": len(ttff) + len(interval),
+            "max_active": max_active,
+            "storage": self.storage,
+            "budget_bytes": self.budget,
+        }
+
+
+def sequential(requests, storage="f32", device=0, on_finish=None):
+    """Baseline: the same requests one at a time in arrival order, each on
+    its own with Sim.run_coupled (per-scene launches, no batching)."""
+    reqs = sorted(requests, key=lambda r: (r["arrival"], r["rid"]))
+    t0 = time.perf_counter()
+    scene_steps = cell_steps = 0
+    for req in reqs:
+        sim, solid = workloads.build(req["spec"], storage, device)
+        sim.run_coupled(solid, req["steps"], frame_every=req["frame_every"])
+        scene_steps += req["steps"]
+        cell_steps += req["steps"] * sim.n
+        if on_finish is not None:
+            on_finish(req["rid"], sim, solid)
+        sim.close()
+    wall = time.perf_counter() - t0
+    return {"requests": len(reqs), "wall_s": wall, "scene_steps": scene_steps,
+            "scene_steps_per_s": scene_steps / wall, "mlups": cell_steps / wall / 1e6,
+            "storage": storage}

@@ -1165,9 +1165,12 @@ struct lbm_batch {
   int *dTileStart = nullptr;  // [n + 1]
   int3 *dTileGrid = nullptr;  // [n]
   int tilesCap = 0;
-  uint8_t *pinned = nullptr;  // frame ring of one chunk
+  uint8_t *pinned = nullptr;  // one frame of every scene
   size_t pinnedCap = 0;
-  long long launches = 0;  // batched fused launches executed
+  long long launches = 0;            // batched fused launches executed
+  cudaGraphExec_t exec = nullptr;    // captured 2-step chunk
+  std::vector<long long> execKey;    // what it baked in
+  std::vector<long long> execDelta;  // per-scene launches in one chunk
 };
 
 namespace {
@@ -1284,6 +1287,7 @@ int lbm_batch_destroy(lbm_batch *b) {
   if (b->dTileStart) cudaFree(b->dTileStart);
   if (b->dTileGrid) cudaFree(b->dTileGrid);
   if (b->pinned) cudaFreeHost(b->pinned);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
   delete b;
   return LBM_OK;
 }
@@ -1322,15 +1326,12 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
   const int ctas = std::min(tiles, ops->fused_batch_ctas(b->rows, b->device));
   const size_t ab = ops->fused_args_bytes();
 
-  // chunk of steps replayed as one graph: an even number (the ping-pong
-  // halves return to their parity) holding a whole number of frames
-  int G = 2;
-  if (wantFrames) G = frame_every % 2 == 0 ? frame_every : 2 * frame_every;
-  const bool graph = use_graph && nsteps >= G;
-  if (!graph) G = wantFrames ? frame_every : 1;
-  const int framesPerChunk = wantFrames ? G / frame_every : 0;
-  std::vector<size_t> slot(n + 1, 0);  // pinned offsets of each scene's frames in one chunk
-  for (int s = 0; s < n; s++) slot[s + 1] = slot[s] + (size_t)framesPerChunk * 2 * b->sims[s]->n;
+  // Graph mode replays a captured chunk of 2 steps (the ping-pong halves
+  // return to their parity); frames are taken between chunks, so graph mode
+  // needs an even frame_every (an odd one runs eagerly).
+  const bool graph = use_graph && nsteps >= 2 && (!wantFrames || frame_every % 2 == 0);
+  std::vector<size_t> slot(n + 1, 0);  // pinned offset of each scene's frame
+  for (int s = 0; s < n; s++) slot[s + 1] = slot[s] + (wantFrames ? 2 * (size_t)b->sims[s]->n : 0);
   if (slot[n] > b->pinnedCap) {
     if (b->pinned) cudaFreeHost(b->pinned);
     b->pinned = nullptr;
@@ -1339,7 +1340,7 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
   }
 
   // one coupled step of every scene: per-scene branches around the shared fused launch
-  auto emit_step = [&](int parity, int stepInChunk) -> int {
+  auto emit_step = [&](int parity) -> int {
     BCK(cudaEventRecord(b->fork, b->origin));
     for (int s = 0; s < n; s++) {
       lbm_sim *h = b->sims[s];
@@ -1352,78 +1353,90 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
                      n, b->rows, ctas, b->origin);
     BCK(cudaGetLastError());
     BCK(cudaEventRecord(b->fork, b->origin));
-    const bool frameDue = wantFrames && (stepInChunk + 1) % frame_every == 0;
-    const int fIdx = wantFrames ? (stepInChunk + 1) / frame_every - 1 : 0;
     for (int s = 0; s < n; s++) {
       lbm_sim *h = b->sims[s];
       BCK(cudaStreamWaitEvent(h->stream, b->fork, 0));
       BSIM(h, coupled_post(h, ctx[s]));
       h->cur = 1 - h->cur;
-      if (frameDue) BSIM(h, coupled_frame(h, b->pinned + slot[s] + (size_t)fIdx * 2 * h->n));
       BCK(cudaEventRecord(b->joins[s], h->stream));
       BCK(cudaStreamWaitEvent(b->origin, b->joins[s], 0));
     }
     return LBM_OK;
   };
-  // frames of chunk `chunk` (count of them; fewer in a final partial chunk)
-  auto copy_frames = [&](long long chunk, int count) -> int {
-    if (!wantFrames || count <= 0) return LBM_OK;
+  // RG8 volume of every scene into frames[s][idx]
+  auto take_frame = [&](long long idx) -> int {
+    BCK(cudaEventRecord(b->fork, b->origin));
+    for (int s = 0; s < n; s++) {
+      lbm_sim *h = b->sims[s];
+      BCK(cudaStreamWaitEvent(h->stream, b->fork, 0));
+      BSIM(h, coupled_frame(h, b->pinned + slot[s]));
+      BCK(cudaEventRecord(b->joins[s], h->stream));
+      BCK(cudaStreamWaitEvent(b->origin, b->joins[s], 0));
+    }
     BCK(cudaStreamSynchronize(b->origin));
     for (int s = 0; s < n; s++) {
       const size_t one = 2 * (size_t)b->sims[s]->n;
-      memcpy(frames[s] + (size_t)chunk * framesPerChunk * one, b->pinned + slot[s], (size_t)count * one);
+      memcpy(frames[s] + (size_t)idx * one, b->pinned + slot[s], one);
     }
     return LBM_OK;
   };
 
-  long long done = 0, chunk = 0;
+  // the captured 2-step graph, reused while nothing it baked in has changed
   if (graph) {
-    std::vector<long long> l0(n);
-    for (int s = 0; s < n; s++) l0[s] = b->sims[s]->launches;
-    cudaGraph_t gr = nullptr;
-    cudaGraphExec_t ex = nullptr;
-    BCK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
-    int erc = LBM_OK;
-    for (int i = 0; i < G && erc == LBM_OK; i++) erc = emit_step(i & 1, i);
-    cudaError_t ce = cudaStreamEndCapture(b->origin, &gr);
-    if (erc != LBM_OK || ce != cudaSuccess) {
-      if (gr) cudaGraphDestroy(gr);
-      cudaGetLastError();
-      for (int s = 0; s < n; s++) b->sims[s]->launches = l0[s];
-      if (erc != LBM_OK) return erc;
-      return bcuda(b, "cudaStreamEndCapture", ce);
+    std::vector<long long> key = {b->rows, b->zchunk, (long long)(uintptr_t)b->dArgs,
+                                  (long long)(uintptr_t)b->dTileStart, ctas};
+    for (int s = 0; s < n; s++) {
+      lbm_sim *h = b->sims[s];
+      const long long v[] = {(long long)(uintptr_t)h,           h->cur,      ctx[s].ns,
+                             ctx[s].slotCells,                  ctx[s].maxU, ctx[s].maxChunks,
+                             ctx[s].redChunks,                  (long long)(uintptr_t)h->impAcc,
+                             (long long)(uintptr_t)h->partials, (long long)(uintptr_t)h->counts};
+      key.insert(key.end(), v, v + 10);
     }
-    ce = cudaGraphInstantiate(&ex, gr, 0);
-    cudaGraphDestroy(gr);
-    if (ce != cudaSuccess) return bcuda(b, "cudaGraphInstantiate", ce);
-    const long long chunks = nsteps / G;
-    for (; chunk < chunks; chunk++) {
-      ce = cudaGraphLaunch(ex, b->origin);
+    if (!b->exec || key != b->execKey) {
+      if (b->exec) cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+      std::vector<long long> l0(n);
+      for (int s = 0; s < n; s++) l0[s] = b->sims[s]->launches;
+      cudaGraph_t gr = nullptr;
+      BCK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+      int erc = emit_step(0);
+      if (erc == LBM_OK) erc = emit_step(1);
+      cudaError_t ce = cudaStreamEndCapture(b->origin, &gr);
+      b->execDelta.assign(n, 0);
+      for (int s = 0; s < n; s++) {
+        b->execDelta[s] = b->sims[s]->launches - l0[s];
+        b->sims[s]->launches = l0[s];  // counted when the graph runs
+      }
+      if (erc != LBM_OK || ce != cudaSuccess) {
+        if (gr) cudaGraphDestroy(gr);
+        cudaGetLastError();
+        if (erc != LBM_OK) return erc;
+        return bcuda(b, "cudaStreamEndCapture", ce);
+      }
+      ce = cudaGraphInstantiate(&b->exec, gr, 0);
+      cudaGraphDestroy(gr);
       if (ce != cudaSuccess) {
-        cudaGraphExecDestroy(ex);
-        return bcuda(b, "cudaGraphLaunch", ce);
+        b->exec = nullptr;
+        return bcuda(b, "cudaGraphInstantiate", ce);
       }
-      b->launches += G;
-      if ((rc = copy_frames(chunk, framesPerChunk))) {
-        cudaGraphExecDestroy(ex);
-        return rc;
-      }
+      b->execKey = key;
     }
-    cudaGraphExecDestroy(ex);
-    // the captured steps ran chunks times; the host flips during capture cancel (G even)
-    for (int s = 0; s < n; s++) b->sims[s]->launches = l0[s] + (b->sims[s]->launches - l0[s]) * chunks;
-    done = chunks * G;
   }
-  // the rest eagerly, chunk by chunk so frames land in the pinned ring in order
+
+  long long done = 0;
   while (done < nsteps) {
-    const long long len = std::min<long long>(G, nsteps - done);
-    for (long long i = 0; i < len; i++) {
-      if ((rc = emit_step((int)((done + i) & 1), (int)i))) return rc;
+    if (graph && nsteps - done >= 2) {
+      BCK(cudaGraphLaunch(b->exec, b->origin));
+      for (int s = 0; s < n; s++) b->sims[s]->launches += b->execDelta[s];
+      b->launches += 2;
+      done += 2;
+    } else {
+      if ((rc = emit_step((int)(done & 1)))) return rc;
       b->launches++;
+      done++;
     }
-    if (wantFrames && (rc = copy_frames(chunk, (int)(len / frame_every)))) return rc;
-    done += len;
-    chunk++;
+    if (wantFrames && done % frame_every == 0 && (rc = take_frame(done / frame_every - 1))) return rc;
   }
   BCK(cudaStreamSynchronize(b->origin));
   for (int s = 0; s < n; s++)

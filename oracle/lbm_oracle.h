@@ -18,9 +18,9 @@
  * check finiteness, phi range and max|u|), and no JavaScript engine exists on
  * this machine.  tests/golden/make_golden.py runs the reference's own
  * lattices.js / solid.js / sim.js, translated mechanically into Python by
- * tests/golden/jsmini.py, and commits the results as tests/golden/*.npz;
- * tests/test_golden_cpu.py requires this oracle to reproduce every field,
- * set, sphere state and impulse of those fixtures bit for bit.
+ * tests/golden/jsmini.py, and commits the results as .npz fixtures in
+ * tests/golden; tests/test_golden_cpu.py requires this oracle to reproduce
+ * every field, set, sphere state and impulse of those fixtures bit for bit.
  *
  * Multi-sphere scenes (the batched workload) use a composite solid: a cell is
  * SOLID when any sphere contains it, and the first containing sphere (lowest

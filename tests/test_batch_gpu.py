@@ -52,16 +52,19 @@ def _state(sim, solid):
     return fields, [b.state() for b in spheres_of(solid)]
 
 
-@pytest.mark.parametrize("use_graph,nsteps", [(True, 24), (True, 17), (False, 13)])
-def test_batch_equals_scenes_alone(gpu, use_graph, nsteps):
+@pytest.mark.parametrize("use_graph,nsteps,every", [(True, 24, 4), (True, 17, 4), (False, 13, 5),
+                                                    (True, 13, 5)])
+def test_batch_equals_scenes_alone(gpu, use_graph, nsteps, every):
+    """Graph replay (2-step chunks, frames between chunks), a trailing eager
+    step, eager mode, and an odd frame cadence (which runs eagerly)."""
     alone = _build(gpu)
     want = []
     for sim, solid in alone:
-        frames = sim.run_coupled(solid, nsteps, frame_every=5)
+        frames = sim.run_coupled(solid, nsteps, frame_every=every)
         want.append((frames, _state(sim, solid)))
     mixed = _build(gpu)
     with gpu.Batch(mixed) as batch:
-        got = batch.run(nsteps, frame_every=5, use_graph=use_graph)
+        got = batch.run(nsteps, frame_every=every, use_graph=use_graph)
         assert batch.launch_count() == nsteps
     for i, ((sim, solid), (wframes, (wf, ws))) in enumerate(zip(mixed, want)):
         assert np.array_equal(got[i], wframes), f"scene {i}: frames differ"
@@ -80,8 +83,9 @@ def test_batch_continues_across_runs_and_configs(gpu):
     with gpu.Batch(mixed) as batch:
         batch.set_config(8, 16)
         batch.run(4)
+        batch.run(2)  # the cached graph is replayed
         batch.set_config(2, 7)
-        batch.run(6)
+        batch.run(4)
         ms = batch.time_fused(4, 32, reps=2)
         assert ms > 0
     for (sim, solid), (rsim, rsolid) in zip(mixed, ref):
