@@ -10,6 +10,9 @@ runs many such scenes on one GPU at once:
     footprint (lbm_footprint_bytes plus the per-scene working buffers) fits
     the memory budget; a request that does not fit waits until running scenes
     finish and release theirs;
+  * an admitted scene is built and initialised on a worker thread, on its
+    own stream, while the running scenes keep stepping; it joins at the next
+    tick after it is ready;
   * each scene's lattices stay on the device from admission to completion;
   * every tick the active scenes advance together as one Batch (one
     persistent fused launch per step, the step sequence replayed as a CUDA
@@ -30,6 +33,7 @@ from __future__ import annotations
 
 import collections
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -109,21 +113,34 @@ class Server:
         ticks = 0
         t0 = time.perf_counter()
         clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: float("inf"))
+        pool = ThreadPoolExecutor(max_workers=2, thread_name_prefix="lbm-build")
+        building = []  # (req, fp, future) admitted, not yet built
         try:
-            while queue or active:
+            while queue or active or building:
                 now = clock()
                 for req in admit(list(queue), used, self.budget, now,
                                  lambda r: footprint(r["spec"], self.storage)):
                     queue.popleft()
-                    sim, solid = workloads.build(req["spec"], self.storage, self.device)
                     fp = footprint(req["spec"], self.storage)
                     used += fp
-                    active.append(dict(req=req, sim=sim, solid=solid, done=0, fp=fp, frames=0, last=None))
+                    building.append((req, fp, pool.submit(workloads.build, req["spec"], self.storage,
+                                                          self.device)))
+                if building and not active:
+                    building[0][2].result()  # nothing to step meanwhile
+                still_building = []
+                for req, fp, fut in building:
+                    if fut.done():
+                        sim, solid = fut.result()
+                        active.append(dict(req=req, sim=sim, solid=solid, done=0, fp=fp, frames=0, last=None))
+                    else:
+                        still_building.append((req, fp, fut))
+                building = still_building
                 if not active:
                     # idle until the next arrival
-                    wait = queue[0]["arrival"] - (time.perf_counter() - t0)
-                    if wait > 0:
-                        time.sleep(wait)
+                    if queue:
+                        wait = queue[0]["arrival"] - (time.perf_counter() - t0)
+                        if wait > 0:
+                            time.sleep(wait)
                     continue
                 max_active = max(max_active, len(active))
                 ids = [a["req"]["rid"] for a in active]
@@ -170,6 +187,12 @@ class Server:
                 batch.close()
             for a in active:
                 a["sim"].close()
+            for _, _, fut in building:
+                try:
+                    fut.result()[0].close()
+                except Exception:
+                    pass
+            pool.shutdown(wait=True)
         wall = time.perf_counter() - t0
         return {
             "requests": len(reqs),

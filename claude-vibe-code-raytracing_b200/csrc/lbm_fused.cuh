@@ -296,9 +296,28 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
           eu += (Real)ez * uz;
           eq += (Real)ez * Qz;
         }
-        const Real fk = om1 * C::dec(L.fv[k], (Real)D::w) + (Real)D::w * (C0 + ev + eu * eq);
         const int fb = ez < 0 ? fbM : (ez == 0 ? fbZ : fbP);
-        if (nd) ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
+        // f*_k = (1 - w) f_k + (w_k T + w_k e.V) with T = (e.u)(e.Q) + C0.  The
+        // opposite direction has the same T and the negated w_k e.V, exactly
+        // (every negation is exact), so a tile cell evaluates opposite pairs
+        // (k odd, k + 1) together and still gets, bit for bit, what a halo
+        // cell evaluating one direction alone gets.
+        if constexpr (MODE == 0 && k > 0) {
+          if constexpr (k & 1) {
+            using O = D27<D::opp>;
+            const Real T = eu * eq + C0, wev = (Real)D::w * ev, wT = (Real)D::w * T;
+            const Real fk = om1 * C::dec(L.fv[k], (Real)D::w) + (wT + wev);
+            const Real fo = om1 * C::dec(L.fv[D::opp], (Real)O::w) + (wT - wev);
+            constexpr int fbo = O::ez < 0 ? 0 : (O::ez == 0 ? 1 : 2);
+            const int fbO = fbo == 0 ? fbM : (fbo == 1 ? fbZ : fbP);
+            ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
+            ring[sm_at(fbO + slot27(D::opp) * NC, RING, 7)] = fo;
+          }
+        } else {
+          const Real T = eu * eq + C0, wev = (Real)D::w * ev, wT = (Real)D::w * T;
+          const Real fk = om1 * C::dec(L.fv[k], (Real)D::w) + (wT + wev);
+          if (nd) ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
+        }
         if constexpr (k < Q7) {
           using E = D7<k>;
           Real ed = 0;
