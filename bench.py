@@ -81,11 +81,8 @@ def dist_init(args):
 def max_over_ranks(v, ws, local):
     if ws == 1:
         return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from b200lbm import placement
+    return placement.max_over_ranks(v)
 
 
 def barrier(ws):
@@ -221,16 +218,19 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, dev):
+def run_batch(args, dev, ws=1, rank=0):
     """64 seeded scenes of mixed sizes (FP16 storage) stepped together: one
     persistent fused launch per step, the steps replayed as a CUDA graph, tile
-    shape from the autotuner; beside it the same scenes one after another."""
+    shape from the autotuner; beside it the same scenes one after another.
+    With N ranks each GPU takes whole scenes (placement.shard by cells); the
+    line reports all ranks' cells over the slowest rank's time."""
     import torch
 
-    from b200lbm import Batch, autotune, workloads
+    from b200lbm import Batch, autotune, placement, workloads
     torch.cuda.set_device(dev)
     storage = "f16" if args.storage == "f32" else args.storage
     specs = workloads.scene_specs(args.scenes, seed=0)
+    specs = placement.shard(specs, ws, workloads.cells)[rank]
     scenes = [workloads.build(sp, storage, dev) for sp in specs]
     cells = sum(sim.n for sim, _ in scenes)
     K = args.steps if args.steps != 2000 else 100
@@ -256,11 +256,17 @@ def run_batch(args, dev):
     dt_seq = time.perf_counter() - t0
     for sim, _ in scenes:
         sim.close()
+    if ws > 1:
+        cells = placement.sum_over_ranks(cells)
+        dt_graph, dt_eager, dt_seq = (placement.max_over_ranks(v) for v in (dt_graph, dt_eager, dt_seq))
+    if rank != 0:
+        return
     line = {
         "metric": f"batched MLUPS, {args.scenes} seeded scenes of mixed sizes", "value": cells * K / dt_graph / 1e6,
-        "unit": UNIT, "n_gpus": 1, "steps": K, "higher_is_better": True, "dtype": storage,
-        "data": "synthetic",
+        "unit": UNIT, "n_gpus": ws, "steps": K, "higher_is_better": True, "dtype": storage,
+        "data": "synthetic", "scaling": "strong",
         "config": {"workload": f"{args.scenes} scenes, edges U[32,160], pool 30-60% of ny, 1-3 spheres",
+                   "parallelism": f"whole scenes per GPU x{ws}",
                    "cells": cells, "storage": storage, "tile": [rows, zchunk],
                    "timings_ms": {f"{r}x{z}": t for (r, z), t in timings.items()}},
         "ms_per_step": dt_graph / K * 1e3,
@@ -273,25 +279,33 @@ def run_batch(args, dev):
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args, dev):
+def run_serve(args, dev, ws=1, rank=0):
     """A seeded Poisson request stream (20/s, mixed sizes, 10% at 256^3,
     500-5000 steps, a frame every 20 steps) through the continuous-batching
     server (FP16 storage), and the same requests one at a time with plain
     FP32 per-scene launches."""
     import torch
 
-    from b200lbm import serve, workloads
+    from b200lbm import placement, serve, workloads
     torch.cuda.set_device(dev)
     reqs = workloads.request_stream(args.requests, seed=0)
+    reqs = placement.shard(reqs, ws, lambda r: workloads.cells(r["spec"]) * r["steps"])[rank]
     storage = "f16" if args.storage == "f32" else args.storage
     clocks = Clocks(dev)
     clocks.start()
     rep = serve.Server(storage=storage, device=dev).run(reqs, realtime=True)
     clk = clocks.stop()
     seq = serve.sequential(reqs, storage="f32", device=dev)
+    if ws > 1:
+        for r in (rep, seq):
+            r["scene_steps"] = placement.sum_over_ranks(r["scene_steps"])
+            r["wall_s"] = placement.max_over_ranks(r["wall_s"])
+            r["scene_steps_per_s"] = r["scene_steps"] / r["wall_s"]
+    if rank != 0:
+        return
     line = {
         "metric": "served scene-steps/s, Poisson request stream of mixed-size scenes",
-        "value": rep["scene_steps_per_s"], "unit": "scene-steps/s", "n_gpus": 1,
+        "value": rep["scene_steps_per_s"], "unit": "scene-steps/s", "n_gpus": ws,
         "higher_is_better": True, "dtype": storage, "data": "synthetic",
         "config": {"workload": f"{args.requests} requests, Poisson 20/s, sizes U[32,160]^3 + 10% 256^3, "
                                "500-5000 steps, RG8 frame every 20 steps", "storage": storage},
@@ -362,8 +376,14 @@ def main():
         run_reference(args, ws, rank)
         return
     if args.workload != "scene":
-        if rank == 0:
-            {"batch": run_batch, "serve": run_serve, "precision": run_precision}[args.workload](args, local)
+        if args.workload == "precision":
+            if rank == 0:
+                run_precision(args, local)
+        else:
+            {"batch": run_batch, "serve": run_serve}[args.workload](args, local, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     import torch
 
