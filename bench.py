@@ -55,10 +55,11 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rows", type=int, default=0)
     ap.add_argument("--zchunk", type=int, default=0)
-    ap.add_argument("--workload", default="scene", choices=["scene", "batch", "serve", "precision"],
+    ap.add_argument("--workload", default="scene", choices=["scene", "batch", "serve", "precision", "render"],
                     help="scene: the 256^3 line (default); batch: 64 seeded scenes stepped together; "
                          "serve: a Poisson request stream through the continuous-batching server; "
-                         "precision: FP32/FP16/BF16 storage against an FP64 run")
+                         "precision: FP32/FP16/BF16 storage against an FP64 run; "
+                         "render: the raymarcher, 1920x1080 frames of the 256^3 scene")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--requests", type=int, default=24)
     return ap.parse_args()
@@ -369,6 +370,65 @@ def run_precision(args, dev):
     print(json.dumps(line), flush=True)
 
 
+def run_render(args, dev):
+    """Frames of the reference's renderer (its fragment shader, one CUDA
+    thread per pixel) over the 256^3 scene's RG8 volume: pack + render per
+    frame, CUDA events on the library's stream; beside it the C restatement
+    of the shader on one host core for one frame."""
+    import torch
+
+    import scenes
+    from b200lbm import RigidSphere, Sim
+    from b200lbm._capi import LbmCamera, LbmSphere, check, lib
+    torch.cuda.set_device(dev)
+    size, W, H = args.size, 1920, 1080
+    sim, sol = scenes.cfg2(lambda *a: Sim(*a, storage=args.storage, device=dev), RigidSphere, n=size)
+    sim.run_coupled(sol, 20)
+    L = lib()
+    cam = LbmCamera()
+    L.lbm_camera_default(C.byref(cam))
+    sph = (LbmSphere * 1)()
+    sol.to_c(sph[0])
+    vol = torch.empty(2 * sim.n, dtype=torch.uint8, device=f"cuda:{dev}")
+    img = torch.empty((H, W, 4), dtype=torch.uint8, device=f"cuda:{dev}")
+    stream = torch.cuda.ExternalStream(L.lbm_stream(sim.handle), device=dev)
+    h = sim.handle
+
+    def frame():
+        check(h, L.lbm_pack_volume_device(h, C.c_void_p(vol.data_ptr())))
+        rc = L.lbm_render_volume(C.c_void_p(vol.data_ptr()), sim.nx, sim.ny, sim.nz, sph, C.byref(cam), W, H,
+                                 C.c_void_p(img.data_ptr()), L.lbm_stream(h))
+        assert rc == 0
+
+    for _ in range(3):
+        frame()
+    K = args.steps if args.steps != 2000 else 50
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        frame()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / K
+    from oracle import oracle
+    host = sim.packVolume().copy()
+    t0 = time.perf_counter()
+    oracle.render(host, sim.nx, sim.ny, sim.nz, (sol.cx, sol.cy, sol.cz, sol.r), width=W, height=H)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    sim.close()
+    line = {
+        "metric": f"rendered frames/s, {W}x{H}, {size}^3 RG8 volume (pack + raymarch)", "value": 1e3 / ms,
+        "unit": "frames/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "f32",
+        "ms_per_frame": ms, "steps": K,
+        "config": {"workload": f"gravity-down pool {size}^3, reference start view, 48 march steps",
+                   "width": W, "height": H},
+        "cpu_baseline": {"value": 1e3 / cpu_ms, "unit": "frames/s", "cores": 1, "kind": "port",
+                         "sample": "one frame of oracle/render_oracle.c (the shader restated in C)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
@@ -376,9 +436,9 @@ def main():
         run_reference(args, ws, rank)
         return
     if args.workload != "scene":
-        if args.workload == "precision":
+        if args.workload in ("precision", "render"):
             if rank == 0:
-                run_precision(args, local)
+                {"precision": run_precision, "render": run_render}[args.workload](args, local)
         else:
             {"batch": run_batch, "serve": run_serve}[args.workload](args, local, ws, rank)
         if ws > 1:

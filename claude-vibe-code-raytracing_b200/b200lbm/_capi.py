@@ -52,6 +52,11 @@ class LbmImpulse(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("Fx", "Fy", "Fz", "Tx", "Ty", "Tz")]
 
 
+class LbmCamera(C.Structure):
+    _fields_ = [("azimuth", C.c_double), ("elev", C.c_double), ("dist", C.c_double),
+                ("light", C.c_double * 3)]
+
+
 class LbmError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"lbm error {code}: {msg}")
@@ -112,6 +117,12 @@ _SIGS = [
     ("lbm_batch_time_fused", C.c_int,
      [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     ("lbm_batch_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    ("lbm_camera_default", None, [C.POINTER(LbmCamera)]),
+    ("lbm_render_volume", C.c_int,
+     [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(LbmSphere), C.POINTER(LbmCamera), C.c_int, C.c_int,
+      C.c_void_p, C.c_void_p]),
+    ("lbm_render", C.c_int,
+     [C.c_void_p, C.POINTER(LbmSphere), C.POINTER(LbmCamera), C.c_int, C.c_int, C.c_void_p]),
     ("lbm_absorb_dead_cells_noalloc", C.c_int,
      [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double] + [C.c_void_p] * 6
      + [C.POINTER(LbmSphere), C.c_int, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),

@@ -270,6 +270,24 @@ class Sim:
         for i, b in enumerate(sp):
             b.add_impulse(out[i])
 
+    def render(self, solid=None, width=640, height=480, camera=None):
+        """Renderer.uploadVolume + draw (src/render.js:431-434, 484-513) without
+        a canvas: the current state rendered by the reference's fragment shader
+        on the GPU.  Returns an RGBA8 image, shape (height, width, 4), top row
+        first.  camera: an LbmCamera (default: the reference's start view)."""
+        from ._capi import LbmCamera
+        cam = camera
+        if cam is None:
+            cam = LbmCamera()
+            lib().lbm_camera_default(C.byref(cam))
+        sp = spheres_of(solid)
+        self._sync()
+        arr = to_c_array(sp[:1])
+        img = np.empty((height, width, 4), dtype=np.uint8)
+        check(self._h, lib().lbm_render(self._h, arr if sp else None, C.byref(cam), width, height,
+                                        img.ctypes.data_as(C.c_void_p)))
+        return img
+
     def run_coupled(self, solid, nsteps, frame_every=0):
         """nsteps worker ticks (src/worker.js:96-100: sim.step(solid);
         solid.absorbDeadCells(sim); solid.step(1.0, sim.gravity)) entirely on

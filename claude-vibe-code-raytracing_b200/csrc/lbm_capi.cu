@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "lbm_kernels.cuh"
+#include "lbm_render.h"
 #include "lbm_state.h"
 
 using namespace lbm;
@@ -380,6 +381,7 @@ int get_scalar64(lbm_sim *h, const void *src, double *host) {
 }
 
 void free_all(lbm_sim *h) {
+  if (h->image) cudaFree(h->image);
   void *ptrs[] = {h->F[0], h->F[1], h->H[0], h->H[1], h->tag, h->tagPrev, h->grad[0], h->grad[1],
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
                   h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
@@ -1027,6 +1029,36 @@ int lbm_pack_volume(lbm_sim *h, uint8_t *host_out) {
   h->ops->pack(h, (uint8_t *)h->staging);
   CKL("packVolume");
   CK(copy_async(h, host_out, h->staging, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+int lbm_render(lbm_sim *h, const lbm_sphere *sphere, const lbm_camera *cam, int width, int height,
+               uint8_t *host_out) {
+  if (!h || !cam || !host_out || width < 1 || height < 1 || (long long)width * height > (1LL << 28))
+    return fail(h, LBM_ERR_ARG, "bad render arguments");
+  DeviceGuard g(h->device);
+  int rc = ensure_staging(h, (size_t)h->n * 2);
+  if (rc) return rc;
+  const size_t bytes = (size_t)width * height * 4;
+  if (bytes > h->imageBytes) {
+    if (h->image) {
+      cudaFree(h->image);
+      h->deviceBytes -= h->imageBytes;
+      h->image = nullptr;
+      h->imageBytes = 0;
+    }
+    DALLOC(h->image, bytes);
+    h->imageBytes = bytes;
+  }
+  h->ops->pack(h, (uint8_t *)h->staging);
+  CKL("packVolume");
+  RenderSetup r;
+  render_frame_setup(h->nx, h->ny, h->nz, sphere, cam, width, height, &r);
+  CK(render_launch((const uint8_t *)h->staging, h->nx, h->ny, h->nz, r, width, height, (uint8_t *)h->image,
+                   h->stream));
+  h->launches++;
+  CK(copy_async(h, host_out, h->image, bytes, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return LBM_OK;
 }

@@ -114,6 +114,8 @@ struct lbm_sim {
   lbm::Plan *dPlan = nullptr;  // device step plan read by the kernels
   void *staging = nullptr;
   size_t stagingBytes = 0;
+  void *image = nullptr;  // rendered RGBA8 frame (lbm_render)
+  size_t imageBytes = 0;
   double *dPhiCol = nullptr;
   int *hTotals = nullptr;  // pinned
 

@@ -222,6 +222,31 @@ int lbm_batch_time_fused(lbm_batch *batch, int rows, int zchunk, int reps, doubl
 /* Batched fused launches executed so far. */
 int lbm_batch_launch_count(const lbm_batch *batch, int64_t *count);
 
+/* ---- headless render of the RG8 volume -------------------------------------- */
+/* Orbit camera of the reference's Renderer (src/render.js:405-412, 452-458):
+ * azimuth and elevation in radians, distance in units of the largest grid
+ * edge, light direction (normalised here).  lbm_camera_default fills the
+ * reference's start view: azimuth pi/4, elevation -0.25, distance 2.4,
+ * light (0.35, 0.75, 0.5). */
+typedef struct {
+  double azimuth, elev, dist;
+  double light[3];
+} lbm_camera;
+void lbm_camera_default(lbm_camera *cam);
+/* The reference's fragment shader (src/render.js:19-268: ray march of the
+ * phi = 0.5 surface with refraction, reflection, Beer-Lambert tint, sphere
+ * and sky shading, tonemap) over an RG8 volume in device memory (the
+ * packVolume layout, 2*nx*ny*nz bytes), one thread per pixel, into
+ * width*height RGBA8 pixels in device memory, top row first.  sphere may be
+ * NULL.  Asynchronous on `stream` (a cudaStream_t). */
+int lbm_render_volume(const uint8_t *d_vol, int nx, int ny, int nz, const lbm_sphere *sphere,
+                      const lbm_camera *cam, int width, int height, uint8_t *d_out, void *stream);
+/* Renderer.uploadVolume + draw (src/render.js:431-434, 484-513) for a handle:
+ * packs its current state and renders it; the image (width*height*4 bytes,
+ * top row first) goes to host memory. */
+int lbm_render(lbm_sim *sim, const lbm_sphere *sphere, const lbm_camera *cam, int width, int height,
+               uint8_t *host_out);
+
 /* ---- allocation-free dead-cell sweep --------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory at the point of the call (an engine that owns all device memory

@@ -20,6 +20,7 @@ this module.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -92,6 +93,9 @@ def lib(store="f32"):
         L.or_store_bytes.restype = C.c_int
         assert L.or_store_bytes() == (8 if store == "f64" else 4)
         L.or_sim_create.restype = SP
+        L.or_render.restype = None
+        L.or_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                C.POINTER(C.c_double), C.c_int, C.c_int, C.c_void_p]
         L.or_sim_create.argtypes = [C.c_int, C.c_int, C.c_int]
         L.or_sim_destroy.argtypes = [SP]
         L.or_sim_set_omp.argtypes = [SP, C.c_int]
@@ -309,3 +313,20 @@ class OracleSim:
     def worker_substep(self, solid):
         """sim.step(solid); solid.absorbDeadCells(sim); solid.step(1.0, g) (src/worker.js:96-100)."""
         self._L.or_worker_substep(self._p, *_solid_args(solid))
+
+
+def render(volume, nx, ny, nz, sphere=None, camera=(math.pi * 0.25, -0.25, 2.4, 0.35, 0.75, 0.5),
+           width=640, height=480):
+    """The reference's renderer (src/render.js) restated in C: RGBA8 image of
+    the RG8 `volume` (2*nx*ny*nz bytes), shape (height, width, 4), top row
+    first.  sphere: (cx, cy, cz, r) in cells or None; camera: azimuth,
+    elevation, distance, light direction."""
+    L = lib()
+    vol = np.ascontiguousarray(np.asarray(volume, dtype=np.uint8))
+    assert vol.size == 2 * nx * ny * nz
+    out = np.empty((height, width, 4), dtype=np.uint8)
+    sp = (C.c_double * 4)(*sphere) if sphere is not None else None
+    cam = (C.c_double * 6)(*camera)
+    L.or_render(vol.ctypes.data_as(C.c_void_p), nx, ny, nz, sp, cam, width, height,
+                out.ctypes.data_as(C.c_void_p))
+    return out

@@ -30,7 +30,23 @@ PLAN = {
     "profile": (40, (1, 40), True, False),
     "cfg1": (80, (1, 80), False, True),
     "drop": (60, (60,), False, True),
+    "dam": (120, (120,), False, True),
+    "rise": (120, (120,), False, True),
+    "drag": (220, (220,), False, True),
 }
+
+# test/drag_stress.mjs's path with shorter legs (the same targets), so the
+# translated reference finishes in minutes
+SHORT_DRAG_PATH = [(40, (20, 24, 20)), (40, (30, 24, 20)), (60, (30, 4, 20)), (30, (20, 4, 20)),
+                   (50, (20, 18, 20))]
+
+
+def _drag_prestep(s, sim, sol):
+    scenes.drag_target(sol, s - 1, SHORT_DRAG_PATH)
+
+
+# called before step s (1-based) of a scene
+PRESTEP = {"drag": _drag_prestep}
 
 
 def digest(arr):
@@ -63,7 +79,10 @@ def run_scene(name, SimC, SphC, built=_noop, on_step=None):
     built(sim)
     rec = {"fields": {}, "sphere": [], "impulse_stream": [], "impulse_dead": [],
            "fresh": [], "dead": []}
+    pre = PRESTEP.get(name)
     for s in range(1, steps + 1):
+        if pre is not None:
+            pre(s, sim, sol)
         if on_step is not None:
             on_step(s, sim, sol)
         sim.step(sol)

@@ -88,6 +88,47 @@ def dam(SimC, SphC):
     return sim, solid
 
 
+def rise(SimC, SphC):
+    """src/worker.js:81-90 'rise' preset: a buoyant ball (density 0.5) below the surface."""
+    NX, NY, NZ = 40, 28, 40
+    sim = SimC(NX, NY, NZ)
+    _params(sim, 0.85, 0.7, 0.008, 0.0015)
+    solid = SphC(NX, NY, NZ, cx=NX * 0.5, cy=NY * 0.20, cz=NZ * 0.5, r=4.0, density=1.6)
+    sim.initFlat(NY * 0.25)
+    solid.cx, solid.cy, solid.cz = NX * 0.5, NY * 0.65, NZ * 0.5
+    solid.setRadius(4.0)
+    solid.setDensity(0.5)
+    return sim, solid
+
+
+def drag(SimC, SphC):
+    """test/drag_stress.mjs:6-18: a density-1.4 sphere dragged by its spring
+    (RigidSphere.step, src/solid.js:118-131) along DRAG_PATH."""
+    NX, NY, NZ = 40, 28, 40
+    sim = SimC(NX, NY, NZ)
+    _params(sim, 0.8, 0.7, 0.008, 0.0015)
+    sim.initFlat(NY * 0.25)
+    solid = SphC(NX, NY, NZ, cx=NX * 0.5, cy=NY * 0.65, cz=NZ * 0.5, r=4, density=1.4)
+    solid.dragging = True
+    return sim, solid
+
+
+# (steps, target) legs of test/drag_stress.mjs:20-26: to the floor, along it,
+# up through the interface, along the top, back down through the interface
+DRAG_PATH = [(100, (20, 24, 20)), (100, (30, 24, 20)), (200, (30, 4, 20)), (100, (20, 4, 20)),
+             (200, (20, 18, 20))]
+
+
+def drag_target(solid, step, path=DRAG_PATH):
+    """Set the drag target for (0-based) step `step` of the path."""
+    for n, t in path:
+        if step < n:
+            solid.dragTargetX, solid.dragTargetY, solid.dragTargetZ = t
+            return
+        step -= n
+    solid.dragTargetX, solid.dragTargetY, solid.dragTargetZ = path[-1][1]
+
+
 def mirrored_pool(sim, level, W):
     """Liquid below y = level (phi = 1/2 (1 + tanh(2 (level - y)/W))) on every
     cell, h = w7 * phi, then seedHydrostatic -- the dam-preset pattern
@@ -147,7 +188,7 @@ def cfg2(SimC, SphC, n=256, seed=0):
 
 
 SCENES = {"smoke": smoke, "profile": profile, "bench": bench, "drop": drop, "dam": dam,
-          "cfg1": cfg1}
+          "cfg1": cfg1, "rise": rise, "drag": drag}
 
 
 def substep(sim, solid):

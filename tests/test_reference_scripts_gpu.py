@@ -1,0 +1,102 @@
+"""The reference's own test scripts, run at full length on the CUDA path beside
+the oracle: test/drag_stress.mjs (a sphere dragged along a 700-step path,
+through the interface and back), test/repro_presets.mjs (drop, dam and rise
+presets, 120 steps each) and test/settle.mjs (drop and rise, 1500 steps).
+
+Besides the scripts' own checks (finite state, max|u| <= 1), every run is
+compared with the oracle:
+  * drag: the GPU sphere takes the oracle's state at the start of every step,
+    so the solid mask and the fresh / dead sets must match exactly at all 700
+    steps (the sphere crosses the interface twice at up to ~0.08 cells/step);
+  * presets and settle run free; the sphere trajectory and the fields must
+    stay within the bars below (FP32 evaluation against the reference's
+    double arithmetic with float32 stores).
+"""
+import numpy as np
+import pytest
+
+import scenes
+from scenes import field_err, substep
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import b200lbm
+    return b200lbm
+
+
+def _max_u(sim):
+    ux, uy, uz = (np.asarray(getattr(sim, k), dtype=np.float64) for k in ("ux", "uy", "uz"))
+    return float(np.sqrt(ux * ux + uy * uy + uz * uz).max())
+
+
+def _finite(sim):
+    return all(np.isfinite(np.asarray(getattr(sim, k))).all() for k in ("phi", "rho", "ux", "uy", "uz"))
+
+
+def _sets(sim):
+    tag, prev = np.array(sim.tag), np.array(sim.tagPrev)
+    return np.nonzero((tag == 0) & (prev == 1))[0], np.nonzero((tag == 1) & (prev == 0))[0]
+
+
+def test_drag_stress(gpu, oracle_mod):
+    o, osol = scenes.drag(oracle_mod.OracleSim, oracle_mod.OracleSphere)
+    g, gsol = scenes.drag(gpu.Sim, gpu.RigidSphere)
+    total = sum(n for n, _ in scenes.DRAG_PATH)
+    n_fresh = n_dead = 0
+    for s in range(total):
+        for sol in (osol, gsol):
+            scenes.drag_target(sol, s)
+        for k in ("cx", "cy", "cz", "vx", "vy", "vz", "wx", "wy", "wz"):
+            setattr(gsol, k, getattr(osol, k))
+        o.step(osol)
+        g.step(gsol)
+        ofr, ode = _sets(o)
+        gfr, gde = _sets(g)
+        assert np.array_equal(gfr, ofr) and np.array_equal(gde, ode), f"sets differ at step {s}"
+        n_fresh += len(ofr)
+        n_dead += len(ode)
+        for sim, sol in ((o, osol), (g, gsol)):
+            sol.absorbDeadCells(sim)
+            sol.step(1.0, sim.gravity)
+        if s % 50 == 49:
+            assert _finite(g) and _max_u(g) <= 1.0, s
+    assert n_fresh > 100 and n_dead > 100
+    assert _finite(g) and _max_u(g) <= 1.0
+    rel, _ = field_err(g.phi, o.phi)
+    assert rel <= 2e-3, rel
+
+
+@pytest.mark.parametrize("preset", ["drop", "dam", "rise"])
+def test_repro_presets(gpu, oracle_mod, preset):
+    build = getattr(scenes, preset)
+    o, osol = build(oracle_mod.OracleSim, oracle_mod.OracleSphere)
+    g, gsol = build(gpu.Sim, gpu.RigidSphere)
+    for s in range(120):
+        substep(o, osol)
+        substep(g, gsol)
+    assert _finite(g) and _max_u(g) <= 1.0
+    drift = max(abs(getattr(gsol, k) - getattr(osol, k)) for k in ("cx", "cy", "cz"))
+    assert drift <= 1e-3, drift
+    rel, _ = field_err(g.phi, o.phi)
+    assert rel <= 2e-3, rel
+
+
+@pytest.mark.parametrize("preset", ["drop", "rise"])
+def test_settle(gpu, oracle_mod, preset):
+    """test/settle.mjs: 1500 steps; the sphere comes to rest at the same place."""
+    build = getattr(scenes, preset)
+    o, osol = build(oracle_mod.OracleSim, oracle_mod.OracleSphere)
+    g, gsol = build(gpu.Sim, gpu.RigidSphere)
+    for s in range(1500):
+        substep(o, osol)
+    g.run_coupled(gsol, 1500)
+    assert _finite(g) and _max_u(g) <= 1.0
+    assert abs(gsol.cy - osol.cy) <= 0.05, (gsol.cy, osol.cy)
+    assert max(abs(gsol.cx - osol.cx), abs(gsol.cz - osol.cz)) <= 0.05
+    rel, _ = field_err(g.phi, o.phi)
+    assert rel <= 1e-2, rel
