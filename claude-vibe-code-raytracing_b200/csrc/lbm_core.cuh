@@ -78,6 +78,22 @@ __device__ __forceinline__ void static_for(F &&f) {
   }
 }
 
+// ---------------------------------------------------------------- explicit rounding
+// Arithmetic that must give the same bits wherever it is inlined (the fused
+// collision runs for tile cells and for halo cells of neighbouring tiles):
+// each operation rounds once and the compiler may not contract or reorder it.
+// FP32: mul / add / sub round to nearest, rfma is one fused multiply-add.
+// FP64: rfma is a multiply then an add (the FP64 form follows the reference's
+// unfused double arithmetic).
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __dadd_rn(__dmul_rn(a, b), c); }
+
 // ---------------------------------------------------------------- storage codecs
 // FP32/FP64 store raw populations.  FP16/BF16 store the offset from a
 // reference value: w_k for f, w_k * phi(cell) for h, so the stored numbers are
@@ -100,17 +116,17 @@ struct Codec<double> {
 template <>
 struct Codec<__half> {
   static constexpr bool offset = true;
-  __device__ __forceinline__ static float dec(__half v, float ref) { return __half2float(v) + ref; }
-  __device__ __forceinline__ static __half enc(float v, float ref) { return __float2half_rn(v - ref); }
+  __device__ __forceinline__ static float dec(__half v, float ref) { return __fadd_rn(__half2float(v), ref); }
+  __device__ __forceinline__ static __half enc(float v, float ref) { return __float2half_rn(__fsub_rn(v, ref)); }
 };
 template <>
 struct Codec<__nv_bfloat16> {
   static constexpr bool offset = true;
   __device__ __forceinline__ static float dec(__nv_bfloat16 v, float ref) {
-    return __bfloat162float(v) + ref;
+    return __fadd_rn(__bfloat162float(v), ref);
   }
   __device__ __forceinline__ static __nv_bfloat16 enc(float v, float ref) {
-    return __float2bfloat16_rn(v - ref);
+    return __float2bfloat16_rn(__fsub_rn(v, ref));
   }
 };
 

@@ -63,20 +63,94 @@ constexpr int RING_F_M = 0, RING_F_Z = 18, RING_F_P = 36;  // 2x9, 2x9, 3x9
 constexpr int RING_H_M = 63, RING_H_Z = 65, RING_H_P = 75;  // 2x1, 2x5, 3x1
 constexpr int RING_PLANES = 78;
 
+// Shared memory of one CTA: the post-collision ring, the tags of three planes
+// and, in the STAGE forms, NBUF staging buffers that receive the tile rows' raw
+// populations of a plane by bulk asynchronous copy, plus one mbarrier per
+// buffer and an abort flag.  A 32-cell row starts anywhere inside an 8-cell
+// block, so it spans at most SB = 5 whole blocks.
+#ifndef LBM_STAGE_NBUF
+#define LBM_STAGE_NBUF 1
+#endif
 template <class PopT, int TY>
 struct FusedSmem {
   using Real = typename Prec<PopT>::Real;
   static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;
-  static constexpr size_t bytes = (size_t)RING_PLANES * NC * sizeof(Real) + 3 * NC;
+  static constexpr bool STAGE = TY == 4 && sizeof(PopT) == 2;
+  static constexpr int NBUF = LBM_STAGE_NBUF;
+  static constexpr int SB = 5;
+  static constexpr int ROWF = SB * 8 * Q27, ROWH = SB * 8 * Q7;  // elements per staged row
+  static constexpr size_t ringBytes = (size_t)RING_PLANES * NC * sizeof(Real);
+  static constexpr size_t stageOff = (ringBytes + 3 * NC + 15) / 16 * 16;
+  static constexpr size_t bufBytes = STAGE ? (size_t)TY * (ROWF + ROWH) * sizeof(PopT) : 0;
+  static constexpr size_t barOff = stageOff + NBUF * bufBytes;
+  static constexpr size_t bytes = STAGE ? barOff + 32 : ringBytes + 3 * NC;
   static constexpr int warps = TY + 2;  // TY cell warps, 2 halo warps
   static constexpr int threads = 32 * warps;
+  static_assert((ROWF * sizeof(PopT)) % 16 == 0 && (ROWH * sizeof(PopT)) % 16 == 0,
+                "bulk copies move whole 16-byte units");
 };
 
-// CTAs per SM the register budget is sized for
-template <int TY>
+// CTAs per SM the register budget is sized for (the staged forms are held to
+// 2 (TY = 4) or 3 (TY = 2) CTAs per SM by shared memory)
+template <class PopT, int TY>
 struct FusedOcc {
-  static constexpr int blocks = TY >= 8 ? 2 : (TY >= 4 ? 3 : 5);
+  static constexpr int blocks = FusedSmem<PopT, TY>::STAGE && FusedSmem<PopT, TY>::NBUF == 2
+                                   ? 2
+                                   : (TY >= 8 ? 2 : (TY >= 4 ? 3 : 5));
 };
+
+// ---------------------------------------------------------------- bulk copies
+// cp.async.bulk global -> shared with an mbarrier counting the bytes.  Every
+// wait is bounded (LBM_STAGE_WAIT_NS of %globaltimer); a wait that runs out
+// returns false and the caller records the fault and stops the tile.
+#ifndef LBM_STAGE_WAIT_NS
+#define LBM_STAGE_WAIT_NS 500000000ull
+#endif
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_inval(uint32_t bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try(bar, parity)) return true;
+    if (global_ns() - t0 > LBM_STAGE_WAIT_NS) return false;
+  }
+}
 
 // Directions a halo cell must collide: those pointing into the tile.
 // SX / SY = +-1 select e_x / e_y equal to that value, 0 means any.
@@ -113,6 +187,17 @@ __device__ __forceinline__ bool lbm_ok(bool ok, int code, long long idx) {
 #endif
 }
 
+// Location code recorded when a bounded wait for a staged plane runs out.
+constexpr int FAULT_STAGE_WAIT = 90;
+__device__ __forceinline__ void record_stage_timeout(int q) {
+  if (atomicCAS(&lbm_fault_word[0], 0ull, (unsigned long long)FAULT_STAGE_WAIT) == 0ull) {
+    lbm_fault_word[1] = (unsigned long long)q;
+    lbm_fault_word[2] = blockIdx.x | ((unsigned long long)blockIdx.y << 20) |
+                        ((unsigned long long)blockIdx.z << 40);
+    lbm_fault_word[3] = threadIdx.x | (threadIdx.y << 8);
+  }
+}
+
 template <class T>
 __device__ __forceinline__ T ldg_at(const T *p, long long idx, long long lim, int code) {
   if (!lbm_ok(idx >= 0 && idx < lim, code, idx)) return T();
@@ -146,7 +231,14 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   constexpr int RX = SM::RX, NC = SM::NC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real *ring = reinterpret_cast<Real *>(smem_raw);                        // [78][NC]
-  uint8_t *stag = smem_raw + (size_t)RING_PLANES * NC * sizeof(Real);    // [3][NC]
+  uint8_t *stag = smem_raw + SM::ringBytes;                               // [3][NC]
+  constexpr bool STAGE = SM::STAGE;
+  constexpr int ROWF = SM::ROWF, ROWH = SM::ROWH, BUF = TY * (ROWF + ROWH), NBUF = SM::NBUF;
+  // with two buffers the halo warps' loads are prefetched into registers too
+  constexpr bool HALO_PF = NBUF == 2;
+  PopT *stage = reinterpret_cast<PopT *>(smem_raw + SM::stageOff);        // [2][TY rows F, TY rows H]
+  int *abortF = reinterpret_cast<int *>(smem_raw + SM::barOff + 16);
+  const uint32_t bar0 = smem_u32(smem_raw + SM::barOff);  // mbarrier of buffer b at bar0 + 8b
 
   const auto &s = a.s;
   const SolidSet &ss = *a.ss;
@@ -206,21 +298,10 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
 
   // Load phase: every load comes from a valid, clamped address and none waits
   // on the tag, so a pass costs one memory latency.
-  auto load = [&](auto MODEc, auto SXc, auto SYc, int sx, int sy, bool active, int q, int gx_, int gy_,
-                  LD &L) __attribute__((always_inline)) {
-    constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
+  // The phi stencil, rho, u and tag of cell (gx_, gy_, q).
+  auto load_small = [&](int q, int gx_, int gy_, LD &L) __attribute__((always_inline)) {
     const bool inside = gx_ >= 0 && gx_ < nx && gy_ >= 0 && gy_ < ny && q >= 0 && q < nz;
     const int ci = inside ? q * nxny + gy_ * nx + gx_ : 0;
-    const int bF = (ci >> 3) * (8 * Q27) + (ci & 7);
-    const int bH = (ci >> 3) * (8 * Q7) + (ci & 7);
-    static_for<0, Q27>([&](auto KK) {
-      constexpr int k = decltype(KK)::value;
-      if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
-        const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
-        L.fv[k] = nd ? ldg_at(Fc, bF + 8 * k, nF, 3) : PopT();
-        if constexpr (k < Q7) L.hv[k] = nd ? ldg_at(Hc, bH + 8 * k, nH, 4) : PopT();
-      }
-    });
     uint8_t tg = ldg_at(tagA, ci, nCell, 1);
     const int last = (int)nCell - 1;
     L.p = ldg_at(phiC, ci, nCell, 5);
@@ -239,6 +320,77 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     if (!inside || (!inner && tg == TAG_FLUID)) tg = TAG_WALL;
     L.tg = tg;
   };
+  auto load = [&](auto MODEc, auto SXc, auto SYc, int sx, int sy, bool active, int q, int gx_, int gy_,
+                  LD &L) __attribute__((always_inline)) {
+    constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
+    const bool inside = gx_ >= 0 && gx_ < nx && gy_ >= 0 && gy_ < ny && q >= 0 && q < nz;
+    const int ci = inside ? q * nxny + gy_ * nx + gx_ : 0;
+    const int bF = (ci >> 3) * (8 * Q27) + (ci & 7);
+    const int bH = (ci >> 3) * (8 * Q7) + (ci & 7);
+    static_for<0, Q27>([&](auto KK) {
+      constexpr int k = decltype(KK)::value;
+      if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
+        const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
+        L.fv[k] = nd ? ldg_at(Fc, bF + 8 * k, nF, 3) : PopT();
+        if constexpr (k < Q7) L.hv[k] = nd ? ldg_at(Hc, bH + 8 * k, nH, 4) : PopT();
+      }
+    });
+    load_small(q, gx_, gy_, L);
+  };
+
+  // ---- staging of the tile rows' populations (STAGE forms)
+  // Row r of plane q covers cells row0 .. row0 + min(31, nx - 1 - x0) of the
+  // flat order, i.e. whole blocks (row0 >> 3) .. (last >> 3): one bulk copy
+  // for f and one for h, into buffer q & 1.  Rows past the grid are skipped.
+  const bool producer = STAGE && ty == TY + 1 && tx == 31;  // an idle lane of halo warp B
+  auto issue = [&](int q) __attribute__((always_inline)) {
+    const int buf = q % NBUF;
+    const uint32_t bar = bar0 + 8 * buf;
+    const int span = min(31, nx - 1 - x0);
+    uint32_t total = 0;
+    for (int r = 0; r < TY; r++) {
+      if (y0 + r >= ny) break;
+      const int row0 = (q * ny + y0 + r) * nx + x0;
+      total += (uint32_t)(((row0 + span) >> 3) - (row0 >> 3) + 1) * 8 * (Q27 + Q7) * sizeof(PopT);
+    }
+    mbar_expect(bar, total);
+    for (int r = 0; r < TY; r++) {
+      if (y0 + r >= ny) break;
+      const int row0 = (q * ny + y0 + r) * nx + x0;
+      const int b0 = row0 >> 3, nb = ((row0 + span) >> 3) - b0 + 1;
+      const bool ok = lbm_ok(nb <= SM::SB, 20, nb) &&
+                      lbm_ok((long long)(b0 + nb) * 8 * Q27 <= nF, 21, b0);
+      if (!ok) continue;
+      bulk_g2s(smem_u32(stage + buf * BUF + r * ROWF), Fc + (long long)b0 * 8 * Q27,
+               (uint32_t)(nb * 8 * Q27 * sizeof(PopT)), bar);
+      bulk_g2s(smem_u32(stage + buf * BUF + TY * ROWF + r * ROWH), Hc + (long long)b0 * 8 * Q7,
+               (uint32_t)(nb * 8 * Q7 * sizeof(PopT)), bar);
+    }
+  };
+  uint32_t phase = 0;  // parity of the next wait, one bit per buffer
+  auto stage_wait = [&](int q) __attribute__((always_inline)) {
+    const int buf = q % NBUF;
+    const uint32_t par = (phase >> buf) & 1u;
+    phase ^= 1u << buf;
+    if (!haloWarp && !mbar_wait(bar0 + 8 * buf, par)) {
+      record_stage_timeout(q);
+      *abortF = 1;
+    }
+  };
+  // a cell thread's populations of plane q from the staging buffer
+  auto stage_pops = [&](int q, LD &L) __attribute__((always_inline)) {
+    const PopT *sF = stage + (q % NBUF) * BUF + ty * ROWF;
+    const PopT *sH = stage + (q % NBUF) * BUF + TY * ROWF + ty * ROWH;
+    const int row0 = (q * ny + y) * nx + x0;
+    const bool inside = x < nx && y < ny;
+    const int off = inside ? ((row0 + tx) >> 3) - (row0 >> 3) : 0;
+    const int e = inside ? ((row0 + tx) & 7) : 0;
+    static_for<0, Q27>([&](auto KK) {
+      constexpr int k = decltype(KK)::value;
+      L.fv[k] = sF[sm_at((off * Q27 + k) * 8 + e, ROWF, 22)];
+      if constexpr (k < Q7) L.hv[k] = sH[sm_at((off * Q7 + k) * 8 + e, ROWH, 23)];
+    });
+  };
 
   // Compute phase: collision into ring cell lc of plane q and the cell's tag.
   // Values computed for non-fluid cells land in ring slots that are never
@@ -252,50 +404,60 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     const int hbM = (RING_H_M + (q & 1)) * NC + lc, hbZ = (RING_H_Z + (q & 1) * 5) * NC + lc;
     const int hbP = (RING_H_P + (q % 3)) * NC + lc;
     if (MODE != 2 || active) stag[sm_at((q % 3) * NC + lc, TAGS, 2)] = L.tg;
+    // Every operation below rounds explicitly (rmul / radd / rsub / rfma), so a
+    // tile cell and a halo cell of another tile get the same bits whatever the
+    // compiler would contract in either context.
     const Real p = L.p, ux = L.ux, uy = L.uy, uz = L.uz;
-    const Real gxv = (Real)0.5 * (L.pxp - L.pxm);
-    const Real gyv = (Real)0.5 * (L.pyp - L.pym);
-    const Real gzv = (Real)0.5 * (L.pzp - L.pzm);
-    const Real lap = L.pxp + L.pxm + L.pyp + L.pym + L.pzp + L.pzm - (Real)6 * p;
-    const Real rhoPh = rhoG + p * dRho;
-    const Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lap;
-    const Real Fx = mu * gxv, Fy = mu * gyv + rhoPh * grav, Fz = mu * gzv;
-    const Real u2 = ux * ux + uy * uy + uz * uz;
-    const Real uF = ux * Fx + uy * Fy + uz * Fz;
-    const Real orh = om * rhoPh;
-    const Real C0 = om * L.sumF - (Real)1.5 * orh * u2 - A * uF;
-    const Real orh3 = (Real)3 * orh;
-    const Real Vx = orh3 * ux + A * Fx, Vy = orh3 * uy + A * Fy, Vz = orh3 * uz + A * Fz;
-    const Real A3 = (Real)3 * A, orh45 = (Real)4.5 * orh;
-    const Real Qx = orh45 * ux + A3 * Fx, Qy = orh45 * uy + A3 * Fy, Qz = orh45 * uz + A3 * Fz;
-    const Real gmag = sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + (Real)1e-12;
-    const Real sh = sharpC4 * p * ((Real)1 - p) / gmag;
-    const Real fp = (Real)4 * omP * p;
-    const Real D0 = omP * p;
-    const Real Dx = fp * ux + sh * gxv, Dy = fp * uy + sh * gyv, Dz = fp * uz + sh * gzv;
-    const Real om1 = (Real)1 - om, omP1 = (Real)1 - omP;
+    const Real half = (Real)0.5, one = (Real)1, two = (Real)2;
+    const Real gxv = rmul(half, rsub(L.pxp, L.pxm));
+    const Real gyv = rmul(half, rsub(L.pyp, L.pym));
+    const Real gzv = rmul(half, rsub(L.pzp, L.pzm));
+    const Real lap = rfma((Real)-6, p, radd(radd(radd(radd(radd(L.pxp, L.pxm), L.pyp), L.pym), L.pzp), L.pzm));
+    const Real rhoPh = rfma(p, dRho, rhoG);
+    const Real mu = rfma(-kappa, lap, rmul(rmul(rmul(beta4, p), rsub(p, one)), rfma(two, p, -one)));
+    const Real Fx = rmul(mu, gxv), Fy = rfma(mu, gyv, rmul(rhoPh, grav)), Fz = rmul(mu, gzv);
+    const Real u2 = rfma(uz, uz, rfma(uy, uy, rmul(ux, ux)));
+    const Real uF = rfma(uz, Fz, rfma(uy, Fy, rmul(ux, Fx)));
+    const Real orh = rmul(om, rhoPh);
+    const Real C0 = rfma(-A, uF, rfma(rmul((Real)-1.5, orh), u2, rmul(om, L.sumF)));
+    const Real orh3 = rmul((Real)3, orh);
+    const Real Vx = rfma(A, Fx, rmul(orh3, ux)), Vy = rfma(A, Fy, rmul(orh3, uy)), Vz = rfma(A, Fz, rmul(orh3, uz));
+    const Real A3 = rmul((Real)3, A), orh45 = rmul((Real)4.5, orh);
+    const Real Qx = rfma(A3, Fx, rmul(orh45, ux)), Qy = rfma(A3, Fy, rmul(orh45, uy)),
+               Qz = rfma(A3, Fz, rmul(orh45, uz));
+    const Real gmag = radd(sqrt(rfma(gzv, gzv, rfma(gyv, gyv, rmul(gxv, gxv)))), (Real)1e-12);
+    const Real sh = rmul(rmul(sharpC4, p), rsub(one, p)) / gmag;
+    const Real D0 = rmul(omP, p);
+    const Real fp = rmul((Real)4, D0);
+    const Real Dx = rfma(sh, gxv, rmul(fp, ux)), Dy = rfma(sh, gyv, rmul(fp, uy)), Dz = rfma(sh, gzv, rmul(fp, uz));
+    const Real om1 = rsub(one, om), omP1 = rsub(one, omP);
+    // e.X for a lattice direction (components -1, 0, 1): signed sums, the
+    // first term taken exactly
+    auto edot = [](auto EX, auto EY, auto EZ, Real X, Real Y, Real Z) __attribute__((always_inline)) {
+      constexpr int ex = decltype(EX)::value, ey = decltype(EY)::value, ez = decltype(EZ)::value;
+      Real r = 0;
+      bool first = true;
+      if constexpr (ex != 0) {
+        r = ex > 0 ? X : -X;
+        first = false;
+      }
+      if constexpr (ey != 0) {
+        r = first ? (ey > 0 ? Y : -Y) : (ey > 0 ? radd(r, Y) : rsub(r, Y));
+        first = false;
+      }
+      if constexpr (ez != 0) r = first ? (ez > 0 ? Z : -Z) : (ez > 0 ? radd(r, Z) : rsub(r, Z));
+      return r;
+    };
     static_for<0, Q27>([&](auto KK) {
       constexpr int k = decltype(KK)::value;
       using D = D27<k>;
       constexpr int ex = D::ex, ey = D::ey, ez = D::ez;
       if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
         const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
-        Real ev = 0, eu = 0, eq = 0;
-        if constexpr (ex != 0) {
-          ev += (Real)ex * Vx;
-          eu += (Real)ex * ux;
-          eq += (Real)ex * Qx;
-        }
-        if constexpr (ey != 0) {
-          ev += (Real)ey * Vy;
-          eu += (Real)ey * uy;
-          eq += (Real)ey * Qy;
-        }
-        if constexpr (ez != 0) {
-          ev += (Real)ez * Vz;
-          eu += (Real)ez * uz;
-          eq += (Real)ez * Qz;
-        }
+        const Real ev = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Vx, Vy, Vz);
+        const Real eu = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, ux, uy, uz);
+        const Real eq = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Qx, Qy, Qz);
+        const Real w = (Real)D::w;
         const int fb = ez < 0 ? fbM : (ez == 0 ? fbZ : fbP);
         // f*_k = (1 - w) f_k + (w_k T + w_k e.V) with T = (e.u)(e.Q) + C0.  The
         // opposite direction has the same T and the negated w_k e.V, exactly
@@ -305,28 +467,26 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
         if constexpr (MODE == 0 && k > 0) {
           if constexpr (k & 1) {
             using O = D27<D::opp>;
-            const Real T = eu * eq + C0, wev = (Real)D::w * ev, wT = (Real)D::w * T;
-            const Real fk = om1 * C::dec(L.fv[k], (Real)D::w) + (wT + wev);
-            const Real fo = om1 * C::dec(L.fv[D::opp], (Real)O::w) + (wT - wev);
+            const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
+            const Real fk = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
+            const Real fo = rfma(om1, C::dec(L.fv[D::opp], w), rsub(wT, wev));
             constexpr int fbo = O::ez < 0 ? 0 : (O::ez == 0 ? 1 : 2);
             const int fbO = fbo == 0 ? fbM : (fbo == 1 ? fbZ : fbP);
             ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
             ring[sm_at(fbO + slot27(D::opp) * NC, RING, 7)] = fo;
           }
         } else {
-          const Real T = eu * eq + C0, wev = (Real)D::w * ev, wT = (Real)D::w * T;
-          const Real fk = om1 * C::dec(L.fv[k], (Real)D::w) + (wT + wev);
+          const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
+          const Real fk = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
           if (nd) ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
         }
         if constexpr (k < Q7) {
-          using E = D7<k>;
-          Real ed = 0;
-          if constexpr (ex != 0) ed += (Real)ex * Dx;
-          if constexpr (ey != 0) ed += (Real)ey * Dy;
-          if constexpr (ez != 0) ed += (Real)ez * Dz;
+          const Real w7 = (Real)D7<k>::w;
+          // D3Q7 directions have at most one non-zero component
+          const Real ed = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Dx, Dy, Dz);
           Real href = 0;
-          if constexpr (C::offset) href = (Real)E::w * p;
-          const Real hk = omP1 * C::dec(L.hv[k], href) + (Real)E::w * (D0 + ed);
+          if constexpr (C::offset) href = rmul(w7, p);
+          const Real hk = rfma(omP1, C::dec(L.hv[k], href), rmul(w7, k == 0 ? D0 : radd(D0, ed)));
           const int hb = ez < 0 ? hbM : (ez == 0 ? hbZ : hbP);
           if (nd) ring[sm_at(hb + (ez == 0 ? k : 0) * NC, RING, 8)] = hk;
         }
@@ -343,14 +503,25 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   // and below the tile (both rows loaded before either is computed); halo
   // warp B the side columns and corners.
   // (lambdas are forced inline: an outlined closure would live in local memory)
-  auto collide_plane = [&](int q, Real &ogx, Real &ogy, Real &ogz, Real &olap,
-                           Real &ophi) __attribute__((always_inline)) {
+  // STAGE forms: the loads of plane q are issued one plane early (prefetch)
+  // into Lc (cell warps: phi stencil, rho, u, tag; halo warp A: the row above;
+  // halo warp B: its side cell) and Lb (halo warp A: the row below); the cell
+  // warps' populations arrive in the staging buffer.
+  LD Lc, Lb;
+  auto prefetch = [&](int q) __attribute__((always_inline)) {
     if (!haloWarp) {
-      LD L;
-      load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
-      compute(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, L, ogx, ogy, ogz, olap, ophi);
+      load_small(q, x, y, Lc);
+    } else if constexpr (!HALO_PF) {
     } else if (haloA) {
-      Real d0, d1, d2, d3, d4;
+      load(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, x, y0 - 1, Lc);
+      load(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, x, y0 + TY, Lb);
+    } else {
+      load(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, x0 - 1 + sideLx, y0 - 1 + sideLy, Lc);
+    }
+  };
+  auto halo_plane = [&](int q) __attribute__((always_inline)) {
+    Real d0, d1, d2, d3, d4;
+    if (haloA) {
       LD top, bot;
       load(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, x, y0 - 1, top);
       load(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, x, y0 + TY, bot);
@@ -358,26 +529,79 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       compute(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, (TY + 1) * RX + tx + 1, bot, d0, d1, d2, d3,
               d4);
     } else {
-      Real d0, d1, d2, d3, d4;
       LD L;
       load(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, x0 - 1 + sideLx, y0 - 1 + sideLy, L);
       compute(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, sideLy * RX + sideLx, L, d0, d1,
               d2, d3, d4);
     }
   };
+  auto collide_staged = [&](int q, Real &ogx, Real &ogy, Real &ogz, Real &olap,
+                            Real &ophi) __attribute__((always_inline)) {
+    stage_wait(q);
+    if (!haloWarp) {
+      stage_pops(q, Lc);
+      compute(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, Lc, ogx, ogy, ogz, olap, ophi);
+    } else if constexpr (!HALO_PF) {
+      halo_plane(q);
+    } else if (haloA) {
+      Real d0, d1, d2, d3, d4;
+      compute(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, tx + 1, Lc, d0, d1, d2, d3, d4);
+      compute(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, (TY + 1) * RX + tx + 1, Lb, d0, d1, d2, d3,
+              d4);
+    } else {
+      Real d0, d1, d2, d3, d4;
+      compute(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, sideLy * RX + sideLx, Lc, d0, d1,
+              d2, d3, d4);
+    }
+  };
+  auto collide_plane = [&](int q, Real &ogx, Real &ogy, Real &ogz, Real &olap,
+                           Real &ophi) __attribute__((always_inline)) {
+    if constexpr (STAGE) {
+      collide_staged(q, ogx, ogy, ogz, olap, ophi);
+    } else if (!haloWarp) {
+      LD L;
+      load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
+      compute(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, L, ogx, ogy, ogz, olap, ophi);
+    } else {
+      halo_plane(q);
+    }
+  };
 
   Real gxC = 0, gyC = 0, gzC = 0, lapC = 0, phC = 0;
   Real gxN = 0, gyN = 0, gzN = 0, lapN = 0, phN = 0;
-  collide_plane(zb - 1, gxN, gyN, gzN, lapN, phN);
-  collide_plane(zb, gxC, gyC, gzC, lapC, phC);
-
   const bool colActive = !haloWarp && x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
 
-  for (int z = zb; z < ze; z++) {
-    collide_plane(z + 1, gxN, gyN, gzN, lapN, phN);
+  if constexpr (STAGE) {
+    if (producer) {
+      for (int b = 0; b < NBUF; b++) mbar_init(bar0 + 8 * b);
+      mbar_init_fence();
+      *abortF = 0;
+    }
     __syncthreads();
-    const int sC = z % 3;
-    const uint8_t tagI = colActive ? stag[sm_at(sC * NC + own, TAGS, 9)] : TAG_WALL;
+    if (producer)
+      for (int b = 0; b < NBUF; b++) issue(zb - 1 + b);
+    prefetch(zb - 1);
+  }
+
+  // Iteration q collides plane q and pulls plane q - 1 (planes zb-1 .. ze are
+  // collided, zb .. ze-1 pulled).  In the STAGE forms the copy of plane q + 2
+  // goes out as soon as plane q's buffer is read, and the register loads of
+  // plane q + 1 right after plane q's collision.
+  int q = zb - 1;
+  for (; q <= ze; q++) {
+    collide_plane(q, gxN, gyN, gzN, lapN, phN);
+    if constexpr (STAGE) {
+      if (q < ze) prefetch(q + 1);
+    }
+    __syncthreads();
+    if constexpr (STAGE) {
+      if (*abortF) break;
+      if (producer && q + NBUF <= ze) issue(q + NBUF);
+    }
+    // pull plane z = q - 1 (nothing while z < zb)
+    const int z = q - 1;
+    const int sC = (z + 3) % 3;
+    const uint8_t tagI = colActive && z >= zb ? stag[sm_at(sC * NC + own, TAGS, 9)] : TAG_WALL;
     const int i = z * nxny + y * nx + x;
     const int bF = (i >> 3) * (8 * Q27) + (i & 7);
     const int bH = (i >> 3) * (8 * Q7) + (i & 7);
@@ -407,7 +631,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       const int obHM = (RING_H_M + (z & 1)) * NC + own;
       const int obHP = (RING_H_P + (z % 3)) * NC + own;
       const int tbM = ((z + 1) % 3) * NC + own, tbZ = sC * NC + own, tbP = ((z + 2) % 3) * NC + own;
-      const Real rhoPhOld = rhoG + phC * dRho;
+      const Real rhoPhOld = rfma(phC, dRho, rhoG);
       Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
       Real hn[Q7];
       uint32_t solidM = 0;
@@ -484,19 +708,22 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
         constexpr int k = decltype(KK)::value;
         st_at(Hn, bH + 8 * k, nH, 17, C::enc(hn[k], (Real)D7<k>::w * p));
       });
-      const Real rhoPhN = rhoG + p * dRho;
-      const Real mu = beta4 * p * (p - (Real)1) * ((Real)2 * p - (Real)1) - kappa * lapC;
-      const Real Fx = mu * gxC, Fy = mu * gyC + rhoPhN * grav, Fz = mu * gzC;
-      const Real inv = (Real)1 / rhoPhN;
-      Real uxn = (mx + (Real)0.5 * Fx) * inv;
-      Real uyn = (my + (Real)0.5 * Fy) * inv;
-      Real uzn = (mz + (Real)0.5 * Fz) * inv;
-      const Real u2 = uxn * uxn + uyn * uyn + uzn * uzn;
+      // explicitly rounded like the collision, so every instance of this
+      // kernel (tile shapes, staged or not, batched or not) gives the same bits
+      const Real one = (Real)1, half = (Real)0.5;
+      const Real rhoPhN = rfma(p, dRho, rhoG);
+      const Real mu = rfma(-kappa, lapC, rmul(rmul(rmul(beta4, p), rsub(p, one)), rfma((Real)2, p, -one)));
+      const Real Fx = rmul(mu, gxC), Fy = rfma(mu, gyC, rmul(rhoPhN, grav)), Fz = rmul(mu, gzC);
+      const Real inv = one / rhoPhN;
+      Real uxn = rmul(rfma(half, Fx, mx), inv);
+      Real uyn = rmul(rfma(half, Fy, my), inv);
+      Real uzn = rmul(rfma(half, Fz, mz), inv);
+      const Real u2 = rfma(uzn, uzn, rfma(uyn, uyn, rmul(uxn, uxn)));
       if (u2 > (Real)(0.2 * 0.2)) {
         const Real sc = (Real)0.2 / sqrt(u2);
-        uxn *= sc;
-        uyn *= sc;
-        uzn *= sc;
+        uxn = rmul(uxn, sc);
+        uyn = rmul(uyn, sc);
+        uzn = rmul(uzn, sc);
       }
       st_at(s.rho[nxt], i, nCell, 18, rhoN);
       st_at(s.phi[nxt], i, nCell, 18, p);
@@ -511,11 +738,23 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     lapC = lapN;
     phC = phN;
   }
+
+  if constexpr (STAGE) {
+    if (q <= ze && producer) {
+      // stopped at plane q: let the copies of planes q .. q + NBUF - 1 land
+      // (bounded) before the buffers are released
+      mbar_wait(bar0 + 8 * (q % NBUF), ((phase >> (q % NBUF)) & 1u) ^ 1u);
+      if (NBUF == 2 && q + 1 <= ze) mbar_wait(bar0 + 8 * ((q + 1) % NBUF), (phase >> ((q + 1) % NBUF)) & 1u);
+    }
+    __syncthreads();
+    if (producer)
+      for (int b = 0; b < NBUF; b++) mbar_inval(bar0 + 8 * b);
+  }
 }
 
 // One scene: the grid is its tiles.
 template <class PopT, int TY>
-__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY>::blocks)
     k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
   fused_tile<PopT, TY>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
@@ -525,7 +764,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
 // gives its own grid, physics constants and state.  CTAs stride over the
 // tiles, so one launch of about one wave advances every scene by a step.
 template <class PopT, int TY>
-__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<TY>::blocks)
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY>::blocks)
     k_fused_batch(const FusedArgs<PopT> *__restrict__ args, const int *__restrict__ tileStart,
                   const int3 *__restrict__ tileGrid, int nscenes) {
   const int total = tileStart[nscenes];

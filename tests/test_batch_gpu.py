@@ -94,3 +94,27 @@ def test_batch_continues_across_runs_and_configs(gpu):
         for k in ("phi", "rho", "ux", "f"):
             assert np.array_equal(a[k], b[k]), k
         assert sa == sb
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_reduced_storage_independent_of_tile_shape(gpu, storage):
+    """Reduced storage has a staged form of the fused kernel at 4 rows per CTA
+    (populations brought in by bulk asynchronous copies) and a plain form at
+    2 and 8 rows; a scene stepped through all three, in a batch, ends bit for
+    bit where the same scene run alone (staged form) ends."""
+    import functools
+    SimS = functools.partial(gpu.Sim, storage=storage)
+    ref = [bld(SimS, gpu.RigidSphere) for bld in BUILDERS]
+    for sim, solid in ref:
+        sim.run_coupled(solid, 12)
+    mixed = [bld(SimS, gpu.RigidSphere) for bld in BUILDERS]
+    with gpu.Batch(mixed) as batch:
+        for rows, zchunk in ((8, 16), (4, 32), (2, 7), (4, 5)):
+            batch.set_config(rows, zchunk)
+            batch.run(3, use_graph=False)
+    for i, ((sim, solid), (rsim, rsolid)) in enumerate(zip(mixed, ref)):
+        a, sa = _state(sim, solid)
+        b, sb = _state(rsim, rsolid)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), f"scene {i}: {k} differs"
+        assert sa == sb, f"scene {i}: sphere state differs"
