@@ -294,10 +294,27 @@ void shift_boxes(lbm_sim *h, const Box &now) {
   h->boxLast = now;
 }
 
+// Synchronizes the handle's stream and reports a fused step that was
+// abandoned because a bounded wait ran out (LBM_ERR_TIMEOUT; the status is
+// cleared, the fields of that step are not valid).  Copies queued before the
+// call complete with it.
+int sync_status(lbm_sim *h) {
+  CK(copy_async(h, h->hTotals + 2, h->totals + 2, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->hTotals[2] != 0) {
+    h->hTotals[2] = 0;
+    CK(cudaMemsetAsync(h->totals + 2, 0, sizeof(int), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return fail(h, LBM_ERR_TIMEOUT,
+                "fused step abandoned: a staged plane did not arrive within the bounded wait");
+  }
+  return LBM_OK;
+}
+
 int fetch_out(lbm_sim *h, const double *d_src, int ns, lbm_impulse *out) {
   if (!out || ns == 0) return LBM_OK;
   CK(copy_async(h, h->hOut, d_src, (size_t)ns * 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  if (int rc = sync_status(h)) return rc;
   for (int b = 0; b < ns; b++) {
     out[b].Fx = h->hOut[6 * b + 0];
     out[b].Fy = h->hOut[6 * b + 1];
@@ -508,7 +525,7 @@ int coupled_finish(lbm_sim *h, lbm_sphere *sp, int ns) {
   CK(copy_async(h, &h->hPlan, h->dPlan, sizeof(Plan), cudaMemcpyDeviceToHost, h->stream));
   if (ns > 0)
     CK(copy_async(h, sp, h->dSph, ns * sizeof(lbm_sphere), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  if (int rc = sync_status(h)) return rc;
   h->boxLast = h->hPlan.boxLast;
   h->boxLastLast = h->hPlan.boxLastLast;
   h->fullRetagSteps = h->hPlan.fullRetag;
@@ -579,15 +596,15 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
     h->listCap = h->n;
     DALLOC(h->fresh, h->listCap * sizeof(int));
     DALLOC(h->dead, h->listCap * sizeof(int));
-    DALLOC(h->totals, 2 * sizeof(int));
-    CK(cudaMemsetAsync(h->totals, 0, 2 * sizeof(int), h->stream));
+    DALLOC(h->totals, 3 * sizeof(int));
+    CK(cudaMemsetAsync(h->totals, 0, 3 * sizeof(int), h->stream));
     DALLOC(h->dOut, 2 * LBM_MAX_SPHERES * 6 * sizeof(double));
     DALLOC(h->dSph, LBM_MAX_SPHERES * sizeof(lbm_sphere));
     DALLOC(h->dPlan, sizeof(Plan));
     CK(cudaMemsetAsync(h->dPlan, 0, sizeof(Plan), h->stream));
     DALLOC(h->dPhiCol, (size_t)ny * sizeof(double));
     CK(cudaMallocHost((void **)&h->hOut, 2 * LBM_MAX_SPHERES * 6 * sizeof(double)));
-    CK(cudaMallocHost((void **)&h->hTotals, 2 * sizeof(int)));
+    CK(cudaMallocHost((void **)&h->hTotals, 3 * sizeof(int)));
     CK(cudaStreamSynchronize(h->stream));
     return LBM_OK;
   };
@@ -1086,7 +1103,12 @@ int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_ev
 int lbm_synchronize(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);
-  CK(cudaStreamSynchronize(h->stream));
+  return sync_status(h);
+}
+
+int lbm_test_withhold_stage_copy(lbm_sim *h, int on) {
+  if (!h) return LBM_ERR_ARG;
+  h->withholdStage = on != 0;
   return LBM_OK;
 }
 

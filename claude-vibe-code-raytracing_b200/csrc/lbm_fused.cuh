@@ -46,6 +46,8 @@ struct FusedArgs {
   int zchunk;
   double om, omP, A, beta4, kappa, rhoG, dRho, gravity, sharpC4;
   const SolidSet *ss;
+  int *status;   // set non-zero when a bounded wait of the step runs out
+  int withhold;  // test hook: the staged forms do not issue each tile's first copy
 };
 
 // slot of direction k within its e_z group (0..8 for D3Q27)
@@ -104,7 +106,12 @@ struct FusedOcc {
 // wait is bounded (LBM_STAGE_WAIT_NS of %globaltimer); a wait that runs out
 // returns false and the caller records the fault and stops the tile.
 #ifndef LBM_STAGE_WAIT_NS
-#define LBM_STAGE_WAIT_NS 500000000ull
+#define LBM_STAGE_WAIT_NS 1000000000ull
+#endif
+// a wait also needs this many polls before it gives up, so time during which
+// the context was not running does not count as waiting
+#ifndef LBM_STAGE_WAIT_POLLS
+#define LBM_STAGE_WAIT_POLLS 65536u
 #endif
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -146,9 +153,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
-  for (;;) {
+  for (uint32_t polls = 0;; polls++) {
     if (mbar_try(bar, parity)) return true;
-    if (global_ns() - t0 > LBM_STAGE_WAIT_NS) return false;
+    if (polls >= LBM_STAGE_WAIT_POLLS && global_ns() - t0 > LBM_STAGE_WAIT_NS) return false;
   }
 }
 
@@ -374,6 +381,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     phase ^= 1u << buf;
     if (!haloWarp && !mbar_wait(bar0 + 8 * buf, par)) {
       record_stage_timeout(q);
+      if (a.status) atomicOr(a.status, 1);
       *abortF = 1;
     }
   };
@@ -579,7 +587,8 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     }
     __syncthreads();
     if (producer)
-      for (int b = 0; b < NBUF; b++) issue(zb - 1 + b);
+      for (int b = 0; b < NBUF; b++)
+        if (!(a.withhold && b == 0)) issue(zb - 1 + b);
     prefetch(zb - 1);
   }
 
@@ -743,7 +752,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     if (q <= ze && producer) {
       // stopped at plane q: let the copies of planes q .. q + NBUF - 1 land
       // (bounded) before the buffers are released
-      mbar_wait(bar0 + 8 * (q % NBUF), ((phase >> (q % NBUF)) & 1u) ^ 1u);
+      if (!(a.withhold && q == zb - 1)) mbar_wait(bar0 + 8 * (q % NBUF), ((phase >> (q % NBUF)) & 1u) ^ 1u);
       if (NBUF == 2 && q + 1 <= ze) mbar_wait(bar0 + 8 * ((q + 1) % NBUF), (phase >> ((q + 1) % NBUF)) & 1u);
     }
     __syncthreads();

@@ -283,6 +283,8 @@ class Ops final : public OpsBase {
     a.gravity = k.gravity;
     a.sharpC4 = 4 * k.sharpC;
     a.ss = &h->dPlan->ss;
+    a.status = h->totals + 2;
+    a.withhold = h->withholdStage ? 1 : 0;
     return a;
   }
   size_t fused_args_bytes() const override { return sizeof(FusedArgs<PopT>); }

@@ -84,6 +84,7 @@ struct lbm_sim {
   lbm::OpsBase *ops = nullptr;
   lbm::FusedCfg cfg;
   bool fusedOK = true;  // the fused kernel's 32-bit indexing covers this grid
+  bool withholdStage = false;  // test hook: the staged fused kernel withholds its first copy
 
   // device memory
   void *F[2] = {nullptr, nullptr};
@@ -99,7 +100,7 @@ struct lbm_sim {
   long long listCap = 0;
   int2 *counts = nullptr;
   long long countsCap = 0;
-  int *totals = nullptr;  // device [2]: n_fresh, n_dead
+  int *totals = nullptr;  // device [3]: n_fresh, n_dead, fused-step status (non-zero: a bounded wait ran out)
   bool listsValid = false;
 
   double *impAcc = nullptr;  // per-cell impulse slots of every sphere
@@ -117,7 +118,7 @@ struct lbm_sim {
   void *image = nullptr;  // rendered RGBA8 frame (lbm_render)
   size_t imageBytes = 0;
   double *dPhiCol = nullptr;
-  int *hTotals = nullptr;  // pinned
+  int *hTotals = nullptr;  // pinned [3]
 
   lbm::Box boxLast{{1, 1, 1}, {0, 0, 0}};
   lbm::Box boxLastLast{{1, 1, 1}, {0, 0, 0}};

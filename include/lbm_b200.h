@@ -163,7 +163,11 @@ int lbm_pack_volume_device(lbm_sim *sim, void *device_out);
 int lbm_run_coupled(lbm_sim *sim, lbm_sphere *spheres, int nspheres, int nsteps,
                     int frame_every, uint8_t *frames);
 
-/* Wait for all work queued on the handle's stream. */
+/* Wait for all work queued on the handle's stream.  Returns LBM_ERR_TIMEOUT
+ * when a fused step since the last check was abandoned because one of its
+ * bounded device waits ran out (its fields are not valid; the handle stays
+ * usable, e.g. after lbm_init_flat).  lbm_step, lbm_run_coupled,
+ * lbm_absorb_dead_cells and lbm_batch_run report the same when they return. */
 int lbm_synchronize(lbm_sim *sim);
 /* CUDA stream of the handle (cudaStream_t), for callers that enqueue around it. */
 void *lbm_stream(lbm_sim *sim);
@@ -183,6 +187,12 @@ int lbm_launch_count(const lbm_sim *sim, int64_t *count);
  * (x | y<<8)}, all zero when none. */
 int lbm_checked_build(void);
 int lbm_fault_record(lbm_sim *sim, int64_t out[4]);
+/* Test hook for the bounded waits: while on, the fused kernel's staged forms
+ * (FP16/BF16 storage, 4 rows per CTA) do not issue the first plane copy of
+ * each tile, so that plane's wait runs out (about a second), the step is
+ * abandoned and LBM_ERR_TIMEOUT is reported; the fault record then holds
+ * location code 90.  No effect on the other forms. */
+int lbm_test_withhold_stage_copy(lbm_sim *sim, int on);
 /* Host->device and device->host bytes this handle has copied since creation. */
 int lbm_transfer_bytes(const lbm_sim *sim, uint64_t *h2d, uint64_t *d2h);
 /* Time the fused step kernel with CUDA events on the handle's stream.
