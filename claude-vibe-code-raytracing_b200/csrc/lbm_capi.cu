@@ -544,7 +544,7 @@ size_t lbm_footprint_bytes(int nx, int ny, int nz, int storage) {
   if (nx < 3 || ny < 3 || nz < 3 || storage < 0 || storage > 3) return 0;
   long long n = (long long)nx * ny * nz;
   size_t pb = pop_bytes_of(storage), mb = mac_bytes_of(storage);
-  size_t bytes = 2 * (size_t)pop_elems(n, 27 + 7) * pb;  // F, H ping-pong
+  size_t bytes = 2 * (size_t)(pop_elems(n, 27) + pop_elems(n, 7)) * pb;  // F, H ping-pong
   bytes += 2 * 5 * (size_t)n * mb;                     // macros ping-pong
   bytes += 2 * (size_t)n;                              // tag, tagPrev
   bytes += 2 * (size_t)n * sizeof(int);                // fresh / dead lists

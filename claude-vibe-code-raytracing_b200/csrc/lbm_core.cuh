@@ -131,15 +131,26 @@ struct Codec<__nv_bfloat16> {
 };
 
 // ---------------------------------------------------------------- population layout
-// Populations are stored in blocks of 8 consecutive cells (flat cell order),
-// direction-major inside a block: element (k, i) of a Q-direction lattice is at
-// ((i >> 3) * Q + k) * 8 + (i & 7).  A warp touching 32 consecutive cells reads
-// whole 32-byte sectors, and the offset between directions is a constant.
+// Populations are stored in blocks of 8 consecutive cells (flat cell order).
+// Inside a block the directions form groups of four (the last group padded),
+// and a cell's four values of a group are adjacent: element (k, i) of a
+// Q-direction lattice is at
+//   ((i >> 3) * G + (k >> 2)) * 32 + (i & 7) * 4 + (k & 3),   G = (Q + 3) / 4.
+// One cell's group is a single 16-byte (FP32) or 8-byte (FP16/BF16) vector,
+// and a warp reading one group of 32 consecutive cells reads whole lines.
+template <int Q>
+struct PopGroups {
+  static constexpr int G = (Q + 3) / 4;  // groups per cell
+  static constexpr int BLOCK = 32 * G;   // elements per 8-cell block
+};
+// offset of direction k inside its cell's part of a block
+__host__ __device__ __forceinline__ constexpr int pofs(int k) { return (k >> 2) * 32 + (k & 3); }
 template <int Q>
 __host__ __device__ __forceinline__ long long pidx(int k, long long i) {
-  return ((i >> 3) * Q + k) * 8 + (i & 7);
+  return (i >> 3) * PopGroups<Q>::BLOCK + (i & 7) * 4 + pofs(k);
 }
-__host__ __device__ inline long long pop_elems(long long n, int Q) { return (n + 7) / 8 * 8 * Q; }
+// elements of a Q-direction lattice over n cells (whole blocks)
+__host__ __device__ inline long long pop_elems(long long n, int Q) { return (n + 7) / 8 * 32 * ((Q + 3) / 4); }
 
 // ---------------------------------------------------------------- scene view
 // Device pointers of one scene.  Index c in [0,1] selects a ping-pong half:

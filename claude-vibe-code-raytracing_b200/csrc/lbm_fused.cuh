@@ -80,7 +80,7 @@ struct FusedSmem {
   static constexpr bool STAGE = TY == 4 && sizeof(PopT) == 2;
   static constexpr int NBUF = LBM_STAGE_NBUF;
   static constexpr int SB = 5;
-  static constexpr int ROWF = SB * 8 * Q27, ROWH = SB * 8 * Q7;  // elements per staged row
+  static constexpr int ROWF = SB * PopGroups<Q27>::BLOCK, ROWH = SB * PopGroups<Q7>::BLOCK;  // per staged row
   static constexpr size_t ringBytes = (size_t)RING_PLANES * NC * sizeof(Real);
   static constexpr size_t stageOff = (ringBytes + 3 * NC + 15) / 16 * 16;
   static constexpr size_t bufBytes = STAGE ? (size_t)TY * (ROWF + ROWH) * sizeof(PopT) : 0;
@@ -166,6 +166,15 @@ constexpr bool halo_dir() {
   return (SX == 0 || kDir[K][0] == SX) && (SY == 0 || kDir[K][1] == SY);
 }
 
+// does direction group g (directions 4g .. 4g+3) hold a direction a halo cell
+// of side (SX, SY) needs?
+template <int SX, int SY, int Q, int G>
+constexpr bool halo_group() {
+  for (int k = 4 * G; k < 4 * G + 4 && k < Q; k++)
+    if ((SX == 0 || kDir[k][0] == SX) && (SY == 0 || kDir[k][1] == SY)) return true;
+  return false;
+}
+
 template <int V>
 using IC = std::integral_constant<int, V>;
 
@@ -218,6 +227,73 @@ __device__ __forceinline__ int sm_at(int idx, int lim, int code) {
   return lbm_ok(idx >= 0 && idx < lim, code, idx) ? idx : 0;
 }
 
+// One cell's group of four populations (adjacent and aligned to the group's
+// size): one 16-byte access for FP32, 8 bytes for FP16/BF16, two 16-byte
+// accesses for FP64.
+template <class PopT>
+__device__ __forceinline__ void ld4_global(const PopT *p, PopT (&o)[4]) {
+  if constexpr (sizeof(PopT) == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+    memcpy(o, &t, 16);
+  } else if constexpr (sizeof(PopT) == 8) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    memcpy(o, &a, 16);
+    memcpy(o + 2, &b, 16);
+  } else {
+    const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
+    memcpy(o, &t, 8);
+  }
+}
+template <class PopT>
+__device__ __forceinline__ void ld4_shared(const PopT *p, PopT (&o)[4]) {
+  if constexpr (sizeof(PopT) == 4) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    memcpy(o, &t, 16);
+  } else if constexpr (sizeof(PopT) == 8) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0];
+    const double2 b = reinterpret_cast<const double2 *>(p)[1];
+    memcpy(o, &a, 16);
+    memcpy(o + 2, &b, 16);
+  } else {
+    const uint2 t = *reinterpret_cast<const uint2 *>(p);
+    memcpy(o, &t, 8);
+  }
+}
+template <class PopT>
+__device__ __forceinline__ void st4_global(PopT *p, const PopT (&v)[4]) {
+  if constexpr (sizeof(PopT) == 4) {
+    float4 t;
+    memcpy(&t, v, 16);
+    *reinterpret_cast<float4 *>(p) = t;
+  } else if constexpr (sizeof(PopT) == 8) {
+    double2 a, b;
+    memcpy(&a, v, 16);
+    memcpy(&b, v + 2, 16);
+    reinterpret_cast<double2 *>(p)[0] = a;
+    reinterpret_cast<double2 *>(p)[1] = b;
+  } else {
+    uint2 t;
+    memcpy(&t, v, 8);
+    *reinterpret_cast<uint2 *>(p) = t;
+  }
+}
+// bounds-checked forms (group of elements idx .. idx + 3); a load that is not
+// wanted or out of range gives zeros
+template <class PopT>
+__device__ __forceinline__ void ldg4_at(const PopT *p, long long idx, long long lim, int code, bool want,
+                                        PopT (&o)[4]) {
+  if (want && lbm_ok(idx >= 0 && idx + 3 < lim, code, idx)) {
+    ld4_global(p + idx, o);
+  } else {
+    o[0] = o[1] = o[2] = o[3] = PopT();
+  }
+}
+template <class PopT>
+__device__ __forceinline__ void st4_at(PopT *p, long long idx, long long lim, int code, const PopT (&v)[4]) {
+  if (lbm_ok(idx >= 0 && idx + 3 < lim, code, idx)) st4_global(p + idx, v);
+}
+
 // Everything the collision of one cell reads from global memory.
 template <class PopT>
 struct CellLoad {
@@ -263,6 +339,8 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   const int nx = s.nx, ny = s.ny, nz = s.nz, nxny = nx * ny;
   const long long nCell = s.n, nF = pop_elems(s.n, Q27), nH = pop_elems(s.n, Q7);
   constexpr int RING = RING_PLANES * NC, TAGS = 3 * NC;
+  constexpr int G27 = PopGroups<Q27>::G, G7 = PopGroups<Q7>::G;
+  constexpr int BLK27 = PopGroups<Q27>::BLOCK, BLK7 = PopGroups<Q7>::BLOCK;
   const Real om = (Real)a.om, omP = (Real)a.omP, A = (Real)a.A;
   const Real beta4 = (Real)a.beta4, kappa = (Real)a.kappa, rhoG = (Real)a.rhoG;
   const Real dRho = (Real)a.dRho, grav = (Real)a.gravity, sharpC4 = (Real)a.sharpC4;
@@ -332,16 +410,30 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
     const bool inside = gx_ >= 0 && gx_ < nx && gy_ >= 0 && gy_ < ny && q >= 0 && q < nz;
     const int ci = inside ? q * nxny + gy_ * nx + gx_ : 0;
-    const int bF = (ci >> 3) * (8 * Q27) + (ci & 7);
-    const int bH = (ci >> 3) * (8 * Q7) + (ci & 7);
-    static_for<0, Q27>([&](auto KK) {
-      constexpr int k = decltype(KK)::value;
-      if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
-        const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
-        L.fv[k] = nd ? ldg_at(Fc, bF + 8 * k, nF, 3) : PopT();
-        if constexpr (k < Q7) L.hv[k] = nd ? ldg_at(Hc, bH + 8 * k, nH, 4) : PopT();
-      }
-    });
+    const int bF = (ci >> 3) * BLK27 + (ci & 7) * 4;
+    const int bH = (ci >> 3) * BLK7 + (ci & 7) * 4;
+    // whole groups of four directions, loaded when any of their directions is needed
+    auto groups = [&](auto QQ, auto NG, const PopT *src, int base, long long lim, int code,
+                      PopT *dst) __attribute__((always_inline)) {
+      constexpr int Q = decltype(QQ)::value;
+      static_for<0, decltype(NG)::value>([&](auto GG) {
+        constexpr int g = decltype(GG)::value;
+        if constexpr (MODE != 1 || halo_group<SX, SY, Q, g>()) {
+          bool nd = false;
+          static_for<4 * g, (4 * g + 4 < Q ? 4 * g + 4 : Q)>([&](auto KK) {
+            nd = nd || needs(MODEc, SXc, SYc, KK, sx, sy, active);
+          });
+          PopT t[4];
+          ldg4_at(src, base + 32 * g, lim, code, nd, t);
+          static_for<4 * g, (4 * g + 4 < Q ? 4 * g + 4 : Q)>([&](auto KK) {
+            constexpr int k = decltype(KK)::value;
+            dst[k] = t[k & 3];
+          });
+        }
+      });
+    };
+    groups(IC<Q27>{}, IC<G27>{}, Fc, bF, nF, 3, L.fv);
+    groups(IC<Q7>{}, IC<G7>{}, Hc, bH, nH, 4, L.hv);
     load_small(q, gx_, gy_, L);
   };
 
@@ -358,7 +450,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     for (int r = 0; r < TY; r++) {
       if (y0 + r >= ny) break;
       const int row0 = (q * ny + y0 + r) * nx + x0;
-      total += (uint32_t)(((row0 + span) >> 3) - (row0 >> 3) + 1) * 8 * (Q27 + Q7) * sizeof(PopT);
+      total += (uint32_t)(((row0 + span) >> 3) - (row0 >> 3) + 1) * (BLK27 + BLK7) * sizeof(PopT);
     }
     mbar_expect(bar, total);
     for (int r = 0; r < TY; r++) {
@@ -366,12 +458,12 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       const int row0 = (q * ny + y0 + r) * nx + x0;
       const int b0 = row0 >> 3, nb = ((row0 + span) >> 3) - b0 + 1;
       const bool ok = lbm_ok(nb <= SM::SB, 20, nb) &&
-                      lbm_ok((long long)(b0 + nb) * 8 * Q27 <= nF, 21, b0);
+                      lbm_ok((long long)(b0 + nb) * BLK27 <= nF, 21, b0);
       if (!ok) continue;
-      bulk_g2s(smem_u32(stage + buf * BUF + r * ROWF), Fc + (long long)b0 * 8 * Q27,
-               (uint32_t)(nb * 8 * Q27 * sizeof(PopT)), bar);
-      bulk_g2s(smem_u32(stage + buf * BUF + TY * ROWF + r * ROWH), Hc + (long long)b0 * 8 * Q7,
-               (uint32_t)(nb * 8 * Q7 * sizeof(PopT)), bar);
+      bulk_g2s(smem_u32(stage + buf * BUF + r * ROWF), Fc + (long long)b0 * BLK27,
+               (uint32_t)(nb * BLK27 * sizeof(PopT)), bar);
+      bulk_g2s(smem_u32(stage + buf * BUF + TY * ROWF + r * ROWH), Hc + (long long)b0 * BLK7,
+               (uint32_t)(nb * BLK7 * sizeof(PopT)), bar);
     }
   };
   uint32_t phase = 0;  // parity of the next wait, one bit per buffer
@@ -393,10 +485,21 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     const bool inside = x < nx && y < ny;
     const int off = inside ? ((row0 + tx) >> 3) - (row0 >> 3) : 0;
     const int e = inside ? ((row0 + tx) & 7) : 0;
-    static_for<0, Q27>([&](auto KK) {
-      constexpr int k = decltype(KK)::value;
-      L.fv[k] = sF[sm_at((off * Q27 + k) * 8 + e, ROWF, 22)];
-      if constexpr (k < Q7) L.hv[k] = sH[sm_at((off * Q7 + k) * 8 + e, ROWH, 23)];
+    static_for<0, G27>([&](auto GG) {
+      constexpr int g = decltype(GG)::value;
+      PopT t[4];
+      ld4_shared(sF + sm_at((off * G27 + g) * 32 + e * 4, ROWF - 3, 22), t);
+      static_for<4 * g, (4 * g + 4 < Q27 ? 4 * g + 4 : Q27)>([&](auto KK) {
+        constexpr int k = decltype(KK)::value;
+        L.fv[k] = t[k & 3];
+      });
+      if constexpr (g < G7) {
+        ld4_shared(sH + sm_at((off * G7 + g) * 32 + e * 4, ROWH - 3, 23), t);
+        static_for<4 * g, (4 * g + 4 < Q7 ? 4 * g + 4 : Q7)>([&](auto KK) {
+          constexpr int k = decltype(KK)::value;
+          L.hv[k] = t[k & 3];
+        });
+      }
     });
   };
 
@@ -612,15 +715,23 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     const int sC = (z + 3) % 3;
     const uint8_t tagI = colActive && z >= zb ? stag[sm_at(sC * NC + own, TAGS, 9)] : TAG_WALL;
     const int i = z * nxny + y * nx + x;
-    const int bF = (i >> 3) * (8 * Q27) + (i & 7);
-    const int bH = (i >> 3) * (8 * Q7) + (i & 7);
+    const int bF = (i >> 3) * BLK27 + (i & 7) * 4;
+    const int bH = (i >> 3) * BLK7 + (i & 7) * 4;
     if (tagI == TAG_SOLID) {
       // Solid cells are not updated; carry their state into the next half so
       // both halves hold the reference's stale values.
 #pragma unroll 1
-      for (int k = 0; k < Q27; k++) st_at(Fn, bF + 8 * k, nF, 10, ldg_at(Fc, bF + 8 * k, nF, 10));
+      for (int g = 0; g < G27; g++) {
+        PopT t[4];
+        ldg4_at(Fc, bF + 32 * g, nF, 10, true, t);
+        st4_at(Fn, bF + 32 * g, nF, 10, t);
+      }
 #pragma unroll 1
-      for (int k = 0; k < Q7; k++) st_at(Hn, bH + 8 * k, nH, 11, ldg_at(Hc, bH + 8 * k, nH, 11));
+      for (int g = 0; g < G7; g++) {
+        PopT t[4];
+        ldg4_at(Hc, bH + 32 * g, nH, 11, true, t);
+        st4_at(Hn, bH + 32 * g, nH, 11, t);
+      }
       st_at(s.phi[nxt], i, nCell, 12, ldg_at(phiC, i, nCell, 12));
       st_at(s.rho[nxt], i, nCell, 12, ldg_at(rhoC, i, nCell, 12));
       st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
@@ -643,6 +754,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       const Real rhoPhOld = rfma(phC, dRho, rhoG);
       Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
       Real hn[Q7];
+      PopT enc4[4];  // the current group's encoded values, stored as one vector
       uint32_t solidM = 0;
       static_for<0, Q27>([&](auto KK) {
         constexpr int k = decltype(KK)::value;
@@ -659,7 +771,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
         // of the cell's own opposite value (moving-wall term added below)
         const Real fk = ring[sm_at(fl ? sbF + slot27(k) * NC + so : obF + slot27(o) * NC, RING, 14)];
         solidM |= (uint32_t)(ts == TAG_SOLID) << k;
-        st_at(Fn, bF + 8 * k, nF, 15, C::enc(fk, (Real)D::w));
+        enc4[k & 3] = C::enc(fk, (Real)D::w);
+        if constexpr ((k & 3) == 3 || k == Q27 - 1) {
+          if constexpr (k == Q27 - 1) enc4[3] = PopT();  // pad of the last group
+          st4_at(Fn, bF + pofs(k & ~3), nF, 15, enc4);
+        }
         rhoA += fk;
         if constexpr (ex != 0) mx += (Real)ex * fk;
         if constexpr (ey != 0) my += (Real)ey * fk;
@@ -695,7 +811,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
           const int obF = oz < 0 ? obFM : (oz == 0 ? sbFZ : obFP);
           const Real fopp = ring[sm_at(obF + c_slot27[o] * NC, RING, 19)];
           const Real fk = fopp + corr;
-          st_at(Fn, bF + 8 * k, nF, 15, C::enc(fk, w));
+          st_at(Fn, bF + pofs(k), nF, 15, C::enc(fk, w));
           rhoA += corr;
           mx += (Real)ex * corr;
           my += (Real)ey * corr;
@@ -715,7 +831,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       const Real p = hsum < (Real)0 ? (Real)0 : hsum > (Real)1 ? (Real)1 : hsum;
       static_for<0, Q7>([&](auto KK) {
         constexpr int k = decltype(KK)::value;
-        st_at(Hn, bH + 8 * k, nH, 17, C::enc(hn[k], (Real)D7<k>::w * p));
+        enc4[k & 3] = C::enc(hn[k], (Real)D7<k>::w * p);
+        if constexpr ((k & 3) == 3 || k == Q7 - 1) {
+          if constexpr (k == Q7 - 1) enc4[3] = PopT();
+          st4_at(Hn, bH + pofs(k & ~3), nH, 17, enc4);
+        }
       });
       // explicitly rounded like the collision, so every instance of this
       // kernel (tile shapes, staged or not, batched or not) gives the same bits
