@@ -219,6 +219,11 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def _shape_name(rows, zchunk):
+    """'4x32', or '4sx32' for the staged 4-row form."""
+    return f"{rows & 0xff}{'s' if rows & 0x100 else ''}x{zchunk}"
+
+
 def run_batch(args, dev, ws=1, rank=0):
     """64 seeded scenes of mixed sizes (FP16 storage) stepped together: one
     persistent fused launch per step, the steps replayed as a CUDA graph, tile
@@ -268,8 +273,8 @@ def run_batch(args, dev, ws=1, rank=0):
         "data": "synthetic", "scaling": "strong",
         "config": {"workload": f"{args.scenes} scenes, edges U[32,160], pool 30-60% of ny, 1-3 spheres",
                    "parallelism": f"whole scenes per GPU x{ws}",
-                   "cells": cells, "storage": storage, "tile": [rows, zchunk],
-                   "timings_ms": {f"{r}x{z}": t for (r, z), t in timings.items()}},
+                   "cells": cells, "storage": storage, "tile": _shape_name(rows, zchunk),
+                   "timings_ms": {_shape_name(r, z): t for (r, z), t in timings.items()}},
         "ms_per_step": dt_graph / K * 1e3,
         "eager_mlups": cells * K / dt_eager / 1e6,
         "sequential_mlups": cells * K / dt_seq / 1e6,

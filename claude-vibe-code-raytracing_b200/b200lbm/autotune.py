@@ -1,7 +1,7 @@
 """Tile-shape autotuner for batched steps.
 
 The fused kernel's tile shape -- rows per CTA (2, 4 or 8 cell warps plus two
-halo warps) and z planes per CTA -- trades halo recomputation and shared-memory
+halo warps, or the staged 4-row form for FP16/BF16) and z planes per CTA -- trades halo recomputation and shared-memory
 occupancy against the number of tiles in flight; the best shape depends on the
 mix of grid sizes.  tune() times each candidate shape with
 lbm_batch_time_fused on the batch's own current state (the timed launches only
@@ -17,7 +17,16 @@ import json
 import math
 import os
 
+# rows | STAGED: the staged form of the 4-row tile (FP16/BF16 storage only),
+# whose tile rows arrive in shared memory by bulk asynchronous copy
+STAGED = 0x100
 CANDIDATES = [(4, 32), (4, 16), (8, 16), (8, 32), (2, 32), (4, 64)]
+CANDIDATES_REDUCED = CANDIDATES + [(4 | STAGED, 32), (4 | STAGED, 16)]
+
+
+def candidates_for(storage):
+    """Tile shapes worth timing for a storage form."""
+    return CANDIDATES_REDUCED if storage in ("f16", "bf16") else CANDIDATES
 
 _cache: dict = {}
 _loaded = False
@@ -58,7 +67,7 @@ def signature(dims, storage):
     return f"{storage}:n{n}:c{c}"
 
 
-def tune(batch, dims, storage, reps=3, candidates=CANDIDATES, force=False):
+def tune(batch, dims, storage, reps=3, candidates=None, force=False):
     """Pick and set the fastest tile shape for `batch` (which has run at least
     one step).  Returns (rows, zchunk, timings): timings maps each measured
     shape to ms per launch, and is empty when the cache answered."""
@@ -69,7 +78,7 @@ def tune(batch, dims, storage, reps=3, candidates=CANDIDATES, force=False):
         batch.set_config(rows, zchunk)
         return rows, zchunk, {}
     timings = {}
-    for rows, zchunk in candidates:
+    for rows, zchunk in candidates or candidates_for(storage):
         timings[(rows, zchunk)] = batch.time_fused(rows, zchunk, reps=reps)
     rows, zchunk = min(timings, key=timings.get)
     _cache[key] = [rows, zchunk]

@@ -44,7 +44,8 @@ class Batch:
             raise LbmError(rc, (lib().lbm_batch_last_error(self._b) or b"").decode(errors="replace"))
 
     def set_config(self, rows, zchunk):
-        """Fused tile shape: rows per CTA (2, 4, 8) and z planes per CTA."""
+        """Fused tile shape: rows per CTA (2, 4, 8, or 4 | autotune.STAGED for the
+        staged FP16/BF16 form) and z planes per CTA."""
         self._check(lib().lbm_batch_set_config(self._b, int(rows), int(zchunk)))
 
     def run(self, nsteps, frame_every=0, use_graph=True):

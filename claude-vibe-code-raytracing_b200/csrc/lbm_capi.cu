@@ -1192,8 +1192,9 @@ int lbm_fused_timing_query(lbm_sim *h, double *total_ms, int64_t *launches) {
 
 int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
   if (!h) return LBM_ERR_ARG;
-  if (!(rows == 2 || rows == 4 || rows == 8) || zchunk < 1)
-    return fail(h, LBM_ERR_ARG, "rows must be 2, 4 or 8 and zchunk >= 1");
+  if (!h->ops->shape_ok(rows) || zchunk < 1)
+    return fail(h, LBM_ERR_ARG,
+                "rows must be 2, 4 or 8 (4 | LBM_FUSED_STAGED with FP16/BF16 storage) and zchunk >= 1");
   if (h->ops->fused_smem(rows) > 227 * 1024)
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;
@@ -1261,7 +1262,8 @@ int batch_tables(lbm_batch *b) {
   for (int s = 0; s < n; s++) {
     lbm_sim *h = b->sims[s];
     for (int p = 0; p < 2; p++) ops->fused_args(h, h->cur ^ p, b->zchunk, &args[(p * n + s) * ab]);
-    grid[s] = make_int3((h->nx + 31) / 32, (h->ny + b->rows - 1) / b->rows,
+    const int rows = shape_rows(b->rows);
+    grid[s] = make_int3((h->nx + 31) / 32, (h->ny + rows - 1) / rows,
                         (h->nz - 2 + b->zchunk - 1) / b->zchunk);
     long long t = (long long)start[s] + (long long)grid[s].x * grid[s].y * grid[s].z;
     if (t > (1LL << 30)) return bfail(b, LBM_ERR_CAPACITY, "too many tiles in one batch");
@@ -1291,7 +1293,7 @@ int batch_tables(lbm_batch *b) {
 int batch_tiles(const lbm_batch *b) {
   long long t = 0;
   for (lbm_sim *h : b->sims)
-    t += (long long)((h->nx + 31) / 32) * ((h->ny + b->rows - 1) / b->rows) *
+    t += (long long)((h->nx + 31) / 32) * ((h->ny + shape_rows(b->rows) - 1) / shape_rows(b->rows)) *
          ((h->nz - 2 + b->zchunk - 1) / b->zchunk);
   return (int)t;
 }
@@ -1350,8 +1352,9 @@ const char *lbm_batch_last_error(const lbm_batch *b) { return b ? b->err.c_str()
 
 int lbm_batch_set_config(lbm_batch *b, int rows, int zchunk) {
   if (!b) return LBM_ERR_ARG;
-  if (!(rows == 2 || rows == 4 || rows == 8) || zchunk < 1)
-    return bfail(b, LBM_ERR_ARG, "rows must be 2, 4 or 8 and zchunk >= 1");
+  if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
+    return bfail(b, LBM_ERR_ARG,
+                 "rows must be 2, 4 or 8 (4 | LBM_FUSED_STAGED with FP16/BF16 storage) and zchunk >= 1");
   b->rows = rows;
   b->zchunk = zchunk;
   return LBM_OK;
@@ -1500,8 +1503,9 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
 
 int lbm_batch_time_fused(lbm_batch *b, int rows, int zchunk, int reps, double *ms) {
   if (!b || !ms || reps < 1) return LBM_ERR_ARG;
-  if (!(rows == 2 || rows == 4 || rows == 8) || zchunk < 1)
-    return bfail(b, LBM_ERR_ARG, "rows must be 2, 4 or 8 and zchunk >= 1");
+  if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
+    return bfail(b, LBM_ERR_ARG,
+                 "rows must be 2, 4 or 8 (4 | LBM_FUSED_STAGED with FP16/BF16 storage) and zchunk >= 1");
   DeviceGuard g(b->device);
   const int keepRows = b->rows, keepZ = b->zchunk;
   b->rows = rows;

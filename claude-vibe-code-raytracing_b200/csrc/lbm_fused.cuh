@@ -66,18 +66,20 @@ constexpr int RING_H_M = 63, RING_H_Z = 65, RING_H_P = 75;  // 2x1, 2x5, 3x1
 constexpr int RING_PLANES = 78;
 
 // Shared memory of one CTA: the post-collision ring, the tags of three planes
-// and, in the STAGE forms, NBUF staging buffers that receive the tile rows' raw
-// populations of a plane by bulk asynchronous copy, plus one mbarrier per
-// buffer and an abort flag.  A 32-cell row starts anywhere inside an 8-cell
-// block, so it spans at most SB = 5 whole blocks.
+// and, in the staged form (STG: FP16/BF16 storage, 4 rows), NBUF staging
+// buffers that receive the tile rows' raw populations of a plane by bulk
+// asynchronous copy, plus one mbarrier per buffer and an abort flag.  A
+// 32-cell row starts anywhere inside an 8-cell block, so it spans at most
+// SB = 5 whole blocks.  The staged form is a tile shape of its own
+// (LBM_FUSED_STAGED), chosen where it measures faster.
 #ifndef LBM_STAGE_NBUF
 #define LBM_STAGE_NBUF 1
 #endif
-template <class PopT, int TY>
+template <class PopT, int TY, bool STG = false>
 struct FusedSmem {
   using Real = typename Prec<PopT>::Real;
   static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;
-  static constexpr bool STAGE = TY == 4 && sizeof(PopT) == 2;
+  static constexpr bool STAGE = STG && TY == 4 && sizeof(PopT) == 2;
   static constexpr int NBUF = LBM_STAGE_NBUF;
   static constexpr int SB = 5;
   static constexpr int ROWF = SB * PopGroups<Q27>::BLOCK, ROWH = SB * PopGroups<Q7>::BLOCK;  // per staged row
@@ -94,9 +96,9 @@ struct FusedSmem {
 
 // CTAs per SM the register budget is sized for (the staged forms are held to
 // 2 (TY = 4) or 3 (TY = 2) CTAs per SM by shared memory)
-template <class PopT, int TY>
+template <class PopT, int TY, bool STG = false>
 struct FusedOcc {
-  static constexpr int blocks = FusedSmem<PopT, TY>::STAGE && FusedSmem<PopT, TY>::NBUF == 2
+  static constexpr int blocks = FusedSmem<PopT, TY, STG>::STAGE && FusedSmem<PopT, TY, STG>::NBUF == 2
                                    ? 2
                                    : (TY >= 8 ? 2 : (TY >= 4 ? 3 : 5));
 };
@@ -305,11 +307,11 @@ struct CellLoad {
 };
 
 // One tile (bx, by) of 32 x TY columns over z-chunk bz of one scene.
-template <class PopT, int TY>
+template <class PopT, int TY, bool STG>
 __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int by, int bz) {
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
-  using SM = FusedSmem<PopT, TY>;
+  using SM = FusedSmem<PopT, TY, STG>;
   using LD = CellLoad<PopT>;
   constexpr int RX = SM::RX, NC = SM::NC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -755,7 +757,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
       Real hn[Q7];
       PopT enc4[4];  // the current group's encoded values, stored as one vector
-      uint32_t solidM = 0;
+      uint32_t orTags = 0;  // OR of the source tags: bit TAG_SOLID set iff a source is SOLID
       static_for<0, Q27>([&](auto KK) {
         constexpr int k = decltype(KK)::value;
         using D = D27<k>;
@@ -770,7 +772,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
         // fluid source: its post-collision value; otherwise halfway bounce-back
         // of the cell's own opposite value (moving-wall term added below)
         const Real fk = ring[sm_at(fl ? sbF + slot27(k) * NC + so : obF + slot27(o) * NC, RING, 14)];
-        solidM |= (uint32_t)(ts == TAG_SOLID) << k;
+        orTags |= ts;
         enc4[k & 3] = C::enc(fk, (Real)D::w);
         if constexpr ((k & 3) == 3 || k == Q27 - 1) {
           if constexpr (k == Q27 - 1) enc4[3] = PopT();  // pad of the last group
@@ -792,7 +794,16 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       // Links to SOLID sources (rare): Ladd moving-wall term
       // 2 w_k rho_phase(phi_old) (e_k . u_s) / cs^2 and the FP64 momentum
       // exchange -(f_opp + f_k) e_k at the solid cell (src/sim.js:517-536).
-      if (solidM) {
+      static_assert(TAG_FLUID == 0 && (TAG_SOLID & TAG_WALL) == 0, "tag bits");
+      if (orTags & TAG_SOLID) {
+        uint32_t solidM = 0;
+#pragma unroll 1
+        for (int k = 1; k < Q27; k++) {
+          const int ez = dcomp(k, 2);
+          const int tb = ez < 0 ? tbM : (ez == 0 ? tbZ : tbP);
+          const int so = -dcomp(k, 1) * RX - dcomp(k, 0);
+          if (stag[sm_at(tb + so, TAGS, 13)] == TAG_SOLID) solidM |= 1u << k;
+        }
         double acc[6] = {0, 0, 0, 0, 0, 0};
         int owner = -1;
         for (uint32_t m = solidM; m; m &= m - 1) {
@@ -882,18 +893,18 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
 }
 
 // One scene: the grid is its tiles.
-template <class PopT, int TY>
-__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY>::blocks)
+template <class PopT, int TY, bool STG>
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks)
     k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
-  fused_tile<PopT, TY>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fused_tile<PopT, TY, STG>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many scenes in one persistent launch: tile w of the batch belongs to the
 // scene s with tileStart[s] <= w < tileStart[s+1]; each scene's descriptor
 // gives its own grid, physics constants and state.  CTAs stride over the
 // tiles, so one launch of about one wave advances every scene by a step.
-template <class PopT, int TY>
-__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY>::blocks)
+template <class PopT, int TY, bool STG>
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks)
     k_fused_batch(const FusedArgs<PopT> *__restrict__ args, const int *__restrict__ tileStart,
                   const int3 *__restrict__ tileGrid, int nscenes) {
   const int total = tileStart[nscenes];
@@ -907,7 +918,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY>::blocks)
     const int3 g = tileGrid[lo];
     const int t = w - tileStart[lo];
     const int bx = t % g.x, by = (t / g.x) % g.y, bz = t / (g.x * g.y);
-    fused_tile<PopT, TY>(args[lo], bx, by, bz);
+    fused_tile<PopT, TY, STG>(args[lo], bx, by, bz);
     __syncthreads();  // the next tile reuses shared memory
   }
 }

@@ -250,20 +250,39 @@ class Ops final : public OpsBase {
     h->launches++;
   }
 
-  template <int TY>
+  // Tile shapes: rows 2, 4, 8, and rows 4 | LBM_FUSED_STAGED (the staged form,
+  // FP16/BF16 storage only).  f(IC<rows>, staged) is called with the shape's
+  // compile-time form.
+  template <class F>
+  static void with_shape(int shape, F &&f) {
+    switch (shape) {
+      case 2: f(IC<2>{}, std::false_type{}); break;
+      case 4: f(IC<4>{}, std::false_type{}); break;
+      case 4 | LBM_FUSED_STAGED:
+        if constexpr (sizeof(PopT) == 2) f(IC<4>{}, std::true_type{});
+        else f(IC<4>{}, std::false_type{});
+        break;
+      default: f(IC<8>{}, std::false_type{}); break;
+    }
+  }
+  bool shape_ok(int shape) const override {
+    return shape == 2 || shape == 4 || shape == 8 || (shape == (4 | LBM_FUSED_STAGED) && sizeof(PopT) == 2);
+  }
+
+  template <int TY, bool STG>
   void launch_fused(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
-    constexpr size_t smem = FusedSmem<PopT, TY>::bytes;
+    constexpr size_t smem = FusedSmem<PopT, TY, STG>::bytes;
     // the shared-memory opt-in is per device
     static unsigned long long attrSet = 0;
     const unsigned long long bit = 1ull << (h->device & 63);
     if (!(attrSet & bit)) {
-      cudaFuncSetAttribute(k_fused_step<PopT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_fused_step<PopT, TY, STG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
       attrSet |= bit;
     }
-    dim3 block(32, FusedSmem<PopT, TY>::warps);  // TY cell warps and two halo warps
+    dim3 block(32, FusedSmem<PopT, TY, STG>::warps);  // TY cell warps and two halo warps
     dim3 grid((h->nx + 31) / 32, (h->ny + TY - 1) / TY, (h->nz - 2 + zchunk - 1) / zchunk);
-    k_fused_step<PopT, TY><<<grid, block, smem, h->stream>>>(a);
+    k_fused_step<PopT, TY, STG><<<grid, block, smem, h->stream>>>(a);
     h->launches++;
   }
 
@@ -292,52 +311,41 @@ class Ops final : public OpsBase {
     FusedArgs<PopT> a = make_args(h, cur, zchunk);
     memcpy(out, &a, sizeof(a));
   }
-  template <int TY>
+  template <int TY, bool STG>
   int batch_ctas(int device) {
-    constexpr size_t smem = FusedSmem<PopT, TY>::bytes;
+    constexpr size_t smem = FusedSmem<PopT, TY, STG>::bytes;
     static unsigned long long attrSet = 0;
     const unsigned long long bit = 1ull << (device & 63);
     if (!(attrSet & bit)) {
-      cudaFuncSetAttribute(k_fused_batch<PopT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_fused_batch<PopT, TY, STG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
       attrSet |= bit;
     }
     int per = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_batch<PopT, TY>,
-                                                  FusedSmem<PopT, TY>::threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_batch<PopT, TY, STG>,
+                                                  FusedSmem<PopT, TY, STG>::threads, smem);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per) * std::max(1, sms);
   }
-  int fused_batch_ctas(int ty, int device) override {
-    switch (ty) {
-      case 2: return batch_ctas<2>(device);
-      case 4: return batch_ctas<4>(device);
-      default: return batch_ctas<8>(device);
-    }
+  int fused_batch_ctas(int shape, int device) override {
+    int r = 0;
+    with_shape(shape, [&](auto T, auto S) { r = batch_ctas<decltype(T)::value, decltype(S)::value>(device); });
+    return r;
   }
-  template <int TY>
-  void batch_launch(const void *d_args, const int *d_tileStart, const int3 *d_tileGrid, int n, int ctas,
-                    cudaStream_t st) {
-    dim3 block(32, FusedSmem<PopT, TY>::warps);
-    k_fused_batch<PopT, TY><<<ctas, block, FusedSmem<PopT, TY>::bytes, st>>>(
-        (const FusedArgs<PopT> *)d_args, d_tileStart, d_tileGrid, n);
-  }
-  void fused_batch(const void *d_args, const int *d_tileStart, const int3 *d_tileGrid, int nscenes, int ty,
+  void fused_batch(const void *d_args, const int *d_tileStart, const int3 *d_tileGrid, int nscenes, int shape,
                    int ctas, cudaStream_t st) override {
-    switch (ty) {
-      case 2: batch_launch<2>(d_args, d_tileStart, d_tileGrid, nscenes, ctas, st); break;
-      case 4: batch_launch<4>(d_args, d_tileStart, d_tileGrid, nscenes, ctas, st); break;
-      default: batch_launch<8>(d_args, d_tileStart, d_tileGrid, nscenes, ctas, st); break;
-    }
+    with_shape(shape, [&](auto T, auto S) {
+      constexpr int TY = decltype(T)::value;
+      constexpr bool STG = decltype(S)::value;
+      dim3 block(32, FusedSmem<PopT, TY, STG>::warps);
+      k_fused_batch<PopT, TY, STG><<<ctas, block, FusedSmem<PopT, TY, STG>::bytes, st>>>(
+          (const FusedArgs<PopT> *)d_args, d_tileStart, d_tileGrid, nscenes);
+    });
   }
 
   void fused_step(lbm_sim *h, const FusedCfg &cfg) override {
     FusedArgs<PopT> a = make_args(h, h->cur, cfg.zchunk);
-    switch (cfg.ty) {
-      case 2: launch_fused<2>(h, a, cfg.zchunk); break;
-      case 4: launch_fused<4>(h, a, cfg.zchunk); break;
-      default: launch_fused<8>(h, a, cfg.zchunk); break;
-    }
+    with_shape(cfg.ty, [&](auto T, auto S) { launch_fused<decltype(T)::value, decltype(S)::value>(h, a, cfg.zchunk); });
   }
 
   cudaError_t read_fault(lbm_sim *h, unsigned long long out[4]) override {
@@ -350,12 +358,10 @@ class Ops final : public OpsBase {
     return cudaMemcpyToSymbol(lbm_fault_word, zero, sizeof(zero));
   }
 
-  size_t fused_smem(int ty) const override {
-    switch (ty) {
-      case 2: return FusedSmem<PopT, 2>::bytes;
-      case 4: return FusedSmem<PopT, 4>::bytes;
-      default: return FusedSmem<PopT, 8>::bytes;
-    }
+  size_t fused_smem(int shape) const override {
+    size_t r = 0;
+    with_shape(shape, [&](auto T, auto S) { r = FusedSmem<PopT, decltype(T)::value, decltype(S)::value>::bytes; });
+    return r;
   }
 
   void pack(lbm_sim *h, uint8_t *d_out) override {

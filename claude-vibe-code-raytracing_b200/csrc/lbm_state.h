@@ -18,9 +18,13 @@ namespace lbm {
 
 // Launch configuration of the fused step kernel.
 struct FusedCfg {
-  int ty = 4;       // cell rows per CTA (CTA = 32 x (ty + 2) threads)
+  int ty = 4;       // tile shape: cell rows per CTA (CTA = 32 x (rows + 2) threads),
+                    // | LBM_FUSED_STAGED for the staged form
   int zchunk = 32;  // z planes marched per CTA
 };
+
+// cell rows per CTA of a tile shape
+inline int shape_rows(int shape) { return shape & 0xff; }
 
 class OpsBase {
  public:
@@ -66,6 +70,8 @@ class OpsBase {
                            int nscenes, int ty, int ctas, cudaStream_t st) = 0;
   // Fault record of the bounds-checked build (all zero otherwise); cleared on read.
   virtual cudaError_t read_fault(lbm_sim *h, unsigned long long out[4]) = 0;
+  // a tile shape this storage form supports (rows 2, 4, 8; 4 | LBM_FUSED_STAGED for FP16/BF16)
+  virtual bool shape_ok(int shape) const = 0;
 };
 
 OpsBase *make_ops_f32();

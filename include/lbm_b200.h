@@ -187,8 +187,8 @@ int lbm_launch_count(const lbm_sim *sim, int64_t *count);
  * (x | y<<8)}, all zero when none. */
 int lbm_checked_build(void);
 int lbm_fault_record(lbm_sim *sim, int64_t out[4]);
-/* Test hook for the bounded waits: while on, the fused kernel's staged forms
- * (FP16/BF16 storage, 4 rows per CTA) do not issue the first plane copy of
+/* Test hook for the bounded waits: while on, the fused kernel's staged form
+ * (rows 4 | LBM_FUSED_STAGED) does not issue the first plane copy of
  * each tile, so that plane's wait runs out (about a second), the step is
  * abandoned and LBM_ERR_TIMEOUT is reported; the fault record then holds
  * location code 90.  No effect on the other forms. */
@@ -200,7 +200,12 @@ int lbm_transfer_bytes(const lbm_sim *sim, uint64_t *h2d, uint64_t *d2h);
  * synchronises the stream and returns the summed kernel time and launch count. */
 int lbm_fused_timing(lbm_sim *sim, int enable);
 int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
-/* Fused-kernel launch shape: rows per CTA (2, 4 or 8) and z planes per CTA. */
+/* Fused-kernel launch shape: rows per CTA (2, 4 or 8) and z planes per CTA.
+ * rows = 4 | LBM_FUSED_STAGED selects the staged form (FP16/BF16 storage
+ * only): each tile row's populations of the next plane arrive in shared
+ * memory by bulk asynchronous copy, waited on with bounded mbarrier waits.
+ * Every shape gives the same results bit for bit. */
+#define LBM_FUSED_STAGED 0x100
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
 
 /* ---- batches: many scenes stepped together ---------------------------------- */

@@ -98,18 +98,19 @@ def test_batch_continues_across_runs_and_configs(gpu):
 
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
 def test_reduced_storage_independent_of_tile_shape(gpu, storage):
-    """Reduced storage has a staged form of the fused kernel at 4 rows per CTA
-    (populations brought in by bulk asynchronous copies) and a plain form at
-    2 and 8 rows; a scene stepped through all three, in a batch, ends bit for
-    bit where the same scene run alone (staged form) ends."""
+    """Reduced storage has a staged form of the fused kernel (4 | STAGED:
+    populations brought in by bulk asynchronous copies) beside the plain 2, 4
+    and 8 row forms; a scene stepped through all of them, in a batch, ends bit
+    for bit where the same scene run alone with the default shape ends."""
     import functools
     SimS = functools.partial(gpu.Sim, storage=storage)
+    shapes = ((8, 16), (4 | 0x100, 32), (2, 7), (4 | 0x100, 5), (4, 9))
     ref = [bld(SimS, gpu.RigidSphere) for bld in BUILDERS]
     for sim, solid in ref:
-        sim.run_coupled(solid, 12)
+        sim.run_coupled(solid, 3 * len(shapes))
     mixed = [bld(SimS, gpu.RigidSphere) for bld in BUILDERS]
     with gpu.Batch(mixed) as batch:
-        for rows, zchunk in ((8, 16), (4, 32), (2, 7), (4, 5)):
+        for rows, zchunk in shapes:
             batch.set_config(rows, zchunk)
             batch.run(3, use_graph=False)
     for i, ((sim, solid), (rsim, rsolid)) in enumerate(zip(mixed, ref)):

@@ -1,13 +1,13 @@
 """Bounded device waits of the fused step.
 
-The staged forms of the fused kernel (FP16/BF16 storage, 4 rows per CTA) wait
-on an mbarrier for each plane's bulk copy.  Every such wait is bounded: when
-it runs out the tile stops, the step is abandoned, the library returns
-LBM_ERR_TIMEOUT and the fault record holds location code 90.  The test makes
-the wait run out by withholding the copy it waits for
-(lbm_test_withhold_stage_copy), so nothing faults or hangs, and then shows the
-handle and the CUDA context still work: the same scene re-initialised steps
-bit for bit like a fresh one.
+The staged form of the fused kernel (FP16/BF16 storage, tile shape
+4 | LBM_FUSED_STAGED) waits on an mbarrier for each plane's bulk copy.  Every
+such wait is bounded: when it runs out the tile stops, the step is abandoned,
+the library returns LBM_ERR_TIMEOUT and the fault record holds location code
+90.  The test makes the wait run out by withholding the copy it waits for
+(lbm_test_withhold_stage_copy), so nothing faults or hangs, and then shows
+the handle and the CUDA context still work: the same scene re-initialised
+steps bit for bit like a fresh one.
 """
 import ctypes as C
 
@@ -19,6 +19,7 @@ import scenes
 pytestmark = pytest.mark.gpu
 
 FAULT_STAGE_WAIT = 90
+STAGED = 0x100
 
 
 @pytest.fixture(scope="module")
@@ -43,7 +44,7 @@ def test_withheld_copy_times_out_and_handle_recovers(gpu, storage):
     sim = _scene(gpu, storage)
     sim._sync()
     h = sim.handle
-    _capi.check(h, L.lbm_set_fused_config(h, 4, 32))
+    _capi.check(h, L.lbm_set_fused_config(h, 4 | STAGED, 32))
     rec = (C.c_int64 * 4)()
     _capi.check(h, L.lbm_fault_record(h, rec))  # clear any earlier record
 
@@ -60,7 +61,7 @@ def test_withheld_copy_times_out_and_handle_recovers(gpu, storage):
     sim.run_coupled(None, 6)
     fresh = _scene(gpu, storage)
     fresh._sync()
-    _capi.check(fresh.handle, L.lbm_set_fused_config(fresh.handle, 4, 32))
+    _capi.check(fresh.handle, L.lbm_set_fused_config(fresh.handle, 4 | STAGED, 32))
     fresh.run_coupled(None, 6)
     for k in ("phi", "rho", "ux", "f", "h"):
         a, b = np.array(getattr(sim, k)), np.array(getattr(fresh, k))
