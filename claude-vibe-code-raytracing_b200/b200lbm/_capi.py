@@ -93,6 +93,10 @@ _SIGS = [
      [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
     ("lbm_pack_volume", C.c_int, [C.c_void_p, C.c_void_p]),
     ("lbm_pack_volume_device", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("lbm_host_alloc", C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
+    ("lbm_pack_volume_async", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("lbm_wait_frames", C.c_int, [C.c_void_p]),
+    ("lbm_host_free", C.c_int, [C.c_void_p]),
     ("lbm_run_coupled", C.c_int,
      [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.c_int, C.c_int, C.c_void_p]),
     ("lbm_synchronize", C.c_int, [C.c_void_p]),

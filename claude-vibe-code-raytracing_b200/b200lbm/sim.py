@@ -25,6 +25,37 @@ from . import _capi
 from ._capi import FIELDS, LbmImpulse, LbmParams, check, lib
 from .solid import impulse_array, spheres_of, to_c_array
 
+
+class _HostBlock:
+    """Owns one lbm_host_alloc block; freed when the last array using it goes."""
+
+    def __init__(self, nbytes):
+        p = C.c_void_p()
+        rc = lib().lbm_host_alloc(nbytes, C.byref(p))
+        if rc != _capi.OK:
+            raise _capi.LbmError(rc, f"lbm_host_alloc({nbytes}) failed")
+        self.ptr = p.value
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().lbm_host_free(C.c_void_p(self.ptr))
+            self.ptr = None
+
+
+def pinned_empty(nbytes):
+    """A uint8 numpy array of nbytes in page-locked host memory."""
+    block = _HostBlock(nbytes)
+    arr = np.ctypeslib.as_array((C.c_uint8 * nbytes).from_address(block.ptr))
+    arr = arr.view(_PinnedArray)
+    arr._block = block  # keeps the memory alive as long as the array (or a view of it)
+    return arr
+
+
+class _PinnedArray(np.ndarray):
+    def __array_finalize__(self, obj):
+        if obj is not None:
+            self._block = getattr(obj, "_block", None)
+
 _PARAM_NAMES = ("tau", "tauPhi", "sigma", "gravity", "rhoL", "rhoG", "W", "mobility")
 # upload order: phi before h (h may be stored relative to phi), tags last
 _UPLOAD_ORDER = ("phi", "rho", "ux", "uy", "uz", "f", "f2", "h", "h2", "usx", "usy", "usz",
@@ -327,6 +358,27 @@ class Sim:
             raise ValueError("packVolume needs a contiguous uint8 buffer of 2*n bytes")
         check(self._h, lib().lbm_pack_volume(self._h, buf.ctypes.data_as(C.c_void_p)))
         return out
+
+    def packVolumeAsync(self, out):
+        """packVolume that returns at once: the frame is copied into `out`
+        (a frameBuffer) while the steps queued after this call run.  `out`
+        holds the frame after waitFrames(); do not read or reuse it before."""
+        self._sync()
+        buf = np.asarray(out).view(np.ndarray)
+        if buf.dtype != np.uint8 or buf.size < self.n * 2 or not buf.flags.c_contiguous:
+            raise ValueError("packVolumeAsync needs a contiguous uint8 buffer of 2*n bytes")
+        check(self._h, lib().lbm_pack_volume_async(self._h, buf.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def waitFrames(self):
+        """Wait until every packVolumeAsync copy has reached its buffer."""
+        check(self._h, lib().lbm_wait_frames(self._h))
+
+    def frameBuffer(self):
+        """A page-locked uint8 buffer of 2*n bytes for packVolume: the
+        device-to-host copy of each frame then runs at full link speed (a
+        pageable numpy buffer goes through driver staging buffers)."""
+        return pinned_empty(self.n * 2)
 
     # ------------------------------------------------------------ extras
     def field64(self, name):

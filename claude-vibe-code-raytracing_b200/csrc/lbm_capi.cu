@@ -412,6 +412,11 @@ void free_all(lbm_sim *h) {
   for (cudaEvent_t e : h->evStop) cudaEventDestroy(e);
   if (h->hOut) cudaFreeHost(h->hOut);
   if (h->hTotals) cudaFreeHost(h->hTotals);
+  if (h->copyStream) cudaStreamSynchronize(h->copyStream);
+  if (h->frameDev) cudaFree(h->frameDev);
+  if (h->evPacked) cudaEventDestroy(h->evPacked);
+  if (h->evCopied) cudaEventDestroy(h->evCopied);
+  if (h->copyStream) cudaStreamDestroy(h->copyStream);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -1038,6 +1043,38 @@ int lbm_pack_volume_device(lbm_sim *h, void *dev_out) {
   return LBM_OK;
 }
 
+int lbm_host_alloc(size_t bytes, void **out) {
+  if (!out || bytes == 0) return LBM_ERR_ARG;
+  *out = nullptr;
+  return cudaMallocHost(out, bytes) == cudaSuccess ? LBM_OK : LBM_ERR_OOM;
+}
+
+int lbm_host_free(void *p) {
+  if (!p) return LBM_OK;
+  return cudaFreeHost(p) == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+}
+
+int lbm_pack_volume_async(lbm_sim *h, uint8_t *host_out) {
+  if (!h || !host_out) return fail(h, LBM_ERR_ARG, "null");
+  DeviceGuard g(h->device);
+  if (!h->copyStream) {
+    CK(cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->evPacked, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->evCopied, cudaEventDisableTiming));
+  }
+  if (!h->frameDev) DALLOC(h->frameDev, (size_t)h->n * 2);
+  // the device frame is reused: the previous copy out of it must be done
+  if (h->copyPending) CK(cudaStreamWaitEvent(h->stream, h->evCopied, 0));
+  h->ops->pack(h, (uint8_t *)h->frameDev);
+  CKL("packVolume");
+  CK(cudaEventRecord(h->evPacked, h->stream));
+  CK(cudaStreamWaitEvent(h->copyStream, h->evPacked, 0));
+  CK(copy_async(h, host_out, h->frameDev, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->copyStream));
+  CK(cudaEventRecord(h->evCopied, h->copyStream));
+  h->copyPending = true;
+  return LBM_OK;
+}
+
 int lbm_pack_volume(lbm_sim *h, uint8_t *host_out) {
   if (!h || !host_out) return fail(h, LBM_ERR_ARG, "null");
   DeviceGuard g(h->device);
@@ -1100,9 +1137,21 @@ int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_ev
   return coupled_finish(h, sp, ns);
 }
 
+int lbm_wait_frames(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  if (h->copyPending) {
+    CK(cudaEventSynchronize(h->evCopied));
+    h->copyPending = false;
+  }
+  return LBM_OK;
+}
+
 int lbm_synchronize(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);
+  int rc = lbm_wait_frames(h);
+  if (rc) return rc;
   return sync_status(h);
 }
 

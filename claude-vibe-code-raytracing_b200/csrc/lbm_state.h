@@ -122,6 +122,13 @@ struct lbm_sim {
   void *staging = nullptr;
   size_t stagingBytes = 0;
   void *image = nullptr;  // rendered RGBA8 frame (lbm_render)
+  // lbm_pack_volume_async: packed frame on the device, copied to the host on
+  // copyStream; evPacked orders the copy after the pack, evCopied the next
+  // pack after the copy
+  void *frameDev = nullptr;
+  cudaStream_t copyStream = nullptr;
+  cudaEvent_t evPacked = nullptr, evCopied = nullptr;
+  bool copyPending = false;
   size_t imageBytes = 0;
   double *dPhiCol = nullptr;
   int *hTotals = nullptr;  // pinned [3]

@@ -152,6 +152,22 @@ int lbm_absorb_dead_cells(lbm_sim *sim, const lbm_sphere *spheres, int nspheres,
 /* Sim.packVolume(out) (src/sim.js:586-600): 2*n bytes, R = (clamp01(phi)*255)|0,
  * G = 255 on SOLID cells. */
 int lbm_pack_volume(lbm_sim *sim, uint8_t *host_out);
+/* Page-locked host memory for the buffers a host reads every frame (packed
+ * volumes, rendered images): device-to-host copies into it run at full link
+ * speed, while a pageable destination is copied through driver staging
+ * buffers at a fraction of that.  No counterpart in the reference (a Web
+ * Worker posts an ArrayBuffer).  Free with lbm_host_free. */
+int lbm_host_alloc(size_t bytes, void **out);
+int lbm_host_free(void *p);
+/* packVolume without waiting: the frame is packed on the handle's stream and
+ * copied to host_out on a separate copy stream, so the copy overlaps the steps
+ * queued after this call.  host_out (2*n bytes, best page-locked) holds the
+ * frame once lbm_wait_frames (or lbm_synchronize) returns; the caller must not
+ * read or reuse it before.  A later call waits on the device for the previous
+ * copy before packing again.  No counterpart in the reference, whose worker
+ * packs synchronously and posts the buffer (src/worker.js:102-111). */
+int lbm_pack_volume_async(lbm_sim *sim, uint8_t *host_out);
+int lbm_wait_frames(lbm_sim *sim);
 /* Same, into device memory, asynchronous on the handle's stream. */
 int lbm_pack_volume_device(lbm_sim *sim, void *device_out);
 
