@@ -66,21 +66,18 @@ constexpr int RING_H_M = 63, RING_H_Z = 65, RING_H_P = 75;  // 2x1, 2x5, 3x1
 constexpr int RING_PLANES = 78;
 
 // Shared memory of one CTA: the post-collision ring, the tags of three planes
-// and, in the staged form (STG: FP16/BF16 storage, 4 rows), NBUF staging
-// buffers that receive the tile rows' raw populations of a plane by bulk
-// asynchronous copy, plus one mbarrier per buffer and an abort flag.  A
+// and, in the staged form (STG: FP16/BF16 storage, 4 rows), a staging buffer
+// that receives the tile rows' raw populations of a plane by bulk
+// asynchronous copy, plus its mbarrier and an abort flag.  A
 // 32-cell row starts anywhere inside an 8-cell block, so it spans at most
 // SB = 5 whole blocks.  The staged form is a tile shape of its own
 // (LBM_FUSED_STAGED), chosen where it measures faster.
-#ifndef LBM_STAGE_NBUF
-#define LBM_STAGE_NBUF 1
-#endif
 template <class PopT, int TY, bool STG = false>
 struct FusedSmem {
   using Real = typename Prec<PopT>::Real;
   static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;
   static constexpr bool STAGE = STG && TY == 4 && sizeof(PopT) == 2;
-  static constexpr int NBUF = LBM_STAGE_NBUF;
+  static constexpr int NBUF = 1;  // the buffer of plane q + 1 is filled while plane q is pulled
   static constexpr int SB = 5;
   static constexpr int ROWF = SB * PopGroups<Q27>::BLOCK, ROWH = SB * PopGroups<Q7>::BLOCK;  // per staged row
   static constexpr size_t ringBytes = (size_t)RING_PLANES * NC * sizeof(Real);
@@ -98,9 +95,7 @@ struct FusedSmem {
 // 2 (TY = 4) or 3 (TY = 2) CTAs per SM by shared memory)
 template <class PopT, int TY, bool STG = false>
 struct FusedOcc {
-  static constexpr int blocks = FusedSmem<PopT, TY, STG>::STAGE && FusedSmem<PopT, TY, STG>::NBUF == 2
-                                   ? 2
-                                   : (TY >= 8 ? 2 : (TY >= 4 ? 3 : 5));
+  static constexpr int blocks = TY >= 8 ? 2 : (TY >= 4 ? 3 : 5);
 };
 
 // ---------------------------------------------------------------- bulk copies
@@ -319,8 +314,6 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   uint8_t *stag = smem_raw + SM::ringBytes;                               // [3][NC]
   constexpr bool STAGE = SM::STAGE;
   constexpr int ROWF = SM::ROWF, ROWH = SM::ROWH, BUF = TY * (ROWF + ROWH), NBUF = SM::NBUF;
-  // with two buffers the halo warps' loads are prefetched into registers too
-  constexpr bool HALO_PF = NBUF == 2;
   PopT *stage = reinterpret_cast<PopT *>(smem_raw + SM::stageOff);        // [2][TY rows F, TY rows H]
   int *abortF = reinterpret_cast<int *>(smem_raw + SM::barOff + 16);
   const uint32_t bar0 = smem_u32(smem_raw + SM::barOff);  // mbarrier of buffer b at bar0 + 8b
@@ -616,21 +609,12 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   // and below the tile (both rows loaded before either is computed); halo
   // warp B the side columns and corners.
   // (lambdas are forced inline: an outlined closure would live in local memory)
-  // STAGE forms: the loads of plane q are issued one plane early (prefetch)
-  // into Lc (cell warps: phi stencil, rho, u, tag; halo warp A: the row above;
-  // halo warp B: its side cell) and Lb (halo warp A: the row below); the cell
-  // warps' populations arrive in the staging buffer.
-  LD Lc, Lb;
+  // Staged form: the cell warps' phi stencil, rho, u and tag of plane q are
+  // loaded one plane early (prefetch) into Lc; their populations arrive in
+  // the staging buffer; the halo warps load as in the plain form.
+  LD Lc;
   auto prefetch = [&](int q) __attribute__((always_inline)) {
-    if (!haloWarp) {
-      load_small(q, x, y, Lc);
-    } else if constexpr (!HALO_PF) {
-    } else if (haloA) {
-      load(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, x, y0 - 1, Lc);
-      load(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, x, y0 + TY, Lb);
-    } else {
-      load(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, x0 - 1 + sideLx, y0 - 1 + sideLy, Lc);
-    }
+    if (!haloWarp) load_small(q, x, y, Lc);
   };
   auto halo_plane = [&](int q) __attribute__((always_inline)) {
     Real d0, d1, d2, d3, d4;
@@ -654,17 +638,8 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     if (!haloWarp) {
       stage_pops(q, Lc);
       compute(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, Lc, ogx, ogy, ogz, olap, ophi);
-    } else if constexpr (!HALO_PF) {
-      halo_plane(q);
-    } else if (haloA) {
-      Real d0, d1, d2, d3, d4;
-      compute(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, tx + 1, Lc, d0, d1, d2, d3, d4);
-      compute(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, (TY + 1) * RX + tx + 1, Lb, d0, d1, d2, d3,
-              d4);
     } else {
-      Real d0, d1, d2, d3, d4;
-      compute(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, sideLy * RX + sideLx, Lc, d0, d1,
-              d2, d3, d4);
+      halo_plane(q);
     }
   };
   auto collide_plane = [&](int q, Real &ogx, Real &ogy, Real &ogz, Real &olap,
@@ -698,9 +673,10 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   }
 
   // Iteration q collides plane q and pulls plane q - 1 (planes zb-1 .. ze are
-  // collided, zb .. ze-1 pulled).  In the STAGE forms the copy of plane q + 2
-  // goes out as soon as plane q's buffer is read, and the register loads of
-  // plane q + 1 right after plane q's collision.
+  // collided, zb .. ze-1 pulled).  In the staged form the copy of plane q + 1
+  // goes out as soon as plane q's buffer is read (after the first barrier),
+  // and the cell warps' register loads of plane q + 1 right after plane q's
+  // collision.
   int q = zb - 1;
   for (; q <= ze; q++) {
     collide_plane(q, gxN, gyN, gzN, lapN, phN);
@@ -881,10 +857,9 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
 
   if constexpr (STAGE) {
     if (q <= ze && producer) {
-      // stopped at plane q: let the copies of planes q .. q + NBUF - 1 land
-      // (bounded) before the buffers are released
+      // stopped at plane q: let the copy of plane q land (bounded) before the
+      // buffer is released (the copy of plane q + 1 was not issued)
       if (!(a.withhold && q == zb - 1)) mbar_wait(bar0 + 8 * (q % NBUF), ((phase >> (q % NBUF)) & 1u) ^ 1u);
-      if (NBUF == 2 && q + 1 <= ze) mbar_wait(bar0 + 8 * ((q + 1) % NBUF), (phase >> ((q + 1) % NBUF)) & 1u);
     }
     __syncthreads();
     if (producer)
@@ -918,7 +893,16 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks
     const int3 g = tileGrid[lo];
     const int t = w - tileStart[lo];
     const int bx = t % g.x, by = (t / g.x) % g.y, bz = t / (g.x * g.y);
-    fused_tile<PopT, TY, STG>(args[lo], bx, by, bz);
+    // the scene's descriptor in shared memory: its fields are re-read there
+    // instead of being held in registers through the tile
+    __shared__ FusedArgs<PopT> sa;
+    constexpr int WORDS = sizeof(FusedArgs<PopT>) / 4;
+    static_assert(sizeof(FusedArgs<PopT>) % 4 == 0, "descriptor copied in words");
+    const int lin = threadIdx.y * blockDim.x + threadIdx.x;
+    if (lin < WORDS)
+      reinterpret_cast<uint32_t *>(&sa)[lin] = reinterpret_cast<const uint32_t *>(args + lo)[lin];
+    __syncthreads();
+    fused_tile<PopT, TY, STG>(sa, bx, by, bz);
     __syncthreads();  // the next tile reuses shared memory
   }
 }
