@@ -47,7 +47,7 @@ struct FusedArgs {
   double om, omP, A, beta4, kappa, rhoG, dRho, gravity, sharpC4;
   const SolidSet *ss;
   int *status;   // set non-zero when a bounded wait of the step runs out
-  int withhold;  // test hook: the staged forms do not issue each tile's first copy
+  int withhold;  // test hook: the staged form does not issue each tile's first copy
 };
 
 // slot of direction k within its e_z group (0..8 for D3Q27)
@@ -91,8 +91,8 @@ struct FusedSmem {
                 "bulk copies move whole 16-byte units");
 };
 
-// CTAs per SM the register budget is sized for (the staged forms are held to
-// 2 (TY = 4) or 3 (TY = 2) CTAs per SM by shared memory)
+// CTAs per SM the register budget is sized for (the staged 4-row form, with
+// its staging buffer beside the ring, still fits 3 per SM)
 template <class PopT, int TY, bool STG = false>
 struct FusedOcc {
   static constexpr int blocks = TY >= 8 ? 2 : (TY >= 4 ? 3 : 5);
@@ -432,7 +432,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     load_small(q, gx_, gy_, L);
   };
 
-  // ---- staging of the tile rows' populations (STAGE forms)
+  // ---- staging of the tile rows' populations (staged form)
   // Row r of plane q covers cells row0 .. row0 + min(31, nx - 1 - x0) of the
   // flat order, i.e. whole blocks (row0 >> 3) .. (last >> 3): one bulk copy
   // for f and one for h, into buffer q & 1.  Rows past the grid are skipped.
