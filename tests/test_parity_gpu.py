@@ -130,13 +130,23 @@ def test_phase_by_phase_matches_oracle(gpu, oracle_mod):
 
 
 def test_sets_bit_exact_with_moving_sphere(gpu, oracle_mod):
-    """The drop preset with the sphere falling through the interface: given the
-    oracle's sphere state every step, the solid mask and the fresh / dead sets
-    match exactly (src/sim.js:214-310, src/solid.js:87-101)."""
+    """The drop preset with the sphere falling through the interface, 400 steps
+    (the length that pins the trajectory, the fresh / dead sets and the
+    impulses): given the oracle's sphere state every step, the solid mask and
+    the fresh / dead sets match exactly (src/sim.js:214-310,
+    src/solid.js:87-101), and each step's momentum exchange plus dead-cell
+    impulse agrees with the oracle's.  F and T are compared per component
+    against the largest |F| (|T|) of the run: the sphere falls on the axis, so
+    Fx, Fz and the torques are near-zero sums whose own relative error is
+    FP32 rounding noise.  Measured: |dF| <= 5.6e-5 max|F|, |dT| <= 2.7e-3
+    max|T|."""
     (o, osol), (g, gsol) = _pair(scenes.drop, gpu, oracle_mod, sigma=0.012, gravity=0.0012)
     moved = 0
     n_fresh = n_dead = 0
-    for s in range(150):
+    F = ("Fx", "Fy", "Fz")
+    T = ("Tx", "Ty", "Tz")
+    fo, fg = [], []
+    for s in range(400):
         _copy_sphere(gsol, osol)
         o.step(osol)
         g.step(gsol)
@@ -148,21 +158,34 @@ def test_sets_bit_exact_with_moving_sphere(gpu, oracle_mod):
         n_fresh += len(ofr)
         n_dead += len(ode)
         osol.absorbDeadCells(o)
+        gsol.absorbDeadCells(g)
+        fo.append([getattr(osol, k) for k in F + T])
+        fg.append([getattr(gsol, k) for k in F + T])
         osol.step(1.0, o.gravity)
+        gsol.step(1.0, g.gravity)  # clears its accumulators; its state is replaced next step
         moved += abs(osol.vy) > 0
     assert moved > 50 and n_fresh > 0 and n_dead > 0
+    fo, fg = np.array(fo), np.array(fg)
+    d = np.abs(fg - fo)
+    assert d[:, :3].max() <= 2e-4 * np.abs(fo[:, :3]).max(), d[:, :3].max(axis=0)
+    assert d[:, 3:].max() <= 1e-2 * np.abs(fo[:, 3:]).max(), d[:, 3:].max(axis=0)
 
 
 def test_drop_trajectory(gpu, oracle_mod):
-    """Free-running drop preset: the sphere trajectory and the fields track the oracle."""
+    """Free-running drop preset, 400 steps: the sphere trajectory and the
+    fields track the oracle (measured: drift <= 3e-6 cells, phi rel-L2 <=
+    1.8e-5)."""
     (o, osol), (g, gsol) = _pair(scenes.drop, gpu, oracle_mod, sigma=0.012, gravity=0.0012)
-    for s in range(120):
+    worst = 0.0
+    cy0 = osol.cy
+    for s in range(400):
         substep(o, osol)
         substep(g, gsol)
-    drift = max(abs(gsol.cx - osol.cx), abs(gsol.cy - osol.cy), abs(gsol.cz - osol.cz))
-    assert drift <= 1e-3, drift
+        worst = max(worst, abs(gsol.cx - osol.cx), abs(gsol.cy - osol.cy), abs(gsol.cz - osol.cz))
+    assert worst <= 2e-5, worst
+    assert osol.cy - cy0 > 3  # the sphere fell through the interface (gravity along +y here)
     rel, _ = field_err(g.phi, o.phi)
-    assert rel <= 1e-3, rel
+    assert rel <= 1e-4, rel
 
 
 def test_impulse_matches_oracle(gpu, oracle_mod):
