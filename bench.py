@@ -55,11 +55,13 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--rows", type=int, default=0)
     ap.add_argument("--zchunk", type=int, default=0)
-    ap.add_argument("--workload", default="scene", choices=["scene", "batch", "serve", "precision", "render"],
+    ap.add_argument("--workload", default="scene",
+                    choices=["scene", "batch", "serve", "precision", "render", "phases"],
                     help="scene: the 256^3 line (default); batch: 64 seeded scenes stepped together; "
                          "serve: a Poisson request stream through the continuous-batching server; "
                          "precision: FP32/FP16/BF16 storage against an FP64 run; "
-                         "render: the raymarcher, 1920x1080 frames of the 256^3 scene")
+                         "render: the raymarcher, 1920x1080 frames of the 256^3 scene; "
+                         "phases: test/bench_phases.mjs, the seven Sim phases timed one by one")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--requests", type=int, default=24)
     return ap.parse_args()
@@ -434,6 +436,84 @@ def run_render(args, dev):
     print(json.dumps(line), flush=True)
 
 
+PHASES = ("retagCells", "handleFreshCells", "computePhiGradients", "collidePhase", "streamPhase",
+          "collideHydro", "streamHydroAndMacro")
+
+
+def _call_phase(sim, sol, name):
+    if name in ("retagCells", "streamHydroAndMacro"):
+        getattr(sim, name)(sol)
+    elif name == "handleFreshCells":
+        sim.handleFreshCells(sol)
+    else:
+        getattr(sim, name)()
+
+
+def run_phases(args, dev):
+    """test/bench_phases.mjs on the device: the seven Sim phases called one by
+    one through the public API (each timed with CUDA events on the handle's
+    stream), after 20 coupled warm-up steps, at the harness's 40x28x40 and at
+    256^3; beside them the fused step (Sim.step) on the same state and, at
+    40x28x40, the oracle's phases on one host thread."""
+    import torch
+
+    import scenes
+    from b200lbm import RigidSphere, Sim
+    from b200lbm._capi import lib
+    from oracle import oracle
+
+    torch.cuda.set_device(dev)
+    out = {}
+    for label, build, reps in (("40x28x40", lambda S, R: scenes.bench(S, R), 80),
+                               (f"{args.size}^3", lambda S, R: scenes.cfg2(S, R, n=args.size), 10)):
+        sim, sol = build(Sim, RigidSphere)
+        for _ in range(20):
+            scenes.substep(sim, sol)
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(lib().lbm_stream(sim.handle))
+        ms = {p: 0.0 for p in PHASES + ("step (fused)",)}
+        for _ in range(reps):
+            for p in PHASES + ("step (fused)",):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                if p == "step (fused)":
+                    sim.step(sol)
+                else:
+                    _call_phase(sim, sol, p)
+                e1.record(stream)
+                e1.synchronize()
+                ms[p] += e0.elapsed_time(e1)
+        per = {p: v / reps for p, v in ms.items()}
+        total = sum(per[p] for p in PHASES)
+        out[label] = {"ms": per, "phases_total_ms": total,
+                      "share": {p: per[p] / total for p in PHASES},
+                      "mlups_phases": sim.n / (total * 1e-3) * 1e-6,
+                      "mlups_fused": sim.n / (per["step (fused)"] * 1e-3) * 1e-6}
+        sim.close()
+    o, osol = scenes.bench(oracle.OracleSim, oracle.OracleSphere)
+    for _ in range(20):
+        scenes.substep(o, osol)
+    cpu = {p: 0.0 for p in PHASES}
+    reps = 10
+    for _ in range(reps):
+        for p in PHASES:
+            t0 = time.perf_counter()
+            _call_phase(o, osol, p)
+            cpu[p] += (time.perf_counter() - t0) * 1e3
+    cpu = {p: v / reps for p, v in cpu.items()}
+    line = {
+        "metric": "per-phase ms of one step (test/bench_phases.mjs breakdown)",
+        "value": out[f"{args.size}^3"]["phases_total_ms"], "unit": "ms per step (seven phases)",
+        "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "test/bench_phases.mjs scene (40x28x40) and the gravity-down pool "
+                               f"{args.size}^3, 20 warm-up ticks, phases called one by one"},
+        "gpu": out,
+        "cpu_baseline": {"ms": cpu, "total_ms": sum(cpu.values()), "cores": 1, "kind": "port",
+                         "sample": f"40x28x40, {reps} repetitions of the seven oracle phases"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
@@ -441,9 +521,10 @@ def main():
         run_reference(args, ws, rank)
         return
     if args.workload != "scene":
-        if args.workload in ("precision", "render"):
+        if args.workload in ("precision", "render", "phases"):
             if rank == 0:
-                {"precision": run_precision, "render": run_render}[args.workload](args, local)
+                {"precision": run_precision, "render": run_render,
+                 "phases": run_phases}[args.workload](args, local)
         else:
             {"batch": run_batch, "serve": run_serve}[args.workload](args, local, ws, rank)
         if ws > 1:
