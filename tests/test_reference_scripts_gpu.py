@@ -1,7 +1,8 @@
 """The reference's own test scripts, run at full length on the CUDA path beside
 the oracle: test/drag_stress.mjs (a sphere dragged along a 700-step path,
 through the interface and back), test/repro_presets.mjs (drop, dam and rise
-presets, 120 steps each) and test/settle.mjs (drop and rise, 1500 steps).
+presets, 120 steps each), test/settle.mjs (drop and rise, 1500 steps) and
+test/sphere_profile.mjs (the smoke scene's vertical phi profile, 80 steps).
 
 Besides the scripts' own checks (finite state, max|u| <= 1), every run is
 compared with the oracle:
@@ -100,3 +101,36 @@ def test_settle(gpu, oracle_mod, preset):
     assert max(abs(gsol.cx - osol.cx), abs(gsol.cz - osol.cz)) <= 0.05
     rel, _ = field_err(g.phi, o.phi)
     assert rel <= 1e-2, rel
+
+
+def _sphere_profile_scene(SimC, SphC):
+    """test/sphere_profile.mjs:5-18: the smoke scene with a sphere r=2, density 1.5 at (6, 3, 6)."""
+    sim = SimC(12, 12, 12)
+    sim.initFlat(6)
+    scenes._params(sim, 0.7, 0.7, 0.012, 0.0012)
+    return sim, SphC(12, 12, 12, cx=6, cy=3, cz=6, r=2.0, density=1.5)
+
+
+def _profile(sim):
+    """What test/sphere_profile.mjs:20-35 prints: the mean phi over the grid and
+    the mean phi of each y layer over the interior x, z."""
+    phi = np.asarray(sim.phi, dtype=np.float64).reshape(sim.nz, sim.ny, sim.nx)
+    return phi.mean(), phi[1:-1, :, 1:-1].mean(axis=(0, 2))
+
+
+def test_sphere_profile(gpu, oracle_mod):
+    """test/sphere_profile.mjs: 80 steps, the profile printed every 10 steps.
+    The printed quantities (2-3 decimals in the script) agree with the oracle's
+    to 1e-5, and the sphere height to 1e-5 cells (the sphere-centre bar of the
+    parity tests)."""
+    o, osol = _sphere_profile_scene(oracle_mod.OracleSim, oracle_mod.OracleSphere)
+    g, gsol = _sphere_profile_scene(gpu.Sim, gpu.RigidSphere)
+    for s in range(1, 81):
+        substep(o, osol)
+        substep(g, gsol)
+        if s % 10 == 0:
+            (oa, oc), (ga, gc) = _profile(o), _profile(g)
+            assert abs(ga - oa) <= 1e-5, (s, ga, oa)
+            assert np.abs(gc - oc).max() <= 1e-5, (s, np.abs(gc - oc).max())
+            assert abs(gsol.cy - osol.cy) <= 1e-5, (s, gsol.cy, osol.cy)
+            assert _finite(g)
