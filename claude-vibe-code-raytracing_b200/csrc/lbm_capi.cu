@@ -578,7 +578,7 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
   h->device = device;
   h->ops = ops;
   h->n = (long long)nx * ny * nz;
-  h->fusedOK = pop_elems(h->n, 27) < (1LL << 31) - 1;
+  h->fusedOK = h->n < (1LL << 31) - 64;  // cell indices are 32-bit in the fused kernel
   h->params = lbm_params{0.6, 0.7, 0.012, 0.0010, 1.0, 0.05, 4.0, 0.02};  // src/sim.js:88-95
   int rc = LBM_OK;
   auto body = [&]() -> int {
@@ -1339,6 +1339,14 @@ int batch_tables(lbm_batch *b) {
   return LBM_OK;
 }
 
+// the batch's shape for a launch: SHAPE_WIDE when any scene needs 64-bit
+// population offsets
+int launch_shape(const lbm_batch *b, int rows) {
+  for (lbm_sim *h : b->sims)
+    if (needs_wide(h->n)) return rows | SHAPE_WIDE;
+  return rows;
+}
+
 int batch_tiles(const lbm_batch *b) {
   long long t = 0;
   for (lbm_sim *h : b->sims)
@@ -1429,7 +1437,7 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
   int rc = batch_tables(b);
   if (rc) return rc;
   const int tiles = batch_tiles(b);
-  const int ctas = std::min(tiles, ops->fused_batch_ctas(b->rows, b->device));
+  const int ctas = std::min(tiles, ops->fused_batch_ctas(launch_shape(b, b->rows), b->device));
   const size_t ab = ops->fused_args_bytes();
 
   // Graph mode replays a captured chunk of 2 steps (the ping-pong halves
@@ -1456,7 +1464,7 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
       BCK(cudaStreamWaitEvent(b->origin, b->joins[s], 0));
     }
     ops->fused_batch((const unsigned char *)b->dArgs + (size_t)parity * n * ab, b->dTileStart, b->dTileGrid,
-                     n, b->rows, ctas, b->origin);
+                     n, launch_shape(b, b->rows), ctas, b->origin);
     BCK(cudaGetLastError());
     BCK(cudaEventRecord(b->fork, b->origin));
     for (int s = 0; s < n; s++) {
@@ -1561,16 +1569,18 @@ int lbm_batch_time_fused(lbm_batch *b, int rows, int zchunk, int reps, double *m
   b->zchunk = zchunk;
   int rc = batch_tables(b);
   OpsBase *ops = b->sims[0]->ops;
-  const int ctas = std::min(batch_tiles(b), ops->fused_batch_ctas(rows, b->device));
+  const int ctas = std::min(batch_tiles(b), ops->fused_batch_ctas(launch_shape(b, rows), b->device));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (rc == LBM_OK) {
     for (lbm_sim *h : b->sims) cudaStreamSynchronize(h->stream);
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    ops->fused_batch(b->dArgs, b->dTileStart, b->dTileGrid, (int)b->sims.size(), rows, ctas, b->origin);
+    ops->fused_batch(b->dArgs, b->dTileStart, b->dTileGrid, (int)b->sims.size(), launch_shape(b, rows), ctas,
+                     b->origin);
     cudaEventRecord(e0, b->origin);
     for (int r = 0; r < reps; r++)
-      ops->fused_batch(b->dArgs, b->dTileStart, b->dTileGrid, (int)b->sims.size(), rows, ctas, b->origin);
+      ops->fused_batch(b->dArgs, b->dTileStart, b->dTileGrid, (int)b->sims.size(), launch_shape(b, rows), ctas,
+                     b->origin);
     cudaEventRecord(e1, b->origin);
     cudaError_t e = cudaEventSynchronize(e1);
     float t = 0;

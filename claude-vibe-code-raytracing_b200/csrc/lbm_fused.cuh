@@ -302,8 +302,11 @@ struct CellLoad {
 };
 
 // One tile (bx, by) of 32 x TY columns over z-chunk bz of one scene.
-template <class PopT, int TY, bool STG>
+// WIDE: 64-bit population offsets, for grids whose populations exceed 2^31
+// elements (more than ~76 M cells); 32-bit offsets otherwise.
+template <class PopT, int TY, bool STG, bool WIDE>
 __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int by, int bz) {
+  using POff = std::conditional_t<WIDE, long long, int>;
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
   using SM = FusedSmem<PopT, TY, STG>;
@@ -405,10 +408,10 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
     const bool inside = gx_ >= 0 && gx_ < nx && gy_ >= 0 && gy_ < ny && q >= 0 && q < nz;
     const int ci = inside ? q * nxny + gy_ * nx + gx_ : 0;
-    const int bF = (ci >> 3) * BLK27 + (ci & 7) * 4;
-    const int bH = (ci >> 3) * BLK7 + (ci & 7) * 4;
+    const POff bF = (POff)(ci >> 3) * BLK27 + (ci & 7) * 4;
+    const POff bH = (POff)(ci >> 3) * BLK7 + (ci & 7) * 4;
     // whole groups of four directions, loaded when any of their directions is needed
-    auto groups = [&](auto QQ, auto NG, const PopT *src, int base, long long lim, int code,
+    auto groups = [&](auto QQ, auto NG, const PopT *src, POff base, long long lim, int code,
                       PopT *dst) __attribute__((always_inline)) {
       constexpr int Q = decltype(QQ)::value;
       static_for<0, decltype(NG)::value>([&](auto GG) {
@@ -693,8 +696,8 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     const int sC = (z + 3) % 3;
     const uint8_t tagI = colActive && z >= zb ? stag[sm_at(sC * NC + own, TAGS, 9)] : TAG_WALL;
     const int i = z * nxny + y * nx + x;
-    const int bF = (i >> 3) * BLK27 + (i & 7) * 4;
-    const int bH = (i >> 3) * BLK7 + (i & 7) * 4;
+    const POff bF = (POff)(i >> 3) * BLK27 + (i & 7) * 4;
+    const POff bH = (POff)(i >> 3) * BLK7 + (i & 7) * 4;
     if (tagI == TAG_SOLID) {
       // Solid cells are not updated; carry their state into the next half so
       // both halves hold the reference's stale values.
@@ -868,17 +871,17 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
 }
 
 // One scene: the grid is its tiles.
-template <class PopT, int TY, bool STG>
+template <class PopT, int TY, bool STG, bool WIDE>
 __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks)
     k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
-  fused_tile<PopT, TY, STG>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fused_tile<PopT, TY, STG, WIDE>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many scenes in one persistent launch: tile w of the batch belongs to the
 // scene s with tileStart[s] <= w < tileStart[s+1]; each scene's descriptor
 // gives its own grid, physics constants and state.  CTAs stride over the
 // tiles, so one launch of about one wave advances every scene by a step.
-template <class PopT, int TY, bool STG>
+template <class PopT, int TY, bool STG, bool WIDE>
 __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks)
     k_fused_batch(const FusedArgs<PopT> *__restrict__ args, const int *__restrict__ tileStart,
                   const int3 *__restrict__ tileGrid, int nscenes) {
@@ -902,7 +905,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks
     if (lin < WORDS)
       reinterpret_cast<uint32_t *>(&sa)[lin] = reinterpret_cast<const uint32_t *>(args + lo)[lin];
     __syncthreads();
-    fused_tile<PopT, TY, STG>(sa, bx, by, bz);
+    fused_tile<PopT, TY, STG, WIDE>(sa, bx, by, bz);
     __syncthreads();  // the next tile reuses shared memory
   }
 }

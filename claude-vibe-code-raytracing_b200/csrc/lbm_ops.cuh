@@ -251,38 +251,44 @@ class Ops final : public OpsBase {
   }
 
   // Tile shapes: rows 2, 4, 8, and rows 4 | LBM_FUSED_STAGED (the staged form,
-  // FP16/BF16 storage only).  f(IC<rows>, staged) is called with the shape's
-  // compile-time form.
+  // FP16/BF16 storage only); SHAPE_WIDE marks a launch over a grid whose
+  // populations need 64-bit offsets.  f(IC<rows>, staged, wide) is called with
+  // the shape's compile-time form.
   template <class F>
   static void with_shape(int shape, F &&f) {
-    switch (shape) {
-      case 2: f(IC<2>{}, std::false_type{}); break;
-      case 4: f(IC<4>{}, std::false_type{}); break;
+    const bool wide = (shape & SHAPE_WIDE) != 0;
+    auto go = [&](auto T, auto S) {
+      if (wide) f(T, S, std::true_type{});
+      else f(T, S, std::false_type{});
+    };
+    switch (shape & ~SHAPE_WIDE) {
+      case 2: go(IC<2>{}, std::false_type{}); break;
+      case 4: go(IC<4>{}, std::false_type{}); break;
       case 4 | LBM_FUSED_STAGED:
-        if constexpr (sizeof(PopT) == 2) f(IC<4>{}, std::true_type{});
-        else f(IC<4>{}, std::false_type{});
+        if constexpr (sizeof(PopT) == 2) go(IC<4>{}, std::true_type{});
+        else go(IC<4>{}, std::false_type{});
         break;
-      default: f(IC<8>{}, std::false_type{}); break;
+      default: go(IC<8>{}, std::false_type{}); break;
     }
   }
   bool shape_ok(int shape) const override {
     return shape == 2 || shape == 4 || shape == 8 || (shape == (4 | LBM_FUSED_STAGED) && sizeof(PopT) == 2);
   }
 
-  template <int TY, bool STG>
+  template <int TY, bool STG, bool WIDE>
   void launch_fused(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
     constexpr size_t smem = FusedSmem<PopT, TY, STG>::bytes;
     // the shared-memory opt-in is per device
     static unsigned long long attrSet = 0;
     const unsigned long long bit = 1ull << (h->device & 63);
     if (!(attrSet & bit)) {
-      cudaFuncSetAttribute(k_fused_step<PopT, TY, STG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_fused_step<PopT, TY, STG, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
       attrSet |= bit;
     }
     dim3 block(32, FusedSmem<PopT, TY, STG>::warps);  // TY cell warps and two halo warps
     dim3 grid((h->nx + 31) / 32, (h->ny + TY - 1) / TY, (h->nz - 2 + zchunk - 1) / zchunk);
-    k_fused_step<PopT, TY, STG><<<grid, block, smem, h->stream>>>(a);
+    k_fused_step<PopT, TY, STG, WIDE><<<grid, block, smem, h->stream>>>(a);
     h->launches++;
   }
 
@@ -311,41 +317,46 @@ class Ops final : public OpsBase {
     FusedArgs<PopT> a = make_args(h, cur, zchunk);
     memcpy(out, &a, sizeof(a));
   }
-  template <int TY, bool STG>
+  template <int TY, bool STG, bool WIDE>
   int batch_ctas(int device) {
     constexpr size_t smem = FusedSmem<PopT, TY, STG>::bytes;
     static unsigned long long attrSet = 0;
     const unsigned long long bit = 1ull << (device & 63);
     if (!(attrSet & bit)) {
-      cudaFuncSetAttribute(k_fused_batch<PopT, TY, STG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_fused_batch<PopT, TY, STG, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
       attrSet |= bit;
     }
     int per = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_batch<PopT, TY, STG>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_batch<PopT, TY, STG, WIDE>,
                                                   FusedSmem<PopT, TY, STG>::threads, smem);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per) * std::max(1, sms);
   }
   int fused_batch_ctas(int shape, int device) override {
     int r = 0;
-    with_shape(shape, [&](auto T, auto S) { r = batch_ctas<decltype(T)::value, decltype(S)::value>(device); });
+    with_shape(shape, [&](auto T, auto S, auto W) {
+      r = batch_ctas<decltype(T)::value, decltype(S)::value, decltype(W)::value>(device);
+    });
     return r;
   }
   void fused_batch(const void *d_args, const int *d_tileStart, const int3 *d_tileGrid, int nscenes, int shape,
                    int ctas, cudaStream_t st) override {
-    with_shape(shape, [&](auto T, auto S) {
+    with_shape(shape, [&](auto T, auto S, auto W) {
       constexpr int TY = decltype(T)::value;
       constexpr bool STG = decltype(S)::value;
       dim3 block(32, FusedSmem<PopT, TY, STG>::warps);
-      k_fused_batch<PopT, TY, STG><<<ctas, block, FusedSmem<PopT, TY, STG>::bytes, st>>>(
+      k_fused_batch<PopT, TY, STG, decltype(W)::value><<<ctas, block, FusedSmem<PopT, TY, STG>::bytes, st>>>(
           (const FusedArgs<PopT> *)d_args, d_tileStart, d_tileGrid, nscenes);
     });
   }
 
   void fused_step(lbm_sim *h, const FusedCfg &cfg) override {
     FusedArgs<PopT> a = make_args(h, h->cur, cfg.zchunk);
-    with_shape(cfg.ty, [&](auto T, auto S) { launch_fused<decltype(T)::value, decltype(S)::value>(h, a, cfg.zchunk); });
+    const int shape = cfg.ty | (needs_wide(h->n) ? SHAPE_WIDE : 0);
+    with_shape(shape, [&](auto T, auto S, auto W) {
+      launch_fused<decltype(T)::value, decltype(S)::value, decltype(W)::value>(h, a, cfg.zchunk);
+    });
   }
 
   cudaError_t read_fault(lbm_sim *h, unsigned long long out[4]) override {
@@ -360,7 +371,7 @@ class Ops final : public OpsBase {
 
   size_t fused_smem(int shape) const override {
     size_t r = 0;
-    with_shape(shape, [&](auto T, auto S) { r = FusedSmem<PopT, decltype(T)::value, decltype(S)::value>::bytes; });
+    with_shape(shape, [&](auto T, auto S, auto) { r = FusedSmem<PopT, decltype(T)::value, decltype(S)::value>::bytes; });
     return r;
   }
 

@@ -25,6 +25,10 @@ struct FusedCfg {
 
 // cell rows per CTA of a tile shape
 inline int shape_rows(int shape) { return shape & 0xff; }
+// internal shape bit: the launch covers a grid whose D3Q27 populations exceed
+// 2^31 elements, so the fused kernel uses 64-bit population offsets
+constexpr int SHAPE_WIDE = 0x200;
+inline bool needs_wide(long long cells) { return pop_elems(cells, 27) >= (1LL << 31) - 64; }
 
 class OpsBase {
  public:
