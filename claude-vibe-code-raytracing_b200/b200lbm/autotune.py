@@ -87,5 +87,53 @@ def tune(batch, dims, storage, reps=3, candidates=None, force=False):
     return rows, zchunk, timings
 
 
+_pending: dict = {}  # signature -> {shape: ms} timed so far by Incremental
+
+
+class Incremental:
+    """The same choice as tune(), spread over several calls: each step() times
+    one candidate shape on the live batch, so a serving loop that calls it once
+    per tick never holds one tick's frames for the whole candidate list.  The
+    timings of a signature accumulate across batches (a serving loop builds a
+    new batch whenever its members change); once every candidate has been
+    timed the fastest is set and cached under the signature, as tune() would.
+    Until then the batch keeps its current shape.  A signature already in the
+    cache is applied at once."""
+
+    def __init__(self, batch, dims, storage, reps=3, candidates=None):
+        _load()
+        self.batch = batch
+        self.key = signature(dims, storage)
+        self.reps = reps
+        self.candidates = list(candidates or candidates_for(storage))
+        self.done = False
+        if self.key in _cache:
+            batch.set_config(*_cache[self.key])
+            self.done = True
+
+    def step(self):
+        """Time the next untimed candidate; returns True once the shape is chosen and set."""
+        if self.done:
+            return True
+        if self.key in _cache:  # finished meanwhile by another batch of the same signature
+            self.batch.set_config(*_cache[self.key])
+            self.done = True
+            return True
+        timings = _pending.setdefault(self.key, {})
+        todo = [c for c in self.candidates if c not in timings]
+        if todo:
+            rows, zchunk = todo[0]
+            timings[(rows, zchunk)] = self.batch.time_fused(rows, zchunk, reps=self.reps)
+        if all(c in timings for c in self.candidates):
+            best = min(self.candidates, key=timings.get)
+            _cache[self.key] = list(best)
+            _pending.pop(self.key, None)
+            _save()
+            self.batch.set_config(*best)
+            self.done = True
+        return self.done
+
+
 def clear():
     _cache.clear()
+    _pending.clear()

@@ -107,6 +107,7 @@ class Server:
         used = 0
         batch = None
         members = None
+        tuner = None
         ttff, interval, done_at = [], [], {}
         scene_steps = cell_steps = 0
         max_active = 0
@@ -149,13 +150,15 @@ class Server:
                         batch.close()
                     batch = Batch([(a["sim"], a["solid"]) for a in active])
                     members = ids
-                    tuned = False
+                    tuner = None
                 frames = batch.run(tick, frame_every=every, use_graph=self.use_graph)
                 ticks += 1
-                if self.tune and not tuned:
-                    autotune.tune(batch, [(a["sim"].nx, a["sim"].ny, a["sim"].nz) for a in active],
-                                  self.storage)
-                    tuned = True
+                if self.tune:
+                    # one candidate tile shape per tick: no tick waits for the whole list
+                    if tuner is None:
+                        tuner = autotune.Incremental(
+                            batch, [(a["sim"].nx, a["sim"].ny, a["sim"].nz) for a in active], self.storage)
+                    tuner.step()
                 t = time.perf_counter() - t0
                 for a, fr in zip(active, frames):
                     for j in range(fr.shape[0]):

@@ -59,3 +59,49 @@ def test_autotune_signature_buckets():
     assert a == b
     assert autotune.signature([(64, 64, 64)] * 5, "f16") != a
     assert autotune.signature([(64, 64, 64)] * 3, "f32") != a
+
+
+class _FakeBatch:
+    """time_fused returns a fixed time per shape; set_config records the shape."""
+
+    def __init__(self, times):
+        self.times = times
+        self.timed = []
+        self.shape = None
+
+    def time_fused(self, rows, zchunk, reps=3):
+        self.timed.append((rows, zchunk))
+        return self.times[(rows, zchunk)]
+
+    def set_config(self, rows, zchunk):
+        self.shape = (rows, zchunk)
+
+
+def test_incremental_tuner_times_one_candidate_per_step():
+    autotune.clear()
+    cands = [(4, 32), (4, 16), (8, 16)]
+    times = {(4, 32): 7.1, (4, 16): 6.9, (8, 16): 7.5}
+    b = _FakeBatch(times)
+    t = autotune.Incremental(b, [(64, 64, 64)] * 3, "f16", candidates=cands)
+    assert not t.done and b.shape is None
+    assert t.step() is False and b.timed == [(4, 32)] and b.shape is None
+    assert t.step() is False and len(b.timed) == 2
+    assert t.step() is True and b.shape == (4, 16)  # the fastest, set after the last candidate
+    assert t.step() is True and len(b.timed) == 3   # nothing more is timed
+    # timings of one signature accumulate across batches (members changed)
+    autotune.clear()
+    b4, b5 = _FakeBatch(times), _FakeBatch(times)
+    t4 = autotune.Incremental(b4, [(64, 64, 64)] * 3, "f16", candidates=cands)
+    t4.step()
+    t5 = autotune.Incremental(b5, [(62, 64, 64)] * 4, "f16", candidates=cands)
+    assert t5.step() is False and b5.timed == [(4, 16)]
+    assert t5.step() is True and b5.shape == (4, 16) and b5.timed == [(4, 16), (8, 16)]
+    assert t4.step() is True and b4.shape == (4, 16) and b4.timed == [(4, 32)]
+    # the same signature later is answered from the cache at once, like tune()
+    b2 = _FakeBatch(times)
+    t2 = autotune.Incremental(b2, [(60, 64, 64)] * 4, "f16", candidates=cands)
+    assert t2.done and b2.shape == (4, 16) and b2.timed == []
+    b3 = _FakeBatch(times)
+    assert autotune.tune(b3, [(64, 64, 64)] * 3, "f16", candidates=cands)[:2] == (4, 16)
+    assert b3.timed == []
+    autotune.clear()
