@@ -6,8 +6,9 @@
 //   1. plane z+1 is collided: every cell thread loads its cell's 27 + 7
 //      populations, phi stencil, rho and u, evaluates the reference's BGK
 //      collisions (collideHydro src/sim.js:406-464, collidePhase
-//      src/sim.js:324-364) in registers and writes the post-collision values
-//      into a shared-memory ring; meanwhile the halo warps collide the
+//      src/sim.js:324-364) in registers and, after a barrier that ends the
+//      previous plane's pull, writes the post-collision values into a
+//      shared-memory ring; meanwhile the halo warps collide the
 //      one-cell in-plane halo, only for the directions that point into the
 //      tile (halo warp A: the rows above and below, halo warp B: the side
 //      columns and corners);
@@ -301,6 +302,18 @@ struct CellLoad {
   uint8_t tg;
 };
 
+// What the collision of one cell puts into the shared-memory ring: its
+// post-collision populations and its tag.  Halo warp A's two cells (the rows
+// above and below the tile) share one: their direction sets (e_y = +1 and
+// e_y = -1) are disjoint, and the lower row's tag goes to tg2.
+template <class PopT>
+struct CellOut {
+  using Real = typename Prec<PopT>::Real;
+  Real f[Q27];
+  Real h[Q7];
+  uint8_t tg, tg2;
+};
+
 // One tile (bx, by) of 32 x TY columns over z-chunk bz of one scene.
 // WIDE: 64-bit population offsets, for grids whose populations exceed 2^31
 // elements (more than ~76 M cells); 32-bit offsets otherwise.
@@ -311,6 +324,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   using C = Codec<PopT>;
   using SM = FusedSmem<PopT, TY, STG>;
   using LD = CellLoad<PopT>;
+  using CO = CellOut<PopT>;
   constexpr int RX = SM::RX, NC = SM::NC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real *ring = reinterpret_cast<Real *>(smem_raw);                        // [78][NC]
@@ -501,18 +515,40 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     });
   };
 
-  // Compute phase: collision into ring cell lc of plane q and the cell's tag.
-  // Values computed for non-fluid cells land in ring slots that are never
-  // read as sources.  Returns gradient, laplacian and phi of the cell.
-  auto compute = [&](auto MODEc, auto SXc, auto SYc, int sx, int sy, bool active, int q, int lc,
-                     const LD &L, Real &ogx, Real &ogy, Real &ogz, Real &olap,
-                     Real &ophi) __attribute__((always_inline)) {
+  // Emit phase: the collided values and the tag of a cell into ring cell lc of
+  // plane q.  Values computed for non-fluid cells land in ring slots that are
+  // never read as sources.
+  auto emit = [&](auto MODEc, auto SXc, auto SYc, int sx, int sy, bool active, int q, int lc,
+                  const CO &o) __attribute__((always_inline)) {
     constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
     const int fbM = (RING_F_M + (q & 1) * 9) * NC + lc, fbZ = (RING_F_Z + (q & 1) * 9) * NC + lc;
     const int fbP = (RING_F_P + (q % 3) * 9) * NC + lc;
     const int hbM = (RING_H_M + (q & 1)) * NC + lc, hbZ = (RING_H_Z + (q & 1) * 5) * NC + lc;
     const int hbP = (RING_H_P + (q % 3)) * NC + lc;
-    if (MODE != 2 || active) stag[sm_at((q % 3) * NC + lc, TAGS, 2)] = L.tg;
+    if (MODE != 2 || active) stag[sm_at((q % 3) * NC + lc, TAGS, 2)] = (MODE == 1 && SY < 0) ? o.tg2 : o.tg;
+    static_for<0, Q27>([&](auto KK) {
+      constexpr int k = decltype(KK)::value;
+      using D = D27<k>;
+      constexpr int ez = D::ez;
+      if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
+        const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
+        const int fb = ez < 0 ? fbM : (ez == 0 ? fbZ : fbP);
+        if (nd) ring[sm_at(fb + slot27(k) * NC, RING, 7)] = o.f[k];
+        if constexpr (k < Q7) {
+          const int hb = ez < 0 ? hbM : (ez == 0 ? hbZ : hbP);
+          if (nd) ring[sm_at(hb + (ez == 0 ? k : 0) * NC, RING, 8)] = o.h[k];
+        }
+      }
+    });
+  };
+
+  // Compute phase: the collision of one cell into registers (o), for emit.
+  // Returns gradient, laplacian and phi of the cell.
+  auto compute = [&](auto MODEc, auto SXc, auto SYc, const LD &L, CO &o, Real &ogx, Real &ogy, Real &ogz, Real &olap,
+                     Real &ophi) __attribute__((always_inline)) {
+    constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
+    if constexpr (MODE == 1 && SY < 0) o.tg2 = L.tg;
+    else o.tg = L.tg;
     // Every operation below rounds explicitly (rmul / radd / rsub / rfma), so a
     // tile cell and a halo cell of another tile get the same bits whatever the
     // compiler would contract in either context.
@@ -562,12 +598,10 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       using D = D27<k>;
       constexpr int ex = D::ex, ey = D::ey, ez = D::ez;
       if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
-        const bool nd = needs(MODEc, SXc, SYc, KK, sx, sy, active);
         const Real ev = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Vx, Vy, Vz);
         const Real eu = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, ux, uy, uz);
         const Real eq = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Qx, Qy, Qz);
         const Real w = (Real)D::w;
-        const int fb = ez < 0 ? fbM : (ez == 0 ? fbZ : fbP);
         // f*_k = (1 - w) f_k + (w_k T + w_k e.V) with T = (e.u)(e.Q) + C0.  The
         // opposite direction has the same T and the negated w_k e.V, exactly
         // (every negation is exact), so a tile cell evaluates opposite pairs
@@ -575,19 +609,13 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
         // cell evaluating one direction alone gets.
         if constexpr (MODE == 0 && k > 0) {
           if constexpr (k & 1) {
-            using O = D27<D::opp>;
             const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
-            const Real fk = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
-            const Real fo = rfma(om1, C::dec(L.fv[D::opp], w), rsub(wT, wev));
-            constexpr int fbo = O::ez < 0 ? 0 : (O::ez == 0 ? 1 : 2);
-            const int fbO = fbo == 0 ? fbM : (fbo == 1 ? fbZ : fbP);
-            ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
-            ring[sm_at(fbO + slot27(D::opp) * NC, RING, 7)] = fo;
+            o.f[k] = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
+            o.f[D::opp] = rfma(om1, C::dec(L.fv[D::opp], w), rsub(wT, wev));
           }
         } else {
           const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
-          const Real fk = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
-          if (nd) ring[sm_at(fb + slot27(k) * NC, RING, 7)] = fk;
+          o.f[k] = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
         }
         if constexpr (k < Q7) {
           const Real w7 = (Real)D7<k>::w;
@@ -595,9 +623,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
           const Real ed = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Dx, Dy, Dz);
           Real href = 0;
           if constexpr (C::offset) href = rmul(w7, p);
-          const Real hk = rfma(omP1, C::dec(L.hv[k], href), rmul(w7, k == 0 ? D0 : radd(D0, ed)));
-          const int hb = ez < 0 ? hbM : (ez == 0 ? hbZ : hbP);
-          if (nd) ring[sm_at(hb + (ez == 0 ? k : 0) * NC, RING, 8)] = hk;
+          o.h[k] = rfma(omP1, C::dec(L.hv[k], href), rmul(w7, k == 0 ? D0 : radd(D0, ed)));
         }
       }
     });
@@ -619,42 +645,53 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   auto prefetch = [&](int q) __attribute__((always_inline)) {
     if (!haloWarp) load_small(q, x, y, Lc);
   };
-  auto halo_plane = [&](int q) __attribute__((always_inline)) {
+  auto halo_plane = [&](int q, CO &o) __attribute__((always_inline)) {
     Real d0, d1, d2, d3, d4;
     if (haloA) {
       LD top, bot;
       load(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, x, y0 - 1, top);
       load(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, x, y0 + TY, bot);
-      compute(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, tx + 1, top, d0, d1, d2, d3, d4);
-      compute(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, (TY + 1) * RX + tx + 1, bot, d0, d1, d2, d3,
-              d4);
+      compute(IC<1>{}, IC<0>{}, IC<1>{}, top, o, d0, d1, d2, d3, d4);
+      compute(IC<1>{}, IC<0>{}, IC<-1>{}, bot, o, d0, d1, d2, d3, d4);
     } else {
       LD L;
       load(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, x0 - 1 + sideLx, y0 - 1 + sideLy, L);
-      compute(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, sideLy * RX + sideLx, L, d0, d1,
-              d2, d3, d4);
+      compute(IC<2>{}, IC<0>{}, IC<0>{}, L, o, d0, d1, d2, d3, d4);
     }
   };
-  auto collide_staged = [&](int q, Real &ogx, Real &ogy, Real &ogz, Real &olap,
+  auto collide_staged = [&](int q, CO &o, Real &ogx, Real &ogy, Real &ogz, Real &olap,
                             Real &ophi) __attribute__((always_inline)) {
     stage_wait(q);
     if (!haloWarp) {
       stage_pops(q, Lc);
-      compute(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, Lc, ogx, ogy, ogz, olap, ophi);
+      compute(IC<0>{}, IC<0>{}, IC<0>{}, Lc, o, ogx, ogy, ogz, olap, ophi);
     } else {
-      halo_plane(q);
+      halo_plane(q, o);
     }
   };
-  auto collide_plane = [&](int q, Real &ogx, Real &ogy, Real &ogz, Real &olap,
+  // collide plane q into registers (o: a cell warp's cell, halo warp A's two
+  // rows, halo warp B's side cell) ...
+  auto collide_plane = [&](int q, CO &o, Real &ogx, Real &ogy, Real &ogz, Real &olap,
                            Real &ophi) __attribute__((always_inline)) {
     if constexpr (STAGE) {
-      collide_staged(q, ogx, ogy, ogz, olap, ophi);
+      collide_staged(q, o, ogx, ogy, ogz, olap, ophi);
     } else if (!haloWarp) {
       LD L;
       load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
-      compute(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, L, ogx, ogy, ogz, olap, ophi);
+      compute(IC<0>{}, IC<0>{}, IC<0>{}, L, o, ogx, ogy, ogz, olap, ophi);
     } else {
-      halo_plane(q);
+      halo_plane(q, o);
+    }
+  };
+  // ... and from registers into the ring
+  auto emit_plane = [&](int q, const CO &o) __attribute__((always_inline)) {
+    if (!haloWarp) {
+      emit(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, own, o);
+    } else if (haloA) {
+      emit(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, tx + 1, o);
+      emit(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, (TY + 1) * RX + tx + 1, o);
+    } else {
+      emit(IC<2>{}, IC<0>{}, IC<0>{}, sideSx, sideSy, sideAct, q, sideLy * RX + sideLx, o);
     }
   };
 
@@ -676,15 +713,26 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   }
 
   // Iteration q collides plane q and pulls plane q - 1 (planes zb-1 .. ze are
-  // collided, zb .. ze-1 pulled).  In the staged form the copy of plane q + 1
+  // collided, zb .. ze-1 pulled).  Plain form: load and collide plane q into
+  // registers, barrier (every warp has pulled plane q - 2), write the ring,
+  // barrier, pull plane q - 1.  Staged form: collide into the ring, barrier,
+  // pull, barrier.  In the staged form the copy of plane q + 1
   // goes out as soon as plane q's buffer is read (after the first barrier),
   // and the cell warps' register loads of plane q + 1 right after plane q's
   // collision.
   int q = zb - 1;
   for (; q <= ze; q++) {
-    collide_plane(q, gxN, gyN, gzN, lapN, phN);
+    CO o;
+    collide_plane(q, o, gxN, gyN, gzN, lapN, phN);
     if constexpr (STAGE) {
+      emit_plane(q, o);
       if (q < ze) prefetch(q + 1);
+    } else {
+      // plane q's slots of the ring are free once every warp has pulled
+      // plane q - 2; a warp that gets here early has its loads and collision
+      // of plane q behind it
+      __syncthreads();
+      emit_plane(q, o);
     }
     __syncthreads();
     if constexpr (STAGE) {
@@ -850,7 +898,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       st_at(s.uy[nxt], i, nCell, 18, uyn);
       st_at(s.uz[nxt], i, nCell, 18, uzn);
     }
-    __syncthreads();
+    if constexpr (STAGE) __syncthreads();
     gxC = gxN;
     gyC = gyN;
     gzC = gzN;
