@@ -228,6 +228,15 @@ class Sim:
     def _moved(self):
         self.__dict__["_version"] += 1
 
+    def _completed(self, rc, apply):
+        """After a call that steps: the device state moved; the results are
+        applied when the steps completed (also when the NaN watchdog then
+        reported a non-finite field), and a non-zero status raises."""
+        self._moved()
+        if rc in (_capi.OK, _capi.ERR_NAN):
+            apply()
+        check(self._h, rc)
+
     # ------------------------------------------------------------ reference API
     def idx(self, x, y, z):
         return ((z * self.ny) + y) * self.nx + x
@@ -285,10 +294,8 @@ class Sim:
         self._sync()
         arr = to_c_array(sp)
         out = impulse_array(len(sp))
-        check(self._h, lib().lbm_stream_hydro_and_macro(self._h, arr, len(sp), out))
-        self._moved()
-        for i, b in enumerate(sp):
-            b.add_impulse(out[i])
+        rc = lib().lbm_stream_hydro_and_macro(self._h, arr, len(sp), out)
+        self._completed(rc, lambda: [b.add_impulse(out[i]) for i, b in enumerate(sp)])
 
     def step(self, solid):
         """src/sim.js:202-210, as one fused device step."""
@@ -296,10 +303,8 @@ class Sim:
         self._sync()
         arr = to_c_array(sp)
         out = impulse_array(len(sp))
-        check(self._h, lib().lbm_step(self._h, arr, len(sp), out))
-        self._moved()
-        for i, b in enumerate(sp):
-            b.add_impulse(out[i])
+        rc = lib().lbm_step(self._h, arr, len(sp), out)
+        self._completed(rc, lambda: [b.add_impulse(out[i]) for i, b in enumerate(sp)])
 
     def render(self, solid=None, width=640, height=480, camera=None):
         """Renderer.uploadVolume + draw (src/render.js:431-434, 484-513) without
@@ -330,11 +335,8 @@ class Sim:
         nfr = nsteps // frame_every if frame_every > 0 else 0
         frames = np.empty((nfr, 2 * self.n), dtype=np.uint8) if nfr else None
         ptr = frames.ctypes.data_as(C.POINTER(C.c_uint8)) if nfr else None
-        check(self._h, lib().lbm_run_coupled(self._h, arr, len(sp), nsteps,
-                                             frame_every if nfr else 0, ptr))
-        self._moved()
-        for i, b in enumerate(sp):
-            b.from_c(arr[i])
+        rc = lib().lbm_run_coupled(self._h, arr, len(sp), nsteps, frame_every if nfr else 0, ptr)
+        self._completed(rc, lambda: [b.from_c(arr[i]) for i, b in enumerate(sp)])
         return frames
 
     def _absorb_dead(self, spheres):
@@ -391,6 +393,13 @@ class Sim:
 
     def synchronize(self):
         check(self._h, lib().lbm_synchronize(self._h))
+
+    def setNanWatchdog(self, every):
+        """Scan phi, rho and u for NaN/Inf after every `every` completed steps and
+        raise LbmError (code ERR_NAN) naming the first such cell; 0 (the
+        default) turns the scan off, as in the reference, where a blow-up only
+        shows as NaN in the fields."""
+        check(self._h, lib().lbm_set_nan_watchdog(self._h, int(every)))
 
     def last_sets(self):
         """(fresh, dead) cell index arrays found at the last retag, scan order."""

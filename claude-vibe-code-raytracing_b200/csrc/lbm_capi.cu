@@ -311,6 +311,28 @@ int sync_status(lbm_sim *h) {
   return LBM_OK;
 }
 
+// NaN/Inf watchdog, opt-in (the reference lets a blow-up show as NaN in the
+// fields): once watchEvery steps have completed since the last scan, the
+// current phi, rho and u are scanned and a non-finite value fails the call.
+int watch_after(lbm_sim *h, long long steps) {
+  if (h->watchEvery <= 0) return LBM_OK;
+  h->watchSteps += steps;
+  if (h->watchSteps < h->watchEvery) return LBM_OK;
+  h->watchSteps = 0;
+  if (!h->dWatch) DALLOC(h->dWatch, sizeof(unsigned long long));
+  CK(cudaMemsetAsync(h->dWatch, 0xFF, sizeof(unsigned long long), h->stream));
+  h->ops->watch_finite(h, h->dWatch);
+  CKL("NaN watchdog");
+  unsigned long long first = 0;
+  CK(copy_async(h, &first, h->dWatch, sizeof first, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (first == ~0ull) return LBM_OK;
+  const long long i = (long long)first, nxny = (long long)h->nx * h->ny;
+  return fail(h, LBM_ERR_NAN,
+              "non-finite phi, rho or u at cell " + std::to_string(i) + " (x " + std::to_string(i % h->nx) +
+                  ", y " + std::to_string((i / h->nx) % h->ny) + ", z " + std::to_string(i / nxny) + ")");
+}
+
 int fetch_out(lbm_sim *h, const double *d_src, int ns, lbm_impulse *out) {
   if (!out || ns == 0) return LBM_OK;
   CK(copy_async(h, h->hOut, d_src, (size_t)ns * 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -402,7 +424,7 @@ void free_all(lbm_sim *h) {
   void *ptrs[] = {h->F[0], h->F[1], h->H[0], h->H[1], h->tag, h->tagPrev, h->grad[0], h->grad[1],
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
                   h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
-                  h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan};
+                  h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan, h->dWatch};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int c = 0; c < 2; c++)
@@ -973,7 +995,8 @@ int lbm_stream_hydro_and_macro(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_imp
     h->bfActive = false;
   }
   if ((rc = reduce_impulses(h, h->dOut))) return rc;
-  return fetch_out(h, h->dOut, ns, out);
+  if ((rc = fetch_out(h, h->dOut, ns, out))) return rc;
+  return watch_after(h, 1);
 }
 
 int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
@@ -1017,7 +1040,8 @@ int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   if ((rc = reduce_impulses(h, h->dOut))) return rc;
   h->cur = 1 - h->cur;
   shift_boxes(h, now);
-  return fetch_out(h, h->dOut, ns, out);
+  if ((rc = fetch_out(h, h->dOut, ns, out))) return rc;
+  return watch_after(h, 1);
 }
 
 int lbm_absorb_dead_cells(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
@@ -1134,7 +1158,8 @@ int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_ev
       frame++;
     }
   }
-  return coupled_finish(h, sp, ns);
+  if ((rc = coupled_finish(h, sp, ns))) return rc;
+  return watch_after(h, nsteps);
 }
 
 int lbm_wait_frames(lbm_sim *h) {
@@ -1153,6 +1178,14 @@ int lbm_synchronize(lbm_sim *h) {
   int rc = lbm_wait_frames(h);
   if (rc) return rc;
   return sync_status(h);
+}
+
+int lbm_set_nan_watchdog(lbm_sim *h, int every) {
+  if (!h) return LBM_ERR_ARG;
+  if (every < 0) return fail(h, LBM_ERR_ARG, "every must be >= 0 (0 turns the watchdog off)");
+  h->watchEvery = every;
+  h->watchSteps = 0;
+  return LBM_OK;
 }
 
 int lbm_test_withhold_stage_copy(lbm_sim *h, int on) {
@@ -1555,6 +1588,7 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
   BCK(cudaStreamSynchronize(b->origin));
   for (int s = 0; s < n; s++)
     BSIM(b->sims[s], coupled_finish(b->sims[s], nspheres[s] ? spheres[s] : nullptr, nspheres[s]));
+  for (int s = 0; s < n; s++) BSIM(b->sims[s], watch_after(b->sims[s], nsteps));
   return LBM_OK;
 }
 

@@ -769,4 +769,25 @@ __global__ void k_pack(Scene<PopT, typename Prec<PopT>::Real> s, int cur, uint8_
   reinterpret_cast<uchar2 *>(out)[i] = o;
 }
 
+// NaN/Inf watchdog: the lowest index of a cell whose phi, rho or u is not
+// finite is min-ed into *first, which the caller sets to ~0 beforehand (rho
+// alone would not do: rho = sum f > 0.01 ? sum f : 0.01 turns a NaN sum into
+// 0.01, src/sim.js:546).  The loop strides by whole blocks, so every warp
+// takes the same trips and one lane per warp that sees such a cell does the
+// atomic.
+template <class PopT>
+__global__ void k_watch_finite(Scene<PopT, typename Prec<PopT>::Real> s, int cur, unsigned long long *first) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < s.n; i0 += stride) {
+    const long long i = i0 + threadIdx.x;
+    bool bad = false;
+    if (i < s.n)
+      bad = !isfinite((double)s.phi[cur][i]) || !isfinite((double)s.rho[cur][i]) ||
+            !isfinite((double)s.ux[cur][i]) || !isfinite((double)s.uy[cur][i]) ||
+            !isfinite((double)s.uz[cur][i]);
+    const unsigned m = __ballot_sync(0xffffffffu, bad);
+    if (m && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicMin(first, (unsigned long long)i);
+  }
+}
+
 }  // namespace lbm

@@ -379,6 +379,11 @@ class Ops final : public OpsBase {
     k_pack<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur, d_out);
     h->launches++;
   }
+  void watch_finite(lbm_sim *h, unsigned long long *d_first) override {
+    k_watch_finite<PopT><<<std::min(nblocks(h->n, 256), 148u * 8u), 256, 0, h->stream>>>(scene(h), h->cur,
+                                                                                        d_first);
+    h->launches++;
+  }
   void upload_pops(lbm_sim *h, bool isH, int half, const float *d_aos, long long c0,
                    long long cells) override {
     k_aos_to_soa<PopT><<<nblocks(cells, 256), 256, 0, h->stream>>>(scene(h), isH ? 1 : 0, half,

@@ -50,6 +50,7 @@ class OpsBase {
   virtual void absorb_dead(lbm_sim *h, double *d_out) = 0;
   virtual void fused_step(lbm_sim *h, const FusedCfg &cfg) = 0;
   virtual void pack(lbm_sim *h, uint8_t *d_out) = 0;
+  virtual void watch_finite(lbm_sim *h, unsigned long long *d_first) = 0;
   // Reference-layout float32 <-> device storage for population fields.
   // half: 0 = both halves (current state), 1 = [cur], 2 = [1-cur].
   virtual void upload_pops(lbm_sim *h, bool isH, int half, const float *d_aos, long long c0,
@@ -136,6 +137,10 @@ struct lbm_sim {
   size_t imageBytes = 0;
   double *dPhiCol = nullptr;
   int *hTotals = nullptr;  // pinned [3]
+  // NaN/Inf watchdog (lbm_set_nan_watchdog): off while watchEvery is 0
+  int watchEvery = 0;
+  long long watchSteps = 0;            // steps completed since the last scan
+  unsigned long long *dWatch = nullptr;  // device: lowest non-finite cell index
 
   lbm::Box boxLast{{1, 1, 1}, {0, 0, 0}};
   lbm::Box boxLastLast{{1, 1, 1}, {0, 0, 0}};

@@ -185,6 +185,17 @@ int lbm_run_coupled(lbm_sim *sim, lbm_sphere *spheres, int nspheres, int nsteps,
  * usable, e.g. after lbm_init_flat).  lbm_step, lbm_run_coupled,
  * lbm_absorb_dead_cells and lbm_batch_run report the same when they return. */
 int lbm_synchronize(lbm_sim *sim);
+/* NaN/Inf watchdog, off by default (every = 0): the reference lets a
+ * numerical blow-up show as NaN in the fields and raises nothing.  With
+ * every > 0, once every steps have completed since the last scan, the call
+ * that completed them (lbm_step, lbm_stream_hydro_and_macro, lbm_run_coupled
+ * at its end, lbm_batch_run at its end, for each of its scenes) scans the
+ * current phi, rho and u (one extra pass, 20 B per cell at FP32) and returns
+ * LBM_ERR_NAN when one is NaN or infinite; lbm_last_error names the lowest
+ * such cell.  The step itself has completed: its fields stay as computed.
+ * Replaces nothing in the reference; the status code is listed with the
+ * other error codes above. */
+int lbm_set_nan_watchdog(lbm_sim *sim, int every);
 /* CUDA stream of the handle (cudaStream_t), for callers that enqueue around it. */
 void *lbm_stream(lbm_sim *sim);
 

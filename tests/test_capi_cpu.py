@@ -54,3 +54,9 @@ def test_product_path_fails_loudly_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(_capi, "_lib", None)
     with pytest.raises(ImportError):
         _capi.lib()
+
+
+def test_nan_watchdog_argument_checks():
+    from b200lbm import _capi
+    L = _capi.lib()
+    assert L.lbm_set_nan_watchdog(None, 1) == _capi.ERR_ARG
