@@ -245,11 +245,12 @@ int launch_compaction(lbm_sim *h, long long maxChunks) {
   }
   int rc = ensure_counts(h, maxChunks);
   if (rc) return rc;
-  k_compact_count<<<(unsigned)maxChunks, COMPACT_THREADS, 0, h->stream>>>(h->tag, h->tagPrev, h->nx,
-                                                                            h->ny, h->dPlan, h->counts);
+  const unsigned ctas = (unsigned)std::min<long long>(maxChunks, SWEEP_CTAS);
+  k_compact_count<<<ctas, COMPACT_THREADS, 0, h->stream>>>(h->tag, h->tagPrev, h->nx, h->ny, h->dPlan,
+                                                           h->counts);
   k_compact_scan<<<1, 1024, 0, h->stream>>>(h->counts, h->dPlan, h->totals);
-  k_compact_emit<<<(unsigned)maxChunks, COMPACT_THREADS, 0, h->stream>>>(
-      h->tag, h->tagPrev, h->nx, h->ny, h->dPlan, h->counts, h->fresh, h->dead, (int)h->listCap);
+  k_compact_emit<<<ctas, COMPACT_THREADS, 0, h->stream>>>(h->tag, h->tagPrev, h->nx, h->ny, h->dPlan,
+                                                          h->counts, h->fresh, h->dead, (int)h->listCap);
   h->launches += 3;
   CKL("fresh/dead compaction");
   h->listsValid = true;

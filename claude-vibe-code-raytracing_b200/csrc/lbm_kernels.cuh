@@ -372,26 +372,32 @@ template <class PopT>
 __global__ void k_retag_box(Scene<PopT, typename Prec<PopT>::Real> s, const Plan *__restrict__ P) {
   const SolidSet &ss = P->ss;
   const Box bx = P->U;
-  long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  int dx = bx.hi[0] - bx.lo[0] + 1, dy = bx.hi[1] - bx.lo[1] + 1, dz = bx.hi[2] - bx.lo[2] + 1;
-  if (l >= (long long)dx * dy * dz) return;
-  int x = bx.lo[0] + (int)(l % dx);
-  int y = bx.lo[1] + (int)((l / dx) % dy);
-  int z = bx.lo[2] + (int)(l / ((long long)dx * dy));
-  long long i = cell_index(x, y, z, s.nx, s.ny);
-  uint8_t old = s.tag[i];
-  s.tagPrev[i] = old;
-  if (x == 0 || x == s.nx - 1 || y == 0 || y == s.ny - 1 || z == 0 || z == s.nz - 1) {
-    s.tag[i] = TAG_WALL;
-    return;
+  const int dx = bx.hi[0] - bx.lo[0] + 1, dy = bx.hi[1] - bx.lo[1] + 1, dz = bx.hi[2] - bx.lo[2] + 1;
+  const long long total = (long long)dx * dy * dz;
+  // grid-stride over the box the plan holds (launches are sized for the
+  // largest box the step may plan, which can be far larger)
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < total;
+       l += (long long)gridDim.x * blockDim.x) {
+    const int x = bx.lo[0] + (int)(l % dx);
+    const int y = bx.lo[1] + (int)((l / dx) % dy);
+    const int z = bx.lo[2] + (int)(l / ((long long)dx * dy));
+    const long long i = cell_index(x, y, z, s.nx, s.ny);
+    s.tagPrev[i] = s.tag[i];
+    if (x == 0 || x == s.nx - 1 || y == 0 || y == s.ny - 1 || z == 0 || z == s.nz - 1)
+      s.tag[i] = TAG_WALL;
+    else
+      s.tag[i] = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) >= 0 ? TAG_SOLID : TAG_FLUID;
   }
-  s.tag[i] = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) >= 0 ? TAG_SOLID : TAG_FLUID;
 }
 
 // Count fresh (FLUID, was SOLID) and dead (SOLID, was FLUID) cells per chunk
 // of the box's linear (scan) order.
 constexpr int COMPACT_CHUNK = 2048;
 constexpr int COMPACT_THREADS = 256;
+// Most CTAs a box sweep (retag, compaction) launches: the kernels stride over
+// the box or its chunks, so a step whose planned box is small does not pay
+// for the empty CTAs of a launch sized for the largest possible box.
+constexpr unsigned SWEEP_CTAS = 148 * 4;
 
 __device__ __forceinline__ void box_cell(const Box &bx, long long l, int &x, int &y, int &z) {
   int dx = bx.hi[0] - bx.lo[0] + 1, dy = bx.hi[1] - bx.lo[1] + 1;
@@ -405,35 +411,39 @@ static __global__ void k_compact_count(const uint8_t *tag, const uint8_t *tagPre
   __shared__ int sf[COMPACT_THREADS / 32], sd[COMPACT_THREADS / 32];
   const Box bx = P->U;
   const long long total = P->ucells;
-  if ((int)blockIdx.x >= P->nchunks) return;
-  long long base = (long long)blockIdx.x * COMPACT_CHUNK;
-  int nf = 0, nd = 0;
-  for (int j = threadIdx.x; j < COMPACT_CHUNK; j += blockDim.x) {
-    long long l = base + j;
-    if (l >= total) break;
-    int x, y, z;
-    box_cell(bx, l, x, y, z);
-    long long i = cell_index(x, y, z, nx, ny);
-    uint8_t t = tag[i], p = tagPrev[i];
-    nf += (t == TAG_FLUID && p == TAG_SOLID);
-    nd += (t == TAG_SOLID && p == TAG_FLUID);
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    nf += __shfl_xor_sync(0xffffffffu, nf, o);
-    nd += __shfl_xor_sync(0xffffffffu, nd, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sf[threadIdx.x >> 5] = nf;
-    sd[threadIdx.x >> 5] = nd;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int a = 0, b = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
-      a += sf[w];
-      b += sd[w];
+  const int nchunks = P->nchunks;
+  // CTAs stride over the chunks (block-uniform trip count)
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const long long base = (long long)c * COMPACT_CHUNK;
+    int nf = 0, nd = 0;
+    for (int j = threadIdx.x; j < COMPACT_CHUNK; j += blockDim.x) {
+      long long l = base + j;
+      if (l >= total) break;
+      int x, y, z;
+      box_cell(bx, l, x, y, z);
+      long long i = cell_index(x, y, z, nx, ny);
+      uint8_t t = tag[i], p = tagPrev[i];
+      nf += (t == TAG_FLUID && p == TAG_SOLID);
+      nd += (t == TAG_SOLID && p == TAG_FLUID);
     }
-    counts[blockIdx.x] = make_int2(a, b);
+    for (int o = 16; o > 0; o >>= 1) {
+      nf += __shfl_xor_sync(0xffffffffu, nf, o);
+      nd += __shfl_xor_sync(0xffffffffu, nd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      sf[threadIdx.x >> 5] = nf;
+      sd[threadIdx.x >> 5] = nd;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int a = 0, b = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+        a += sf[w];
+        b += sd[w];
+      }
+      counts[c] = make_int2(a, b);
+    }
+    __syncthreads();  // sf / sd are rewritten for the next chunk
   }
 }
 
@@ -479,57 +489,61 @@ static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev
   __shared__ int runF, runD;
   const Box bx = P->U;
   const long long total = P->ucells;
-  if ((int)blockIdx.x >= P->nchunks) return;
-  long long base = (long long)blockIdx.x * COMPACT_CHUNK;
-  if (threadIdx.x == 0) {
-    runF = offsets[blockIdx.x].x;
-    runD = offsets[blockIdx.x].y;
-  }
-  __syncthreads();
+  const int nchunks = P->nchunks;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int j0 = 0; j0 < COMPACT_CHUNK; j0 += blockDim.x) {
-    long long l = base + j0 + threadIdx.x;
-    bool isF = false, isD = false;
-    long long i = 0;
-    if (l < total && j0 + (int)threadIdx.x < COMPACT_CHUNK) {
-      int x, y, z;
-      box_cell(bx, l, x, y, z);
-      i = cell_index(x, y, z, nx, ny);
-      uint8_t t = tag[i], p = tagPrev[i];
-      isF = (t == TAG_FLUID && p == TAG_SOLID);
-      isD = (t == TAG_SOLID && p == TAG_FLUID);
-    }
-    unsigned bf = __ballot_sync(0xffffffffu, isF), bd = __ballot_sync(0xffffffffu, isD);
-    if (lane == 0) {
-      wf[warp] = __popc(bf);
-      wd[warp] = __popc(bd);
-    }
-    __syncthreads();
-    int offF = runF, offD = runD;
-    for (int w = 0; w < warp; w++) {
-      offF += wf[w];
-      offD += wd[w];
-    }
-    unsigned below = (1u << lane) - 1u;
-    if (isF) {
-      int pos = offF + __popc(bf & below);
-      if (pos < cap) fresh[pos] = (int)i;
-    }
-    if (isD) {
-      int pos = offD + __popc(bd & below);
-      if (pos < cap) dead[pos] = (int)i;
-    }
-    __syncthreads();
+  // CTAs stride over the chunks (block-uniform trip count); the inner loop
+  // ends on a barrier, so runF / runD are free to be reset for the next chunk
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const long long base = (long long)c * COMPACT_CHUNK;
     if (threadIdx.x == 0) {
-      int a = 0, b = 0;
-      for (int w = 0; w < nw; w++) {
-        a += wf[w];
-        b += wd[w];
-      }
-      runF += a;
-      runD += b;
+      runF = offsets[c].x;
+      runD = offsets[c].y;
     }
     __syncthreads();
+    for (int j0 = 0; j0 < COMPACT_CHUNK; j0 += blockDim.x) {
+      long long l = base + j0 + threadIdx.x;
+      bool isF = false, isD = false;
+      long long i = 0;
+      if (l < total && j0 + (int)threadIdx.x < COMPACT_CHUNK) {
+        int x, y, z;
+        box_cell(bx, l, x, y, z);
+        i = cell_index(x, y, z, nx, ny);
+        uint8_t t = tag[i], p = tagPrev[i];
+        isF = (t == TAG_FLUID && p == TAG_SOLID);
+        isD = (t == TAG_SOLID && p == TAG_FLUID);
+      }
+      unsigned bf = __ballot_sync(0xffffffffu, isF), bd = __ballot_sync(0xffffffffu, isD);
+      if (lane == 0) {
+        wf[warp] = __popc(bf);
+        wd[warp] = __popc(bd);
+      }
+      __syncthreads();
+      int offF = runF, offD = runD;
+      for (int w = 0; w < warp; w++) {
+        offF += wf[w];
+        offD += wd[w];
+      }
+      unsigned below = (1u << lane) - 1u;
+      if (isF) {
+        int pos = offF + __popc(bf & below);
+        if (pos < cap) fresh[pos] = (int)i;
+      }
+      if (isD) {
+        int pos = offD + __popc(bd & below);
+        if (pos < cap) dead[pos] = (int)i;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int a = 0, b = 0;
+        for (int w = 0; w < nw; w++) {
+          a += wf[w];
+          b += wd[w];
+        }
+        runF += a;
+        runD += b;
+      }
+      __syncthreads();
+    }
   }
 }
 

@@ -233,7 +233,7 @@ class Ops final : public OpsBase {
   }
   void retag_box(lbm_sim *h, long long maxCells) override {
     if (maxCells <= 0) return;
-    k_retag_box<PopT><<<nblocks(maxCells, 256), 256, 0, h->stream>>>(scene(h), h->dPlan);
+    k_retag_box<PopT><<<std::min(nblocks(maxCells, 256), SWEEP_CTAS), 256, 0, h->stream>>>(scene(h), h->dPlan);
     h->launches++;
   }
   void fresh_fill(lbm_sim *h) override {
