@@ -101,23 +101,37 @@ __device__ __forceinline__ double rfma(double a, double b, double c) { return __
 template <class S>
 struct Codec;
 
+// enc4: one cell's group of four values at once, element for element what
+// enc gives (the 16-bit forms convert pairs with one packing conversion, each
+// element rounded to nearest even as by the scalar conversion).
 template <>
 struct Codec<float> {
   static constexpr bool offset = false;
   __device__ __forceinline__ static float dec(float v, float) { return v; }
   __device__ __forceinline__ static float enc(float v, float) { return v; }
+  __device__ __forceinline__ static void enc4(const float (&v)[4], const float (&)[4], float (&o)[4]) {
+    o[0] = v[0], o[1] = v[1], o[2] = v[2], o[3] = v[3];
+  }
 };
 template <>
 struct Codec<double> {
   static constexpr bool offset = false;
   __device__ __forceinline__ static double dec(double v, double) { return v; }
   __device__ __forceinline__ static double enc(double v, double) { return v; }
+  __device__ __forceinline__ static void enc4(const double (&v)[4], const double (&)[4], double (&o)[4]) {
+    o[0] = v[0], o[1] = v[1], o[2] = v[2], o[3] = v[3];
+  }
 };
 template <>
 struct Codec<__half> {
   static constexpr bool offset = true;
   __device__ __forceinline__ static float dec(__half v, float ref) { return __fadd_rn(__half2float(v), ref); }
   __device__ __forceinline__ static __half enc(float v, float ref) { return __float2half_rn(__fsub_rn(v, ref)); }
+  __device__ __forceinline__ static void enc4(const float (&v)[4], const float (&r)[4], __half (&o)[4]) {
+    const __half2 a = __floats2half2_rn(__fsub_rn(v[0], r[0]), __fsub_rn(v[1], r[1]));
+    const __half2 b = __floats2half2_rn(__fsub_rn(v[2], r[2]), __fsub_rn(v[3], r[3]));
+    o[0] = __low2half(a), o[1] = __high2half(a), o[2] = __low2half(b), o[3] = __high2half(b);
+  }
 };
 template <>
 struct Codec<__nv_bfloat16> {
@@ -127,6 +141,12 @@ struct Codec<__nv_bfloat16> {
   }
   __device__ __forceinline__ static __nv_bfloat16 enc(float v, float ref) {
     return __float2bfloat16_rn(__fsub_rn(v, ref));
+  }
+  __device__ __forceinline__ static void enc4(const float (&v)[4], const float (&r)[4],
+                                              __nv_bfloat16 (&o)[4]) {
+    const __nv_bfloat162 a = __floats2bfloat162_rn(__fsub_rn(v[0], r[0]), __fsub_rn(v[1], r[1]));
+    const __nv_bfloat162 b = __floats2bfloat162_rn(__fsub_rn(v[2], r[2]), __fsub_rn(v[3], r[3]));
+    o[0] = __low2bfloat16(a), o[1] = __high2bfloat16(a), o[2] = __low2bfloat16(b), o[3] = __high2bfloat16(b);
   }
 };
 

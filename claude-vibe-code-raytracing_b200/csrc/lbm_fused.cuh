@@ -783,7 +783,8 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       const Real rhoPhOld = rfma(phC, dRho, rhoG);
       Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
       Real hn[Q7];
-      PopT enc4[4];  // the current group's encoded values, stored as one vector
+      Real val4[4], ref4[4];  // the current group's values and offsets, encoded and stored as one vector
+      PopT enc4[4];
       uint32_t orTags = 0;  // OR of the source tags: bit TAG_SOLID set iff a source is SOLID
       static_for<0, Q27>([&](auto KK) {
         constexpr int k = decltype(KK)::value;
@@ -800,9 +801,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
         // of the cell's own opposite value (moving-wall term added below)
         const Real fk = ring[sm_at(fl ? sbF + slot27(k) * NC + so : obF + slot27(o) * NC, RING, 14)];
         orTags |= ts;
-        enc4[k & 3] = C::enc(fk, (Real)D::w);
+        val4[k & 3] = fk;
+        ref4[k & 3] = (Real)D::w;
         if constexpr ((k & 3) == 3 || k == Q27 - 1) {
-          if constexpr (k == Q27 - 1) enc4[3] = PopT();  // pad of the last group
+          if constexpr (k == Q27 - 1) val4[3] = ref4[3] = 0;  // pad of the last group: encodes to +0
+          C::enc4(val4, ref4, enc4);
           st4_at(Fn, bF + pofs(k & ~3), nF, 15, enc4);
         }
         rhoA += fk;
@@ -869,9 +872,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       const Real p = hsum < (Real)0 ? (Real)0 : hsum > (Real)1 ? (Real)1 : hsum;
       static_for<0, Q7>([&](auto KK) {
         constexpr int k = decltype(KK)::value;
-        enc4[k & 3] = C::enc(hn[k], (Real)D7<k>::w * p);
+        val4[k & 3] = hn[k];
+        ref4[k & 3] = (Real)D7<k>::w * p;
         if constexpr ((k & 3) == 3 || k == Q7 - 1) {
-          if constexpr (k == Q7 - 1) enc4[3] = PopT();
+          if constexpr (k == Q7 - 1) val4[3] = ref4[3] = 0;
+          C::enc4(val4, ref4, enc4);
           st4_at(Hn, bH + pofs(k & ~3), nH, 17, enc4);
         }
       });
