@@ -518,7 +518,9 @@ int coupled_pre(lbm_sim *h, const CoupledCtx &c) {
   if (rc) return rc;
   h->ops->fresh_fill(h);
   if (c.ns > 0) {
-    k_zero_targets<<<148 * 4, 256, 0, h->stream>>>(h->dPlan, h->impAcc);
+    // sized for the most slots the plan can use (small spheres need few CTAs)
+    const unsigned zc = std::min(nblocks((long long)c.ns * c.slotCells * 6, 256), SWEEP_CTAS);
+    k_zero_targets<<<zc, 256, 0, h->stream>>>(h->dPlan, h->impAcc);
     h->launches++;
   }
   CKL("coupled step (before the fused kernel)");
