@@ -165,6 +165,13 @@ def ncu_traffic(size, storage):
         return None
 
 
+def scene_config(size, storage, ws):
+    """The workload description both arms (this library and --impl reference) print."""
+    return {"workload": f"gravity-down pool {size}^3 with a density-2 sphere r={24 * size // 256}",
+            "grid": [size] * 3, "storage": storage, "parallelism": f"replicas x{ws}",
+            "l2": "state > 126 MB L2, no flush needed"}
+
+
 def cpu_baseline(size, steps, threads=None):
     """The oracle (CPU restatement of src/sim.js + src/solid.js) on the same scene,
     OpenMP over the host's cores; `steps` timed steps after one warm-up."""
@@ -194,7 +201,8 @@ def run_reference(args, ws, rank):
     threads = os.cpu_count()
     sim, sol = scenes.cfg2(oracle.OracleSim, oracle.OracleSphere, n=size)
     sim.set_threads(threads)
-    for _ in range(max(1, min(args.warmup, 2))):
+    warm = max(1, min(args.warmup, 2))  # a CPU step of the full scene takes seconds
+    for _ in range(warm):
         scenes.substep(sim, sol)
     t0 = time.perf_counter()
     done = 0
@@ -207,11 +215,10 @@ def run_reference(args, ws, rank):
     v = size ** 3 / dt * 1e-6
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": done, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "steps": done, "warmup": warm, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 math, f32 storage",
         "data": "synthetic",
-        "config": {"workload": f"gravity-down pool {size}^3, sphere r={24 * size // 256}",
-                   "grid": [size] * 3, "storage": "f32", "l2": "state > L2, no flush"},
+        "config": scene_config(size, "f32", args.gpus),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{done} of {args.steps} steps of the {size}^3 scene "
                                    f"(bounded to ~{budget_s:.0f} s), CPU restatement of the "
@@ -638,10 +645,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
-            "config": {"workload": f"gravity-down pool {size}^3 with a density-2 sphere r={24 * size // 256}",
-                       "grid": [size] * 3, "storage": args.storage, "parallelism": f"replicas x{ws}",
-                       "l2": "state 5.3 GB > 126 MB L2, no flush needed",
-                       "fused_rows": args.rows or 4, "zchunk": args.zchunk or 32},
+            "config": scene_config(size, args.storage, ws),
+            "tile": {"fused_rows": args.rows or 4, "zchunk": args.zchunk or 32},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,

@@ -15,7 +15,8 @@ sample for the 40x28x40 scenes (keeps the files small; the oracle must match
 the digests bit for bit, the GPU compares against the samples).
 
 Usage (needs the reference sources; runs in about three minutes):
-    python tests/golden/make_golden.py [--ref /root/reference] [--only smoke ...]
+    python tests/golden/make_golden.py --ref <reference checkout> [--only smoke ...]
+(or set LBM_REFERENCE_DIR to the reference checkout instead of --ref).
 """
 import argparse
 import array
@@ -79,9 +80,12 @@ def reference_classes(ns):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("LBM_REFERENCE_DIR"),
+                    help="root of the reference checkout (holds src/sim.js); default $LBM_REFERENCE_DIR")
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give --ref <reference checkout> or set LBM_REFERENCE_DIR")
     ns = load_reference(args.ref)
     SimC, SphC, built = reference_classes(ns)
 

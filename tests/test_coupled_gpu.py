@@ -1,0 +1,218 @@
+"""Parity of the device-resident worker tick (Sim.run_coupled -> lbm_run_coupled:
+the device step plan k_plan, the fused step, the impulse reductions, the
+dead-cell sweep and the FP64 RigidSphere.step k_sphere_step, src/worker.js:96-100)
+against the oracle's tick (Sim.step, RigidSphere.absorbDeadCells,
+RigidSphere.step; src/sim.js:202-210, src/solid.js:87-210).  This is the path
+bench.py times.
+
+Two kinds of run:
+  * given state: before every step the GPU sphere takes the oracle's state, so
+    the solid mask, the fresh / dead sets (exact) and the sphere state after the
+    device integrator (within FP32 force noise) are compared step by step;
+  * free running: the GPU trajectory and fields are compared with the oracle's
+    after the whole run, and one long lbm_run_coupled call is compared bit for
+    bit with the same steps taken one call at a time.
+
+Scenes: the drop preset (src/worker.js:23-53; the sphere falls through the
+interface), test/drag_stress.mjs (the drag-spring branch of src/solid.js:118-131),
+a 'kick' scene (gravity 0, which takes the `gravity || 0.001` fallback of
+src/solid.js:141; the speed cap of :159-164, rotation and damping of :177-192
+and the wall clamp of :199-205), and the 256^3 benchmark scene at reduced and
+full size.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import scenes
+from scenes import field_err, substep
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("cx", "cy", "cz", "vx", "vy", "vz", "wx", "wy", "wz")
+# sphere state after one tick from identical inputs: the device integrator sees
+# the FP32 path's momentum exchange (|dF| <= 2e-4 max|F|), so velocities and
+# positions differ by ~dF/m; a snap or cap decision taken at its threshold
+# could move one component by up to the snap size 1e-4, which the bar covers
+TOL_STEP = 2e-5
+# FP32 fields against the oracle (the bars of tests/test_parity_gpu.py)
+TOL_REL, TOL_INF = 2e-5, 2e-4
+TOL_REL_U, TOL_INF_U = 1e-2, 2e-2
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import b200lbm
+    return b200lbm
+
+
+def _copy_state(dst, src):
+    for k in ("cx", "cy", "cz", "r", "vx", "vy", "vz", "wx", "wy", "wz", "dragging", "dragTargetX",
+              "dragTargetY", "dragTargetZ"):
+        setattr(dst, k, getattr(src, k))
+
+
+def _oracle_sets(o_sim):
+    tag, prev = np.asarray(o_sim.tag), np.asarray(o_sim.tagPrev)
+    return np.nonzero((tag == 0) & (prev == 1))[0], np.nonzero((tag == 1) & (prev == 0))[0]
+
+
+def _check_fields(o, g, tag, rel=TOL_REL, inf=TOL_INF, rel_u=TOL_REL_U, inf_u=TOL_INF_U):
+    out = {}
+    for name in ("phi", "rho"):
+        r, li = field_err(getattr(g, name), getattr(o, name))
+        out[name] = (r, li)
+        assert r <= rel and li <= inf, f"{tag} {name}: rel {r:.3e} linf {li:.3e}"
+    umax = max(np.abs(np.asarray(o.ux)).max(), np.abs(np.asarray(o.uy)).max(),
+               np.abs(np.asarray(o.uz)).max(), 1e-30)
+    for name in ("ux", "uy", "uz"):
+        r, li = field_err(getattr(g, name), getattr(o, name), norm=umax)
+        out[name] = (r, li)
+        assert r <= rel_u and li <= inf_u, f"{tag} {name}: rel {r:.3e} linf/umax {li:.3e}"
+    return out
+
+
+def kick(SimC, SphC):
+    """Drop-preset pool with gravity 0 and a sphere thrown sideways at 0.11
+    cells/step (above the 0.08 speed cap), spinning, towards the +x wall."""
+    sim = SimC(40, 28, 40)
+    scenes._params(sim, 0.85, 0.7, 0.008, 0.0)
+    sim.initFlat(28 * 0.25)
+    sol = SphC(40, 28, 40, cx=33.0, cy=15.0, cz=20.0, r=4.0, density=1.6)
+    sol.vx, sol.vy, sol.vz = 0.09, -0.06, 0.03
+    sol.wx, sol.wy, sol.wz = 0.01, -0.004, 0.02
+    return sim, sol
+
+
+def _given_state(gpu, oracle_mod, build, steps, drag_path=None, **kw):
+    """Step the oracle's tick and the device tick from the same sphere state
+    every step.  Returns (#steps the sphere moved, #fresh, #dead, worst state
+    difference)."""
+    o, osol = build(oracle_mod.OracleSim, oracle_mod.OracleSphere, **kw)
+    g, gsol = build(gpu.Sim, gpu.RigidSphere, **kw)
+    moved = n_fresh = n_dead = 0
+    worst = 0.0
+    for s in range(steps):
+        if drag_path is not None:
+            scenes.drag_target(osol, s, drag_path)
+        _copy_state(gsol, osol)
+        before = osol.cy
+        substep(o, osol)
+        g.run_coupled(gsol, 1)
+        fr, de = g.last_sets()
+        ofr, ode = _oracle_sets(o)
+        assert np.array_equal(np.asarray(g.tag), np.asarray(o.tag)), f"tags differ at step {s}"
+        assert np.array_equal(fr, ofr), f"fresh set differs at step {s}"
+        assert np.array_equal(de, ode), f"dead set differs at step {s}"
+        n_fresh += len(ofr)
+        n_dead += len(ode)
+        d = max(abs(getattr(gsol, k) - getattr(osol, k)) for k in STATE)
+        assert d <= TOL_STEP, (s, {k: (getattr(gsol, k), getattr(osol, k)) for k in STATE})
+        worst = max(worst, d)
+        moved += osol.cy != before
+    return moved, n_fresh, n_dead, worst, (o, g)
+
+
+def test_coupled_drop_given_state(gpu, oracle_mod):
+    """Drop preset, 400 ticks through lbm_run_coupled."""
+    moved, nf, nd, worst, _ = _given_state(gpu, oracle_mod, scenes.drop, 400, sigma=0.012, gravity=0.0012)
+    assert moved > 50 and nf > 0 and nd > 0, (moved, nf, nd)
+
+
+def test_coupled_drag_given_state(gpu, oracle_mod):
+    """test/drag_stress.mjs (700 ticks): the device integrator's drag spring
+    pulls the sphere to the floor, along it, up through the interface and back."""
+    moved, nf, nd, worst, (o, g) = _given_state(gpu, oracle_mod, scenes.drag, sum(n for n, _ in scenes.DRAG_PATH),
+                                                drag_path=scenes.DRAG_PATH)
+    assert moved > 300 and nf > 100 and nd > 100, (moved, nf, nd)
+    rel, _ = field_err(g.phi, o.phi)
+    assert rel <= 2e-3, rel
+
+
+def test_coupled_kick_given_state(gpu, oracle_mod):
+    """Zero gravity (the `gravity || 0.001` fallback), the speed cap, spin with
+    its damping and snap, and the wall clamp, 80 ticks."""
+    o, osol = kick(oracle_mod.OracleSim, oracle_mod.OracleSphere)
+    g, gsol = kick(gpu.Sim, gpu.RigidSphere)
+    clamped = capped = spun = 0
+    for s in range(80):
+        _copy_state(gsol, osol)
+        speed0 = (osol.vx ** 2 + osol.vy ** 2 + osol.vz ** 2) ** 0.5
+        substep(o, osol)
+        g.run_coupled(gsol, 1)
+        assert np.array_equal(np.asarray(g.tag), np.asarray(o.tag)), s
+        fr, de = g.last_sets()
+        ofr, ode = _oracle_sets(o)
+        assert np.array_equal(fr, ofr) and np.array_equal(de, ode), s
+        for k in STATE:
+            assert abs(getattr(gsol, k) - getattr(osol, k)) <= TOL_STEP, (s, k, getattr(gsol, k), getattr(osol, k))
+        clamped += osol.cx == 40 - 1 - (osol.r + 1.5)
+        capped += speed0 > 0.08
+        spun += osol.wz != 0
+    assert clamped > 0 and capped > 0 and spun > 0, (clamped, capped, spun)
+
+
+def test_coupled_drop_free_running(gpu, oracle_mod):
+    """Drop preset, 400 free-running ticks: one lbm_run_coupled call per tick
+    and one call of 400 ticks are bit-identical, and both track the oracle
+    (trajectory within 2e-5 cells at every tick, fields within the FP32 bars)."""
+    kw = dict(sigma=0.012, gravity=0.0012)
+    o, osol = scenes.drop(oracle_mod.OracleSim, oracle_mod.OracleSphere, **kw)
+    g, gsol = scenes.drop(gpu.Sim, gpu.RigidSphere, **kw)
+    g2, gsol2 = scenes.drop(gpu.Sim, gpu.RigidSphere, **kw)
+    worst = 0.0
+    cy0 = osol.cy
+    for s in range(400):
+        substep(o, osol)
+        g.run_coupled(gsol, 1)
+        worst = max(worst, *(abs(getattr(gsol, k) - getattr(osol, k)) for k in ("cx", "cy", "cz")))
+    assert worst <= 2e-5, worst
+    assert osol.cy - cy0 > 3
+    g2.run_coupled(gsol2, 400)
+    assert gsol2.state() == gsol.state()
+    for k in ("phi", "rho", "ux", "uy", "uz", "f", "h", "tag"):
+        assert np.array_equal(np.asarray(getattr(g2, k)), np.asarray(getattr(g, k))), k
+    rel, _ = field_err(g.phi, o.phi)
+    assert rel <= 1e-4, rel
+    rel, _ = field_err(g.rho, o.rho)
+    assert rel <= 1e-4, rel
+
+
+def _cfg2_pair(gpu, oracle_mod, n):
+    o, osol = scenes.cfg2(oracle_mod.OracleSim, oracle_mod.OracleSphere, n=n)
+    o.set_threads(os.cpu_count() or 1)
+    g, gsol = scenes.cfg2(gpu.Sim, gpu.RigidSphere, n=n)
+    return (o, osol), (g, gsol)
+
+
+@pytest.mark.parametrize("n,steps", [(64, 80), (96, 80)])
+def test_cfg2_reduced_matches_oracle(gpu, oracle_mod, n, steps):
+    """The benchmark scene (liquid below a seeded +-0.5-cell wavy interface,
+    g = -1e-5, density-2 sphere, tau 0.6, tauPhi 0.8) scaled to n^3, stepped
+    by the timed path (one lbm_run_coupled call) against the oracle's ticks:
+    phi and rho within the FP32 bars, u within its bar, tags exact, sphere
+    state within 1e-6."""
+    (o, osol), (g, gsol) = _cfg2_pair(gpu, oracle_mod, n)
+    for _ in range(steps):
+        substep(o, osol)
+    g.run_coupled(gsol, steps)
+    _check_fields(o, g, f"cfg2 n={n}")
+    assert np.array_equal(np.asarray(g.tag), np.asarray(o.tag))
+    for k in STATE:
+        assert abs(getattr(gsol, k) - getattr(osol, k)) <= 1e-6, k
+
+
+def test_cfg2_full_size_matches_oracle(gpu, oracle_mod):
+    """The 256^3 benchmark scene itself, 20 ticks of the timed path against
+    the oracle (OpenMP over the host's cores, ~1 s per tick)."""
+    (o, osol), (g, gsol) = _cfg2_pair(gpu, oracle_mod, 256)
+    for _ in range(20):
+        substep(o, osol)
+    g.run_coupled(gsol, 20)
+    _check_fields(o, g, "cfg2 n=256")
+    assert np.array_equal(np.asarray(g.tag), np.asarray(o.tag))
+    for k in STATE:
+        assert abs(getattr(gsol, k) - getattr(osol, k)) <= 1e-6, k

@@ -31,10 +31,18 @@ def gpu():
     return b200lbm
 
 
-def _scene(gpu, centre, r, seed):
-    """The bench scene with random fields and a sphere placed on them: the first
-    retag turns every cell of the sphere FLUID -> SOLID (all of them dead)."""
-    sim, sol = scenes.bench(gpu.Sim, gpu.RigidSphere)
+def _large(SimC, SphC):
+    """110^3 pool for a sphere whose search box nearly fills the array."""
+    sim = SimC(110, 110, 110)
+    scenes._params(sim, 0.7, 0.7, 0.012, 0.00135)
+    sim.initFlat(30)
+    return sim, SphC(110, 110, 110, cx=55, cy=55, cz=55, r=10, density=1.6)
+
+
+def _scene(gpu, centre, r, seed, build=scenes.bench):
+    """A scene with random fields and a sphere placed on them: the first retag
+    turns every cell of the sphere FLUID -> SOLID (all of them dead)."""
+    sim, sol = build(gpu.Sim, gpu.RigidSphere)
     rng = np.random.default_rng(seed)
     sim.phi[:] = rng.uniform(-0.1, 1.1, sim.n).astype(np.float32)
     for name in ("ux", "uy", "uz"):
@@ -77,6 +85,24 @@ def test_no_alloc_matches_handle_based_two_calls(gpu):
         sim, sol = _scene(gpu, centre, r, seed)
         tag, prev = np.array(sim.tag), np.array(sim.tagPrev)
         assert np.count_nonzero((tag == 1) & (prev == 0)) > 100
+        want = _handle_based(gpu, sim, sol)
+        got = _no_alloc(gpu, sim, sol)
+        assert np.all(np.isfinite(got)), (n, got)
+        for k, a, b in zip(KEYS, got, want):
+            assert abs(a - b) <= TOL * max(1.0, abs(b)), (n, k, a, b)
+        sim.close()
+
+
+def test_no_alloc_near_capacity(gpu):
+    """A sphere of radius 49 in a 110^3 grid: its search box is 101^3 =
+    1,030,301 cells (98% of the 2^20 limit) with ~490,000 dead cells, then a
+    small sphere on other fields right after it."""
+    cases = [((55.3, 55.6, 54.8), 49.0, 21, _large), ((20.6, 9.4, 19.9), 4.1, 22, scenes.bench)]
+    for n, (centre, r, seed, build) in enumerate(cases):
+        sim, sol = _scene(gpu, centre, r, seed, build)
+        tag, prev = np.array(sim.tag), np.array(sim.tagPrev)
+        ndead = np.count_nonzero((tag == 1) & (prev == 0))
+        assert ndead > (400000 if n == 0 else 100), ndead
         want = _handle_based(gpu, sim, sol)
         got = _no_alloc(gpu, sim, sol)
         assert np.all(np.isfinite(got)), (n, got)
