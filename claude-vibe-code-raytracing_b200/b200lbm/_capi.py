@@ -99,6 +99,8 @@ _SIGS = [
     ("lbm_host_free", C.c_int, [C.c_void_p]),
     ("lbm_run_coupled", C.c_int,
      [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    ("lbm_sphere_step_host", C.c_int,
+     [C.POINTER(LbmSphere), C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
     ("lbm_synchronize", C.c_int, [C.c_void_p]),
     ("lbm_stream", C.c_void_p, [C.c_void_p]),
     ("lbm_last_sets", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

@@ -11,6 +11,7 @@
 
 #include "lbm_kernels.cuh"
 #include "lbm_render.h"
+#include "lbm_sphere.cuh"
 #include "lbm_state.h"
 
 using namespace lbm;
@@ -575,8 +576,8 @@ size_t lbm_footprint_bytes(int nx, int ny, int nz, int storage) {
   long long n = (long long)nx * ny * nz;
   size_t pb = pop_bytes_of(storage), mb = mac_bytes_of(storage);
   size_t bytes = 2 * (size_t)(pop_elems(n, 27) + pop_elems(n, 7)) * pb;  // F, H ping-pong
-  bytes += 2 * 5 * (size_t)n * mb;                     // macros ping-pong
-  bytes += 2 * (size_t)n;                              // tag, tagPrev
+  bytes += 2 * 5 * (size_t)(n + ARRAY_PAD) * mb;       // macros ping-pong
+  bytes += 2 * (size_t)(n + ARRAY_PAD);                // tag, tagPrev
   bytes += 2 * (size_t)n * sizeof(int);                // fresh / dead lists
   return bytes;
 }
@@ -614,15 +615,17 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
       DALLOC(h->H[c], pop_elems(h->n, 7) * pb);
       CK(cudaMemsetAsync(h->F[c], 0, pop_elems(h->n, 27) * pb, h->stream));
       CK(cudaMemsetAsync(h->H[c], 0, pop_elems(h->n, 7) * pb, h->stream));
+      // macro and tag arrays carry a tail pad: the pipelined step copies rows
+      // rounded out to 16-byte units, which can reach past the last cell
       for (int a = 0; a < 5; a++) {
-        DALLOC(h->mac[c][a], h->n * mb);
-        CK(cudaMemsetAsync(h->mac[c][a], 0, h->n * mb, h->stream));
+        DALLOC(h->mac[c][a], (h->n + ARRAY_PAD) * mb);
+        CK(cudaMemsetAsync(h->mac[c][a], 0, (h->n + ARRAY_PAD) * mb, h->stream));
       }
     }
-    DALLOC(h->tag, h->n);
-    DALLOC(h->tagPrev, h->n);
-    CK(cudaMemsetAsync(h->tag, 0, h->n, h->stream));
-    CK(cudaMemsetAsync(h->tagPrev, 0, h->n, h->stream));
+    DALLOC(h->tag, h->n + ARRAY_PAD);
+    DALLOC(h->tagPrev, h->n + ARRAY_PAD);
+    CK(cudaMemsetAsync(h->tag, 0, h->n + ARRAY_PAD, h->stream));
+    CK(cudaMemsetAsync(h->tagPrev, 0, h->n + ARRAY_PAD, h->stream));
     h->listCap = h->n;
     DALLOC(h->fresh, h->listCap * sizeof(int));
     DALLOC(h->dead, h->listCap * sizeof(int));
@@ -1165,6 +1168,12 @@ int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_ev
   return watch_after(h, nsteps);
 }
 
+int lbm_sphere_step_host(lbm_sphere *spheres, int n, double dt, double gravity, int nx, int ny, int nz) {
+  if (n < 0 || (n > 0 && !spheres) || nx < 3 || ny < 3 || nz < 3) return LBM_ERR_ARG;
+  for (int b = 0; b < n; b++) lbm::sphere_step_fp64(spheres[b], dt, gravity, nx, ny, nz);
+  return LBM_OK;
+}
+
 int lbm_wait_frames(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);
@@ -1591,7 +1600,18 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
   BCK(cudaStreamSynchronize(b->origin));
   for (int s = 0; s < n; s++)
     BSIM(b->sims[s], coupled_finish(b->sims[s], nspheres[s] ? spheres[s] : nullptr, nspheres[s]));
-  for (int s = 0; s < n; s++) BSIM(b->sims[s], watch_after(b->sims[s], nsteps));
+  // every scene's watchdog advances and scans; the first scene that reports
+  // gives the batch's status and message
+  int first = LBM_OK;
+  std::string firstMsg;
+  for (int s = 0; s < n; s++) {
+    const int rc_ = watch_after(b->sims[s], nsteps);
+    if (rc_ != LBM_OK && first == LBM_OK) {
+      first = rc_;
+      firstMsg = "scene " + std::to_string(s) + ": " + b->sims[s]->err;
+    }
+  }
+  if (first != LBM_OK) return bfail(b, first, firstMsg);
   return LBM_OK;
 }
 

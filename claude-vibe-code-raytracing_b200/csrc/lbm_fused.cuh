@@ -314,6 +314,119 @@ struct CellOut {
   uint8_t tg, tg2;
 };
 
+// Physics constants of the fused collision in the storage form's arithmetic type.
+template <class Real>
+struct CollK {
+  Real om, omP, A, beta4, kappa, rhoG, dRho, grav, sharpC4;
+};
+template <class PopT>
+__device__ __forceinline__ CollK<typename Prec<PopT>::Real> coll_consts(const FusedArgs<PopT> &a) {
+  using Real = typename Prec<PopT>::Real;
+  return CollK<Real>{(Real)a.om,   (Real)a.omP,  (Real)a.A,    (Real)a.beta4,  (Real)a.kappa,
+                     (Real)a.rhoG, (Real)a.dRho, (Real)a.gravity, (Real)a.sharpC4};
+}
+
+// e.X for a lattice direction (components -1, 0, 1): signed sums, the first
+// term taken exactly
+template <int ex, int ey, int ez, class Real>
+__device__ __forceinline__ Real edot(Real X, Real Y, Real Z) {
+  Real r = 0;
+  bool first = true;
+  if constexpr (ex != 0) {
+    r = ex > 0 ? X : -X;
+    first = false;
+  }
+  if constexpr (ey != 0) {
+    r = first ? (ey > 0 ? Y : -Y) : (ey > 0 ? radd(r, Y) : rsub(r, Y));
+    first = false;
+  }
+  if constexpr (ez != 0) r = first ? (ez > 0 ? Z : -Z) : (ez > 0 ? radd(r, Z) : rsub(r, Z));
+  return r;
+}
+
+// The collision of one cell into registers (o).  MODE 0: every direction (a
+// tile cell; opposite pairs evaluated together); MODE 1: the directions of the
+// compile-time halo side (SX, SY); MODE 2: every direction, one at a time (a
+// halo cell whose side is known at run time).  Returns gradient, laplacian
+// and phi of the cell.  Every operation rounds explicitly (rmul / radd / rsub
+// / rfma), so a tile cell and a halo cell of another tile get the same bits
+// whatever the compiler would contract in either context.
+template <class PopT, int MODE, int SX, int SY>
+__device__ __forceinline__ void collide_cell(const CollK<typename Prec<PopT>::Real> &K, const CellLoad<PopT> &L,
+                                             CellOut<PopT> &o, typename Prec<PopT>::Real &ogx,
+                                             typename Prec<PopT>::Real &ogy, typename Prec<PopT>::Real &ogz,
+                                             typename Prec<PopT>::Real &olap, typename Prec<PopT>::Real &ophi) {
+  using Real = typename Prec<PopT>::Real;
+  using C = Codec<PopT>;
+  if constexpr (MODE == 1 && SY < 0) o.tg2 = L.tg;
+  else o.tg = L.tg;
+  const Real om = K.om, omP = K.omP, A = K.A, beta4 = K.beta4, kappa = K.kappa, rhoG = K.rhoG;
+  const Real dRho = K.dRho, grav = K.grav, sharpC4 = K.sharpC4;
+  const Real p = L.p, ux = L.ux, uy = L.uy, uz = L.uz;
+  const Real half = (Real)0.5, one = (Real)1, two = (Real)2;
+  const Real gxv = rmul(half, rsub(L.pxp, L.pxm));
+  const Real gyv = rmul(half, rsub(L.pyp, L.pym));
+  const Real gzv = rmul(half, rsub(L.pzp, L.pzm));
+  const Real lap = rfma((Real)-6, p, radd(radd(radd(radd(radd(L.pxp, L.pxm), L.pyp), L.pym), L.pzp), L.pzm));
+  const Real rhoPh = rfma(p, dRho, rhoG);
+  const Real mu = rfma(-kappa, lap, rmul(rmul(rmul(beta4, p), rsub(p, one)), rfma(two, p, -one)));
+  const Real Fx = rmul(mu, gxv), Fy = rfma(mu, gyv, rmul(rhoPh, grav)), Fz = rmul(mu, gzv);
+  const Real u2 = rfma(uz, uz, rfma(uy, uy, rmul(ux, ux)));
+  const Real uF = rfma(uz, Fz, rfma(uy, Fy, rmul(ux, Fx)));
+  const Real orh = rmul(om, rhoPh);
+  const Real C0 = rfma(-A, uF, rfma(rmul((Real)-1.5, orh), u2, rmul(om, L.sumF)));
+  const Real orh3 = rmul((Real)3, orh);
+  const Real Vx = rfma(A, Fx, rmul(orh3, ux)), Vy = rfma(A, Fy, rmul(orh3, uy)), Vz = rfma(A, Fz, rmul(orh3, uz));
+  const Real A3 = rmul((Real)3, A), orh45 = rmul((Real)4.5, orh);
+  const Real Qx = rfma(A3, Fx, rmul(orh45, ux)), Qy = rfma(A3, Fy, rmul(orh45, uy)),
+             Qz = rfma(A3, Fz, rmul(orh45, uz));
+  const Real gmag = radd(sqrt(rfma(gzv, gzv, rfma(gyv, gyv, rmul(gxv, gxv)))), (Real)1e-12);
+  const Real sh = rmul(rmul(sharpC4, p), rsub(one, p)) / gmag;
+  const Real D0 = rmul(omP, p);
+  const Real fp = rmul((Real)4, D0);
+  const Real Dx = rfma(sh, gxv, rmul(fp, ux)), Dy = rfma(sh, gyv, rmul(fp, uy)), Dz = rfma(sh, gzv, rmul(fp, uz));
+  const Real om1 = rsub(one, om), omP1 = rsub(one, omP);
+  static_for<0, Q27>([&](auto KK) {
+    constexpr int k = decltype(KK)::value;
+    using D = D27<k>;
+    constexpr int ex = D::ex, ey = D::ey, ez = D::ez;
+    if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
+      const Real ev = edot<ex, ey, ez>(Vx, Vy, Vz);
+      const Real eu = edot<ex, ey, ez>(ux, uy, uz);
+      const Real eq = edot<ex, ey, ez>(Qx, Qy, Qz);
+      const Real w = (Real)D::w;
+      // f*_k = (1 - w) f_k + (w_k T + w_k e.V) with T = (e.u)(e.Q) + C0.  The
+      // opposite direction has the same T and the negated w_k e.V, exactly
+      // (every negation is exact), so a tile cell evaluates opposite pairs
+      // (k odd, k + 1) together and still gets, bit for bit, what a halo
+      // cell evaluating one direction alone gets.
+      if constexpr (MODE == 0 && k > 0) {
+        if constexpr (k & 1) {
+          const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
+          o.f[k] = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
+          o.f[D::opp] = rfma(om1, C::dec(L.fv[D::opp], w), rsub(wT, wev));
+        }
+      } else {
+        const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
+        o.f[k] = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
+      }
+      if constexpr (k < Q7) {
+        const Real w7 = (Real)D7<k>::w;
+        // D3Q7 directions have at most one non-zero component
+        const Real ed = edot<ex, ey, ez>(Dx, Dy, Dz);
+        Real href = 0;
+        if constexpr (C::offset) href = rmul(w7, p);
+        o.h[k] = rfma(omP1, C::dec(L.hv[k], href), rmul(w7, k == 0 ? D0 : radd(D0, ed)));
+      }
+    }
+  });
+  ogx = gxv;
+  ogy = gyv;
+  ogz = gzv;
+  olap = lap;
+  ophi = p;
+}
+
 // One tile (bx, by) of 32 x TY columns over z-chunk bz of one scene.
 // WIDE: 64-bit population offsets, for grids whose populations exceed 2^31
 // elements (more than ~76 M cells); 32-bit offsets otherwise.
@@ -543,95 +656,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   };
 
   // Compute phase: the collision of one cell into registers (o), for emit.
-  // Returns gradient, laplacian and phi of the cell.
+  const CollK<Real> K = coll_consts(a);
   auto compute = [&](auto MODEc, auto SXc, auto SYc, const LD &L, CO &o, Real &ogx, Real &ogy, Real &ogz, Real &olap,
                      Real &ophi) __attribute__((always_inline)) {
-    constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
-    if constexpr (MODE == 1 && SY < 0) o.tg2 = L.tg;
-    else o.tg = L.tg;
-    // Every operation below rounds explicitly (rmul / radd / rsub / rfma), so a
-    // tile cell and a halo cell of another tile get the same bits whatever the
-    // compiler would contract in either context.
-    const Real p = L.p, ux = L.ux, uy = L.uy, uz = L.uz;
-    const Real half = (Real)0.5, one = (Real)1, two = (Real)2;
-    const Real gxv = rmul(half, rsub(L.pxp, L.pxm));
-    const Real gyv = rmul(half, rsub(L.pyp, L.pym));
-    const Real gzv = rmul(half, rsub(L.pzp, L.pzm));
-    const Real lap = rfma((Real)-6, p, radd(radd(radd(radd(radd(L.pxp, L.pxm), L.pyp), L.pym), L.pzp), L.pzm));
-    const Real rhoPh = rfma(p, dRho, rhoG);
-    const Real mu = rfma(-kappa, lap, rmul(rmul(rmul(beta4, p), rsub(p, one)), rfma(two, p, -one)));
-    const Real Fx = rmul(mu, gxv), Fy = rfma(mu, gyv, rmul(rhoPh, grav)), Fz = rmul(mu, gzv);
-    const Real u2 = rfma(uz, uz, rfma(uy, uy, rmul(ux, ux)));
-    const Real uF = rfma(uz, Fz, rfma(uy, Fy, rmul(ux, Fx)));
-    const Real orh = rmul(om, rhoPh);
-    const Real C0 = rfma(-A, uF, rfma(rmul((Real)-1.5, orh), u2, rmul(om, L.sumF)));
-    const Real orh3 = rmul((Real)3, orh);
-    const Real Vx = rfma(A, Fx, rmul(orh3, ux)), Vy = rfma(A, Fy, rmul(orh3, uy)), Vz = rfma(A, Fz, rmul(orh3, uz));
-    const Real A3 = rmul((Real)3, A), orh45 = rmul((Real)4.5, orh);
-    const Real Qx = rfma(A3, Fx, rmul(orh45, ux)), Qy = rfma(A3, Fy, rmul(orh45, uy)),
-               Qz = rfma(A3, Fz, rmul(orh45, uz));
-    const Real gmag = radd(sqrt(rfma(gzv, gzv, rfma(gyv, gyv, rmul(gxv, gxv)))), (Real)1e-12);
-    const Real sh = rmul(rmul(sharpC4, p), rsub(one, p)) / gmag;
-    const Real D0 = rmul(omP, p);
-    const Real fp = rmul((Real)4, D0);
-    const Real Dx = rfma(sh, gxv, rmul(fp, ux)), Dy = rfma(sh, gyv, rmul(fp, uy)), Dz = rfma(sh, gzv, rmul(fp, uz));
-    const Real om1 = rsub(one, om), omP1 = rsub(one, omP);
-    // e.X for a lattice direction (components -1, 0, 1): signed sums, the
-    // first term taken exactly
-    auto edot = [](auto EX, auto EY, auto EZ, Real X, Real Y, Real Z) __attribute__((always_inline)) {
-      constexpr int ex = decltype(EX)::value, ey = decltype(EY)::value, ez = decltype(EZ)::value;
-      Real r = 0;
-      bool first = true;
-      if constexpr (ex != 0) {
-        r = ex > 0 ? X : -X;
-        first = false;
-      }
-      if constexpr (ey != 0) {
-        r = first ? (ey > 0 ? Y : -Y) : (ey > 0 ? radd(r, Y) : rsub(r, Y));
-        first = false;
-      }
-      if constexpr (ez != 0) r = first ? (ez > 0 ? Z : -Z) : (ez > 0 ? radd(r, Z) : rsub(r, Z));
-      return r;
-    };
-    static_for<0, Q27>([&](auto KK) {
-      constexpr int k = decltype(KK)::value;
-      using D = D27<k>;
-      constexpr int ex = D::ex, ey = D::ey, ez = D::ez;
-      if constexpr (MODE != 1 || halo_dir<SX, SY, k>()) {
-        const Real ev = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Vx, Vy, Vz);
-        const Real eu = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, ux, uy, uz);
-        const Real eq = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Qx, Qy, Qz);
-        const Real w = (Real)D::w;
-        // f*_k = (1 - w) f_k + (w_k T + w_k e.V) with T = (e.u)(e.Q) + C0.  The
-        // opposite direction has the same T and the negated w_k e.V, exactly
-        // (every negation is exact), so a tile cell evaluates opposite pairs
-        // (k odd, k + 1) together and still gets, bit for bit, what a halo
-        // cell evaluating one direction alone gets.
-        if constexpr (MODE == 0 && k > 0) {
-          if constexpr (k & 1) {
-            const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
-            o.f[k] = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
-            o.f[D::opp] = rfma(om1, C::dec(L.fv[D::opp], w), rsub(wT, wev));
-          }
-        } else {
-          const Real T = rfma(eu, eq, C0), wev = rmul(w, ev), wT = rmul(w, T);
-          o.f[k] = rfma(om1, C::dec(L.fv[k], w), radd(wT, wev));
-        }
-        if constexpr (k < Q7) {
-          const Real w7 = (Real)D7<k>::w;
-          // D3Q7 directions have at most one non-zero component
-          const Real ed = edot(IC<ex>{}, IC<ey>{}, IC<ez>{}, Dx, Dy, Dz);
-          Real href = 0;
-          if constexpr (C::offset) href = rmul(w7, p);
-          o.h[k] = rfma(omP1, C::dec(L.hv[k], href), rmul(w7, k == 0 ? D0 : radd(D0, ed)));
-        }
-      }
-    });
-    ogx = gxv;
-    ogy = gyv;
-    ogz = gzv;
-    olap = lap;
-    ophi = p;
+    collide_cell<PopT, decltype(MODEc)::value, decltype(SXc)::value, decltype(SYc)::value>(K, L, o, ogx, ogy, ogz,
+                                                                                         olap, ophi);
   };
 
   // Collide plane q: cell warps their own cells; halo warp A the rows above

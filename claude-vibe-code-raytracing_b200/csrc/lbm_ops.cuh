@@ -6,8 +6,9 @@
 
 #include <algorithm>
 
-#include "lbm_fused.cuh"
+#include "lbm_fused_pipe.cuh"
 #include "lbm_kernels.cuh"
+#include "lbm_sphere.cuh"
 #include "lbm_state.h"
 
 namespace lbm {
@@ -63,91 +64,20 @@ __global__ void k_reencode_h(Scene<PopT, typename Prec<PopT>::Real> s, int half,
   }
 }
 
-// RigidSphere.step(1.0, gravity) (src/solid.js:104-210) on the device, one
-// thread per sphere, FP64 round-to-nearest intrinsics in the reference's
-// evaluation order.  The momentum-exchange and dead-cell impulses of the step
-// are added first, as RigidSphere.applyImpulseAtCell would have.
-__device__ __forceinline__ double js_max0(double v) {
-  if (v != v) return v;
-  if (v == 0) return signbit(v) ? 0.0 : v;
-  return v > 0 ? v : 0.0;
-}
-__device__ __forceinline__ double js_min0(double v) {
-  if (v != v) return v;
-  if (v == 0) return signbit(v) ? v : 0.0;
-  return v < 0 ? v : 0.0;
-}
-
+// The device-resident loop's RigidSphere.step(1.0, gravity), one thread per
+// sphere: the momentum-exchange and dead-cell impulses of the step are added
+// first, as RigidSphere.applyImpulseAtCell would have.
 static __global__ void k_sphere_step(lbm_sphere *sph, int nsph, double gravity, const double *fluid,
-                              const double *dead, int nx, int ny, int nz) {
+                                     const double *dead, int nx, int ny, int nz) {
   int b = threadIdx.x;
   if (blockIdx.x != 0 || b >= nsph) return;
   lbm_sphere s = sph[b];
-  const double dt = 1.0;
   double *F[6] = {&s.Fx, &s.Fy, &s.Fz, &s.Tx, &s.Ty, &s.Tz};
   for (int j = 0; j < 6; j++) {
     if (fluid) *F[j] = __dadd_rn(*F[j], fluid[6 * b + j]);
     if (dead) *F[j] = __dadd_rn(*F[j], dead[6 * b + j]);
   }
-  s.Fy = __dadd_rn(s.Fy, __dmul_rn(s.mass, gravity));
-  if (s.dragging) {
-    double k = __dmul_rn(0.004, s.mass);
-    double cD = __dmul_rn(2.0, __dsqrt_rn(__dmul_rn(k, s.mass)));
-    s.Fx = __dadd_rn(s.Fx, __dsub_rn(__dmul_rn(k, __dsub_rn(s.dragTargetX, s.cx)), __dmul_rn(cD, s.vx)));
-    s.Fy = __dadd_rn(s.Fy, __dsub_rn(__dmul_rn(k, __dsub_rn(s.dragTargetY, s.cy)), __dmul_rn(cD, s.vy)));
-    s.Fz = __dadd_rn(s.Fz, __dsub_rn(__dmul_rn(k, __dsub_rn(s.dragTargetZ, s.cz)), __dmul_rn(cD, s.vz)));
-  }
-  double gsel = (gravity == 0 || gravity != gravity) ? 0.001 : gravity;
-  double accCap = __dmul_rn(3.5, fabs(gsel));
-  {
-    double ax = __ddiv_rn(s.Fx, s.mass);
-    double ay = __ddiv_rn(s.Fy, s.mass);
-    double az = __ddiv_rn(s.Fz, s.mass);
-    double a2 = __dadd_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)), __dmul_rn(az, az));
-    double c2 = __dmul_rn(accCap, accCap);
-    double sc = a2 > c2 ? __ddiv_rn(accCap, __dsqrt_rn(a2)) : 1.0;
-    s.vx = __dadd_rn(s.vx, __dmul_rn(__dmul_rn(dt, ax), sc));
-    s.vy = __dadd_rn(s.vy, __dmul_rn(__dmul_rn(dt, ay), sc));
-    s.vz = __dadd_rn(s.vz, __dmul_rn(__dmul_rn(dt, az), sc));
-  }
-  s.wx = __dadd_rn(s.wx, __ddiv_rn(__dmul_rn(dt, s.Tx), s.I));
-  s.wy = __dadd_rn(s.wy, __ddiv_rn(__dmul_rn(dt, s.Ty), s.I));
-  s.wz = __dadd_rn(s.wz, __ddiv_rn(__dmul_rn(dt, s.Tz), s.I));
-  const double BODY_UMAX = 0.08;
-  double sp2 = __dadd_rn(__dadd_rn(__dmul_rn(s.vx, s.vx), __dmul_rn(s.vy, s.vy)), __dmul_rn(s.vz, s.vz));
-  if (sp2 > __dmul_rn(BODY_UMAX, BODY_UMAX)) {
-    double sc = __ddiv_rn(BODY_UMAX, __dsqrt_rn(sp2));
-    s.vx = __dmul_rn(s.vx, sc);
-    s.vy = __dmul_rn(s.vy, sc);
-    s.vz = __dmul_rn(s.vz, sc);
-  }
-  s.vx = __dmul_rn(s.vx, 0.98);
-  s.vy = __dmul_rn(s.vy, 0.98);
-  s.vz = __dmul_rn(s.vz, 0.98);
-  s.wx = __dmul_rn(s.wx, 0.95);
-  s.wy = __dmul_rn(s.wy, 0.95);
-  s.wz = __dmul_rn(s.wz, 0.95);
-  const double SNAP = 0.0001;
-  if (fabs(s.vx) < SNAP) s.vx = 0;
-  if (fabs(s.vy) < SNAP) s.vy = 0;
-  if (fabs(s.vz) < SNAP) s.vz = 0;
-  if (fabs(s.wx) < SNAP) s.wx = 0;
-  if (fabs(s.wy) < SNAP) s.wy = 0;
-  if (fabs(s.wz) < SNAP) s.wz = 0;
-  s.cx = __dadd_rn(s.cx, __dmul_rn(dt, s.vx));
-  s.cy = __dadd_rn(s.cy, __dmul_rn(dt, s.vy));
-  s.cz = __dadd_rn(s.cz, __dmul_rn(dt, s.vz));
-  double m = __dadd_rn(s.r, 1.5);
-  double limX = __dsub_rn((double)(nx - 1), m), limY = __dsub_rn((double)(ny - 1), m);
-  double limZ = __dsub_rn((double)(nz - 1), m);
-  if (s.cx < m) { s.cx = m; s.vx = js_max0(s.vx); }
-  if (s.cx > limX) { s.cx = limX; s.vx = js_min0(s.vx); }
-  if (s.cy < m) { s.cy = m; s.vy = js_max0(s.vy); }
-  if (s.cy > limY) { s.cy = limY; s.vy = js_min0(s.vy); }
-  if (s.cz < m) { s.cz = m; s.vz = js_max0(s.vz); }
-  if (s.cz > limZ) { s.cz = limZ; s.vz = js_min0(s.vz); }
-  s.Fx = s.Fy = s.Fz = 0;
-  s.Tx = s.Ty = s.Tz = 0;
+  sphere_step_fp64(s, 1.0, gravity, nx, ny, nz);
   sph[b] = s;
 }
 
@@ -265,30 +195,60 @@ class Ops final : public OpsBase {
       case 2: go(IC<2>{}, std::false_type{}); break;
       case 4: go(IC<4>{}, std::false_type{}); break;
       case 4 | LBM_FUSED_STAGED:
-        if constexpr (sizeof(PopT) == 2) go(IC<4>{}, std::true_type{});
+        if constexpr (kPipe) go(IC<4>{}, std::true_type{});
+        else go(IC<4>{}, std::false_type{});
+        break;
+      case 6 | LBM_FUSED_STAGED:
+        if constexpr (kPipe) go(IC<6>{}, std::true_type{});
         else go(IC<4>{}, std::false_type{});
         break;
       default: go(IC<8>{}, std::false_type{}); break;
     }
   }
+  // the pipelined form (4 | LBM_FUSED_STAGED) keeps FP32 values in its ring:
+  // FP32, FP16 and BF16 storage
+  static constexpr bool kPipe = sizeof(Real) == 4;
   bool shape_ok(int shape) const override {
-    return shape == 2 || shape == 4 || shape == 8 || (shape == (4 | LBM_FUSED_STAGED) && sizeof(PopT) == 2);
+    return shape == 2 || shape == 4 || shape == 8 ||
+           ((shape == (4 | LBM_FUSED_STAGED) || shape == (6 | LBM_FUSED_STAGED)) && kPipe);
+  }
+  // shared memory and threads of a launch of either form
+  template <int TY, bool PIPE>
+  static constexpr size_t smem_of() {
+    if constexpr (PIPE) return PipeSmem<PopT, TY>::bytes;
+    else return FusedSmem<PopT, TY, false>::bytes;
+  }
+  template <int TY, bool PIPE>
+  static constexpr int warps_of() {
+    if constexpr (PIPE) return PipeSmem<PopT, TY>::warps;
+    else return FusedSmem<PopT, TY, false>::warps;
+  }
+  template <int TY, bool PIPE, bool WIDE>
+  static auto step_kernel() {
+    if constexpr (PIPE) return k_fused_pipe<PopT, TY, WIDE>;
+    else return k_fused_step<PopT, TY, false, WIDE>;
+  }
+  template <int TY, bool PIPE, bool WIDE>
+  static auto batch_kernel() {
+    if constexpr (PIPE) return k_fused_pipe_batch<PopT, TY, WIDE>;
+    else return k_fused_batch<PopT, TY, false, WIDE>;
   }
 
   template <int TY, bool STG, bool WIDE>
   void launch_fused(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
-    constexpr size_t smem = FusedSmem<PopT, TY, STG>::bytes;
+    constexpr size_t smem = smem_of<TY, STG>();
+    const auto kern = step_kernel<TY, STG, WIDE>();
     // the shared-memory opt-in is per device
     static unsigned long long attrSet = 0;
     const unsigned long long bit = 1ull << (h->device & 63);
     if (!(attrSet & bit)) {
-      cudaFuncSetAttribute(k_fused_step<PopT, TY, STG, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       attrSet |= bit;
     }
-    dim3 block(32, FusedSmem<PopT, TY, STG>::warps);  // TY cell warps and two halo warps
+    dim3 block(32, warps_of<TY, STG>());  // TY cell warps and the halo warps
     dim3 grid((h->nx + 31) / 32, (h->ny + TY - 1) / TY, (h->nz - 2 + zchunk - 1) / zchunk);
-    k_fused_step<PopT, TY, STG, WIDE><<<grid, block, smem, h->stream>>>(a);
+    kern<<<grid, block, smem, h->stream>>>(a);
     h->launches++;
   }
 
@@ -319,17 +279,17 @@ class Ops final : public OpsBase {
   }
   template <int TY, bool STG, bool WIDE>
   int batch_ctas(int device) {
-    constexpr size_t smem = FusedSmem<PopT, TY, STG>::bytes;
+    constexpr size_t smem = smem_of<TY, STG>();
+    const auto kern = batch_kernel<TY, STG, WIDE>();
     static unsigned long long attrSet = 0;
     const unsigned long long bit = 1ull << (device & 63);
     if (!(attrSet & bit)) {
-      cudaFuncSetAttribute(k_fused_batch<PopT, TY, STG, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       attrSet |= bit;
     }
     int per = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_batch<PopT, TY, STG, WIDE>,
-                                                  FusedSmem<PopT, TY, STG>::threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * warps_of<TY, STG>(), smem);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per) * std::max(1, sms);
   }
@@ -345,8 +305,8 @@ class Ops final : public OpsBase {
     with_shape(shape, [&](auto T, auto S, auto W) {
       constexpr int TY = decltype(T)::value;
       constexpr bool STG = decltype(S)::value;
-      dim3 block(32, FusedSmem<PopT, TY, STG>::warps);
-      k_fused_batch<PopT, TY, STG, decltype(W)::value><<<ctas, block, FusedSmem<PopT, TY, STG>::bytes, st>>>(
+      dim3 block(32, warps_of<TY, STG>());
+      batch_kernel<TY, STG, decltype(W)::value>()<<<ctas, block, smem_of<TY, STG>(), st>>>(
           (const FusedArgs<PopT> *)d_args, d_tileStart, d_tileGrid, nscenes);
     });
   }
@@ -371,7 +331,7 @@ class Ops final : public OpsBase {
 
   size_t fused_smem(int shape) const override {
     size_t r = 0;
-    with_shape(shape, [&](auto T, auto S, auto) { r = FusedSmem<PopT, decltype(T)::value, decltype(S)::value>::bytes; });
+    with_shape(shape, [&](auto T, auto S, auto) { r = smem_of<decltype(T)::value, decltype(S)::value>(); });
     return r;
   }
 

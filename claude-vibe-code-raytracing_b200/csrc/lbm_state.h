@@ -29,6 +29,9 @@ inline int shape_rows(int shape) { return shape & 0xff; }
 // 2^31 elements, so the fused kernel uses 64-bit population offsets
 constexpr int SHAPE_WIDE = 0x200;
 inline bool needs_wide(long long cells) { return pop_elems(cells, 27) >= (1LL << 31) - 64; }
+// elements of tail pad after every macro and tag array (row copies of the
+// pipelined step are rounded out to 16-byte units)
+constexpr long long ARRAY_PAD = 64;
 
 class OpsBase {
  public:

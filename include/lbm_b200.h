@@ -179,6 +179,15 @@ int lbm_pack_volume_device(lbm_sim *sim, void *device_out);
 int lbm_run_coupled(lbm_sim *sim, lbm_sphere *spheres, int nspheres, int nsteps,
                     int frame_every, uint8_t *frames);
 
+/* RigidSphere.step(dt, gravity) (src/solid.js:104-210) on the host, in FP64
+ * with the reference's operation order (the device-resident loop runs the
+ * same code): for each sphere, gravity and the drag spring are added to the
+ * accumulated Fx..Tz, then the capped, damped, snapped and wall-clamped
+ * update of velocity, spin and centre; Fx..Tz are cleared.  nx, ny, nz give
+ * the clamp walls.  Needs no device; for hosts (the Node addon) whose sphere
+ * state lives in this struct. */
+int lbm_sphere_step_host(lbm_sphere *spheres, int n, double dt, double gravity, int nx, int ny, int nz);
+
 /* Wait for all work queued on the handle's stream.  Returns LBM_ERR_TIMEOUT
  * when a fused step since the last check was abandoned because one of its
  * bounded device waits ran out (its fields are not valid; the handle stays

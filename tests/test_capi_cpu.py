@@ -31,9 +31,11 @@ def test_footprint_is_host_only():
     L = _capi.lib()
     n = 256 ** 3
     b = L.lbm_footprint_bytes(256, 256, 256, _capi.STORE_F32)
-    # populations in 8-cell blocks of 4-direction groups: 27 -> 28 and 7 -> 8 slots
+    # populations in 8-cell blocks of 4-direction groups: 27 -> 28 and 7 -> 8 slots;
+    # macro and tag arrays carry a 64-element tail pad
     blocks = (n + 7) // 8
-    assert b == 2 * (28 + 8) * 8 * blocks * 4 + 2 * 5 * n * 4 + 2 * n + 2 * n * 4
+    pad = 64
+    assert b == 2 * (28 + 8) * 8 * blocks * 4 + 2 * 5 * (n + pad) * 4 + 2 * (n + pad) + 2 * n * 4
     b16 = L.lbm_footprint_bytes(256, 256, 256, _capi.STORE_F16)
     assert b16 < b
     assert L.lbm_footprint_bytes(2, 8, 8, 0) == 0
