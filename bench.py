@@ -64,6 +64,8 @@ def parse():
                          "phases: test/bench_phases.mjs, the seven Sim phases timed one by one")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line without its fp16 / batch / served objects")
     return ap.parse_args()
 
 
@@ -233,12 +235,14 @@ def _shape_name(rows, zchunk):
     return f"{rows & 0xff}{'s' if rows & 0x100 else ''}x{zchunk}"
 
 
-def run_batch(args, dev, ws=1, rank=0):
+def batch_result(args, dev, ws=1, rank=0, steps=100):
     """64 seeded scenes of mixed sizes (FP16 storage) stepped together: one
     persistent fused launch per step, the steps replayed as a CUDA graph, tile
     shape from the autotuner; beside it the same scenes one after another.
     With N ranks each GPU takes whole scenes (placement.shard by cells); the
-    line reports all ranks' cells over the slowest rank's time."""
+    result counts all ranks' cells over the slowest rank's time.  The batched
+    fused kernel's roofline: 177 B per interior cell of every scene over its
+    CUDA-event time (lbm_batch_time_fused)."""
     import torch
 
     from b200lbm import Batch, autotune, placement, workloads
@@ -248,7 +252,8 @@ def run_batch(args, dev, ws=1, rank=0):
     specs = placement.shard(specs, ws, workloads.cells)[rank]
     scenes = [workloads.build(sp, storage, dev) for sp in specs]
     cells = sum(sim.n for sim, _ in scenes)
-    K = args.steps if args.steps != 2000 else 100
+    interior = sum((sim.nx - 2) * (sim.ny - 2) * (sim.nz - 2) for sim, _ in scenes)
+    K = steps
     with Batch(scenes) as batch:
         batch.run(2)
         rows, zchunk, timings = autotune.tune(batch, [sp["dims"] for sp in specs], storage, force=True)
@@ -267,6 +272,7 @@ def run_batch(args, dev, ws=1, rank=0):
         batch.run(K, use_graph=False)
         dt_eager = time.perf_counter() - t0
         fused = batch.launch_count() - l0
+        fused_ms = batch.time_fused(rows, zchunk, reps=10)
     t0 = time.perf_counter()
     for sim, solid in scenes:
         sim.run_coupled(solid, K)
@@ -276,27 +282,44 @@ def run_batch(args, dev, ws=1, rank=0):
     if ws > 1:
         cells = placement.sum_over_ranks(cells)
         dt_graph, dt_eager, dt_seq = (placement.max_over_ranks(v) for v in (dt_graph, dt_eager, dt_seq))
-    if rank != 0:
-        return
-    line = {
-        "metric": f"batched MLUPS, {args.scenes} seeded scenes of mixed sizes", "value": cells * K / dt_graph / 1e6,
-        "unit": UNIT, "n_gpus": ws, "steps": K, "higher_is_better": True, "dtype": storage,
-        "data": "synthetic", "scaling": "strong",
-        "config": {"workload": f"{args.scenes} scenes, edges U[32,160], pool 30-60% of ny, 1-3 spheres",
-                   "parallelism": f"whole scenes per GPU x{ws}",
-                   "cells": cells, "storage": storage, "tile": _shape_name(rows, zchunk),
-                   "timings_ms": {_shape_name(r, z): t for (r, z), t in timings.items()}},
-        "ms_per_step": dt_graph / K * 1e3,
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_CELL[storage] * interior / (fused_ms * 1e-3) / 1e9
+    return {
+        "mlups": cells * K / dt_graph / 1e6, "unit": UNIT, "steps": K, "storage": storage,
+        "ms_per_step": dt_graph / K * 1e3, "cells": cells, "scenes": args.scenes,
         "eager_mlups": cells * K / dt_eager / 1e6,
         "sequential_mlups": cells * K / dt_seq / 1e6,
         "batched_fused_launches": fused,
-        "timing": "wall clock around whole runs (host work included), after a synchronize",
+        "tile": _shape_name(rows, zchunk),
+        "timings_ms": {_shape_name(r, z): t for (r, z), t in timings.items()},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "k_fused_batch",
+                     "kernel_ms": fused_ms, "bytes_per_cell": BYTES_PER_CELL[storage],
+                     "cells_per_launch": interior},
+        "timing": "wall clock around whole runs (host work included), after a synchronize; "
+                  "kernel_ms by CUDA events (rank 0's scenes)",
         "clocks": clk,
+    }
+
+
+def run_batch(args, dev, ws=1, rank=0):
+    r = batch_result(args, dev, ws, rank, steps=args.steps if args.steps != 2000 else 100)
+    if rank != 0:
+        return
+    line = {
+        "metric": f"batched MLUPS, {args.scenes} seeded scenes of mixed sizes", "value": r["mlups"],
+        "unit": UNIT, "n_gpus": ws, "steps": r["steps"], "higher_is_better": True, "dtype": r["storage"],
+        "data": "synthetic", "scaling": "strong",
+        "config": {"workload": f"{args.scenes} scenes, edges U[32,160], pool 30-60% of ny, 1-3 spheres",
+                   "parallelism": f"whole scenes per GPU x{ws}", "cells": r["cells"], "storage": r["storage"],
+                   "tile": r["tile"], "timings_ms": r["timings_ms"]},
+        **{k: r[k] for k in ("ms_per_step", "eager_mlups", "sequential_mlups", "batched_fused_launches",
+                             "roofline", "timing", "clocks")},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args, dev, ws=1, rank=0):
+def serve_result(args, dev, ws=1, rank=0):
     """A seeded Poisson request stream (20/s, mixed sizes, 10% at 256^3,
     500-5000 steps, a frame every 20 steps) through the continuous-batching
     server (FP16 storage), and the same requests one at a time with plain
@@ -318,17 +341,27 @@ def run_serve(args, dev, ws=1, rank=0):
             r["scene_steps"] = placement.sum_over_ranks(r["scene_steps"])
             r["wall_s"] = placement.max_over_ranks(r["wall_s"])
             r["scene_steps_per_s"] = r["scene_steps"] / r["wall_s"]
+    return {
+        "scene_steps_per_s": rep["scene_steps_per_s"], "unit": "scene-steps/s", "storage": storage,
+        "frame_interval_s": rep["frame_interval_s"], "ttff_s": rep["ttff_s"],
+        "workload": f"{args.requests} requests, Poisson 20/s, sizes U[32,160]^3 + 10% 256^3, "
+                    "500-5000 steps, RG8 frame every 20 steps",
+        "served": rep, "sequential_plain_f32": seq,
+        "speedup_vs_sequential": rep["scene_steps_per_s"] / seq["scene_steps_per_s"],
+        "clocks": clk,
+    }
+
+
+def run_serve(args, dev, ws=1, rank=0):
+    r = serve_result(args, dev, ws, rank)
     if rank != 0:
         return
     line = {
         "metric": "served scene-steps/s, Poisson request stream of mixed-size scenes",
-        "value": rep["scene_steps_per_s"], "unit": "scene-steps/s", "n_gpus": ws,
-        "higher_is_better": True, "dtype": storage, "data": "synthetic",
-        "config": {"workload": f"{args.requests} requests, Poisson 20/s, sizes U[32,160]^3 + 10% 256^3, "
-                               "500-5000 steps, RG8 frame every 20 steps", "storage": storage},
-        "served": rep, "sequential_plain_f32": seq,
-        "speedup_vs_sequential": rep["scene_steps_per_s"] / seq["scene_steps_per_s"],
-        "clocks": clk,
+        "value": r["scene_steps_per_s"], "unit": "scene-steps/s", "n_gpus": ws,
+        "higher_is_better": True, "dtype": r["storage"], "data": "synthetic",
+        "config": {"workload": r["workload"], "storage": r["storage"]},
+        **{k: r[k] for k in ("served", "sequential_plain_f32", "speedup_vs_sequential", "clocks")},
     }
     print(json.dumps(line), flush=True)
 
@@ -525,6 +558,54 @@ def run_phases(args, dev):
     print(json.dumps(line), flush=True)
 
 
+def kernel_name(rows):
+    return "k_fused_pipe" if rows & 0x100 else "k_fused_step"
+
+
+def scene_form(args, storage, steps, dev, ws, local):
+    """The 256^3 scene in another storage form: `steps` device-resident steps
+    after the warm-up, CUDA events on the library's stream (max over ranks),
+    and the fused kernel's roofline."""
+    import torch
+
+    import scenes
+    from b200lbm import RigidSphere, Sim
+    from b200lbm._capi import LbmSphere, check, lib
+    L = lib()
+    size = args.size
+    sim, sol = scenes.cfg2(lambda *a: Sim(*a, storage=storage, device=dev), RigidSphere, n=size)
+    h = sim.handle
+    if args.rows:
+        check(h, L.lbm_set_fused_config(h, args.rows, args.zchunk or 32))
+    rows, zchunk = sim.fused_config()
+    sph = (LbmSphere * 1)()
+    sol.to_c(sph[0])
+    stream = torch.cuda.ExternalStream(L.lbm_stream(h), device=dev)
+    check(h, L.lbm_run_coupled(h, sph, 1, args.warmup, 0, None))
+    check(h, L.lbm_fused_timing(h, 1))
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    check(h, L.lbm_run_coupled(h, sph, 1, steps, 0, None))
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), ws, local)
+    fms, fn = C.c_double(), C.c_int64()
+    check(h, L.lbm_fused_timing_query(h, C.byref(fms), C.byref(fn)))
+    sim.close()
+    per_launch = fms.value / max(1, fn.value)
+    interior = (size - 2) ** 3
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_CELL[storage] * interior / (per_launch * 1e-3) / 1e9
+    return {"storage": storage, "mlups": ws * size ** 3 * steps / (ms * 1e-3) * 1e-6, "unit": UNIT,
+            "steps": steps, "ms_per_step": ms / steps, "tile": _shape_name(rows, zchunk),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "kernel": kernel_name(rows),
+                         "kernel_ms": per_launch, "bytes_per_cell": BYTES_PER_CELL[storage],
+                         "cells_per_launch": interior}}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args)
@@ -558,6 +639,7 @@ def main():
     if args.rows:
         check(h, L.lbm_set_fused_config(h, args.rows, args.zchunk or 32))
     sim._sync()
+    rows, zchunk = sim.fused_config()
     sph = (LbmSphere * 1)()
     sol.to_c(sph[0])
     stream = torch.cuda.ExternalStream(L.lbm_stream(h), device=dev)
@@ -639,6 +721,19 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(size, args.cpu_steps)
+    sphere_state = {"cx": sol.cx, "cy": sol.cy, "cz": sol.cz}
+    sim.close()
+
+    # the forms the metric names beside the plain line: FP16 storage on the
+    # same scene, the 64-scene batch, and the served request stream
+    extras = {}
+    if not args.no_extras:
+        if args.storage == "f32":
+            f16 = scene_form(args, "f16", min(args.steps, 1000), dev, ws, local)
+            f16["over_f32"] = f16["mlups"] / value
+            extras["fp16"] = f16
+        extras["batch"] = batch_result(args, dev, ws, rank, steps=100)
+        extras["served"] = serve_result(args, dev, ws, rank)
 
     if rank == 0:
         line = {
@@ -646,11 +741,11 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
             "config": scene_config(size, args.storage, ws),
-            "tile": {"fused_rows": args.rows or 4, "zchunk": args.zchunk or 32},
+            "tile": _shape_name(rows, zchunk),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,
-                         "kernel": "k_fused_step", "kernel_ms": per_launch_ms,
+                         "kernel": kernel_name(rows), "kernel_ms": per_launch_ms,
                          "bytes_per_cell": bpc, "cells_per_launch": interior},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
@@ -658,10 +753,10 @@ def main():
             "gpu_launches": int(c1.value - c0.value),
             "clocks": clk,
             "cpu_baseline": cpu,
-            "sphere": {"cx": sol.cx, "cy": sol.cy, "cz": sol.cz},
+            "sphere": sphere_state,
+            **extras,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -99,6 +99,9 @@ _SIGS = [
     ("lbm_host_free", C.c_int, [C.c_void_p]),
     ("lbm_run_coupled", C.c_int,
      [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    ("lbm_retag_cells_mask", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("lbm_solid_links", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("lbm_sphere_step_host", C.c_int,
      [C.POINTER(LbmSphere), C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
     ("lbm_synchronize", C.c_int, [C.c_void_p]),
@@ -115,6 +118,7 @@ _SIGS = [
     ("lbm_fused_timing", C.c_int, [C.c_void_p, C.c_int]),
     ("lbm_fused_timing_query", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("lbm_set_fused_config", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("lbm_get_fused_config", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("lbm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
     ("lbm_batch_destroy", C.c_int, [C.c_void_p]),
     ("lbm_batch_last_error", C.c_char_p, [C.c_void_p]),

@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _capi
 from ._capi import FIELDS, LbmImpulse, LbmParams, check, lib
-from .solid import impulse_array, spheres_of, to_c_array
+from .solid import evaluate_generic, impulse_array, is_generic, spheres_of, to_c_array
 
 
 class _HostBlock:
@@ -55,6 +55,12 @@ class _PinnedArray(np.ndarray):
     def __array_finalize__(self, obj):
         if obj is not None:
             self._block = getattr(obj, "_block", None)
+
+# D3Q27 velocity set, rest first then opposite pairs (src/lattices.js:34-49)
+_DIRS = ((0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1),
+         (1, 1, 0), (-1, -1, 0), (1, -1, 0), (-1, 1, 0), (1, 0, 1), (-1, 0, -1), (1, 0, -1),
+         (-1, 0, 1), (0, 1, 1), (0, -1, -1), (0, 1, -1), (0, -1, 1), (1, 1, 1), (-1, -1, -1),
+         (1, 1, -1), (-1, -1, 1), (1, -1, 1), (-1, 1, -1), (-1, 1, 1), (1, -1, -1))
 
 _PARAM_NAMES = ("tau", "tauPhi", "sigma", "gravity", "rhoL", "rhoG", "W", "mobility")
 # upload order: phi before h (h may be stored relative to phi), tags last
@@ -263,11 +269,56 @@ class Sim:
         self._moved()
 
     def retagCells(self, solid):
+        if is_generic(solid):
+            return self._retag_generic(solid)
         sp = spheres_of(solid)
         self._sync()
         arr = to_c_array(sp)
         check(self._h, lib().lbm_retag_cells(self._h, arr, len(sp)))
         self._moved()
+
+    # ------------------------------------------------------------ duck-typed solids
+    # Any object with contains / surfaceVelocity / applyImpulseAtCell
+    # (README.md:69-73) runs through the phase-by-phase kernels: its predicates
+    # are evaluated here on the host and uploaded as a mask, and its
+    # momentum exchange comes back as a scan-ordered list of links that is
+    # replayed through its applyImpulseAtCell (src/sim.js:517-536).
+    def _retag_generic(self, solid):
+        mask, us = evaluate_generic(solid, self.nx, self.ny, self.nz)
+        self._sync()
+        check(self._h, lib().lbm_retag_cells_mask(self._h, mask.ctypes.data_as(C.c_void_p),
+                                                  us.ctypes.data_as(C.c_void_p)))
+        self._moved()
+
+    def _links_generic(self, solid):
+        L = lib()
+        cnt = C.c_int()
+        check(self._h, L.lbm_solid_links(self._h, None, None, None, 0, C.byref(cnt)))
+        n = cnt.value
+        if n == 0:
+            return
+        cells = np.empty(n, dtype=np.int32)
+        dirs = np.empty(n, dtype=np.int8)
+        mom = np.empty(n, dtype=np.float64)
+        check(self._h, L.lbm_solid_links(self._h, cells.ctypes.data_as(C.c_void_p), dirs.ctypes.data_as(C.c_void_p),
+                                         mom.ctypes.data_as(C.c_void_p), n, C.byref(cnt)))
+        nx, nxny = self.nx, self.nx * self.ny
+        apply = solid.applyImpulseAtCell
+        for i, k, m in zip(cells.tolist(), dirs.tolist(), mom.tolist()):
+            ex, ey, ez = _DIRS[k]
+            z, r = divmod(i, nxny)
+            y, x = divmod(r, nx)
+            apply(x - ex, y - ey, z - ez, -m * ex, -m * ey, -m * ez)
+
+    def _step_generic(self, solid):
+        """src/sim.js:202-210 for a duck-typed solid, phase by phase."""
+        self._retag_generic(solid)
+        self.handleFreshCells(solid)
+        self.computePhiGradients()
+        self.collidePhase()
+        self.streamPhase()
+        self.collideHydro()
+        self.streamHydroAndMacro(solid)
 
     def handleFreshCells(self, solid=None):
         self._sync()
@@ -290,6 +341,12 @@ class Sim:
         self._moved()
 
     def streamHydroAndMacro(self, solid):
+        if is_generic(solid):
+            self._sync()
+            rc = lib().lbm_stream_hydro_and_macro(self._h, None, 0, None)
+            self._completed(rc, lambda: None)
+            self._links_generic(solid)
+            return
         sp = spheres_of(solid)
         self._sync()
         arr = to_c_array(sp)
@@ -298,7 +355,10 @@ class Sim:
         self._completed(rc, lambda: [b.add_impulse(out[i]) for i, b in enumerate(sp)])
 
     def step(self, solid):
-        """src/sim.js:202-210, as one fused device step."""
+        """src/sim.js:202-210, as one fused device step (phase by phase for a
+        duck-typed solid that is not made of RigidSpheres)."""
+        if is_generic(solid):
+            return self._step_generic(solid)
         sp = spheres_of(solid)
         self._sync()
         arr = to_c_array(sp)
@@ -411,6 +471,18 @@ class Sim:
             self._h, fr.ctypes.data_as(C.POINTER(C.c_int32)), nf.value,
             de.ctypes.data_as(C.POINTER(C.c_int32)), nd.value))
         return fr[:nf.value], de[:nd.value]
+
+    def fused_config(self):
+        """(rows, zchunk): the fused step's launch shape in use."""
+        r, z = C.c_int(), C.c_int()
+        check(self._h, lib().lbm_get_fused_config(self._h, C.byref(r), C.byref(z)))
+        return r.value, z.value
+
+    def set_fused_config(self, rows, zchunk=32):
+        """Fused step launch shape: rows per CTA (2, 4, 8; 4 or 6 | 0x100 for the
+        pipelined form) and z planes per CTA.  Every shape gives the same bits."""
+        self._sync()
+        check(self._h, lib().lbm_set_fused_config(self._h, int(rows), int(zchunk)))
 
     def launch_count(self):
         v = C.c_int64()

@@ -243,6 +243,12 @@ class CompositeSolid:
             b.step(dt, gravity)
 
 
+def is_generic(solid):
+    """A duck-typed solid that is not made of RigidSpheres (README.md:69-73:
+    any object with contains / surfaceVelocity / applyImpulseAtCell)."""
+    return solid is not None and not isinstance(solid, (RigidSphere, CompositeSolid))
+
+
 def spheres_of(solid):
     """The list of RigidSpheres behind a solid argument (None -> [])."""
     if solid is None:
@@ -252,7 +258,32 @@ def spheres_of(solid):
     if isinstance(solid, CompositeSolid):
         return solid.spheres
     raise TypeError(
-        "the device path takes a RigidSphere, a CompositeSolid or None; got " + type(solid).__name__)
+        "the sphere descriptors take a RigidSphere, a CompositeSolid or None; got " + type(solid).__name__)
+
+
+def evaluate_generic(solid, nx, ny, nz):
+    """retagCells' calls of a duck-typed solid (src/sim.js:214-244), in the
+    reference's order: solid.contains(x, y, z) for every interior cell and
+    solid.surfaceVelocity for the cells it contains.  Returns the mask (n
+    bytes) and the surface velocities (3n float32)."""
+    import numpy as np
+    n = nx * ny * nz
+    mask = np.zeros(n, dtype=np.uint8)
+    us = np.zeros(3 * n, dtype=np.float32)
+    tmp = [0.0, 0.0, 0.0]
+    contains, velocity = solid.contains, solid.surfaceVelocity
+    for z in range(1, nz - 1):
+        for y in range(1, ny - 1):
+            base = (z * ny + y) * nx
+            for x in range(1, nx - 1):
+                if contains(x, y, z):
+                    i = base + x
+                    mask[i] = 1
+                    velocity(x, y, z, tmp)
+                    us[3 * i] = tmp[0]
+                    us[3 * i + 1] = tmp[1]
+                    us[3 * i + 2] = tmp[2]
+    return mask, us
 
 
 def to_c_array(spheres):

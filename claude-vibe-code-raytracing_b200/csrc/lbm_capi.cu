@@ -426,7 +426,8 @@ void free_all(lbm_sim *h) {
   void *ptrs[] = {h->F[0], h->F[1], h->H[0], h->H[1], h->tag, h->tagPrev, h->grad[0], h->grad[1],
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
                   h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
-                  h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan, h->dWatch};
+                  h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan, h->dWatch, h->linkChunks,
+                  h->linkBuf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int c = 0; c < 2; c++)
@@ -935,6 +936,73 @@ int lbm_retag_cells(lbm_sim *h, const lbm_sphere *sp, int ns) {
   return LBM_OK;
 }
 
+int lbm_retag_cells_mask(lbm_sim *h, const uint8_t *solid_mask, const float *surface_velocity) {
+  if (!h || !solid_mask) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  const size_t n = (size_t)h->n;
+  const size_t usOff = (n + 255) / 256 * 256;
+  if ((rc = ensure_staging(h, usOff + (surface_velocity ? 12 * n : 0)))) return rc;
+  uint8_t *dMask = (uint8_t *)h->staging;
+  float *dUs = surface_velocity ? (float *)((uint8_t *)h->staging + usOff) : nullptr;
+  CK(copy_async(h, dMask, solid_mask, n, cudaMemcpyHostToDevice, h->stream));
+  if (dUs) CK(copy_async(h, dUs, surface_velocity, 12 * n, cudaMemcpyHostToDevice, h->stream));
+  h->ops->retag_mask(h, dMask, dUs);
+  CKL("retag (mask)");
+  CK(cudaStreamSynchronize(h->stream));  // the staging buffer is reused by the next call
+  // solid cells may be anywhere: a following fused step retags the whole grid
+  h->fullRetagSteps = 2;
+  h->lastRetagBox = interior(h);
+  h->listsValid = false;
+  return LBM_OK;
+}
+
+int lbm_solid_links(lbm_sim *h, int32_t *cells, int8_t *dirs, double *mom, int cap, int *count) {
+  if (!h || !count || cap < 0 || (cap > 0 && (!cells || !dirs || !mom))) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  const long long chunks = (h->n + LINK_CHUNK - 1) / LINK_CHUNK;
+  if (chunks + 1 > h->linkChunksCap) {
+    if (h->linkChunks) {
+      cudaFree(h->linkChunks);
+      h->deviceBytes -= h->linkChunksCap * sizeof(int);
+      h->linkChunks = nullptr;
+    }
+    DALLOC(h->linkChunks, (chunks + 1) * sizeof(int));
+    h->linkChunksCap = chunks + 1;
+  }
+  h->ops->link_count(h, h->linkChunks);
+  CKL("link count");
+  CK(copy_async(h, h->hTotals, h->linkChunks + chunks, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const int total = h->hTotals[0];
+  *count = total;
+  if (cap == 0 || total == 0) return LBM_OK;
+  const int take = std::min(cap, total);
+  const long long per = sizeof(double) + sizeof(int) + 1;
+  if (take > h->linkBufCap) {
+    if (h->linkBuf) {
+      cudaFree(h->linkBuf);
+      h->deviceBytes -= h->linkBufCap * per;
+      h->linkBuf = nullptr;
+    }
+    DALLOC(h->linkBuf, (size_t)take * per);
+    h->linkBufCap = take;
+  }
+  double *dMom = (double *)h->linkBuf;
+  int *dCells = (int *)(dMom + h->linkBufCap);
+  int8_t *dDirs = (int8_t *)(dCells + h->linkBufCap);
+  h->ops->link_emit(h, h->linkChunks, take, dCells, dDirs, dMom);
+  CKL("link emit");
+  CK(copy_async(h, cells, dCells, (size_t)take * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(copy_async(h, dirs, dDirs, (size_t)take, cudaMemcpyDeviceToHost, h->stream));
+  CK(copy_async(h, mom, dMom, (size_t)take * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
 int lbm_handle_fresh_cells(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);
@@ -1293,6 +1361,13 @@ int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;
   h->cfg.zchunk = zchunk;
+  return LBM_OK;
+}
+
+int lbm_get_fused_config(const lbm_sim *h, int *rows, int *zchunk) {
+  if (!h || !rows || !zchunk) return LBM_ERR_ARG;
+  *rows = h->cfg.ty;
+  *zchunk = h->cfg.zchunk;
   return LBM_OK;
 }
 

@@ -169,6 +169,10 @@ template <int Q>
 __host__ __device__ __forceinline__ long long pidx(int k, long long i) {
   return (i >> 3) * PopGroups<Q>::BLOCK + (i & 7) * 4 + pofs(k);
 }
+// elements of tail pad after every macro and tag array: the pipelined step
+// copies rows rounded out to 16-byte units, which can reach past the last cell
+constexpr long long ARRAY_PAD = 64;
+
 // elements of a Q-direction lattice over n cells (whole blocks)
 __host__ __device__ inline long long pop_elems(long long n, int Q) { return (n + 7) / 8 * 32 * ((Q + 3) / 4); }
 

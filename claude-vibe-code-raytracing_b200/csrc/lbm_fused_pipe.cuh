@@ -15,8 +15,8 @@
 //     warps right after the barrier that ends a plane, while the cell warps
 //     pull it, so their latency is off the critical path;
 //   * the ring stores, for each direction, only the cells that can be a
-//     source of that direction for the tile (32 or 33 columns by 4 or 5 rows)
-//     plus the tile itself for bounce-back: 46.7 KB instead of 63.6 KB, which
+//     source of that direction for the tile (33 columns by 4 or 5 rows)
+//     plus the tile itself for bounce-back: 47.3 KB instead of 63.6 KB, which
 //     leaves room for the stage at three CTAs per SM.
 //
 // Results are bit-identical to fused_tile (the collision is the same
@@ -31,14 +31,16 @@ namespace lbm {
 
 // ---------------------------------------------------------------- compact ring
 // Direction k's slot array in one ring copy covers the local columns
-// [cx0, cx0 + W) and rows [ry0, ry0 + H) of the tile (local (0, 0) is the
+// [cx0, cx0 + 33) and rows [ry0, ry0 + H) of the tile (local (0, 0) is the
 // tile's first cell; -1 and 32 / TY are the halo): a direction with e_x = +1
 // is pulled by column 0 from column -1, so its array starts at column -1, and
 // so on.  Every tile cell is inside every array (bounce-back reads the cell's
-// own value of the opposite direction).
+// own value of the opposite direction).  All arrays are 33 wide (one column
+// unused where e_x = 0), so a cell's index in any array is the same
+// per-thread term ty * 33 + tx plus a compile-time constant.
 template <int TY>
 struct PipeRing {
-  static constexpr int W(int k) { return 32 + (kDir[k][0] != 0 ? 1 : 0); }
+  static constexpr int W(int) { return 33; }
   static constexpr int H(int k) { return TY + (kDir[k][1] != 0 ? 1 : 0); }
   static constexpr int CX0(int k) { return kDir[k][0] > 0 ? -1 : 0; }
   static constexpr int RY0(int k) { return kDir[k][1] > 0 ? -1 : 0; }
@@ -71,7 +73,7 @@ struct PipeRing {
 };
 
 // ---------------------------------------------------------------- shared memory
-template <class PopT, int TY>
+template <class PopT, int TY, bool STG = true>
 struct PipeSmem {
   using Real = typename Prec<PopT>::Real;
   using R = PipeRing<TY>;
@@ -89,7 +91,8 @@ struct PipeSmem {
   static constexpr size_t stT = stM + (size_t)4 * TY * MROW * sizeof(Real);
   static constexpr size_t phiOff = stT + (size_t)TY * TROW;
   static constexpr size_t barOff = (phiOff + (size_t)3 * (TY + 2) * PROW * sizeof(Real) + 15) / 16 * 16;
-  static constexpr size_t bytes = barOff + 16;
+  // without the stage (cell warps load from global memory): ring and tags only
+  static constexpr size_t bytes = STG ? barOff + 16 : (tagOff + 3 * NC + 15) / 16 * 16;
   static constexpr int warps = TY + 2;  // TY cell warps, the halo rows above and below, the sides
   static constexpr int threads = 32 * warps;
   static_assert(sizeof(Real) == 4, "the pipelined form holds FP32 arithmetic values in its ring");
@@ -99,12 +102,12 @@ struct PipeSmem {
 };
 
 // ---------------------------------------------------------------- the tile
-template <class PopT, int TY, bool WIDE>
+template <class PopT, int TY, bool STG, bool WIDE>
 __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx, int by, int bz) {
   using POff = std::conditional_t<WIDE, long long, int>;
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
-  using SM = PipeSmem<PopT, TY>;
+  using SM = PipeSmem<PopT, TY, STG>;
   using R = PipeRing<TY>;
   using LD = CellLoad<PopT>;
   using CO = CellOut<PopT>;
@@ -151,7 +154,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   const int x = x0 + tx, y = y0 + ty;
   const int own = (ty + 1) * RX + (tx + 1);  // tag-plane index of a cell warp's cell
   const int span = min(31, nx - 1 - x0);     // last column of the tile's rows
-  const int r32 = ty * 32 + tx, r33 = ty * 33 + tx;
+  const int r33 = ty * 33 + tx;
 
   // Lanes of the side warp: the left half (lanes 0..15) takes the left column
   // (lanes 0..TY-1 for rows 0..TY-1, then the corners at rows -1 and TY), the
@@ -162,9 +165,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   const bool sideAct = sideLane < TY + 2;
   const int sideLx = sideRight ? RX - 1 : 0;                                          // frame column
   const int sideLy = sideLane < TY ? sideLane + 1 : (sideLane == TY ? 0 : TY + 1);   // frame row
-  const int sideSx = sideRight ? -1 : 1;
   const int sideSy = sideLane < TY ? 0 : (sideLane == TY ? 1 : -1);
-  const bool producer = haloSide && tx == 31;
+  const bool producer = STG && haloSide && tx == 31;
 
   // ---- halo loads (plain, into registers), as in fused_tile
   auto needs = [&](auto MODEc, auto SXc, auto SYc, auto KK, int sx, int sy,
@@ -251,7 +253,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       const long long a0 = phi_row0(P, r);
       const long long c1 = ((long long)P * ny + yy) * nx + x0 + span + 1;
       const uint32_t cnt = (uint32_t)((c1 | 3) - a0 + 1);
-      if (!lbm_ok(cnt <= PROW, 30, cnt)) continue;
+      if (!lbm_ok(cnt <= PROW, 30, cnt) || !lbm_ok(a0 + cnt <= nCell + ARRAY_PAD, 40, a0)) continue;
       if (go)
         bulk_g2s(smem_u32(sP + ((P % 3) * (TY + 2) + (r + 1)) * PROW), phiC + a0, cnt * sizeof(Real), bar);
       else
@@ -269,7 +271,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       const uint32_t mcnt = (uint32_t)(((row0 + span) | 3) - m0 + 1);
       const uint32_t tcnt = (uint32_t)(((row0 + span) | 15) - t0 + 1);
       const bool ok = lbm_ok(nb <= (uint32_t)SM::SB, 31, nb) && lbm_ok((b0 + nb) * BLK27 <= nF, 32, b0) &&
-                      lbm_ok(mcnt <= (uint32_t)MROW, 33, mcnt) && lbm_ok(tcnt <= (uint32_t)TROW, 34, tcnt);
+                      lbm_ok(mcnt <= (uint32_t)MROW, 33, mcnt) && lbm_ok(tcnt <= (uint32_t)TROW, 34, tcnt) &&
+                      lbm_ok(m0 + mcnt <= nCell + ARRAY_PAD, 41, m0) && lbm_ok(t0 + tcnt <= nCell + ARRAY_PAD, 42, t0);
       if (!ok) continue;
       if (go) {
         bulk_g2s(smem_u32(sF + r * ROWF), Fc + b0 * BLK27, nb * BLK27 * sizeof(PopT), bar);
@@ -376,7 +379,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         const int base = ez < 0 ? cM : (ez == 0 ? cZ : cP);
         int idx;
         if constexpr (MODE == 0) {
-          idx = base + (R::W(k) == 33 ? r33 : r32) + R::at(27, k, 0, 0);
+          idx = base + r33 + R::at(27, k, 0, 0);
         } else {
           idx = base + R::off(27, k) + (ly - R::RY0(k)) * R::W(k) + (lx - R::CX0(k));
         }
@@ -384,7 +387,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         if constexpr (k < Q7) {
           const int hb = ez < 0 ? hM : (ez == 0 ? hZ : hP);
           int hidx;
-          if constexpr (MODE == 0) hidx = hb + (R::W(k) == 33 ? r33 : r32) + R::at(7, k, 0, 0);
+          if constexpr (MODE == 0) hidx = hb + r33 + R::at(7, k, 0, 0);
           else hidx = hb + R::off(7, k) + (ly - R::RY0(k)) * R::W(k) + (lx - R::CX0(k));
           if (nd) ring[sm_at(hidx, RING, 8)] = o.h[k];
         }
@@ -399,8 +402,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   if (producer) {
     mbar_init(bar);
     mbar_init_fence();
-    *abortF = 0;
   }
+  if (STG && threadIdx.x == 0 && threadIdx.y == 0) *abortF = 0;
   __syncthreads();
   if (producer && !a.withhold) issue(zb - 1, true);
   uint32_t parity = 0;
@@ -409,13 +412,17 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   for (; q <= ze; q++) {
     CO o;
     if (cellWarp) {
-      if (!mbar_wait(bar, parity)) {
-        record_stage_timeout(q);
-        if (a.status) atomicOr(a.status, 1);
-        *abortF = 1;
-      }
       LD L;
-      stage_load(q, L);
+      if constexpr (STG) {
+        if (!mbar_wait(bar, parity)) {
+          record_stage_timeout(q);
+          if (a.status) atomicOr(a.status, 1);
+          *abortF = 1;
+        }
+        stage_load(q, L);
+      } else {
+        load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
+      }
       collide_cell<PopT, 0, 0, 0>(K, L, o, gxN, gyN, gzN, lapN, phN);
     } else {
       // the halo warps load after the barrier that ends the previous plane,
@@ -435,7 +442,9 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     parity ^= 1u;
     // every warp has pulled plane q - 2 and the cell warps have read the stage
     __syncthreads();
-    if (producer && q < ze && !*abortF) issue(q + 1, false);
+    if constexpr (STG) {
+      if (producer && q < ze && !*abortF) issue(q + 1, false);
+    }
     if (cellWarp) {
       emit(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, tx, ty, o);
     } else if (haloRows) {
@@ -447,7 +456,9 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       emit(IC<2>{}, IC<-1>{}, IC<0>{}, -1, sideSy, sideAct, q, sideLx - 1, sideLy - 1, o);
     }
     __syncthreads();
-    if (*abortF) break;
+    if constexpr (STG) {
+      if (*abortF) break;
+    }
 
     // pull plane z = q - 1 (nothing while z < zb)
     const int z = q - 1;
@@ -504,8 +515,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         const uint8_t ts = stag[sm_at(tb + so, TAGS, 13)];
         const bool fl = ts == TAG_FLUID;
         // source (tx - ex, ty - ey) in direction k's array; own cell in o's
-        const int si = sbF + (R::W(k) == 33 ? r33 : r32) + R::at(27, k, -ex, -ey);
-        const int oi = obF + (R::W(o) == 33 ? r33 : r32) + R::at(27, o, 0, 0);
+        const int si = sbF + r33 + R::at(27, k, -ex, -ey);
+        const int oi = obF + r33 + R::at(27, o, 0, 0);
         const Real fk = ring[sm_at(fl ? si : oi, RING, 14)];
         orTags |= ts;
         val4[k & 3] = fk;
@@ -522,8 +533,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         if constexpr (k < Q7) {
           const int sbH = ez < 0 ? sHM : (ez == 0 ? sHZ : sHP);
           const int obH = oz < 0 ? oHM : (oz == 0 ? sHZ : oHP);
-          const int shi = sbH + (R::W(k) == 33 ? r33 : r32) + R::at(7, k, -ex, -ey);
-          const int ohi = obH + (R::W(o) == 33 ? r33 : r32) + R::at(7, o, 0, 0);
+          const int shi = sbH + r33 + R::at(7, k, -ex, -ey);
+          const int ohi = obH + r33 + R::at(7, o, 0, 0);
           const Real hk = ring[sm_at(fl ? shi : ohi, RING, 16)];
           hn[k] = hk;
           hsum += hk;
@@ -560,7 +571,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
           int oi = oz < 0 ? oFM : (oz == 0 ? sFZ : oFP);
           static_for<1, Q27>([&](auto KK) {
             constexpr int kk = decltype(KK)::value;
-            if (kk == o) oi += (R::W(kk) == 33 ? r33 : r32) + R::at(27, kk, 0, 0);
+            if (kk == o) oi += r33 + R::at(27, kk, 0, 0);
           });
           const Real fopp = ring[sm_at(oi, RING, 19)];
           const Real fk = fopp + corr;
@@ -623,27 +634,29 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   // Stopped early (a wait ran out): the copy of stage q was issued (unless
   // withheld) and may still be in flight; let it land (bounded) before the
   // shared memory is released.  Normal exit: every issued copy was waited for.
-  if (q <= ze && producer && !(a.withhold && q == zb - 1)) mbar_wait(bar, parity ^ 1u);
-  __syncthreads();
-  if (producer) mbar_inval(bar);
+  if constexpr (STG) {
+    if (q <= ze && producer && !(a.withhold && q == zb - 1)) mbar_wait(bar, parity ^ 1u);
+    __syncthreads();
+    if (producer) mbar_inval(bar);
+  }
 }
 
 // CTAs per SM the register budget is sized for: 4 rows fit three CTAs per SM
 // in shared memory, 6 rows two
-template <int TY>
+template <int TY, bool STG>
 struct PipeOcc {
   static constexpr int blocks = TY <= 4 ? 3 : 2;
 };
 
-template <class PopT, int TY, bool WIDE>
-__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY>::blocks)
+template <class PopT, int TY, bool STG, bool WIDE>
+__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, STG>::blocks)
     k_fused_pipe(const __grid_constant__ FusedArgs<PopT> a) {
-  fused_tile_pipe<PopT, TY, WIDE>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fused_tile_pipe<PopT, TY, STG, WIDE>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many scenes in one persistent launch (as k_fused_batch)
-template <class PopT, int TY, bool WIDE>
-__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY>::blocks)
+template <class PopT, int TY, bool STG, bool WIDE>
+__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, STG>::blocks)
     k_fused_pipe_batch(const FusedArgs<PopT> *__restrict__ args, const int *__restrict__ tileStart,
                        const int3 *__restrict__ tileGrid, int nscenes) {
   const int total = tileStart[nscenes];
@@ -663,7 +676,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY>::blocks)
     if (lin < WORDS)
       reinterpret_cast<uint32_t *>(&sa)[lin] = reinterpret_cast<const uint32_t *>(args + lo)[lin];
     __syncthreads();
-    fused_tile_pipe<PopT, TY, WIDE>(sa, bx, by, bz);
+    fused_tile_pipe<PopT, TY, STG, WIDE>(sa, bx, by, bz);
     __syncthreads();
   }
 }

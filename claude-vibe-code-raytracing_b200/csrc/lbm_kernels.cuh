@@ -609,6 +609,131 @@ __global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, 
 // per sphere; thread t sums the contiguous t-th share of the list in scan
 // order, then a fixed shared-memory tree adds the shares -- deterministic,
 // and independent of how many dead cells there are per step.
+// ---------------------------------------------------------------- generic solids
+// retagCells(solid) for any duck-typed solid (src/sim.js:214-244): the host
+// has evaluated solid.contains / solid.surfaceVelocity per cell into mask
+// (non-zero = inside) and us (3 floats per cell, x y z; null = at rest).
+template <class PopT>
+__global__ void k_retag_mask(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const uint8_t *__restrict__ mask,
+                             const float *__restrict__ us) {
+  using Real = typename Prec<PopT>::Real;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  int x = (int)(i % nx);
+  long long t = i / nx;
+  int y = (int)(t % ny);
+  int z = (int)(t / ny);
+  s.tagPrev[i] = s.tag[i];
+  s.phi[1 - cur][i] = s.phi[cur][i];
+  if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
+    s.tag[i] = TAG_WALL;
+    s.usx[i] = s.usy[i] = s.usz[i] = (Real)0;
+  } else if (mask[i]) {
+    s.tag[i] = TAG_SOLID;
+    s.usx[i] = us ? (Real)us[3 * i] : (Real)0;
+    s.usy[i] = us ? (Real)us[3 * i + 1] : (Real)0;
+    s.usz[i] = us ? (Real)us[3 * i + 2] : (Real)0;
+  } else {
+    s.tag[i] = TAG_FLUID;
+    s.usx[i] = s.usy[i] = s.usz[i] = (Real)0;
+  }
+}
+
+// Momentum-exchange links of the last hydro stream (after
+// k_stream_hydro_macro, while F[1 - cur] still holds the post-collision f2):
+// for every interior FLUID cell i in scan order and every direction k whose
+// source i - e_k is SOLID, the link (i, k, m) with m = f2_opp(i) + f_k(i), the
+// value src/sim.js:529-531 hands to solid.applyImpulseAtCell (as
+// -m e_k at the solid cell).  Three passes: count per chunk, scan, emit.
+constexpr int LINK_CHUNK = 1024;  // cells per chunk = threads per block
+
+__device__ __forceinline__ uint32_t solid_links(const uint8_t *tag, long long i, int nx, int ny, int nz) {
+  if (tag[i] != TAG_FLUID || !interior_cell(i, nx, ny, nz)) return 0u;
+  uint32_t m = 0;
+  for (int k = 1; k < Q27; k++) {
+    const long long src = i - (((long long)dcomp(k, 2) * ny + dcomp(k, 1)) * nx + dcomp(k, 0));
+    if (tag[src] == TAG_SOLID) m |= 1u << k;
+  }
+  return m;
+}
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *sh, int &total) {
+  // Hillis-Steele over one block of LINK_CHUNK threads
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int d = 1; d < LINK_CHUNK; d <<= 1) {
+    const int a = t >= d ? sh[t - d] : 0;
+    __syncthreads();
+    sh[t] += a;
+    __syncthreads();
+  }
+  total = sh[LINK_CHUNK - 1];
+  const int excl = sh[t] - v;
+  __syncthreads();
+  return excl;
+}
+
+static __global__ void __launch_bounds__(LINK_CHUNK) k_link_count(const uint8_t *tag, int nx, int ny, int nz,
+                                                                 long long n, int *chunkCount) {
+  __shared__ int sh[LINK_CHUNK];
+  const long long i = (long long)blockIdx.x * LINK_CHUNK + threadIdx.x;
+  const int c = i < n ? __popc(solid_links(tag, i, nx, ny, nz)) : 0;
+  int total;
+  block_exclusive_scan(c, sh, total);
+  if (threadIdx.x == 0) chunkCount[blockIdx.x] = total;
+}
+
+// exclusive scan of the chunk counts in place; total into chunkCount[nchunks]
+static __global__ void k_link_scan(int *chunkCount, int nchunks) {
+  __shared__ int part[1024];
+  const int per = (nchunks + blockDim.x - 1) / blockDim.x;
+  const int b0 = threadIdx.x * per, b1 = min(b0 + per, nchunks);
+  int sum = 0;
+  for (int b = b0; b < b1; b++) sum += chunkCount[b];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int t = 0; t < (int)blockDim.x; t++) {
+      const int v = part[t];
+      part[t] = run;
+      run += v;
+    }
+    chunkCount[nchunks] = run;
+  }
+  __syncthreads();
+  int run = part[threadIdx.x];
+  for (int b = b0; b < b1; b++) {
+    const int v = chunkCount[b];
+    chunkCount[b] = run;
+    run += v;
+  }
+}
+
+template <class PopT>
+__global__ void __launch_bounds__(LINK_CHUNK) k_link_emit(Scene<PopT, typename Prec<PopT>::Real> s, int cur,
+                                                         const int *chunkOff, int cap, int *cells,
+                                                         int8_t *dirs, double *mom) {
+  __shared__ int sh[LINK_CHUNK];
+  const long long i = (long long)blockIdx.x * LINK_CHUNK + threadIdx.x;
+  const uint32_t m = i < s.n ? solid_links(s.tag, i, s.nx, s.ny, s.nz) : 0u;
+  int total;
+  int pos = chunkOff[blockIdx.x] + block_exclusive_scan(__popc(m), sh, total);
+  const PopT *f2 = s.F[1 - cur];
+  const PopT *f = s.F[cur];
+  for (uint32_t r = m; r; r &= r - 1, pos++) {
+    const int k = __ffs(r) - 1;
+    if (pos >= cap) break;
+    const double fopp = (double)Codec<PopT>::dec(f2[pidx<27>(opp_of(k), i)], 0);
+    const double fk = (double)Codec<PopT>::dec(f[pidx<27>(k, i)], 0);
+    cells[pos] = (int)i;
+    dirs[pos] = (int8_t)k;
+    mom[pos] = fopp + fk;
+  }
+}
+
 constexpr int DEAD_THREADS = 256;
 
 // (static: Real = float is instantiated by several translation units)

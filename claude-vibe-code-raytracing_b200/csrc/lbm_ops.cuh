@@ -142,6 +142,21 @@ class Ops final : public OpsBase {
     k_retag_full<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur, &h->dPlan->ss);
     h->launches++;
   }
+  void retag_mask(lbm_sim *h, const uint8_t *d_mask, const float *d_us) override {
+    k_retag_mask<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur, d_mask, d_us);
+    h->launches++;
+  }
+  void link_count(lbm_sim *h, int *d_chunks) override {
+    const unsigned chunks = nblocks(h->n, LINK_CHUNK);
+    k_link_count<<<chunks, LINK_CHUNK, 0, h->stream>>>(h->tag, h->nx, h->ny, h->nz, h->n, d_chunks);
+    k_link_scan<<<1, 1024, 0, h->stream>>>(d_chunks, (int)chunks);
+    h->launches += 2;
+  }
+  void link_emit(lbm_sim *h, const int *d_chunks, int cap, int *cells, int8_t *dirs, double *mom) override {
+    k_link_emit<PopT><<<nblocks(h->n, LINK_CHUNK), LINK_CHUNK, 0, h->stream>>>(scene(h), h->cur, d_chunks, cap,
+                                                                                cells, dirs, mom);
+    h->launches++;
+  }
   void collide_phase(lbm_sim *h) override {
     k_collide_phase<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur,
                                                                        make_const(h->params));
@@ -184,6 +199,8 @@ class Ops final : public OpsBase {
   // FP16/BF16 storage only); SHAPE_WIDE marks a launch over a grid whose
   // populations need 64-bit offsets.  f(IC<rows>, staged, wide) is called with
   // the shape's compile-time form.
+  // the compact-ring form without the stage: rows | LBM_FUSED_COMPACT
+  using Compact = std::integral_constant<int, 2>;
   template <class F>
   static void with_shape(int shape, F &&f) {
     const bool wide = (shape & SHAPE_WIDE) != 0;
@@ -192,6 +209,14 @@ class Ops final : public OpsBase {
       else f(T, S, std::false_type{});
     };
     switch (shape & ~SHAPE_WIDE) {
+      case 4 | LBM_FUSED_COMPACT:
+        if constexpr (kPipe) go(IC<4>{}, Compact{});
+        else go(IC<4>{}, std::false_type{});
+        break;
+      case 6 | LBM_FUSED_COMPACT:
+        if constexpr (kPipe) go(IC<6>{}, Compact{});
+        else go(IC<4>{}, std::false_type{});
+        break;
       case 2: go(IC<2>{}, std::false_type{}); break;
       case 4: go(IC<4>{}, std::false_type{}); break;
       case 4 | LBM_FUSED_STAGED:
@@ -210,31 +235,35 @@ class Ops final : public OpsBase {
   static constexpr bool kPipe = sizeof(Real) == 4;
   bool shape_ok(int shape) const override {
     return shape == 2 || shape == 4 || shape == 8 ||
-           ((shape == (4 | LBM_FUSED_STAGED) || shape == (6 | LBM_FUSED_STAGED)) && kPipe);
+           ((shape == (4 | LBM_FUSED_STAGED) || shape == (6 | LBM_FUSED_STAGED) ||
+             shape == (4 | LBM_FUSED_COMPACT) || shape == (6 | LBM_FUSED_COMPACT)) &&
+            kPipe);
   }
-  // shared memory and threads of a launch of either form
-  template <int TY, bool PIPE>
+  // shared memory, warps and kernels of a launch form: FORM 0 the plain
+  // fused kernel, 1 the pipelined form with its stage, 2 the compact ring
+  // without the stage
+  template <int TY, int FORM>
   static constexpr size_t smem_of() {
-    if constexpr (PIPE) return PipeSmem<PopT, TY>::bytes;
-    else return FusedSmem<PopT, TY, false>::bytes;
+    if constexpr (FORM == 0) return FusedSmem<PopT, TY, false>::bytes;
+    else return PipeSmem<PopT, TY, FORM == 1>::bytes;
   }
-  template <int TY, bool PIPE>
+  template <int TY, int FORM>
   static constexpr int warps_of() {
-    if constexpr (PIPE) return PipeSmem<PopT, TY>::warps;
-    else return FusedSmem<PopT, TY, false>::warps;
+    if constexpr (FORM == 0) return FusedSmem<PopT, TY, false>::warps;
+    else return PipeSmem<PopT, TY, FORM == 1>::warps;
   }
-  template <int TY, bool PIPE, bool WIDE>
+  template <int TY, int FORM, bool WIDE>
   static auto step_kernel() {
-    if constexpr (PIPE) return k_fused_pipe<PopT, TY, WIDE>;
-    else return k_fused_step<PopT, TY, false, WIDE>;
+    if constexpr (FORM == 0) return k_fused_step<PopT, TY, false, WIDE>;
+    else return k_fused_pipe<PopT, TY, FORM == 1, WIDE>;
   }
-  template <int TY, bool PIPE, bool WIDE>
+  template <int TY, int FORM, bool WIDE>
   static auto batch_kernel() {
-    if constexpr (PIPE) return k_fused_pipe_batch<PopT, TY, WIDE>;
-    else return k_fused_batch<PopT, TY, false, WIDE>;
+    if constexpr (FORM == 0) return k_fused_batch<PopT, TY, false, WIDE>;
+    else return k_fused_pipe_batch<PopT, TY, FORM == 1, WIDE>;
   }
 
-  template <int TY, bool STG, bool WIDE>
+  template <int TY, int STG, bool WIDE>
   void launch_fused(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
     constexpr size_t smem = smem_of<TY, STG>();
     const auto kern = step_kernel<TY, STG, WIDE>();
@@ -243,7 +272,6 @@ class Ops final : public OpsBase {
     const unsigned long long bit = 1ull << (h->device & 63);
     if (!(attrSet & bit)) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       attrSet |= bit;
     }
     dim3 block(32, warps_of<TY, STG>());  // TY cell warps and the halo warps
@@ -277,7 +305,7 @@ class Ops final : public OpsBase {
     FusedArgs<PopT> a = make_args(h, cur, zchunk);
     memcpy(out, &a, sizeof(a));
   }
-  template <int TY, bool STG, bool WIDE>
+  template <int TY, int STG, bool WIDE>
   int batch_ctas(int device) {
     constexpr size_t smem = smem_of<TY, STG>();
     const auto kern = batch_kernel<TY, STG, WIDE>();
@@ -285,7 +313,6 @@ class Ops final : public OpsBase {
     const unsigned long long bit = 1ull << (device & 63);
     if (!(attrSet & bit)) {
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       attrSet |= bit;
     }
     int per = 0, sms = 0;
@@ -304,7 +331,7 @@ class Ops final : public OpsBase {
                    int ctas, cudaStream_t st) override {
     with_shape(shape, [&](auto T, auto S, auto W) {
       constexpr int TY = decltype(T)::value;
-      constexpr bool STG = decltype(S)::value;
+      constexpr int STG = decltype(S)::value;
       dim3 block(32, warps_of<TY, STG>());
       batch_kernel<TY, STG, decltype(W)::value>()<<<ctas, block, smem_of<TY, STG>(), st>>>(
           (const FusedArgs<PopT> *)d_args, d_tileStart, d_tileGrid, nscenes);

@@ -29,9 +29,7 @@ inline int shape_rows(int shape) { return shape & 0xff; }
 // 2^31 elements, so the fused kernel uses 64-bit population offsets
 constexpr int SHAPE_WIDE = 0x200;
 inline bool needs_wide(long long cells) { return pop_elems(cells, 27) >= (1LL << 31) - 64; }
-// elements of tail pad after every macro and tag array (row copies of the
-// pipelined step are rounded out to 16-byte units)
-constexpr long long ARRAY_PAD = 64;
+
 
 class OpsBase {
  public:
@@ -44,6 +42,11 @@ class OpsBase {
   virtual void gradients(lbm_sim *h) = 0;
   // Kernels of a step read the sphere set and boxes from h->dPlan.
   virtual void retag_full(lbm_sim *h) = 0;
+  // retag from a host-evaluated solid mask and surface velocities (device copies)
+  virtual void retag_mask(lbm_sim *h, const uint8_t *d_mask, const float *d_us) = 0;
+  // momentum-exchange links of the last phase-by-phase hydro stream, scan order
+  virtual void link_count(lbm_sim *h, int *d_chunks) = 0;
+  virtual void link_emit(lbm_sim *h, const int *d_chunks, int cap, int *cells, int8_t *dirs, double *mom) = 0;
   virtual void collide_phase(lbm_sim *h) = 0;
   virtual void stream_phase(lbm_sim *h) = 0;
   virtual void collide_hydro(lbm_sim *h) = 0;
@@ -150,6 +153,11 @@ struct lbm_sim {
   lbm::Box lastRetagBox{{1, 1, 1}, {0, 0, 0}};
   int fullRetagSteps = 0;
   int nsphLast = 0;
+
+  int *linkChunks = nullptr;  // generic-solid link compaction: per-chunk counts, then offsets
+  long long linkChunksCap = 0;
+  void *linkBuf = nullptr;  // the link list (cells, moms, dirs) on the device
+  long long linkBufCap = 0;  // links
 
   size_t deviceBytes = 0;
   long long launches = 0;

@@ -582,6 +582,18 @@ static napi_value js_set_fused_config(napi_env env, napi_callback_info info) {
   return check_sim(env, h, lbm_set_fused_config(h, rows, zchunk));
 }
 
+/* getFusedConfig(h, Int32Array(2)) -> rows, zchunk */
+static napi_value js_get_fused_config(napi_env env, napi_callback_info info) {
+  Args a;
+  if (!args_get(env, info, &a, 2)) return NULL;
+  lbm_sim *h = arg_sim(&a, 0);
+  size_t len = 0;
+  int32_t *d = (int32_t *)arg_typed(&a, 1, napi_int32_array, &len);
+  if (a.failed) return NULL;
+  if (len < 2) return throw_msg(env, LBM_ERR_ARG, "getFusedConfig needs an Int32Array of 2");
+  return check_sim(env, h, lbm_get_fused_config(h, &d[0], &d[1]));
+}
+
 static napi_value js_test_withhold_stage_copy(napi_env env, napi_callback_info info) {
   Args a;
   if (!args_get(env, info, &a, 2)) return NULL;
@@ -777,6 +789,7 @@ static const napi_property_descriptor kExports[] = {
     FN("fusedTiming", js_fused_timing),
     FN("fusedTimingQuery", js_fused_timing_query),
     FN("setFusedConfig", js_set_fused_config),
+    FN("getFusedConfig", js_get_fused_config),
     FN("testWithholdStageCopy", js_test_withhold_stage_copy),
     FN("cameraDefault", js_camera_default),
     FN("render", js_render),

@@ -130,6 +130,14 @@ int lbm_seed_hydrostatic(lbm_sim *sim);
 /* spheres may be NULL with nspheres 0 (the reference's solid === null). */
 int lbm_retag_cells(lbm_sim *sim, const lbm_sphere *spheres, int nspheres);
 int lbm_handle_fresh_cells(lbm_sim *sim);
+/* retagCells(solid) for any duck-typed solid (src/sim.js:214-244, README.md:
+ * 69-73), the generic fallback beside the sphere descriptors: the host has
+ * called solid.contains(x, y, z) for every interior cell (solid_mask[i]
+ * non-zero where it returned true; n bytes) and solid.surfaceVelocity for
+ * those cells (surface_velocity[3*i .. 3*i+2], 3*n floats, or NULL for a
+ * solid at rest).  Boundary cells become WALL whatever the mask says.  The
+ * next fused lbm_step retags the whole grid. */
+int lbm_retag_cells_mask(lbm_sim *sim, const uint8_t *solid_mask, const float *surface_velocity);
 int lbm_compute_phi_gradients(lbm_sim *sim);
 int lbm_collide_phase(lbm_sim *sim);
 int lbm_stream_phase(lbm_sim *sim);
@@ -137,6 +145,16 @@ int lbm_collide_hydro(lbm_sim *sim);
 /* out: one lbm_impulse per sphere (may be NULL). */
 int lbm_stream_hydro_and_macro(lbm_sim *sim, const lbm_sphere *spheres, int nspheres,
                                lbm_impulse *out);
+
+/* The momentum-exchange links of the last lbm_stream_hydro_and_macro, for a
+ * duck-typed solid whose applyImpulseAtCell the host calls itself
+ * (src/sim.js:517-536): in the reference's scan order (cells z, y, x, then
+ * direction k), each FLUID cell i with a SOLID source i - e_k gives
+ * (cells[j] = i, dirs[j] = k, mom[j] = f2_opp(i) + f_k(i)); the impulse at
+ * the solid cell (x - ex, y - ey, z - ez) is -mom * e_k.  *count receives the
+ * number of links; at most cap are written (cap = 0 only counts).  Valid
+ * until the next call that changes f or f2. */
+int lbm_solid_links(lbm_sim *sim, int32_t *cells, int8_t *dirs, double *mom, int cap, int *count);
 
 /* ---- Sim.step (src/sim.js:202-210), fused ---------------------------------- */
 /* retag + fresh cells on the spheres' bounding boxes, then one fused
@@ -242,7 +260,13 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
  * memory by bulk asynchronous copy, waited on with bounded mbarrier waits.
  * Every shape gives the same results bit for bit. */
 #define LBM_FUSED_STAGED 0x100
+/* rows = 4 | LBM_FUSED_COMPACT or 6 | LBM_FUSED_COMPACT: the compact shared-
+ * memory ring of the pipelined form (each direction keeps only the cells that
+ * can source it) with the plain form's register loads (FP32/FP16/BF16). */
+#define LBM_FUSED_COMPACT 0x400
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
+/* The launch shape in use (the default or the last lbm_set_fused_config). */
+int lbm_get_fused_config(const lbm_sim *sim, int *rows, int *zchunk);
 
 /* ---- batches: many scenes stepped together ---------------------------------- */
 /* The reference advances one scene per Web Worker (src/worker.js:94-115); a

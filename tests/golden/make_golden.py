@@ -104,6 +104,7 @@ def main():
                 "pack_bytes": scenarios.run_pack(SimC, SphC, pack, built)}
 
     jobs["absorb_pack"] = absorb_pack
+    jobs["crate"] = lambda: scenarios.crate_fixture(scenarios.run_crate(SimC, built))
     for name, job in jobs.items():
         if args.only and name not in args.only:
             continue

@@ -201,3 +201,42 @@ def run_pack(SimC, SphC, pack, built=_noop):
     sim.phi[:] = pack_phi(sim.n)
     built(sim)
     return np.asarray(pack(sim), dtype=np.uint8).copy()
+
+
+CRATE_STEPS = 40
+
+
+def run_crate(SimC, built=_noop):
+    """A duck-typed solid that is not a sphere (scenes.Crate: a moving box)
+    in the drop preset's pool, CRATE_STEPS worker ticks: per step the force and
+    torque the stream gave it (through its applyImpulseAtCell), the dead-cell
+    impulse, the fresh / dead sets; the fields at the end."""
+    sim, box = scenes.crate(SimC)
+    built(sim)
+    rec = {"impulse_stream": [], "impulse_dead": [], "fresh": [], "dead": []}
+    for s in range(CRATE_STEPS):
+        sim.step(box)
+        fr, de = sets_of(sim)
+        rec["fresh"].append(fr)
+        rec["dead"].append(de)
+        rec["impulse_stream"].append([getattr(box, k) for k in IMPULSE_KEYS])
+        f0 = [getattr(box, k) for k in IMPULSE_KEYS]
+        box.absorbDeadCells(sim)
+        rec["impulse_dead"].append([getattr(box, k) - a for k, a in zip(IMPULSE_KEYS, f0)])
+        box.step(1.0, sim.gravity)
+    rec["fields"] = {fld: as_np(getattr(sim, fld)) for fld in FIELDS + ("tag",)}
+    return rec
+
+
+def crate_fixture(rec):
+    out = {}
+    for fld, a in rec["fields"].items():
+        out[f"sha_{fld}"] = np.array(digest(a))
+        out[f"sample_{fld}"] = a[::SAMPLE_STRIDE].copy()
+    for k in ("impulse_stream", "impulse_dead"):
+        out[k] = np.array(rec[k], dtype=np.float64)
+    out["n_fresh"] = np.array([len(x) for x in rec["fresh"]], dtype=np.int32)
+    out["n_dead"] = np.array([len(x) for x in rec["dead"]], dtype=np.int32)
+    out["fresh"] = np.concatenate(rec["fresh"]).astype(np.int32)
+    out["dead"] = np.concatenate(rec["dead"]).astype(np.int32)
+    return out

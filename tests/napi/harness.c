@@ -117,13 +117,15 @@ int main(int argc, char **argv) {
     napi_value ca[3] = {N(12), N(12), N(12)};
     napi_value h = stub_call(env, "create", 3, ca);
     expect_ok(env, "create");
+    /* test/smoke.mjs:7-15 order: initFlat runs with the constructor's
+     * parameters, the scene's parameters are set after it */
+    napi_value ia[2] = {h, N(6)};
+    stub_call(env, "initFlat", 2, ia);
+    expect_ok(env, "initFlat");
     double params[8] = {0.7, 0.7, 0.012, 0.0012, 1.0, 0.1, 4.0, 0.02};
     napi_value pa[2] = {h, stub_typed(napi_float64_array, params, 8)};
     stub_call(env, "setParams", 2, pa);
     expect_ok(env, "setParams");
-    napi_value ia[2] = {h, N(6)};
-    stub_call(env, "initFlat", 2, ia);
-    expect_ok(env, "initFlat");
     lbm_sphere sp;
     sphere_init(&sp, 6, 3, 6, 2.0, 1.5);
     double imp[6];

@@ -210,3 +210,75 @@ def field_err(a, b, norm=None):
     if norm:
         linf /= norm
     return rel, linf
+
+
+class Crate:
+    """A duck-typed solid that is not a sphere (README.md:69-73: any object
+    with contains / surfaceVelocity / applyImpulseAtCell works): an
+    axis-aligned box moving at a fixed velocity, kinematically (its step only
+    moves it), accumulating the force and torque the fluid exerts.  Its
+    absorbDeadCells follows src/solid.js:87-101 for this body."""
+
+    def __init__(self, lo, hi, vel):
+        self.lo = [float(v) for v in lo]
+        self.hi = [float(v) for v in hi]
+        self.vx, self.vy, self.vz = (float(v) for v in vel)
+        self.Fx = self.Fy = self.Fz = 0.0
+        self.Tx = self.Ty = self.Tz = 0.0
+
+    def centre(self):
+        return [(a + b) * 0.5 for a, b in zip(self.lo, self.hi)]
+
+    def contains(self, x, y, z):
+        p = (x + 0.5, y + 0.5, z + 0.5)
+        return all(self.lo[a] <= p[a] <= self.hi[a] for a in range(3))
+
+    def surfaceVelocity(self, x, y, z, out):
+        out[0] = self.vx
+        out[1] = self.vy
+        out[2] = self.vz
+
+    def applyImpulseAtCell(self, x, y, z, px, py, pz):
+        cx, cy, cz = self.centre()
+        rx, ry, rz = x + 0.5 - cx, y + 0.5 - cy, z + 0.5 - cz
+        self.Fx += px
+        self.Fy += py
+        self.Fz += pz
+        self.Tx += ry * pz - rz * py
+        self.Ty += rz * px - rx * pz
+        self.Tz += rx * py - ry * px
+
+    def absorbDeadCells(self, sim):
+        nx, ny, nz = sim.nx, sim.ny, sim.nz
+        tag, prev, phi = sim.tag, sim.tagPrev, sim.phi
+        ux, uy, uz = sim.ux, sim.uy, sim.uz
+        dRho = sim.rhoL - sim.rhoG
+        # dead cells are inside the box: scan its cells (in the reference's order)
+        rng = [range(max(1, int(self.lo[a] - 1)), min(n - 1, int(self.hi[a]) + 2))
+               for a, n in enumerate((nx, ny, nz))]
+        for z in rng[2]:
+            for y in rng[1]:
+                for x in rng[0]:
+                    i = (z * ny + y) * nx + x
+                    if tag[i] != 1 or prev[i] != 0:
+                        continue
+                    rhoPhase = sim.rhoG + float(phi[i]) * dRho
+                    self.applyImpulseAtCell(x, y, z, rhoPhase * float(ux[i]), rhoPhase * float(uy[i]),
+                                            rhoPhase * float(uz[i]))
+
+    def step(self, dt, gravity):
+        for a, v in enumerate((self.vx, self.vy, self.vz)):
+            self.lo[a] += dt * v
+            self.hi[a] += dt * v
+        self.Fx = self.Fy = self.Fz = 0.0
+        self.Tx = self.Ty = self.Tz = 0.0
+
+
+def crate(SimC, SphC=None):
+    """The drop preset's pool (src/worker.js:23-53; sigma 0.012, g 0.0012) with
+    a moving box instead of the sphere: 6.2 x 5.5 x 6.5 cells, not aligned to
+    the lattice, sliding down and sideways through the liquid."""
+    sim = SimC(40, 28, 40)
+    _params(sim, 0.85, 0.7, 0.012, 0.0012)
+    sim.initFlat(7)
+    return sim, Crate((14.2, 15.6, 17.3), (20.4, 21.1, 23.8), (0.03, -0.05, 0.02))

@@ -19,7 +19,7 @@ EXPECTED = """create destroy lastError getDims deviceBytes footprintBytes setPar
 downloadField downloadFieldF64 initFlat seedHydrostatic retagCells handleFreshCells computePhiGradients
 collidePhase streamPhase collideHydro streamHydroAndMacro step absorbDeadCells packVolume packVolumeAsync
 waitFrames runCoupled sphereStep synchronize setNanWatchdog lastSets launchCount checkedBuild faultRecord
-transferBytes fusedTiming fusedTimingQuery setFusedConfig testWithholdStageCopy cameraDefault render
+transferBytes fusedTiming fusedTimingQuery setFusedConfig getFusedConfig testWithholdStageCopy cameraDefault render
 batchCreate batchDestroy batchSetConfig batchRun batchTimeFused batchLaunchCount""".split()
 
 

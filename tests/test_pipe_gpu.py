@@ -1,6 +1,7 @@
 """The pipelined form of the fused step (tile shapes 4 | LBM_FUSED_STAGED and
 6 | LBM_FUSED_STAGED: tile rows staged in shared memory by bulk asynchronous
-copies, a compact ring) gives, bit for bit, what the plain 4-row form gives --
+copies, a compact ring) and the compact ring with register loads (4 or 6 |
+LBM_FUSED_COMPACT) give, bit for bit, what the plain 4-row form gives --
 for FP32, FP16 and BF16 storage, on grids whose rows start inside an 8-cell
 block (odd nx), with partial tiles in x and y, with moving spheres (SOLID
 links, fresh and dead cells) and a composite solid.  Run alone (lbm_step,
@@ -15,7 +16,9 @@ import scenes
 pytestmark = pytest.mark.gpu
 
 STAGED = 0x100
-PIPE_SHAPES = ((4 | STAGED, 32), (6 | STAGED, 32), (4 | STAGED, 5), (6 | STAGED, 9))
+COMPACT = 0x400
+PIPE_SHAPES = ((4 | STAGED, 32), (6 | STAGED, 32), (4 | STAGED, 5), (6 | STAGED, 9), (4 | COMPACT, 32),
+               (6 | COMPACT, 7))
 
 
 @pytest.fixture(scope="module")
@@ -104,7 +107,9 @@ def test_pipelined_batch_equals_alone(gpu, storage):
         batch.set_config(6 | STAGED, 32)
         batch.run(4)
         batch.set_config(4 | STAGED, 16)
-        batch.run(4, use_graph=False)
+        batch.run(2, use_graph=False)
+        batch.set_config(4 | COMPACT, 32)
+        batch.run(2)
     for i, ((sim, solid), (rsim, rsolid)) in enumerate(zip(mixed, ref)):
         a, sa = _state(sim, solid)
         b, sb = _state(rsim, rsolid)
