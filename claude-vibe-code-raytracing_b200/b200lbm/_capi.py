@@ -121,6 +121,7 @@ _SIGS = [
     ("lbm_get_fused_config", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("lbm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
     ("lbm_batch_destroy", C.c_int, [C.c_void_p]),
+    ("lbm_batch_set_scenes", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     ("lbm_batch_last_error", C.c_char_p, [C.c_void_p]),
     ("lbm_batch_set_config", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("lbm_batch_run", C.c_int,

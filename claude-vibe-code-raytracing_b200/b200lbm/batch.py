@@ -39,6 +39,18 @@ class Batch:
         if rows is not None or zchunk is not None:
             self.set_config(rows or 4, zchunk or 32)
 
+    def set_scenes(self, scenes):
+        """Replace the scenes (a list of (Sim, solid) pairs on the same device
+        and storage form) and keep the batch's stream, tables and frame
+        buffer; the step graph is captured anew at the next run."""
+        scenes = list(scenes)
+        if not scenes:
+            raise ValueError("a batch needs at least one scene")
+        n = len(scenes)
+        handles = (C.c_void_p * n)(*[sim.handle for sim, _ in scenes])
+        self._check(lib().lbm_batch_set_scenes(self._b, handles, n))
+        self.scenes = scenes
+
     def _check(self, rc):
         if rc != 0:
             raise LbmError(rc, (lib().lbm_batch_last_error(self._b) or b"").decode(errors="replace"))

@@ -6,10 +6,11 @@ runs many such scenes on one GPU at once:
 
   * a request names a scene (grid, pool level, spheres; see workloads.py), a
     number of steps and a frame cadence;
-  * admission: requests are taken in arrival order while their device
-    footprint (lbm_footprint_bytes plus the per-scene working buffers) fits
-    the memory budget; a request that does not fit waits until running scenes
-    finish and release theirs;
+  * admission by device footprint (lbm_footprint_bytes plus the per-scene
+    working buffers) against the memory budget, in arrival order, passing
+    over a request that does not fit yet to admit later ones that do -- until
+    the one passed over has waited AGE_LIMIT_S, after which nothing is
+    admitted ahead of it, so a large request still runs when memory frees;
   * an admitted scene is built and initialised on a worker thread, on its
     own stream, while the running scenes keep stepping; it joins at the next
     tick after it is ready;
@@ -19,7 +20,12 @@ runs many such scenes on one GPU at once:
     graph) by one frame interval, and every scene's RG8 volume is streamed
     back to the host;
   * between ticks finished scenes leave and newly arrived ones join, so work
-    that arrives while others run overlaps with them on the device.
+    that arrives while others run overlaps with them on the device; the
+    Batch object is kept and only told its new members (its stream, tables
+    and frame buffer stay; the step graph is captured anew);
+  * the tile shape is tuned incrementally (one candidate per tick) with the
+    timings kept per batch signature, so a membership seen before reuses its
+    shape.
 
 Each scene's results do not depend on what it was batched with: the batch
 gives every scene exactly the results of running it alone (tests/
@@ -53,21 +59,29 @@ def footprint(spec, storage):
     return int(base + _EXTRA_PER_CELL * nx * ny * nz + _EXTRA_FIXED)
 
 
-def admit(queue, used, budget, now, fp):
-    """Requests to admit now: the longest prefix of `queue` (arrival order)
-    that has arrived by `now` and fits in budget - used.  fp(req) -> bytes.
-    A request larger than the whole budget is admitted alone when nothing
-    else is running, so it is not starved forever (it may then fail to
-    allocate, which the caller reports)."""
+# a request passed over for lack of memory blocks later ones after this long
+AGE_LIMIT_S = 2.0
+
+
+def admit(queue, used, budget, now, fp, age_limit=AGE_LIMIT_S):
+    """Requests to admit now, in arrival order, among those that have arrived
+    by `now`: each that fits in budget - used is taken; one that does not fit
+    is passed over while it has waited less than age_limit seconds (later,
+    smaller requests may go ahead of it), and once it has waited longer
+    nothing more is admitted ahead of it.  fp(req) -> bytes.  A request
+    larger than the whole budget is admitted alone when nothing else is
+    running, so it is not starved forever (it may then fail to allocate,
+    which the caller reports)."""
     out = []
     for req in queue:
         if req["arrival"] > now:
             break
         need = fp(req)
-        if used + need > budget and not (used == 0 and not out):
+        if used + need <= budget or (used == 0 and not out):
+            out.append(req)
+            used += need
+        elif now - req["arrival"] >= age_limit:
             break
-        out.append(req)
-        used += need
     return out
 
 
@@ -109,6 +123,8 @@ class Server:
         members = None
         tuner = None
         ttff, interval, done_at = [], [], {}
+        tick_run, tick_tune = [], []  # seconds per tick: the batch's steps + frames, the tuner
+        changes = 0  # membership changes of the batch
         scene_steps = cell_steps = 0
         max_active = 0
         ticks = 0
@@ -121,7 +137,7 @@ class Server:
                 now = clock()
                 for req in admit(list(queue), used, self.budget, now,
                                  lambda r: footprint(r["spec"], self.storage)):
-                    queue.popleft()
+                    queue.remove(req)
                     fp = footprint(req["spec"], self.storage)
                     used += fp
                     building.append((req, fp, pool.submit(workloads.build, req["spec"], self.storage,
@@ -145,13 +161,18 @@ class Server:
                     continue
                 max_active = max(max_active, len(active))
                 ids = [a["req"]["rid"] for a in active]
+                tk0 = time.perf_counter()
                 if ids != members:
-                    if batch is not None:
-                        batch.close()
-                    batch = Batch([(a["sim"], a["solid"]) for a in active])
+                    pairs = [(a["sim"], a["solid"]) for a in active]
+                    if batch is None:
+                        batch = Batch(pairs)
+                    else:
+                        batch.set_scenes(pairs)
                     members = ids
+                    changes += 1
                     tuner = None
                 frames = batch.run(tick, frame_every=every, use_graph=self.use_graph)
+                tk1 = time.perf_counter()
                 ticks += 1
                 if self.tune:
                     # one candidate tile shape per tick: no tick waits for the whole list
@@ -160,6 +181,8 @@ class Server:
                             batch, [(a["sim"].nx, a["sim"].ny, a["sim"].nz) for a in active], self.storage)
                     tuner.step()
                 t = time.perf_counter() - t0
+                tick_run.append(tk1 - tk0)
+                tick_tune.append(t + t0 - tk1)
                 for a, fr in zip(active, frames):
                     for j in range(fr.shape[0]):
                         if a["frames"] == 0:
@@ -208,6 +231,9 @@ class Server:
             "frame_interval_s": percentiles(interval),
             "frames": len(ttff) + len(interval),
             "max_active": max_active,
+            "membership_changes": changes,
+            "tick_run_s": percentiles(tick_run),
+            "tick_tune_s": percentiles(tick_tune),
             "storage": self.storage,
             "budget_bytes": self.budget,
         }

@@ -1525,6 +1525,30 @@ int lbm_batch_destroy(lbm_batch *b) {
   return LBM_OK;
 }
 
+int lbm_batch_set_scenes(lbm_batch *b, lbm_sim *const *sims, int n) {
+  if (!b || !sims || n < 1) return LBM_ERR_ARG;
+  for (int s = 0; s < n; s++) {
+    if (!sims[s]) return bfail(b, LBM_ERR_ARG, "scene " + std::to_string(s) + " is NULL");
+    if (sims[s]->device != b->device || sims[s]->storage != b->storage)
+      return bfail(b, LBM_ERR_ARG, "scene " + std::to_string(s) + " is on another device or storage form");
+    for (int t = 0; t < s; t++)
+      if (sims[t] == sims[s]) return bfail(b, LBM_ERR_ARG, "a scene appears twice");
+  }
+  DeviceGuard g(b->device);
+  BCK(cudaStreamSynchronize(b->origin));
+  while ((int)b->joins.size() < n) {
+    cudaEvent_t ev = nullptr;
+    BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->joins.push_back(ev);
+  }
+  b->sims.assign(sims, sims + n);
+  // the captured graph names the old scenes: the next run captures anew
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+  b->execKey.clear();
+  return LBM_OK;
+}
+
 const char *lbm_batch_last_error(const lbm_batch *b) { return b ? b->err.c_str() : "null batch"; }
 
 int lbm_batch_set_config(lbm_batch *b, int rows, int zchunk) {

@@ -7,9 +7,10 @@
 //
 //   * the tile rows' populations, rho, u and tags of the next plane, and the
 //     phi rows of the plane after it, arrive in a shared-memory stage by bulk
-//     asynchronous copies (cp.async.bulk, completion counted in bytes on one
-//     mbarrier) issued by one producer lane while the current plane is pulled,
-//     so the cell warps never wait on a global load;
+//     asynchronous copies (cp.async.bulk, completion counted in bytes on an
+//     mbarrier), issued by one producer lane as soon as every cell warp has
+//     read the current plane out of the stage (a second mbarrier), so the copy
+//     lands while the current plane is collided and the previous one pulled;
 //   * the halo rows and columns (collided by two halo warps: the rows above
 //     and below, and the side columns with the corners) are loaded by those
 //     warps right after the barrier that ends a plane, while the cell warps
@@ -92,7 +93,8 @@ struct PipeSmem {
   static constexpr size_t phiOff = stT + (size_t)TY * TROW;
   static constexpr size_t barOff = (phiOff + (size_t)3 * (TY + 2) * PROW * sizeof(Real) + 15) / 16 * 16;
   // without the stage (cell warps load from global memory): ring and tags only
-  static constexpr size_t bytes = STG ? barOff + 16 : (tagOff + 3 * NC + 15) / 16 * 16;
+  // two mbarriers (stage full, stage read) and the abort flag
+  static constexpr size_t bytes = STG ? barOff + 32 : (tagOff + 3 * NC + 15) / 16 * 16;
   static constexpr int warps = TY + 2;  // TY cell warps, the halo rows above and below, the sides
   static constexpr int threads = 32 * warps;
   static_assert(sizeof(Real) == 4, "the pipelined form holds FP32 arithmetic values in its ring");
@@ -123,8 +125,9 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   Real *sM = reinterpret_cast<Real *>(smem_raw + SM::stM);          // [4][TY][MROW] rho ux uy uz
   uint8_t *sT = smem_raw + SM::stT;                                 // [TY][TROW]
   Real *sP = reinterpret_cast<Real *>(smem_raw + SM::phiOff);       // [3][TY + 2][PROW]
-  const uint32_t bar = smem_u32(smem_raw + SM::barOff);
-  int *abortF = reinterpret_cast<int *>(smem_raw + SM::barOff + 8);
+  const uint32_t bar = smem_u32(smem_raw + SM::barOff);       // stage q landed (1 arrival + bytes)
+  const uint32_t barE = smem_u32(smem_raw + SM::barOff + 8);  // stage q read (one arrival per cell warp)
+  int *abortF = reinterpret_cast<int *>(smem_raw + SM::barOff + 16);
 
   const auto &s = a.s;
   const SolidSet &ss = *a.ss;
@@ -166,7 +169,9 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   const int sideLx = sideRight ? RX - 1 : 0;                                          // frame column
   const int sideLy = sideLane < TY ? sideLane + 1 : (sideLane == TY ? 0 : TY + 1);   // frame row
   const int sideSy = sideLane < TY ? 0 : (sideLane == TY ? 1 : -1);
-  const bool producer = STG && haloSide && tx == 31;
+  // the producer: lane 0 of cell warp 0 issues each stage as soon as every
+  // cell warp has read the previous one
+  const bool producer = STG && ty == 0 && tx == 0;
 
   // ---- halo loads (plain, into registers), as in fused_tile
   auto needs = [&](auto MODEc, auto SXc, auto SYc, auto KK, int sx, int sy,
@@ -401,6 +406,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
 
   if (producer) {
     mbar_init(bar);
+    mbar_init_count(barE, TY);
     mbar_init_fence();
   }
   if (STG && threadIdx.x == 0 && threadIdx.y == 0) *abortF = 0;
@@ -420,6 +426,15 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
           *abortF = 1;
         }
         stage_load(q, L);
+        __syncwarp();
+        if (tx == 0) mbar_arrive(barE);
+        if (producer) {
+          // every cell warp has its plane-q values in registers: the stage and
+          // the phi slot of plane q - 1 are free for stage q + 1, which now
+          // lands while plane q is collided and plane q - 1 pulled.  A wait
+          // that ran out (set before the arrivals) stops the issuing.
+          if (mbar_wait(barE, parity) && q < ze && !*abortF) issue(q + 1, false);
+        }
       } else {
         load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
       }
@@ -442,9 +457,6 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     parity ^= 1u;
     // every warp has pulled plane q - 2 and the cell warps have read the stage
     __syncthreads();
-    if constexpr (STG) {
-      if (producer && q < ze && !*abortF) issue(q + 1, false);
-    }
     if (cellWarp) {
       emit(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, tx, ty, o);
     } else if (haloRows) {
@@ -637,7 +649,10 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   if constexpr (STG) {
     if (q <= ze && producer && !(a.withhold && q == zb - 1)) mbar_wait(bar, parity ^ 1u);
     __syncthreads();
-    if (producer) mbar_inval(bar);
+    if (producer) {
+      mbar_inval(bar);
+      mbar_inval(barE);
+    }
   }
 }
 

@@ -400,6 +400,48 @@ SIM_SPHERES_OUT(js_stream_hydro_and_macro, lbm_stream_hydro_and_macro)
 SIM_SPHERES_OUT(js_step, lbm_step)
 SIM_SPHERES_OUT(js_absorb_dead_cells, lbm_absorb_dead_cells)
 
+/* retagCellsMask(h, Uint8Array(n) mask, Float32Array(3n) | null velocities):
+ * retagCells for a duck-typed solid evaluated on the host */
+static napi_value js_retag_cells_mask(napi_env env, napi_callback_info info) {
+  Args a;
+  if (!args_get(env, info, &a, 2)) return NULL;
+  lbm_sim *h = arg_sim(&a, 0);
+  size_t mlen = 0, ulen = 0;
+  uint8_t *mask = (uint8_t *)arg_typed(&a, 1, napi_uint8_array, &mlen);
+  float *us = NULL;
+  if (a.argc > 2 && !is_nullish(&a, 2)) us = (float *)arg_typed(&a, 2, napi_float32_array, &ulen);
+  if (a.failed) return NULL;
+  int nx = 0, ny = 0, nz = 0, st = 0;
+  lbm_get_dims(h, &nx, &ny, &nz, &st);
+  const size_t n = (size_t)nx * ny * nz;
+  if (mlen < n || (us && ulen < 3 * n)) return throw_msg(env, LBM_ERR_ARG, "retagCellsMask: n mask bytes, 3n velocities");
+  return check_sim(env, h, lbm_retag_cells_mask(h, mask, us));
+}
+
+/* solidLinks(h, Int32Array cells | null, Int8Array dirs | null, Float64Array mom | null)
+ * -> number of links of the last streamHydroAndMacro (as many written as fit) */
+static napi_value js_solid_links(napi_env env, napi_callback_info info) {
+  Args a;
+  if (!args_get(env, info, &a, 1)) return NULL;
+  lbm_sim *h = arg_sim(&a, 0);
+  int32_t *cells = NULL;
+  int8_t *dirs = NULL;
+  double *mom = NULL;
+  size_t cl = 0, dl = 0, ml = 0;
+  if (a.argc > 3 && !is_nullish(&a, 1)) {
+    cells = (int32_t *)arg_typed(&a, 1, napi_int32_array, &cl);
+    dirs = (int8_t *)arg_typed(&a, 2, napi_int8_array, &dl);
+    mom = (double *)arg_typed(&a, 3, napi_float64_array, &ml);
+  }
+  if (a.failed) return NULL;
+  size_t cap = cl < dl ? cl : dl;
+  cap = cap < ml ? cap : ml;
+  int count = 0;
+  int rc = lbm_solid_links(h, cells, dirs, mom, cells ? (int)cap : 0, &count);
+  if (rc != LBM_OK) return check_sim(env, h, rc);
+  return num(env, (double)count);
+}
+
 /* packVolume(h, Uint8Array(2n)) (src/sim.js:586-600) */
 static napi_value js_pack_volume(napi_env env, napi_callback_info info) {
   Args a;
@@ -766,6 +808,8 @@ static const napi_property_descriptor kExports[] = {
     FN("initFlat", js_init_flat),
     FN("seedHydrostatic", js_seed_hydrostatic),
     FN("retagCells", js_retag_cells),
+    FN("retagCellsMask", js_retag_cells_mask),
+    FN("solidLinks", js_solid_links),
     FN("handleFreshCells", js_handle_fresh_cells),
     FN("computePhiGradients", js_compute_phi_gradients),
     FN("collidePhase", js_collide_phase),

@@ -32,11 +32,13 @@ const DIRS = [
   [1, 1, -1], [-1, -1, 1], [1, -1, 1], [-1, 1, -1], [-1, 1, 1], [1, -1, -1],
 ];
 
+// RigidSpheres behind a solid argument; null for a duck-typed solid of any
+// other kind (README.md:69-73), which takes the generic route below
 function spheresOf(solid) {
   if (solid == null) return [];
   if (solid instanceof RigidSphere) return [solid];
   if (Array.isArray(solid.spheres) && solid.spheres.every((s) => s instanceof RigidSphere)) return solid.spheres;
-  throw new TypeError('the CUDA path takes a RigidSphere, an object with .spheres, or null');
+  return null;
 }
 
 export class Sim {
@@ -140,9 +142,60 @@ export class Sim {
   computePhiGradients() { this._sync(); addon.computePhiGradients(this._h); this._moved(); }
   retagCells(solid) {
     const list = spheresOf(solid);
+    if (list === null) return this._retagGeneric(solid);
     this._sync();
     addon.retagCells(this._h, this._spheres(list));
     this._moved();
+  }
+
+  // ---------------------------------------------------------------- duck-typed solids
+  // contains / surfaceVelocity are called here for every interior cell, in the
+  // reference's order (src/sim.js:214-244), and uploaded as a mask; after the
+  // hydro stream the device returns the momentum-exchange links in scan order
+  // and each is applied through solid.applyImpulseAtCell (src/sim.js:517-536).
+  _retagGeneric(solid) {
+    const { nx, ny, nz } = this;
+    const mask = this._mask ?? (this._mask = new Uint8Array(this.n));
+    const us = this._us ?? (this._us = new Float32Array(3 * this.n));
+    mask.fill(0);
+    us.fill(0);
+    const tmp = [0, 0, 0];
+    for (let z = 1; z < nz - 1; z++) {
+      for (let y = 1; y < ny - 1; y++) {
+        for (let x = 1; x < nx - 1; x++) {
+          if (!solid.contains(x, y, z)) continue;
+          const i = (z * ny + y) * nx + x;
+          mask[i] = 1;
+          solid.surfaceVelocity(x, y, z, tmp);
+          us[3 * i] = tmp[0]; us[3 * i + 1] = tmp[1]; us[3 * i + 2] = tmp[2];
+        }
+      }
+    }
+    this._sync();
+    addon.retagCellsMask(this._h, mask, us);
+    this._moved();
+  }
+  _applyLinks(solid) {
+    const count = addon.solidLinks(this._h);
+    if (count === 0) return;
+    const cells = new Int32Array(count), dirs = new Int8Array(count), mom = new Float64Array(count);
+    addon.solidLinks(this._h, cells, dirs, mom);
+    const { nx } = this, nxny = this.nx * this.ny;
+    for (let j = 0; j < count; j++) {
+      const [ex, ey, ez] = DIRS[dirs[j]];
+      const i = cells[j], z = Math.floor(i / nxny), r = i - z * nxny, y = Math.floor(r / nx), x = r - y * nx;
+      const m = mom[j];
+      solid.applyImpulseAtCell(x - ex, y - ey, z - ez, -m * ex, -m * ey, -m * ez);
+    }
+  }
+  _stepGeneric(solid) {
+    this._retagGeneric(solid);
+    this.handleFreshCells(solid);
+    this.computePhiGradients();
+    this.collidePhase();
+    this.streamPhase();
+    this.collideHydro();
+    this.streamHydroAndMacro(solid);
   }
   handleFreshCells() { this._sync(); addon.handleFreshCells(this._h); this._moved(); }
   collidePhase() { this._sync(); addon.collidePhase(this._h); this._moved(); }
@@ -150,6 +203,7 @@ export class Sim {
   collideHydro() { this._sync(); addon.collideHydro(this._h); this._moved(); }
   _withImpulses(call, solid) {
     const list = spheresOf(solid);
+    if (list === null) throw new TypeError('a duck-typed solid keeps its own absorbDeadCells');
     this._sync();
     try {
       call(this._h, this._spheres(list), this._impulses);
@@ -158,9 +212,25 @@ export class Sim {
     }
     for (let b = 0; b < list.length; b++) list[b].addImpulse(this._impulses, 6 * b);
   }
-  streamHydroAndMacro(solid) { this._withImpulses(addon.streamHydroAndMacro, solid); }
-  // src/sim.js:202-210 as one fused device step
-  step(solid) { this._withImpulses(addon.step, solid); }
+  streamHydroAndMacro(solid) {
+    if (spheresOf(solid) === null) {
+      this._sync();
+      try {
+        addon.streamHydroAndMacro(this._h, null, this._impulses);
+      } finally {
+        this._moved();
+      }
+      this._applyLinks(solid);
+      return;
+    }
+    this._withImpulses(addon.streamHydroAndMacro, solid);
+  }
+  // src/sim.js:202-210 as one fused device step (phase by phase for a
+  // duck-typed solid that is not made of RigidSpheres)
+  step(solid) {
+    if (spheresOf(solid) === null) return this._stepGeneric(solid);
+    this._withImpulses(addon.step, solid);
+  }
   _absorbDeadCells(solid) { this._withImpulses(addon.absorbDeadCells, solid); }
   // src/sim.js:586-600 (the second argument is ignored, as in the reference)
   packVolume(out) {
@@ -174,6 +244,7 @@ export class Sim {
   // state comes back into their RigidSphere objects
   runCoupled(solid, nsteps, frameEvery = 0, frames = null) {
     const list = spheresOf(solid);
+    if (list === null) throw new TypeError('runCoupled integrates RigidSpheres on the device');
     this._sync();
     const buf = this._spheres(list);
     try {

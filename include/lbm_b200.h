@@ -282,6 +282,11 @@ int lbm_get_fused_config(const lbm_sim *sim, int *rows, int *zchunk);
 typedef struct lbm_batch lbm_batch;
 int lbm_batch_create(lbm_sim *const *sims, int n, lbm_batch **out);
 int lbm_batch_destroy(lbm_batch *batch);
+/* Replace the batch's scenes (same device and storage form), keeping its
+ * stream, events, tables and page-locked frame buffer: a continuous-batching
+ * server changes membership between ticks without building a new batch.  The
+ * step graph is captured anew at the next lbm_batch_run. */
+int lbm_batch_set_scenes(lbm_batch *batch, lbm_sim *const *sims, int n);
 const char *lbm_batch_last_error(const lbm_batch *batch);
 int lbm_batch_set_config(lbm_batch *batch, int rows, int zchunk);
 /* nsteps coupled steps of every scene (lbm_run_coupled semantics): spheres[s]

@@ -9,14 +9,16 @@ def _req(rid, arrival, size):
     return dict(rid=rid, arrival=arrival, spec=dict(dims=(size, size, size)), steps=40, frame_every=20)
 
 
-def test_admission_takes_arrived_prefix_within_budget():
+def test_admission_within_budget_with_aging():
     q = [_req(0, 0.0, 10), _req(1, 0.1, 20), _req(2, 0.2, 10), _req(3, 5.0, 10)]
     fp = lambda r: r["spec"]["dims"][0]  # noqa: E731
-    # all arrived but the last; the budget stops at the second request
-    assert [r["rid"] for r in serve.admit(q, 0, 25, 1.0, fp)] == [0]
+    # all arrived but the last; the second does not fit, the third does
+    assert [r["rid"] for r in serve.admit(q, 0, 25, 1.0, fp)] == [0, 2]
     assert [r["rid"] for r in serve.admit(q, 0, 40, 1.0, fp)] == [0, 1, 2]
-    # arrival order is kept: a small request does not overtake a big one
-    assert [r["rid"] for r in serve.admit(q[1:], 10, 25, 1.0, fp)] == []
+    # a request that does not fit is passed over by smaller later ones ...
+    assert [r["rid"] for r in serve.admit(q[1:], 10, 25, 1.0, fp)] == [2]
+    # ... until it has waited the aging bound; then nothing goes ahead of it
+    assert [r["rid"] for r in serve.admit(q[1:], 10, 25, 0.1 + serve.AGE_LIMIT_S, fp)] == []
     # nothing arrived yet
     assert serve.admit(q, 0, 100, -1.0, fp) == []
     # an oversized request runs alone when the device is idle
