@@ -127,7 +127,7 @@ Box interior(const lbm_sim *h) {
 Box spheres_box(const lbm_sim *h, const lbm_sphere *sp, int ns) {
   Box u{{1, 1, 1}, {0, 0, 0}};
   for (int b = 0; b < ns; b++)
-    u = box_union(u, sphere_box(sp[b].cx, sp[b].cy, sp[b].cz, sp[b].r, h->nx, h->ny, h->nz));
+    u = box_union(u, sphere_box(sp[b].cx, sp[b].cy, sp[b].cz - h->zoff, sp[b].r, h->nx, h->ny, h->nz));
   return u;
 }
 
@@ -150,6 +150,10 @@ int set_solids(lbm_sim *h, const lbm_sphere *sp, int ns, bool targets) {
   SolidSet &ss = h->hPlan.ss;
   memset(&ss, 0, sizeof(ss));
   ss.nsph = ns;
+  if (h->slab) {
+    ss.zlo = h->ownLo;
+    ss.zend = h->ownHi + 1;
+  }
   long long off = 0;
   int maxChunks = 1;
   long long offs[LBM_MAX_SPHERES] = {0};
@@ -157,7 +161,10 @@ int set_solids(lbm_sim *h, const lbm_sphere *sp, int ns, bool targets) {
     SphereDesc &d = ss.sph[b];
     d.cx = sp[b].cx;
     d.cy = sp[b].cy;
-    d.cz = sp[b].cz;
+    // a slab works in its local frame: z - zoff, exactly (cz - zoff is exact
+    // for integer zoff, so every contains / surfaceVelocity / torque-arm
+    // difference rounds as it does in the global frame)
+    d.cz = sp[b].cz - h->zoff;
     d.r = sp[b].r;
     d.vx = sp[b].vx;
     d.vy = sp[b].vy;
@@ -167,6 +174,10 @@ int set_solids(lbm_sim *h, const lbm_sphere *sp, int ns, bool targets) {
     d.wz = sp[b].wz;
     if (!targets) continue;
     Box bx = box_grow(sphere_box(d.cx, d.cy, d.cz, d.r, h->nx, h->ny, h->nz), 1, h->nx, h->ny, h->nz);
+    if (h->slab) {  // links of cells outside the owned planes belong to the neighbour
+      bx.lo[2] = std::max(bx.lo[2], h->ownLo);
+      bx.hi[2] = std::min(bx.hi[2], h->ownHi);
+    }
     ImpulseTarget &t = ss.imp[b];
     long long cells = 0;
     if (box_empty(bx)) {
@@ -462,6 +473,9 @@ struct CoupledCtx {
 int coupled_prepare(lbm_sim *h, const lbm_sphere *sp, int ns, bool frames, CoupledCtx &c) {
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
+  if (h->slab)
+    return fail(h, LBM_ERR_UNSUPPORTED,
+                "a z slab steps with lbm_step: its sphere needs every slab's impulses before it moves");
   if (h->bfActive) return fail(h, LBM_ERR_STATE, "a pending body force needs lbm_step");
   if (!h->fusedOK) return fail(h, LBM_ERR_UNSUPPORTED, "grid too large for the fused kernel");
   double rmax = 0;
@@ -1361,6 +1375,63 @@ int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;
   h->cfg.zchunk = zchunk;
+  return LBM_OK;
+}
+
+int lbm_set_slab(lbm_sim *h, int zoff, int own_lo, int own_hi) {
+  if (!h) return LBM_ERR_ARG;
+  if (own_lo < 1 || own_hi > h->nz - 2 || own_lo > own_hi || zoff < 0)
+    return fail(h, LBM_ERR_ARG, "owned planes must lie in 1 .. nz - 2 and zoff >= 0");
+  if (((long long)h->nx * h->ny) % 8 != 0)
+    return fail(h, LBM_ERR_ARG, "slabs need nx * ny divisible by 8 (whole population blocks per plane)");
+  h->slab = true;
+  h->zoff = zoff;
+  h->ownLo = own_lo;
+  h->ownHi = own_hi;
+  h->fullRetagSteps = 2;
+  return LBM_OK;
+}
+
+int lbm_slab_copy_planes(lbm_sim *dst, int dst_plane, const lbm_sim *src, int src_plane, int nplanes) {
+  if (!dst || !src || nplanes < 0) return LBM_ERR_ARG;
+  if (dst->nx != src->nx || dst->ny != src->ny || dst->storage != src->storage)
+    return fail(dst, LBM_ERR_ARG, "slabs of one scene share nx, ny and the storage form");
+  if (dst_plane < 0 || src_plane < 0 || dst_plane + nplanes > dst->nz || src_plane + nplanes > src->nz)
+    return fail(dst, LBM_ERR_ARG, "planes out of range");
+  const long long nxny = (long long)dst->nx * dst->ny;
+  if (nxny % 8 != 0) return fail(dst, LBM_ERR_ARG, "slabs need nx * ny divisible by 8");
+  if (nplanes == 0) return LBM_OK;
+  lbm_sim *h = dst;  // errors are reported on the destination handle
+  DeviceGuard g(dst->device);
+  if (dst->device != src->device) {
+    // NVLink peer copies; an already-enabled peer is fine
+    cudaError_t pe = cudaDeviceEnablePeerAccess(src->device, 0);
+    if (pe != cudaSuccess && pe != cudaErrorPeerAccessAlreadyEnabled) return cuda_fail(dst, "peer access", pe);
+    cudaGetLastError();
+  }
+  // the source's step must be complete
+  CK(cudaStreamSynchronize(src->stream));
+  const size_t pb = dst->ops->pop_bytes(), mb = dst->ops->macro_bytes();
+  auto copy = [&](void *d, const void *s, size_t bytes) -> cudaError_t {
+    if (dst->device == src->device) return cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, dst->stream);
+    return cudaMemcpyPeerAsync(d, dst->device, s, src->device, bytes, dst->stream);
+  };
+  const long long cells = nxny * nplanes;
+  const long long dc = nxny * dst_plane, sc = nxny * src_plane;
+  // populations: whole 8-cell blocks of the current half
+  const struct { int Q; void *d; const void *s; } pops[] = {{27, dst->F[dst->cur], src->F[src->cur]},
+                                                           {7, dst->H[dst->cur], src->H[src->cur]}};
+  for (const auto &p : pops) {
+    const size_t blk = (size_t)32 * ((p.Q + 3) / 4) * pb;  // bytes of one 8-cell block
+    CK(copy((char *)p.d + (size_t)(dc / 8) * blk, (const char *)p.s + (size_t)(sc / 8) * blk,
+            (size_t)(cells / 8) * blk));
+  }
+  for (int a = 0; a < 5; a++)
+    CK(copy((char *)dst->mac[dst->cur][a] + dc * mb, (const char *)src->mac[src->cur][a] + sc * mb,
+            (size_t)cells * mb));
+  CK(copy(dst->tag + dc, src->tag + sc, (size_t)cells));
+  CK(cudaStreamSynchronize(dst->stream));
+  dst->listsValid = false;
   return LBM_OK;
 }
 

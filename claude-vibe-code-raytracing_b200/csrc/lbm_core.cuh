@@ -341,6 +341,9 @@ struct ImpulseTarget {
 
 struct SolidSet {
   int nsph;
+  // z slab: dead cells outside local planes [zlo, zend) give no impulse (their
+  // slab's neighbour owns them); zend = 0 (the default) means no limit
+  int zlo, zend;
   SphereDesc sph[LBM_MAX_SPHERES];
   ImpulseTarget imp[LBM_MAX_SPHERES];
 };

@@ -759,6 +759,7 @@ static __global__ void __launch_bounds__(DEAD_THREADS)
     const long long t = i / nx;
     const int y = (int)(t % ny);
     const int z = (int)(t / ny);
+    if (ss.zend > 0 && (z < ss.zlo || z >= ss.zend)) continue;
     if (owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) != b) continue;
     const double rhoPhase = __dadd_rn(rhoG, __dmul_rn((double)phi[i], dRho));
     impulse_terms(ss.sph[b], x, y, z, __dmul_rn(rhoPhase, (double)ux[i]),

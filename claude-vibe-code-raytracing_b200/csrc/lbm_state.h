@@ -154,6 +154,12 @@ struct lbm_sim {
   int fullRetagSteps = 0;
   int nsphLast = 0;
 
+  // z slab of a larger scene (lbm_set_slab): local plane k is global plane
+  // k + zoff; planes [ownLo, ownHi] are this handle's, the others copies of
+  // its neighbours' (slab = false: the whole grid is the scene)
+  bool slab = false;
+  int zoff = 0, ownLo = 0, ownHi = 0;
+
   int *linkChunks = nullptr;  // generic-solid link compaction: per-chunk counts, then offsets
   long long linkChunksCap = 0;
   void *linkBuf = nullptr;  // the link list (cells, moms, dirs) on the device

@@ -265,6 +265,25 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
  * can source it) with the plain form's register loads (FP32/FP16/BF16). */
 #define LBM_FUSED_COMPACT 0x400
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
+/* ---- one scene in z slabs (several handles, one or more GPUs) -------------- */
+/* Declares the handle a z slab of a larger scene: its local plane k is the
+ * scene's plane k + zoff; local planes own_lo .. own_hi (within 1 .. nz - 2)
+ * are this slab's own, the planes below and above them copies of the
+ * neighbouring slabs' (two planes each side, so the copied plane next to the
+ * owned ones collides with a complete phi stencil; the outermost local plane
+ * is the scene's wall or a copy whose results are discarded).  Spheres keep
+ * the scene's coordinates: the library shifts them into the slab's frame
+ * (exactly: zoff is an integer).  Impulses (lbm_step, lbm_absorb_dead_cells)
+ * cover the owned planes only, so the slabs' impulses add up to the scene's.
+ * Needs nx * ny divisible by 8.  The reference has no counterpart: it is one
+ * scene in one typed-array set (src/sim.js:30-96); this splits scenes larger
+ * than one GPU.  lbm_run_coupled and batches refuse slabs. */
+int lbm_set_slab(lbm_sim *sim, int zoff, int own_lo, int own_hi);
+/* After a step of both: copy nplanes planes (populations, phi, rho, u and tags
+ * of the current state) from src's plane src_plane on to dst's plane
+ * dst_plane -- the halo exchange between neighbouring slabs, device to device
+ * (over NVLink between GPUs, with peer access enabled here).  Synchronous. */
+int lbm_slab_copy_planes(lbm_sim *dst, int dst_plane, const lbm_sim *src, int src_plane, int nplanes);
 /* The launch shape in use (the default or the last lbm_set_fused_config). */
 int lbm_get_fused_config(const lbm_sim *sim, int *rows, int *zchunk);
 

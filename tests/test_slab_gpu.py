@@ -1,0 +1,101 @@
+"""One scene in z slabs (b200lbm.SlabSim: lbm_set_slab, lbm_slab_copy_planes)
+against the same scene in one handle, on one GPU (the slabs are separate
+handles whose copied planes cross by device copies, as they would over
+NVLink between GPUs).
+
+  * the 256^3 benchmark scene scaled to 48^3 (liquid below a wavy interface,
+    so the fields vary in z; the sphere rests): 2 and 3 slabs give every
+    field bit for bit what one handle gives after 30 ticks;
+  * the drop preset (the sphere falls 2 cells, with fresh and dead cells):
+    2 slabs track one handle -- the slabs' impulse sums add in another order,
+    so the sphere differs by FP64 rounding and the fields by what that moves.
+"""
+import numpy as np
+import pytest
+
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("phi", "rho", "ux", "uy", "uz", "f", "h", "tag")
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import b200lbm
+    return b200lbm
+
+
+def _slab_factory(gpu, nslabs):
+    def make(nx, ny, nz):
+        return gpu.SlabSim(nx, ny, nz, nslabs=nslabs)
+    return make
+
+
+def _setup_wavy(sim, n):
+    """scenes.cfg2 at n^3 on either kind of scene (fields written scene-wide)."""
+    s = n / 256.0
+    scenes._params(sim, 0.6, 0.8, 1e-3, -1e-5)
+    sim.initFlat(96 * s)
+    yw = scenes.cfg2_interface(n, n, 0, level=96 * s, wavelength=64 * s)
+    ys = np.arange(n, dtype=np.float64)[None, :, None]
+    phi = (0.5 * (1 + np.tanh(2 * (yw[:, None, :] - ys) / 4.0))).reshape(-1)
+    h = (phi[:, None] * scenes.W7[None, :]).astype(np.float32).reshape(-1)
+    if hasattr(sim, "set_field"):
+        sim.set_field("phi", phi.astype(np.float32))
+        sim.set_field("phiPrev", phi.astype(np.float32))
+        sim.set_field("h", h)
+    else:
+        sim.phi[:] = phi.astype(np.float32)
+        sim.phiPrev[:] = phi.astype(np.float32)
+        sim.h[:] = h
+    sim.seedHydrostatic()
+
+
+def _field(sim, k):
+    return sim.field(k) if hasattr(sim, "field") else np.array(getattr(sim, k))
+
+
+@pytest.mark.parametrize("nslabs", [2, 3])
+def test_slabs_equal_one_handle_bitwise(gpu, nslabs):
+    n = 48
+    one = gpu.Sim(n, n, n)
+    _setup_wavy(one, n)
+    sol1 = gpu.RigidSphere(n, n, n, cx=24.0, cy=37.5, cz=24.0, r=4.5, density=2.0)
+    cut = gpu.SlabSim(n, n, n, nslabs=nslabs)
+    _setup_wavy(cut, n)
+    sol2 = gpu.RigidSphere(n, n, n, cx=24.0, cy=37.5, cz=24.0, r=4.5, density=2.0)
+    for k in FIELDS:
+        assert np.array_equal(_field(cut, k), _field(one, k)), ("initial", k)
+    for _ in range(30):
+        scenes.substep(one, sol1)
+        scenes.substep(cut, sol2)
+    for k in FIELDS:
+        assert np.array_equal(_field(cut, k), _field(one, k)), k
+    assert sol1.state() == sol2.state()
+    cut.close()
+    one.close()
+
+
+def test_slabs_track_one_handle_with_moving_sphere(gpu):
+    kw = dict(sigma=0.012, gravity=0.0012)
+    one, sol1 = scenes.drop(gpu.Sim, gpu.RigidSphere, **kw)
+    cut, sol2 = scenes.drop(_slab_factory(gpu, 2), gpu.RigidSphere, **kw)
+    cz0 = sol1.cy
+    n_dead = 0
+    for s in range(150):
+        scenes.substep(one, sol1)
+        scenes.substep(cut, sol2)
+        tag, prev = np.asarray(one.tag), np.asarray(one.tagPrev)
+        n_dead += int(np.count_nonzero((tag == 1) & (prev == 0)))
+        for k in ("cx", "cy", "cz"):
+            assert abs(getattr(sol1, k) - getattr(sol2, k)) <= 1e-9, (s, k)
+    assert abs(sol1.cy - cz0) > 1.5 and n_dead > 0
+    assert np.array_equal(_field(cut, "tag"), _field(one, "tag"))
+    for k in ("phi", "rho"):
+        a, b = _field(cut, k).astype(np.float64), _field(one, k).astype(np.float64)
+        assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(b), k
+    cut.close()
+    one.close()
