@@ -1,7 +1,8 @@
 """Tile-shape autotuner for batched steps.
 
 The fused kernel's tile shape -- rows per CTA (2, 4 or 8 cell warps plus two
-halo warps, or the staged 4-row form for FP16/BF16) and z planes per CTA -- trades halo recomputation and shared-memory
+halo warps; the compact-ring and pipelined 4- and 6-row forms) and z planes
+per CTA -- trades halo recomputation and shared-memory
 occupancy against the number of tiles in flight; the best shape depends on the
 mix of grid sizes.  tune() times each candidate shape with
 lbm_batch_time_fused on the batch's own current state (the timed launches only
@@ -17,16 +18,19 @@ import json
 import math
 import os
 
-# rows | STAGED: the staged form of the 4-row tile (FP16/BF16 storage only),
-# whose tile rows arrive in shared memory by bulk asynchronous copy
+# rows | STAGED: the pipelined form (tile rows staged in shared memory by bulk
+# asynchronous copies); rows | COMPACT: the compact ring with register loads.
+# Both for FP32, FP16 and BF16 storage.
 STAGED = 0x100
-CANDIDATES = [(4, 32), (4, 16), (8, 16), (8, 32), (2, 32), (4, 64)]
-CANDIDATES_REDUCED = CANDIDATES + [(4 | STAGED, 32), (4 | STAGED, 16)]
+COMPACT = 0x400
+CANDIDATES_F64 = [(4, 32), (4, 16), (8, 16), (8, 32), (2, 32), (4, 64)]
+CANDIDATES = [(6 | COMPACT, 32), (6 | COMPACT, 16), (6 | COMPACT, 64), (4, 32), (4, 16), (8, 16),
+              (4 | COMPACT, 32), (6 | STAGED, 32)]
 
 
 def candidates_for(storage):
     """Tile shapes worth timing for a storage form."""
-    return CANDIDATES_REDUCED if storage in ("f16", "bf16") else CANDIDATES
+    return CANDIDATES_F64 if storage == "f64" else CANDIDATES
 
 _cache: dict = {}
 _loaded = False

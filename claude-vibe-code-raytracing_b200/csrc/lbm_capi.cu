@@ -620,6 +620,10 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
   h->ops = ops;
   h->n = (long long)nx * ny * nz;
   h->fusedOK = h->n < (1LL << 31) - 64;  // cell indices are 32-bit in the fused kernel
+  // default launch shape: the compact-ring 6-row form where the storage form
+  // has it (FP32 values in the ring: FP32, FP16, BF16), the plain 4-row form
+  // for FP64
+  if (ops->shape_ok(6 | LBM_FUSED_COMPACT)) h->cfg.ty = 6 | LBM_FUSED_COMPACT;
   h->params = lbm_params{0.6, 0.7, 0.012, 0.0010, 1.0, 0.05, 4.0, 0.02};  // src/sim.js:88-95
   int rc = LBM_OK;
   auto body = [&]() -> int {
