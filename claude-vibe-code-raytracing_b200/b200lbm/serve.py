@@ -124,6 +124,9 @@ class Server:
         tuner = None
         ttff, interval, done_at = [], [], {}
         tick_run, tick_tune = [], []  # seconds per tick: the batch's steps + frames, the tuner
+        # the rest of a loop iteration: admission and collecting built scenes,
+        # telling the batch its members, retiring finished scenes
+        seg = {"admit": [], "members": [], "retire": []}
         changes = 0  # membership changes of the batch
         scene_steps = cell_steps = 0
         max_active = 0
@@ -134,6 +137,7 @@ class Server:
         building = []  # (req, fp, future) admitted, not yet built
         try:
             while queue or active or building:
+                tl0 = time.perf_counter()
                 now = clock()
                 for req in admit(list(queue), used, self.budget, now,
                                  lambda r: footprint(r["spec"], self.storage)):
@@ -162,6 +166,7 @@ class Server:
                 max_active = max(max_active, len(active))
                 ids = [a["req"]["rid"] for a in active]
                 tk0 = time.perf_counter()
+                seg["admit"].append(tk0 - tl0)
                 if ids != members:
                     pairs = [(a["sim"], a["solid"]) for a in active]
                     if batch is None:
@@ -171,6 +176,8 @@ class Server:
                     members = ids
                     changes += 1
                     tuner = None
+                tkm = time.perf_counter()
+                seg["members"].append(tkm - tk0)
                 frames = batch.run(tick, frame_every=every, use_graph=self.use_graph)
                 tk1 = time.perf_counter()
                 ticks += 1
@@ -181,7 +188,7 @@ class Server:
                             batch, [(a["sim"].nx, a["sim"].ny, a["sim"].nz) for a in active], self.storage)
                     tuner.step()
                 t = time.perf_counter() - t0
-                tick_run.append(tk1 - tk0)
+                tick_run.append(tk1 - tkm)
                 tick_tune.append(t + t0 - tk1)
                 for a, fr in zip(active, frames):
                     for j in range(fr.shape[0]):
@@ -208,6 +215,7 @@ class Server:
                         still.append(a)
                 if len(still) != len(active):
                     active = still
+                seg["retire"].append(time.perf_counter() - t - t0)
         finally:
             if batch is not None:
                 batch.close()
@@ -232,8 +240,9 @@ class Server:
             "frames": len(ttff) + len(interval),
             "max_active": max_active,
             "membership_changes": changes,
-            "tick_run_s": percentiles(tick_run),
-            "tick_tune_s": percentiles(tick_tune),
+            "tick_run_s": percentiles(tick_run, (50, 99, 100)),
+            "tick_tune_s": percentiles(tick_tune, (50, 99, 100)),
+            **{f"{k}_s": percentiles(v, (50, 99, 100)) for k, v in seg.items()},
             "storage": self.storage,
             "budget_bytes": self.budget,
         }

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -57,11 +58,31 @@ size_t pop_bytes_of(int storage) {
 size_t mac_bytes_of(int storage) { return storage == LBM_STORE_F64 ? 8 : 4; }
 
 
+// Device memory comes from the device's stream-ordered pool, allocated and
+// freed on the handle's stream: creating or destroying a scene does not stop
+// the device (a plain cudaFree waits for every stream), so a server can admit
+// and retire scenes while others step.  The pool keeps freed memory for the
+// next scene (release threshold raised once per device).
+void keep_pool(int device) {
+  static std::mutex mu;
+  static unsigned long long done = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  const unsigned long long bit = 1ull << (device & 63);
+  if (done & bit) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done |= bit;
+}
+
 int dalloc(lbm_sim *h, void **p, size_t bytes) {
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
   if (e != cudaSuccess) {
     *p = nullptr;
-    return cuda_fail(h, "cudaMalloc", e);
+    return cuda_fail(h, "cudaMallocAsync", e);
   }
   h->deviceBytes += bytes;
   return LBM_OK;
@@ -85,7 +106,7 @@ cudaError_t copy_async(lbm_sim *h, void *dst, const void *src, size_t bytes, cud
 int ensure_staging(lbm_sim *h, size_t bytes) {
   if (h->stagingBytes >= bytes) return LBM_OK;
   if (h->staging) {
-    cudaFree(h->staging);
+    cudaFreeAsync(h->staging, h->stream);
     h->deviceBytes -= h->stagingBytes;
     h->staging = nullptr;
     h->stagingBytes = 0;
@@ -200,7 +221,7 @@ int set_solids(lbm_sim *h, const lbm_sphere *sp, int ns, bool targets) {
   long long need = std::max(1LL, off * 6);
   if (need > h->impCap) {
     if (h->impAcc) {
-      cudaFree(h->impAcc);
+      cudaFreeAsync(h->impAcc, h->stream);
       h->deviceBytes -= h->impCap * sizeof(double);
       h->impAcc = nullptr;
     }
@@ -211,7 +232,7 @@ int set_solids(lbm_sim *h, const lbm_sphere *sp, int ns, bool targets) {
   long long pneed = (long long)std::max(ns, 1) * maxChunks * 6;
   if (pneed > h->partialsCap) {
     if (h->partials) {
-      cudaFree(h->partials);
+      cudaFreeAsync(h->partials, h->stream);
       h->deviceBytes -= h->partialsCap * sizeof(double);
       h->partials = nullptr;
     }
@@ -238,7 +259,7 @@ int reduce_impulses(lbm_sim *h, double *d_out) {
 int ensure_counts(lbm_sim *h, long long nch) {
   if (nch <= h->countsCap) return LBM_OK;
   if (h->counts) {
-    cudaFree(h->counts);
+    cudaFreeAsync(h->counts, h->stream);
     h->deviceBytes -= h->countsCap * sizeof(int2);
     h->counts = nullptr;
   }
@@ -433,27 +454,30 @@ int get_scalar64(lbm_sim *h, const void *src, double *host) {
 }
 
 void free_all(lbm_sim *h) {
-  if (h->image) cudaFree(h->image);
+  if (h->image) cudaFreeAsync(h->image, h->stream);
   void *ptrs[] = {h->F[0], h->F[1], h->H[0], h->H[1], h->tag, h->tagPrev, h->grad[0], h->grad[1],
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
                   h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
                   h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan, h->dWatch, h->linkChunks,
                   h->linkBuf};
   for (void *p : ptrs)
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, h->stream);
   for (int c = 0; c < 2; c++)
     for (int a = 0; a < 5; a++)
-      if (h->mac[c][a]) cudaFree(h->mac[c][a]);
+      if (h->mac[c][a]) cudaFreeAsync(h->mac[c][a], h->stream);
   for (cudaEvent_t e : h->evStart) cudaEventDestroy(e);
   for (cudaEvent_t e : h->evStop) cudaEventDestroy(e);
   if (h->hOut) cudaFreeHost(h->hOut);
   if (h->hTotals) cudaFreeHost(h->hTotals);
   if (h->copyStream) cudaStreamSynchronize(h->copyStream);
-  if (h->frameDev) cudaFree(h->frameDev);
+  if (h->frameDev) cudaFreeAsync(h->frameDev, h->stream);
   if (h->evPacked) cudaEventDestroy(h->evPacked);
   if (h->evCopied) cudaEventDestroy(h->evCopied);
   if (h->copyStream) cudaStreamDestroy(h->copyStream);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->stream) {
+    cudaStreamSynchronize(h->stream);  // the stream-ordered frees above
+    cudaStreamDestroy(h->stream);
+  }
 }
 
 
@@ -491,7 +515,7 @@ int coupled_prepare(lbm_sim *h, const lbm_sphere *sp, int ns, bool frames, Coupl
   long long need = std::max(1LL, (long long)ns * c.slotCells * 6);
   if (need > h->impCap) {
     if (h->impAcc) {
-      cudaFree(h->impAcc);
+      cudaFreeAsync(h->impAcc, h->stream);
       h->deviceBytes -= h->impCap * sizeof(double);
       h->impAcc = nullptr;
     }
@@ -501,7 +525,7 @@ int coupled_prepare(lbm_sim *h, const lbm_sphere *sp, int ns, bool frames, Coupl
   long long pneed = (long long)std::max(ns, 1) * c.redChunks * 6;
   if (pneed > h->partialsCap) {
     if (h->partials) {
-      cudaFree(h->partials);
+      cudaFreeAsync(h->partials, h->stream);
       h->deviceBytes -= h->partialsCap * sizeof(double);
       h->partials = nullptr;
     }
@@ -627,6 +651,7 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
   h->params = lbm_params{0.6, 0.7, 0.012, 0.0010, 1.0, 0.05, 4.0, 0.02};  // src/sim.js:88-95
   int rc = LBM_OK;
   auto body = [&]() -> int {
+    keep_pool(device);
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     size_t pb = ops->pop_bytes(), mb = ops->macro_bytes();
     for (int c = 0; c < 2; c++) {
@@ -773,19 +798,19 @@ int lbm_upload_field(lbm_sim *h, int field, const void *host, size_t count) {
       void *old = nullptr;
       bool off = !h->ops->phases_supported();
       if (off) {
-        CK(cudaMalloc(&old, n * mb));
+        CK(cudaMallocAsync(&old, n * mb, h->stream));
       }
       for (int c = 0; c < 2; c++) {
         if (off) CK(copy_async(h, old, h->mac[c][0], n * mb, cudaMemcpyDeviceToDevice, h->stream));
         int rc = put_scalar(h, h->mac[c][0], src);
         if (rc) {
-          if (old) cudaFree(old);
+          if (old) cudaFreeAsync(old, h->stream);
           return rc;
         }
         if (off) h->ops->reencode_h(h, c, old);
       }
+      if (old) cudaFreeAsync(old, h->stream);
       cudaError_t e = cudaStreamSynchronize(h->stream);
-      if (old) cudaFree(old);
       if (e != cudaSuccess) return cuda_fail(h, "upload phi", e);
       return LBM_OK;
     }
@@ -984,7 +1009,7 @@ int lbm_solid_links(lbm_sim *h, int32_t *cells, int8_t *dirs, double *mom, int c
   const long long chunks = (h->n + LINK_CHUNK - 1) / LINK_CHUNK;
   if (chunks + 1 > h->linkChunksCap) {
     if (h->linkChunks) {
-      cudaFree(h->linkChunks);
+      cudaFreeAsync(h->linkChunks, h->stream);
       h->deviceBytes -= h->linkChunksCap * sizeof(int);
       h->linkChunks = nullptr;
     }
@@ -1002,7 +1027,7 @@ int lbm_solid_links(lbm_sim *h, int32_t *cells, int8_t *dirs, double *mom, int c
   const long long per = sizeof(double) + sizeof(int) + 1;
   if (take > h->linkBufCap) {
     if (h->linkBuf) {
-      cudaFree(h->linkBuf);
+      cudaFreeAsync(h->linkBuf, h->stream);
       h->deviceBytes -= h->linkBufCap * per;
       h->linkBuf = nullptr;
     }
@@ -1213,7 +1238,7 @@ int lbm_render(lbm_sim *h, const lbm_sphere *sphere, const lbm_camera *cam, int 
   const size_t bytes = (size_t)width * height * 4;
   if (bytes > h->imageBytes) {
     if (h->image) {
-      cudaFree(h->image);
+      cudaFreeAsync(h->image, h->stream);
       h->deviceBytes -= h->imageBytes;
       h->image = nullptr;
       h->imageBytes = 0;
@@ -1513,24 +1538,27 @@ int batch_tables(lbm_batch *b) {
     if (t > (1LL << 30)) return bfail(b, LBM_ERR_CAPACITY, "too many tiles in one batch");
     start[s + 1] = (int)t;
   }
+  // stream-ordered on the batch's stream (no device-wide wait)
+  cudaStream_t st = b->origin;
   if (args.size() > b->argsCap) {
-    if (b->dArgs) cudaFree(b->dArgs);
+    if (b->dArgs) cudaFreeAsync(b->dArgs, st);
     b->dArgs = nullptr;
-    BCK(cudaMalloc(&b->dArgs, args.size()));
+    BCK(cudaMallocAsync(&b->dArgs, args.size(), st));
     b->argsCap = args.size();
   }
   if (n > b->tilesCap) {
-    if (b->dTileStart) cudaFree(b->dTileStart);
-    if (b->dTileGrid) cudaFree(b->dTileGrid);
+    if (b->dTileStart) cudaFreeAsync(b->dTileStart, st);
+    if (b->dTileGrid) cudaFreeAsync(b->dTileGrid, st);
     b->dTileStart = nullptr;
     b->dTileGrid = nullptr;
-    BCK(cudaMalloc(&b->dTileStart, (n + 1) * sizeof(int)));
-    BCK(cudaMalloc(&b->dTileGrid, n * sizeof(int3)));
+    BCK(cudaMallocAsync(&b->dTileStart, (n + 1) * sizeof(int), st));
+    BCK(cudaMallocAsync(&b->dTileGrid, n * sizeof(int3), st));
     b->tilesCap = n;
   }
-  BCK(cudaMemcpy(b->dArgs, args.data(), args.size(), cudaMemcpyHostToDevice));
-  BCK(cudaMemcpy(b->dTileStart, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  BCK(cudaMemcpy(b->dTileGrid, grid.data(), n * sizeof(int3), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpyAsync(b->dArgs, args.data(), args.size(), cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(b->dTileStart, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+  BCK(cudaMemcpyAsync(b->dTileGrid, grid.data(), n * sizeof(int3), cudaMemcpyHostToDevice, st));
+  BCK(cudaStreamSynchronize(st));  // the host vectors go out of scope
   return LBM_OK;
 }
 
@@ -1587,13 +1615,14 @@ int lbm_batch_destroy(lbm_batch *b) {
   if (!b) return LBM_ERR_ARG;
   DeviceGuard g(b->device);
   if (b->origin) cudaStreamSynchronize(b->origin);
+  if (b->dArgs) cudaFreeAsync(b->dArgs, b->origin);
+  if (b->dTileStart) cudaFreeAsync(b->dTileStart, b->origin);
+  if (b->dTileGrid) cudaFreeAsync(b->dTileGrid, b->origin);
+  if (b->origin) cudaStreamSynchronize(b->origin);
   for (cudaEvent_t ev : b->joins)
     if (ev) cudaEventDestroy(ev);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->origin) cudaStreamDestroy(b->origin);
-  if (b->dArgs) cudaFree(b->dArgs);
-  if (b->dTileStart) cudaFree(b->dTileStart);
-  if (b->dTileGrid) cudaFree(b->dTileGrid);
   if (b->pinned) cudaFreeHost(b->pinned);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   delete b;
@@ -1666,10 +1695,12 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
   std::vector<size_t> slot(n + 1, 0);  // pinned offset of each scene's frame
   for (int s = 0; s < n; s++) slot[s + 1] = slot[s] + (wantFrames ? 2 * (size_t)b->sims[s]->n : 0);
   if (slot[n] > b->pinnedCap) {
+    // grown with headroom: page-locking is slow and a server's batch grows often
+    const size_t cap = std::max(slot[n], b->pinnedCap + b->pinnedCap / 2);
     if (b->pinned) cudaFreeHost(b->pinned);
     b->pinned = nullptr;
-    BCK(cudaMallocHost((void **)&b->pinned, slot[n]));
-    b->pinnedCap = slot[n];
+    BCK(cudaMallocHost((void **)&b->pinned, cap));
+    b->pinnedCap = cap;
   }
 
   // one coupled step of every scene: per-scene branches around the shared fused launch
