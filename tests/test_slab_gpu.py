@@ -6,9 +6,11 @@ NVLink between GPUs).
   * the 256^3 benchmark scene scaled to 48^3 (liquid below a wavy interface,
     so the fields vary in z; the sphere rests): 2 and 3 slabs give every
     field bit for bit what one handle gives after 30 ticks;
-  * the drop preset (the sphere falls 2 cells, with fresh and dead cells):
-    2 slabs track one handle -- the slabs' impulse sums add in another order,
-    so the sphere differs by FP64 rounding and the fields by what that moves.
+  * the drop preset (the sphere falls 2 cells, with fresh and dead cells),
+    2 slabs: given the one handle's sphere state before every tick, every
+    field bit for bit and the sphere within FP64 rounding (the slabs'
+    impulse sums add in another order); free-running, the trajectory within
+    the device-against-oracle bar.
 """
 import numpy as np
 import pytest
@@ -79,23 +81,63 @@ def test_slabs_equal_one_handle_bitwise(gpu, nslabs):
     one.close()
 
 
-def test_slabs_track_one_handle_with_moving_sphere(gpu):
+STATE = ("cx", "cy", "cz", "vx", "vy", "vz", "wx", "wy", "wz")
+# the slabs' impulse sums add in another order than the one handle's fixed
+# tree: the forces differ by FP64 rounding (a few ulp of the summed terms)
+TOL_GIVEN = 1e-12
+# free-running, a rounding difference in the sphere moves its surface
+# velocity, which the FP32 fields round differently, and so on; the
+# trajectory bar is the device-against-oracle one
+TOL_FREE = 2e-5
+
+
+def _copy_state(dst, src):
+    for k in STATE + ("r",):
+        setattr(dst, k, getattr(src, k))
+
+
+def test_slabs_equal_one_handle_with_moving_sphere_given_state(gpu):
+    """The drop preset (the sphere falls 2 cells, with fresh and dead cells)
+    with the slabs' sphere given the one handle's state before every tick:
+    every field bit for bit, the sphere after the tick within FP64 rounding."""
     kw = dict(sigma=0.012, gravity=0.0012)
     one, sol1 = scenes.drop(gpu.Sim, gpu.RigidSphere, **kw)
     cut, sol2 = scenes.drop(_slab_factory(gpu, 2), gpu.RigidSphere, **kw)
-    cz0 = sol1.cy
-    n_dead = 0
+    cy0 = sol1.cy
+    n_fresh = n_dead = 0
     for s in range(150):
+        _copy_state(sol2, sol1)
         scenes.substep(one, sol1)
         scenes.substep(cut, sol2)
         tag, prev = np.asarray(one.tag), np.asarray(one.tagPrev)
         n_dead += int(np.count_nonzero((tag == 1) & (prev == 0)))
+        n_fresh += int(np.count_nonzero((tag == 0) & (prev == 1)))
+        for k in ("tag", "phi", "rho"):
+            assert np.array_equal(_field(cut, k), _field(one, k)), (s, k)
+        for k in STATE:
+            assert abs(getattr(sol1, k) - getattr(sol2, k)) <= TOL_GIVEN, (s, k)
+    assert abs(sol1.cy - cy0) > 1.5 and n_dead > 0 and n_fresh > 0
+    for k in FIELDS:
+        assert np.array_equal(_field(cut, k), _field(one, k)), k
+    cut.close()
+    one.close()
+
+
+def test_slabs_track_one_handle_with_moving_sphere(gpu):
+    kw = dict(sigma=0.012, gravity=0.0012)
+    one, sol1 = scenes.drop(gpu.Sim, gpu.RigidSphere, **kw)
+    cut, sol2 = scenes.drop(_slab_factory(gpu, 2), gpu.RigidSphere, **kw)
+    cy0 = sol1.cy
+    worst = 0.0
+    for s in range(150):
+        scenes.substep(one, sol1)
+        scenes.substep(cut, sol2)
         for k in ("cx", "cy", "cz"):
-            assert abs(getattr(sol1, k) - getattr(sol2, k)) <= 1e-9, (s, k)
-    assert abs(sol1.cy - cz0) > 1.5 and n_dead > 0
-    assert np.array_equal(_field(cut, "tag"), _field(one, "tag"))
+            worst = max(worst, abs(getattr(sol1, k) - getattr(sol2, k)))
+    assert abs(sol1.cy - cy0) > 1.5
+    assert worst <= TOL_FREE, worst
     for k in ("phi", "rho"):
         a, b = _field(cut, k).astype(np.float64), _field(one, k).astype(np.float64)
-        assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(b), k
+        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), k
     cut.close()
     one.close()
