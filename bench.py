@@ -231,8 +231,10 @@ def run_reference(args, ws, rank):
 
 
 def _shape_name(rows, zchunk):
-    """'4x32', or '4sx32' for the staged 4-row form."""
-    return f"{rows & 0xff}{'s' if rows & 0x100 else ''}x{zchunk}"
+    """'4x32' for the plain form; a suffix names the compact-ring forms:
+    'c' register loads, 'a' per-thread async copies, 's' bulk-staged rows."""
+    form = "s" if rows & 0x100 else "c" if rows & 0x400 else "a" if rows & 0x800 else ""
+    return f"{rows & 0xff}{form}x{zchunk}"
 
 
 def batch_result(args, dev, ws=1, rank=0, steps=100):
@@ -293,7 +295,7 @@ def batch_result(args, dev, ws=1, rank=0, steps=100):
         "tile": _shape_name(rows, zchunk),
         "timings_ms": {_shape_name(r, z): t for (r, z), t in timings.items()},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "k_fused_batch",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "kernel": kernel_name(rows, batch=True),
                      "kernel_ms": fused_ms, "bytes_per_cell": BYTES_PER_CELL[storage],
                      "cells_per_launch": interior},
         "timing": "wall clock around whole runs (host work included), after a synchronize; "
@@ -558,8 +560,11 @@ def run_phases(args, dev):
     print(json.dumps(line), flush=True)
 
 
-def kernel_name(rows):
-    return "k_fused_pipe" if rows & 0x100 else "k_fused_step"
+def kernel_name(rows, batch=False):
+    """The fused kernel a tile shape launches."""
+    pipe = bool(rows & (0x100 | 0x400 | 0x800))
+    return ("k_fused_pipe" if pipe else "k_fused_step" if not batch else "k_fused_batch") + \
+        ("_batch" if batch and pipe else "")
 
 
 def scene_form(args, storage, steps, dev, ws, local):

@@ -89,6 +89,8 @@ _SIGS = [
     ("lbm_stream_hydro_and_macro", C.c_int,
      [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
     ("lbm_step", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
+    ("lbm_step_begin", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int]),
+    ("lbm_step_end", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
     ("lbm_absorb_dead_cells", C.c_int,
      [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
     ("lbm_pack_volume", C.c_int, [C.c_void_p, C.c_void_p]),

@@ -18,14 +18,15 @@ import json
 import math
 import os
 
-# rows | STAGED: the pipelined form (tile rows staged in shared memory by bulk
-# asynchronous copies); rows | COMPACT: the compact ring with register loads.
-# Both for FP32, FP16 and BF16 storage.
+# Compact-ring forms (FP32, FP16 and BF16 storage): rows | COMPACT register
+# loads, rows | ASYNC per-thread async copies one plane ahead, rows | STAGED
+# tile rows staged by bulk asynchronous copies.  Plain forms: rows 2, 4, 8.
 STAGED = 0x100
 COMPACT = 0x400
+ASYNC = 0x800
 CANDIDATES_F64 = [(4, 32), (4, 16), (8, 16), (8, 32), (2, 32), (4, 64)]
-CANDIDATES = [(6 | COMPACT, 32), (6 | COMPACT, 16), (6 | COMPACT, 64), (4, 32), (4, 16), (8, 16),
-              (4 | COMPACT, 32), (6 | STAGED, 32)]
+CANDIDATES = [(6 | COMPACT, 32), (6 | ASYNC, 32), (6 | COMPACT, 16), (6 | ASYNC, 16), (6 | COMPACT, 64),
+              (4, 32), (4, 16), (8, 16), (4 | COMPACT, 32), (6 | STAGED, 32)]
 
 
 def candidates_for(storage):

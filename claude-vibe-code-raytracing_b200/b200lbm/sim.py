@@ -366,6 +366,25 @@ class Sim:
         rc = lib().lbm_step(self._h, arr, len(sp), out)
         self._completed(rc, lambda: [b.add_impulse(out[i]) for i, b in enumerate(sp)])
 
+    def step_begin(self, solid):
+        """The first half of step (retagCells + handleFreshCells,
+        src/sim.js:203-204); step_end(solid) with the same solid completes it."""
+        if is_generic(solid):
+            raise TypeError("a split step takes spheres (RigidSphere / CompositeSolid)")
+        sp = spheres_of(solid)
+        self._sync()
+        rc = lib().lbm_step_begin(self._h, to_c_array(sp), len(sp))
+        self._moved()
+        check(self._h, rc)
+
+    def step_end(self, solid):
+        sp = spheres_of(solid)
+        self._sync()
+        arr = to_c_array(sp)
+        out = impulse_array(len(sp))
+        rc = lib().lbm_step_end(self._h, arr, len(sp), out)
+        self._completed(rc, lambda: [b.add_impulse(out[i]) for i, b in enumerate(sp)])
+
     def render(self, solid=None, width=640, height=480, camera=None):
         """Renderer.uploadVolume + draw (src/render.js:431-434, 484-513) without
         a canvas: the current state rendered by the reference's fragment shader

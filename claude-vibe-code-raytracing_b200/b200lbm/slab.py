@@ -18,11 +18,10 @@ slabs' impulses are added in slab order, so the solid sees the scene's total.
     phi = scene.field("phi")           # the scene's array, reference layout
 
 Given the same sphere state every cell update is the one a single handle
-makes (the fused step's arithmetic does not depend on the tiling); only the
-order in which the slabs' impulse sums are added differs from the single
-handle's fixed-order reduction.  Fresh cells next to a cut are filled in the
-scene's scan order as long as no chain of fresh cells spans three planes
-across the cut.
+makes (the fused step's arithmetic does not depend on the tiling, and fresh
+cells are filled in the scene's scan order across the cuts, see step); only
+the order in which the slabs' impulse sums are added differs from the single
+handle's fixed-order reduction.
 """
 from __future__ import annotations
 
@@ -82,6 +81,8 @@ class SlabSim:
             check(sim.handle, lib().lbm_set_slab(sim.handle, zoff, own_lo, own_hi))
             self.slabs.append(sim)
         self._ops = exchange_plan(self.plan)
+        self._up = self._ops[0::2]    # per cut: the lower slab's top owned planes go up
+        self._down = self._ops[1::2]  # per cut: the upper slab's bottom owned planes go down
 
     # ------------------------------------------------------------ parameters
     def __getattr__(self, name):
@@ -144,10 +145,22 @@ class SlabSim:
             sim.seedHydrostatic()
 
     def step(self, solid):
-        """Sim.step (src/sim.js:202-210) on every slab, then the plane
-        exchange; the solid collects every slab's momentum exchange."""
+        """Sim.step (src/sim.js:202-210) on every slab; the solid collects
+        every slab's momentum exchange.  handleFreshCells fills a fresh cell
+        from neighbours of which those earlier in the scene's scan order are
+        already filled (src/sim.js:257-300), so the slabs begin their steps
+        (retag + fill of their own planes) in z order, each handing its two
+        top owned planes, filled, to the next slab's copied planes; then each
+        slab's two bottom owned planes, filled, go down to the slab below,
+        every slab ends its step, and the plane exchange follows."""
+        for s, sim in enumerate(self.slabs):
+            sim.step_begin(solid)
+            if s < len(self._up):
+                self._copy(*self._up[s])
+        for op in self._down:
+            self._copy(*op)
         for sim in self.slabs:
-            sim.step(solid)
+            sim.step_end(solid)
         self.exchange()
 
     def _absorb_dead(self, spheres):
@@ -155,10 +168,13 @@ class SlabSim:
         for sim in self.slabs:
             sim._absorb_dead(spheres)
 
+    def _copy(self, dst, dplane, src, splane, k):
+        d, s = self.slabs[dst], self.slabs[src]
+        rc = lib().lbm_slab_copy_planes(d.handle, dplane, s.handle, splane, k)
+        if rc != _capi.OK:
+            raise _capi.LbmError(rc, (lib().lbm_last_error(d.handle) or b"").decode(errors="replace"))
+        d._moved()
+
     def exchange(self):
-        for dst, dplane, src, splane, k in self._ops:
-            d, s = self.slabs[dst], self.slabs[src]
-            rc = lib().lbm_slab_copy_planes(d.handle, dplane, s.handle, splane, k)
-            if rc != _capi.OK:
-                raise _capi.LbmError(rc, (lib().lbm_last_error(d.handle) or b"").decode(errors="replace"))
-            d._moved()
+        for op in self._ops:
+            self._copy(*op)

@@ -1116,10 +1116,11 @@ int lbm_stream_hydro_and_macro(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_imp
   return watch_after(h, 1);
 }
 
-int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
+int lbm_step_begin(lbm_sim *h, const lbm_sphere *sp, int ns) {
   if (!h) return LBM_ERR_ARG;
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
+  if (h->stepBegunNs >= 0) return fail(h, LBM_ERR_STATE, "a step was begun and not ended");
   DeviceGuard g(h->device);
   if (h->bfActive || !h->fusedOK) {
     // A pending external body force is consumed by the phase-by-phase path,
@@ -1127,11 +1128,8 @@ int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
     // fused kernel's 32-bit indexing take the same path.
     if ((rc = lbm_retag_cells(h, sp, ns))) return rc;
     if ((rc = lbm_handle_fresh_cells(h))) return rc;
-    if ((rc = lbm_compute_phi_gradients(h))) return rc;
-    if ((rc = lbm_collide_phase(h))) return rc;
-    if ((rc = lbm_stream_phase(h))) return rc;
-    if ((rc = lbm_collide_hydro(h))) return rc;
-    return lbm_stream_hydro_and_macro(h, sp, ns, out);
+    h->stepBegunNs = ns;
+    return LBM_OK;
   }
   if ((rc = set_solids(h, sp, ns, true))) return rc;
   Box now = spheres_box(h, sp, ns);
@@ -1152,13 +1150,39 @@ int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   if ((rc = launch_compaction(h, h->hPlan.nchunks))) return rc;
   h->ops->fresh_fill(h);
   CKL("fresh cells");
+  h->stepNow = now;
+  h->stepBegunNs = ns;
+  return LBM_OK;
+}
+
+int lbm_step_end(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
+  if (!h) return LBM_ERR_ARG;
+  int rc = check_spheres(h, sp, ns);
+  if (rc) return rc;
+  if (h->stepBegunNs < 0) return fail(h, LBM_ERR_STATE, "lbm_step_end without lbm_step_begin");
+  if (ns != h->stepBegunNs) return fail(h, LBM_ERR_ARG, "lbm_step_end with another sphere count than its begin");
+  h->stepBegunNs = -1;
+  DeviceGuard g(h->device);
+  if (h->bfActive || !h->fusedOK) {
+    if ((rc = lbm_compute_phi_gradients(h))) return rc;
+    if ((rc = lbm_collide_phase(h))) return rc;
+    if ((rc = lbm_stream_phase(h))) return rc;
+    if ((rc = lbm_collide_hydro(h))) return rc;
+    return lbm_stream_hydro_and_macro(h, sp, ns, out);
+  }
   launch_fused(h);
   CKL("fused step");
   if ((rc = reduce_impulses(h, h->dOut))) return rc;
   h->cur = 1 - h->cur;
-  shift_boxes(h, now);
+  shift_boxes(h, h->stepNow);
   if ((rc = fetch_out(h, h->dOut, ns, out))) return rc;
   return watch_after(h, 1);
+}
+
+int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
+  int rc = lbm_step_begin(h, sp, ns);
+  if (rc) return rc;
+  return lbm_step_end(h, sp, ns, out);
 }
 
 int lbm_absorb_dead_cells(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
@@ -1399,7 +1423,7 @@ int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
   if (!h) return LBM_ERR_ARG;
   if (!h->ops->shape_ok(rows) || zchunk < 1)
     return fail(h, LBM_ERR_ARG,
-                "rows must be 2, 4 or 8 (4 | LBM_FUSED_STAGED with FP16/BF16 storage) and zchunk >= 1");
+                "rows must be 2, 4 or 8, or 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED (FP32/FP16/BF16 storage), and zchunk >= 1");
   if (h->ops->fused_smem(rows) > 227 * 1024)
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;
@@ -1659,7 +1683,7 @@ int lbm_batch_set_config(lbm_batch *b, int rows, int zchunk) {
   if (!b) return LBM_ERR_ARG;
   if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
     return bfail(b, LBM_ERR_ARG,
-                 "rows must be 2, 4 or 8 (4 | LBM_FUSED_STAGED with FP16/BF16 storage) and zchunk >= 1");
+                 "rows must be 2, 4 or 8, or 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED (FP32/FP16/BF16 storage), and zchunk >= 1");
   b->rows = rows;
   b->zchunk = zchunk;
   return LBM_OK;
@@ -1824,7 +1848,7 @@ int lbm_batch_time_fused(lbm_batch *b, int rows, int zchunk, int reps, double *m
   if (!b || !ms || reps < 1) return LBM_ERR_ARG;
   if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
     return bfail(b, LBM_ERR_ARG,
-                 "rows must be 2, 4 or 8 (4 | LBM_FUSED_STAGED with FP16/BF16 storage) and zchunk >= 1");
+                 "rows must be 2, 4 or 8, or 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED (FP32/FP16/BF16 storage), and zchunk >= 1");
   DeviceGuard g(b->device);
   const int keepRows = b->rows, keepZ = b->zchunk;
   b->rows = rows;

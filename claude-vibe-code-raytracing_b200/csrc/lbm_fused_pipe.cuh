@@ -1,34 +1,46 @@
-// The pipelined form of the fused LBM step (tile shape 4 | LBM_FUSED_STAGED).
+// The compact-ring forms of the fused LBM step (tile shapes 4 or 6 rows |
+// LBM_FUSED_COMPACT, LBM_FUSED_ASYNC or LBM_FUSED_STAGED).
 //
 // Same algorithm and arithmetic as fused_tile (lbm_fused.cuh): a CTA owns a
-// 32 x 4 column of cells and marches it up a z-chunk; each plane is collided
+// 32 x TY column of cells and marches it up a z-chunk; each plane is collided
 // at its source into a shared-memory ring and pulled from there.  What
-// differs is how the data reach the SM:
+// differs is the ring and how the data reach the SM:
 //
-//   * the tile rows' populations, rho, u and tags of the next plane, and the
-//     phi rows of the plane after it, arrive in a shared-memory stage by bulk
-//     asynchronous copies (cp.async.bulk, completion counted in bytes on an
-//     mbarrier), issued by one producer lane as soon as every cell warp has
-//     read the current plane out of the stage (a second mbarrier), so the copy
-//     lands while the current plane is collided and the previous one pulled;
-//   * the halo rows and columns (collided by two halo warps: the rows above
-//     and below, and the side columns with the corners) are loaded by those
-//     warps right after the barrier that ends a plane, while the cell warps
-//     pull it, so their latency is off the critical path;
 //   * the ring stores, for each direction, only the cells that can be a
-//     source of that direction for the tile (33 columns by 4 or 5 rows)
-//     plus the tile itself for bounce-back: 47.3 KB instead of 63.6 KB, which
-//     leaves room for the stage at three CTAs per SM.
+//     source of that direction for the tile plus the tile itself for
+//     bounce-back (33 columns by TY or TY + 1 rows), so a cell's index in any
+//     direction's array is one per-thread term plus a compile-time constant:
+//     46 KB at 4 rows (three CTAs per SM), 66 KB at 6 rows (two);
+//   * the halo rows and columns are collided by two halo warps (the rows above
+//     and below; the side columns with the corners, one half-warp per side),
+//     which load right after the barrier that ends a plane, while the cell
+//     warps pull it, so their latency is off the critical path;
+//   * the cell warps' loads of the next plane:
+//       - COMPACT: plain loads into registers at the start of each plane;
+//       - ASYNC: each thread copies its own cell of plane q + 1 (populations
+//         by whole groups, rho, u and the phi stencil) into its own
+//         shared-memory slots with per-thread asynchronous copies issued
+//         after it has written plane q into the ring, so the copies land
+//         while plane q - 1 is pulled and no registers are held meanwhile;
+//       - STAGED: the tile rows of plane q + 1 arrive by bulk asynchronous
+//         copies (cp.async.bulk, completion counted in bytes on an mbarrier)
+//         issued by one producer lane as soon as every cell warp has read the
+//         current stage (a second mbarrier).
 //
-// Results are bit-identical to fused_tile (the collision is the same
-// collide_cell, the pull sums in the same order).  FP32, FP16 and BF16
-// storage; the waits for the stage are bounded like every other wait of the
-// library (status word + fault code 90 + LBM_ERR_TIMEOUT).
+// Results are bit-identical to fused_tile in every form (the collision is the
+// same collide_cell, the pull sums in the same order).  FP32, FP16 and BF16
+// storage; the waits for the bulk stage are bounded like every other wait of
+// the library (status word + fault code 90 + LBM_ERR_TIMEOUT).
 #pragma once
 
 #include "lbm_fused.cuh"
 
 namespace lbm {
+
+// launch forms of the compact-ring kernel (the FORM of the launch tables)
+constexpr int PIPE_STAGED = 1;
+constexpr int PIPE_COMPACT = 2;
+constexpr int PIPE_ASYNC = 3;
 
 // ---------------------------------------------------------------- compact ring
 // Direction k's slot array in one ring copy covers the local columns
@@ -74,9 +86,10 @@ struct PipeRing {
 };
 
 // ---------------------------------------------------------------- shared memory
-template <class PopT, int TY, bool STG = true>
+template <class PopT, int TY, int PF>
 struct PipeSmem {
   using Real = typename Prec<PopT>::Real;
+  static constexpr bool STG = PF == PIPE_STAGED, ASY = PF == PIPE_ASYNC;
   using R = PipeRing<TY>;
   static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;  // tag planes keep the full halo frame
   static constexpr int SB = 5;                              // blocks a 32-cell row can span
@@ -92,9 +105,16 @@ struct PipeSmem {
   static constexpr size_t stT = stM + (size_t)4 * TY * MROW * sizeof(Real);
   static constexpr size_t phiOff = stT + (size_t)TY * TROW;
   static constexpr size_t barOff = (phiOff + (size_t)3 * (TY + 2) * PROW * sizeof(Real) + 15) / 16 * 16;
-  // without the stage (cell warps load from global memory): ring and tags only
-  // two mbarriers (stage full, stage read) and the abort flag
-  static constexpr size_t bytes = STG ? barOff + 32 : (tagOff + 3 * NC + 15) / 16 * 16;
+  // the async form's per-thread slots after the tag planes: [G27][32 TY]
+  // groups of f, [G7][32 TY] groups of h, [11][32 TY] words (phi and its six
+  // neighbours, rho, ux, uy, uz)
+  static constexpr int NT = 32 * TY, GB = 4 * (int)sizeof(PopT), NS = 11;
+  static constexpr size_t aF = (tagOff + 3 * NC + 15) / 16 * 16;
+  static constexpr size_t aH = aF + (size_t)PopGroups<Q27>::G * NT * GB;
+  static constexpr size_t aS = aH + (size_t)PopGroups<Q7>::G * NT * GB;
+  // staged: two mbarriers (stage full, stage read) and the abort flag;
+  // compact: ring and tags only
+  static constexpr size_t bytes = STG ? barOff + 32 : ASY ? aS + (size_t)NS * NT * 4 : aF;
   static constexpr int warps = TY + 2;  // TY cell warps, the halo rows above and below, the sides
   static constexpr int threads = 32 * warps;
   static_assert(sizeof(Real) == 4, "the pipelined form holds FP32 arithmetic values in its ring");
@@ -104,12 +124,13 @@ struct PipeSmem {
 };
 
 // ---------------------------------------------------------------- the tile
-template <class PopT, int TY, bool STG, bool WIDE>
+template <class PopT, int TY, int PF, bool WIDE>
 __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx, int by, int bz) {
   using POff = std::conditional_t<WIDE, long long, int>;
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
-  using SM = PipeSmem<PopT, TY, STG>;
+  using SM = PipeSmem<PopT, TY, PF>;
+  constexpr bool STG = SM::STG, ASY = SM::ASY;
   using R = PipeRing<TY>;
   using LD = CellLoad<PopT>;
   using CO = CellOut<PopT>;
@@ -149,7 +170,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   const CollK<Real> K = coll_consts(a);
 
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const bool cellWarp = ty < TY, haloRows = ty == TY, haloSide = ty == TY + 1;
+  const bool cellWarp = ty < TY, haloRows = ty == TY;
   const int x0 = bx * 32, y0 = by * TY;
   const int zb = 1 + bz * a.zchunk;
   const int ze = min(zb + a.zchunk, nz - 1);
@@ -400,6 +421,78 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     });
   };
 
+  // ---- the async form: a cell warp's cell of plane q into this thread's own
+  // slots (every group of f and h, phi and its six neighbours, rho, u) by
+  // per-thread asynchronous copies from the same clamped addresses the plain
+  // load uses; the tag (one byte, no copy size that small) by a plain load
+  // into a register that is held until plane q is collided
+  constexpr int NT = SM::NT, GB = SM::GB;
+  PopT *aF = reinterpret_cast<PopT *>(smem_raw + SM::aF);  // [G27][NT] groups
+  PopT *aH = reinterpret_cast<PopT *>(smem_raw + SM::aH);  // [G7][NT] groups
+  Real *aS = reinterpret_cast<Real *>(smem_raw + SM::aS);  // [11][NT] words
+  const int lin = ty * 32 + tx;
+  auto async_issue = [&](int q, uint8_t &tgq) __attribute__((always_inline)) {
+    const bool inside = x < nx && y < ny && q >= 0 && q < nz;
+    const int ci = inside ? q * nxny + y * nx + x : 0;
+    const POff bF = (POff)(ci >> 3) * BLK27 + (ci & 7) * 4;
+    const POff bH = (POff)(ci >> 3) * BLK7 + (ci & 7) * 4;
+    static_for<0, G27>([&](auto GG) {
+      constexpr int g = decltype(GG)::value;
+      const long long e = (long long)bF + 32 * g;
+      if (lbm_ok(e >= 0 && e + 3 < nF, 3, e)) cp_async<GB>(smem_u32(aF + (g * NT + lin) * 4), Fc + e);
+    });
+    static_for<0, G7>([&](auto GG) {
+      constexpr int g = decltype(GG)::value;
+      const long long e = (long long)bH + 32 * g;
+      if (lbm_ok(e >= 0 && e + 3 < nH, 4, e)) cp_async<GB>(smem_u32(aH + (g * NT + lin) * 4), Hc + e);
+    });
+    const int last = (int)nCell - 1;
+    const int src[SM::NS] = {ci, min(ci + 1, last), max(ci - 1, 0), min(ci + nx, last), max(ci - nx, 0),
+                             min(ci + nxny, last), max(ci - nxny, 0), ci, ci, ci, ci};
+    const Real *arr[SM::NS] = {phiC, phiC, phiC, phiC, phiC, phiC, phiC, rhoC, uxC, uyC, uzC};
+#pragma unroll
+    for (int j = 0; j < SM::NS; j++)
+      if (lbm_ok(src[j] >= 0 && src[j] < nCell, j < 7 ? 5 : 6, src[j]))
+        cp_async<4>(smem_u32(aS + j * NT + lin), arr[j] + src[j]);
+    cp_async_commit();
+    tgq = ldg_at(tagA, ci, nCell, 1);
+  };
+  auto async_load = [&](int q, uint8_t tgq, LD &L) __attribute__((always_inline)) {
+    cp_async_wait_all();
+    static_for<0, G27>([&](auto GG) {
+      constexpr int g = decltype(GG)::value;
+      PopT tv[4];
+      ld4_shared(aF + (g * NT + lin) * 4, tv);
+      static_for<4 * g, (4 * g + 4 < Q27 ? 4 * g + 4 : Q27)>([&](auto KK) {
+        constexpr int k = decltype(KK)::value;
+        L.fv[k] = tv[k & 3];
+      });
+      if constexpr (g < G7) {
+        ld4_shared(aH + (g * NT + lin) * 4, tv);
+        static_for<4 * g, (4 * g + 4 < Q7 ? 4 * g + 4 : Q7)>([&](auto KK) {
+          constexpr int k = decltype(KK)::value;
+          L.hv[k] = tv[k & 3];
+        });
+      }
+    });
+    L.p = aS[0 * NT + lin];
+    L.pxp = aS[1 * NT + lin];
+    L.pxm = aS[2 * NT + lin];
+    L.pyp = aS[3 * NT + lin];
+    L.pym = aS[4 * NT + lin];
+    L.pzp = aS[5 * NT + lin];
+    L.pzm = aS[6 * NT + lin];
+    L.sumF = aS[7 * NT + lin];
+    L.ux = aS[8 * NT + lin];
+    L.uy = aS[9 * NT + lin];
+    L.uz = aS[10 * NT + lin];
+    uint8_t tg = tgq;
+    const bool inside = x < nx && y < ny;
+    const bool inner = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2 && q >= 1 && q <= nz - 2;
+    if (!inside || (!inner && tg == TAG_FLUID)) tg = TAG_WALL;
+    L.tg = tg;
+  };
+
   Real gxC = 0, gyC = 0, gzC = 0, lapC = 0, phC = 0;
   Real gxN = 0, gyN = 0, gzN = 0, lapN = 0, phN = 0;
   const bool colActive = cellWarp && x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
@@ -413,6 +506,10 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   __syncthreads();
   if (producer && !a.withhold) issue(zb - 1, true);
   uint32_t parity = 0;
+  uint8_t tgNext = 0;
+  if constexpr (ASY) {
+    if (cellWarp) async_issue(zb - 1, tgNext);
+  }
 
   int q = zb - 1;
   for (; q <= ze; q++) {
@@ -435,6 +532,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
           // that ran out (set before the arrivals) stops the issuing.
           if (mbar_wait(barE, parity) && q < ze && !*abortF) issue(q + 1, false);
         }
+      } else if constexpr (ASY) {
+        async_load(q, tgNext, L);
       } else {
         load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
       }
@@ -459,6 +558,11 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     __syncthreads();
     if (cellWarp) {
       emit(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, tx, ty, o);
+      // the slots of plane q were read before the barrier above: plane q + 1
+      // now lands while plane q - 1 is pulled
+      if constexpr (ASY) {
+        if (q < ze) async_issue(q + 1, tgNext);
+      }
     } else if (haloRows) {
       emit(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, tx, -1, o);
       emit(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, tx, TY, o);
@@ -658,20 +762,20 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
 
 // CTAs per SM the register budget is sized for: 4 rows fit three CTAs per SM
 // in shared memory, 6 rows two
-template <int TY, bool STG>
+template <int TY, int PF>
 struct PipeOcc {
   static constexpr int blocks = TY <= 4 ? 3 : 2;
 };
 
-template <class PopT, int TY, bool STG, bool WIDE>
-__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, STG>::blocks)
+template <class PopT, int TY, int PF, bool WIDE>
+__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, PF>::blocks)
     k_fused_pipe(const __grid_constant__ FusedArgs<PopT> a) {
-  fused_tile_pipe<PopT, TY, STG, WIDE>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fused_tile_pipe<PopT, TY, PF, WIDE>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many scenes in one persistent launch (as k_fused_batch)
-template <class PopT, int TY, bool STG, bool WIDE>
-__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, STG>::blocks)
+template <class PopT, int TY, int PF, bool WIDE>
+__global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, PF>::blocks)
     k_fused_pipe_batch(const FusedArgs<PopT> *__restrict__ args, const int *__restrict__ tileStart,
                        const int3 *__restrict__ tileGrid, int nscenes) {
   const int total = tileStart[nscenes];
@@ -691,7 +795,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, STG>::blocks)
     if (lin < WORDS)
       reinterpret_cast<uint32_t *>(&sa)[lin] = reinterpret_cast<const uint32_t *>(args + lo)[lin];
     __syncthreads();
-    fused_tile_pipe<PopT, TY, STG, WIDE>(sa, bx, by, bz);
+    fused_tile_pipe<PopT, TY, PF, WIDE>(sa, bx, by, bz);
     __syncthreads();
   }
 }

@@ -552,7 +552,7 @@ static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev
 // for earlier ones exactly as in the reference's single sweep.
 template <class PopT>
 __global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *fresh,
-                             const int *totals, int cap, double rhoL, double rhoG) {
+                             const int *totals, int cap, double rhoL, double rhoG, int zlo, int zend) {
   using Real = typename Prec<PopT>::Real;
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   int nf = totals[0];
@@ -560,6 +560,12 @@ __global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, 
   const int nx = s.nx, ny = s.ny;
   for (int q = 0; q < nf; q++) {
     long long i = fresh[q];
+    // a z slab fills the cells of its own planes only: its copied planes
+    // receive the neighbouring slab's filled values
+    if (zend > 0) {
+      const long long z = i / ((long long)nx * ny);
+      if (z < zlo || z >= zend) continue;
+    }
     double psum = 0, rsum = 0, vxs = 0, vys = 0, vzs = 0;
     int pcnt = 0;
     for (int dz = -1; dz <= 1; dz++)

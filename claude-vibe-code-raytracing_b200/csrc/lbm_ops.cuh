@@ -183,7 +183,8 @@ class Ops final : public OpsBase {
   }
   void fresh_fill(lbm_sim *h) override {
     k_fresh_fill<PopT><<<1, 32, 0, h->stream>>>(scene(h), h->cur, h->fresh, h->totals,
-                                                 (int)h->listCap, h->params.rhoL, h->params.rhoG);
+                                                 (int)h->listCap, h->params.rhoL, h->params.rhoG,
+                                                 h->slab ? h->ownLo : 0, h->slab ? h->ownHi + 1 : 0);
     h->launches++;
   }
   void absorb_dead(lbm_sim *h, double *d_out) override {
@@ -195,12 +196,13 @@ class Ops final : public OpsBase {
     h->launches++;
   }
 
-  // Tile shapes: rows 2, 4, 8, and rows 4 | LBM_FUSED_STAGED (the staged form,
-  // FP16/BF16 storage only); SHAPE_WIDE marks a launch over a grid whose
-  // populations need 64-bit offsets.  f(IC<rows>, staged, wide) is called with
-  // the shape's compile-time form.
-  // the compact-ring form without the stage: rows | LBM_FUSED_COMPACT
-  using Compact = std::integral_constant<int, 2>;
+  // Tile shapes: rows 2, 4, 8 (the plain form, every storage form), and rows
+  // 4 or 6 | LBM_FUSED_COMPACT / LBM_FUSED_ASYNC / LBM_FUSED_STAGED (the
+  // compact-ring forms, which keep FP32 values in their ring: FP32, FP16 and
+  // BF16 storage); SHAPE_WIDE marks a launch over a grid whose populations
+  // need 64-bit offsets.  f(IC<rows>, IC<form>, wide) is called with the
+  // shape's compile-time launch form: 0 plain, PIPE_STAGED, PIPE_COMPACT,
+  // PIPE_ASYNC.
   template <class F>
   static void with_shape(int shape, F &&f) {
     const bool wide = (shape & SHAPE_WIDE) != 0;
@@ -208,59 +210,49 @@ class Ops final : public OpsBase {
       if (wide) f(T, S, std::true_type{});
       else f(T, S, std::false_type{});
     };
+    auto pipe = [&](auto T, auto S) {
+      if constexpr (kPipe) go(T, S);
+      else go(IC<4>{}, IC<0>{});  // not reached: shape_ok refuses these shapes
+    };
     switch (shape & ~SHAPE_WIDE) {
-      case 4 | LBM_FUSED_COMPACT:
-        if constexpr (kPipe) go(IC<4>{}, Compact{});
-        else go(IC<4>{}, std::false_type{});
-        break;
-      case 6 | LBM_FUSED_COMPACT:
-        if constexpr (kPipe) go(IC<6>{}, Compact{});
-        else go(IC<4>{}, std::false_type{});
-        break;
-      case 2: go(IC<2>{}, std::false_type{}); break;
-      case 4: go(IC<4>{}, std::false_type{}); break;
-      case 4 | LBM_FUSED_STAGED:
-        if constexpr (kPipe) go(IC<4>{}, std::true_type{});
-        else go(IC<4>{}, std::false_type{});
-        break;
-      case 6 | LBM_FUSED_STAGED:
-        if constexpr (kPipe) go(IC<6>{}, std::true_type{});
-        else go(IC<4>{}, std::false_type{});
-        break;
-      default: go(IC<8>{}, std::false_type{}); break;
+      case 2: go(IC<2>{}, IC<0>{}); break;
+      case 4: go(IC<4>{}, IC<0>{}); break;
+      case 4 | LBM_FUSED_COMPACT: pipe(IC<4>{}, IC<PIPE_COMPACT>{}); break;
+      case 6 | LBM_FUSED_COMPACT: pipe(IC<6>{}, IC<PIPE_COMPACT>{}); break;
+      case 4 | LBM_FUSED_ASYNC: pipe(IC<4>{}, IC<PIPE_ASYNC>{}); break;
+      case 6 | LBM_FUSED_ASYNC: pipe(IC<6>{}, IC<PIPE_ASYNC>{}); break;
+      case 4 | LBM_FUSED_STAGED: pipe(IC<4>{}, IC<PIPE_STAGED>{}); break;
+      case 6 | LBM_FUSED_STAGED: pipe(IC<6>{}, IC<PIPE_STAGED>{}); break;
+      default: go(IC<8>{}, IC<0>{}); break;
     }
   }
-  // the pipelined form (4 | LBM_FUSED_STAGED) keeps FP32 values in its ring:
-  // FP32, FP16 and BF16 storage
   static constexpr bool kPipe = sizeof(Real) == 4;
   bool shape_ok(int shape) const override {
-    return shape == 2 || shape == 4 || shape == 8 ||
-           ((shape == (4 | LBM_FUSED_STAGED) || shape == (6 | LBM_FUSED_STAGED) ||
-             shape == (4 | LBM_FUSED_COMPACT) || shape == (6 | LBM_FUSED_COMPACT)) &&
-            kPipe);
+    if (shape == 2 || shape == 4 || shape == 8) return true;
+    const int rows = shape & 0xff, form = shape & ~0xff;
+    return kPipe && (rows == 4 || rows == 6) &&
+           (form == LBM_FUSED_COMPACT || form == LBM_FUSED_ASYNC || form == LBM_FUSED_STAGED);
   }
-  // shared memory, warps and kernels of a launch form: FORM 0 the plain
-  // fused kernel, 1 the pipelined form with its stage, 2 the compact ring
-  // without the stage
+  // shared memory, warps and kernels of a launch form
   template <int TY, int FORM>
   static constexpr size_t smem_of() {
     if constexpr (FORM == 0) return FusedSmem<PopT, TY, false>::bytes;
-    else return PipeSmem<PopT, TY, FORM == 1>::bytes;
+    else return PipeSmem<PopT, TY, FORM>::bytes;
   }
   template <int TY, int FORM>
   static constexpr int warps_of() {
     if constexpr (FORM == 0) return FusedSmem<PopT, TY, false>::warps;
-    else return PipeSmem<PopT, TY, FORM == 1>::warps;
+    else return PipeSmem<PopT, TY, FORM>::warps;
   }
   template <int TY, int FORM, bool WIDE>
   static auto step_kernel() {
     if constexpr (FORM == 0) return k_fused_step<PopT, TY, false, WIDE>;
-    else return k_fused_pipe<PopT, TY, FORM == 1, WIDE>;
+    else return k_fused_pipe<PopT, TY, FORM, WIDE>;
   }
   template <int TY, int FORM, bool WIDE>
   static auto batch_kernel() {
     if constexpr (FORM == 0) return k_fused_batch<PopT, TY, false, WIDE>;
-    else return k_fused_pipe_batch<PopT, TY, FORM == 1, WIDE>;
+    else return k_fused_pipe_batch<PopT, TY, FORM, WIDE>;
   }
 
   template <int TY, int STG, bool WIDE>
@@ -331,9 +323,9 @@ class Ops final : public OpsBase {
                    int ctas, cudaStream_t st) override {
     with_shape(shape, [&](auto T, auto S, auto W) {
       constexpr int TY = decltype(T)::value;
-      constexpr int STG = decltype(S)::value;
-      dim3 block(32, warps_of<TY, STG>());
-      batch_kernel<TY, STG, decltype(W)::value>()<<<ctas, block, smem_of<TY, STG>(), st>>>(
+      constexpr int FORM = decltype(S)::value;
+      dim3 block(32, warps_of<TY, FORM>());
+      batch_kernel<TY, FORM, decltype(W)::value>()<<<ctas, block, smem_of<TY, FORM>(), st>>>(
           (const FusedArgs<PopT> *)d_args, d_tileStart, d_tileGrid, nscenes);
     });
   }

@@ -151,6 +151,10 @@ struct lbm_sim {
   lbm::Box boxLast{{1, 1, 1}, {0, 0, 0}};
   lbm::Box boxLastLast{{1, 1, 1}, {0, 0, 0}};
   lbm::Box lastRetagBox{{1, 1, 1}, {0, 0, 0}};
+  // a step split by lbm_step_begin / lbm_step_end: the spheres' box of the
+  // begun step, and how many spheres it was begun with (-1: none begun)
+  lbm::Box stepNow{{1, 1, 1}, {0, 0, 0}};
+  int stepBegunNs = -1;
   int fullRetagSteps = 0;
   int nsphLast = 0;
 

@@ -160,6 +160,16 @@ int lbm_solid_links(lbm_sim *sim, int32_t *cells, int8_t *dirs, double *mom, int
 /* retag + fresh cells on the spheres' bounding boxes, then one fused
  * gradient + collide + pull-stream + bounce-back + macro pass per step. */
 int lbm_step(lbm_sim *sim, const lbm_sphere *spheres, int nspheres, lbm_impulse *out);
+/* lbm_step in two halves, for z slabs of one scene (lbm_set_slab): begin =
+ * retagCells + handleFreshCells (src/sim.js:203-204), end = the rest of the
+ * step with the same spheres.  A slab's fresh cells are filled in the scene's
+ * scan order when the slabs begin in z order with each slab's two top owned
+ * planes copied into the next slab's copied planes after its begin, and the
+ * two bottom owned planes copied down before the lower slab's end.
+ * lbm_step = begin + end.  LBM_ERR_STATE for a begin after a begin or an end
+ * without one. */
+int lbm_step_begin(lbm_sim *sim, const lbm_sphere *spheres, int nspheres);
+int lbm_step_end(lbm_sim *sim, const lbm_sphere *spheres, int nspheres, lbm_impulse *out);
 
 /* RigidSphere.absorbDeadCells(sim) (src/solid.js:87-101): impulse rho(phi)*u
  * of every cell that turned FLUID -> SOLID at the last retag, summed in scan
@@ -254,16 +264,22 @@ int lbm_transfer_bytes(const lbm_sim *sim, uint64_t *h2d, uint64_t *d2h);
  * synchronises the stream and returns the summed kernel time and launch count. */
 int lbm_fused_timing(lbm_sim *sim, int enable);
 int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
-/* Fused-kernel launch shape: rows per CTA (2, 4 or 8) and z planes per CTA.
- * rows = 4 | LBM_FUSED_STAGED selects the staged form (FP16/BF16 storage
- * only): each tile row's populations of the next plane arrive in shared
- * memory by bulk asynchronous copy, waited on with bounded mbarrier waits.
+/* Fused-kernel launch shape: rows per CTA and z planes per CTA.
+ *   rows = 2, 4 or 8: the plain form (every storage form);
+ *   rows = 4 or 6 | LBM_FUSED_COMPACT: the compact shared-memory ring (each
+ *     direction keeps only the cells that can source it) with register loads
+ *     of each plane (FP32/FP16/BF16 storage); 6 | LBM_FUSED_COMPACT is the
+ *     default for those storage forms;
+ *   rows = 4 or 6 | LBM_FUSED_ASYNC: the compact ring, each thread's loads of
+ *     the next plane issued one plane ahead as per-thread asynchronous copies
+ *     into shared memory (FP32/FP16/BF16);
+ *   rows = 4 or 6 | LBM_FUSED_STAGED: the compact ring, the tile rows of the
+ *     next plane staged by bulk asynchronous copies waited on with bounded
+ *     mbarrier waits (FP32/FP16/BF16).
  * Every shape gives the same results bit for bit. */
 #define LBM_FUSED_STAGED 0x100
-/* rows = 4 | LBM_FUSED_COMPACT or 6 | LBM_FUSED_COMPACT: the compact shared-
- * memory ring of the pipelined form (each direction keeps only the cells that
- * can source it) with the plain form's register loads (FP32/FP16/BF16). */
 #define LBM_FUSED_COMPACT 0x400
+#define LBM_FUSED_ASYNC 0x800
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
 /* ---- one scene in z slabs (several handles, one or more GPUs) -------------- */
 /* Declares the handle a z slab of a larger scene: its local plane k is the

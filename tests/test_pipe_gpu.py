@@ -1,7 +1,7 @@
-"""The pipelined form of the fused step (tile shapes 4 | LBM_FUSED_STAGED and
-6 | LBM_FUSED_STAGED: tile rows staged in shared memory by bulk asynchronous
-copies, a compact ring) and the compact ring with register loads (4 or 6 |
-LBM_FUSED_COMPACT) give, bit for bit, what the plain 4-row form gives --
+"""The compact-ring forms of the fused step -- register loads (4 or 6 |
+LBM_FUSED_COMPACT), per-thread asynchronous copies one plane ahead (4 or 6 |
+LBM_FUSED_ASYNC), tile rows staged by bulk asynchronous copies (4 or 6 |
+LBM_FUSED_STAGED) -- give, bit for bit, what the plain 4-row form gives --
 for FP32, FP16 and BF16 storage, on grids whose rows start inside an 8-cell
 block (odd nx), with partial tiles in x and y, with moving spheres (SOLID
 links, fresh and dead cells) and a composite solid.  Run alone (lbm_step,
@@ -17,8 +17,9 @@ pytestmark = pytest.mark.gpu
 
 STAGED = 0x100
 COMPACT = 0x400
+ASYNC = 0x800
 PIPE_SHAPES = ((4 | STAGED, 32), (6 | STAGED, 32), (4 | STAGED, 5), (6 | STAGED, 9), (4 | COMPACT, 32),
-               (6 | COMPACT, 7))
+               (6 | COMPACT, 7), (6 | ASYNC, 32), (4 | ASYNC, 6), (6 | ASYNC, 5))
 
 
 @pytest.fixture(scope="module")
@@ -101,7 +102,7 @@ def test_pipelined_batch_equals_alone(gpu, storage):
     SimS = functools.partial(gpu.Sim, storage=storage)
     ref = [bld(SimS, gpu.RigidSphere) for bld in BUILDERS]
     for sim, solid in ref:
-        sim.run_coupled(solid, 8)
+        sim.run_coupled(solid, 10)
     mixed = [bld(SimS, gpu.RigidSphere) for bld in BUILDERS]
     with gpu.Batch(mixed) as batch:
         batch.set_config(6 | STAGED, 32)
@@ -109,6 +110,8 @@ def test_pipelined_batch_equals_alone(gpu, storage):
         batch.set_config(4 | STAGED, 16)
         batch.run(2, use_graph=False)
         batch.set_config(4 | COMPACT, 32)
+        batch.run(2)
+        batch.set_config(6 | ASYNC, 32)
         batch.run(2)
     for i, ((sim, solid), (rsim, rsolid)) in enumerate(zip(mixed, ref)):
         a, sa = _state(sim, solid)

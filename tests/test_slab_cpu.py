@@ -37,3 +37,57 @@ def test_partition_and_exchange(nz, ns):
 def test_too_many_slabs():
     with pytest.raises(ValueError):
         slab_plan(7, 4)
+
+
+def test_step_order_fills_in_scan_order(monkeypatch):
+    """SlabSim.step's protocol with stand-ins for the handles: slab s + 1
+    begins (retag + fresh fill) only after slab s began and its top owned
+    planes were copied up; every bottom-plane copy down comes after all begins
+    and before any end; the post-step exchange comes last."""
+    import b200lbm.slab as slab
+    log, made = [], []
+
+    class FakeSim:
+        def __init__(self, nx, ny, nz, storage="f32", device=0):
+            self.handle = len(made)
+            made.append(self)
+
+        def step_begin(self, solid):
+            log.append(("begin", self.handle))
+
+        def step_end(self, solid):
+            log.append(("end", self.handle))
+
+        def _moved(self):
+            pass
+
+    class FakeLib:
+        def lbm_set_slab(self, *a):
+            return 0
+
+        def lbm_slab_copy_planes(self, d, dp, s, sp, k):
+            log.append(("copy", d, dp, s, sp, k))
+            return 0
+
+        def lbm_last_error(self, h):
+            return b""
+
+    monkeypatch.setattr(slab, "Sim", FakeSim)
+    monkeypatch.setattr(slab, "lib", lambda: FakeLib())
+    monkeypatch.setattr(slab, "check", lambda h, rc: None)
+    ns = 3
+    scene = slab.SlabSim(8, 8, 48, nslabs=ns)
+    scene.step(None)
+    plan = scene.plan
+    up = [("copy", s + 1, 0, s, plan[s][7] - 1, 2) for s in range(ns - 1)]
+    down = [("copy", s, plan[s][7] + 1, s + 1, plan[s + 1][6], 2) for s in range(ns - 1)]
+    expect = []
+    for s in range(ns):
+        expect.append(("begin", s))
+        if s < ns - 1:
+            expect.append(up[s])
+    expect += down
+    expect += [("end", s) for s in range(ns)]
+    for u, d in zip(up, down):
+        expect += [u, d]
+    assert log == expect
