@@ -96,6 +96,8 @@ _SIGS = [
     ("lbm_pack_volume", C.c_int, [C.c_void_p, C.c_void_p]),
     ("lbm_pack_volume_device", C.c_int, [C.c_void_p, C.c_void_p]),
     ("lbm_host_alloc", C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
+    ("lbm_prepare_device", C.c_int, [C.c_int, C.c_int, C.c_uint64]),
+    ("lbm_trim_device_memory", C.c_int, [C.c_int]),
     ("lbm_pack_volume_async", C.c_int, [C.c_void_p, C.c_void_p]),
     ("lbm_wait_frames", C.c_int, [C.c_void_p]),
     ("lbm_host_free", C.c_int, [C.c_void_p]),

@@ -93,13 +93,30 @@ def percentiles(xs, ps=(50, 99)):
 
 
 class Server:
-    def __init__(self, storage="f16", budget_bytes=None, tick=None, use_graph=True, tune=True, device=0):
+    def __init__(self, storage="f16", budget_bytes=None, tick=None, use_graph=True, tune=True, device=0,
+                 prepare=True):
         self.storage = storage
         self.budget = budget_bytes if budget_bytes is not None else int(0.9 * 180e9)
         self.tick = tick
         self.use_graph = use_graph
         self.tune = tune
         self.device = device
+        self.prepare = prepare
+        self.prepared = None
+
+    def start(self):
+        """Server start-up (once, before the first run; run calls it): load
+        the storage form's fused kernels and grow the device's memory pool to
+        the budget (at most the free memory less 4 GB), so that neither a
+        first launch nor a new scene's allocation stalls a tick.  Records the
+        reserved bytes (0 when the reserve did not fit)."""
+        if self.prepared is not None or not self.prepare:
+            return
+        import torch
+        free, _ = torch.cuda.mem_get_info(self.device)
+        want = max(0, min(self.budget, free - 4 * 2**30))
+        rc = lib().lbm_prepare_device(self.device, STORAGE[self.storage], want)
+        self.prepared = want if rc == 0 else 0
 
     def run(self, requests, realtime=True, on_frame=None, on_finish=None):
         """Serve `requests` (dicts with rid, arrival, spec, steps, frame_every;
@@ -116,6 +133,7 @@ class Server:
         tick = self.tick or every
         if tick % every or any(r["steps"] % tick for r in reqs):
             raise ValueError("the tick must be a multiple of the frame cadence and divide every request")
+        self.start()
         queue = collections.deque(reqs)
         active = []  # dicts: req, sim, solid, done, fp, frames, last
         used = 0
@@ -128,6 +146,7 @@ class Server:
         # telling the batch its members, retiring finished scenes
         seg = {"admit": [], "members": [], "retire": []}
         changes = 0  # membership changes of the batch
+        slow = []  # per tick: (batch run s, membership changed, active, building, cells)
         scene_steps = cell_steps = 0
         max_active = 0
         ticks = 0
@@ -167,7 +186,8 @@ class Server:
                 ids = [a["req"]["rid"] for a in active]
                 tk0 = time.perf_counter()
                 seg["admit"].append(tk0 - tl0)
-                if ids != members:
+                changed = ids != members
+                if changed:
                     pairs = [(a["sim"], a["solid"]) for a in active]
                     if batch is None:
                         batch = Batch(pairs)
@@ -189,6 +209,8 @@ class Server:
                     tuner.step()
                 t = time.perf_counter() - t0
                 tick_run.append(tk1 - tkm)
+                slow.append((tk1 - tkm, changed, len(active), len(building),
+                             sum(a["sim"].n for a in active)))
                 tick_tune.append(t + t0 - tk1)
                 for a, fr in zip(active, frames):
                     for j in range(fr.shape[0]):
@@ -242,6 +264,9 @@ class Server:
             "membership_changes": changes,
             "tick_run_s": percentiles(tick_run, (50, 99, 100)),
             "tick_tune_s": percentiles(tick_tune, (50, 99, 100)),
+            "slowest_ticks": [dict(run_s=r, membership_changed=c, active=a, building=b, cells=n)
+                              for r, c, a, b, n in sorted(slow, key=lambda t: -t[0])[:5]],
+            "reserved_bytes": self.prepared,
             **{f"{k}_s": percentiles(v, (50, 99, 100)) for k, v in seg.items()},
             "storage": self.storage,
             "budget_bytes": self.budget,

@@ -1208,6 +1208,52 @@ int lbm_pack_volume_device(lbm_sim *h, void *dev_out) {
   return LBM_OK;
 }
 
+int lbm_prepare_device(int device, int storage, uint64_t reserve_bytes) {
+  OpsBase *ops = ops_for(storage);
+  int ndev = 0;
+  if (!ops || cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return LBM_ERR_ARG;
+  }
+  DeviceGuard g(device);
+  keep_pool(device);
+  ops->warm(device);
+  if (reserve_bytes == 0) return LBM_OK;
+  // one allocation of the reserve, freed again: the pool keeps its memory
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return LBM_ERR_CUDA;
+  }
+  int rc = LBM_OK;
+  void *p = nullptr;
+  if (cudaMallocAsync(&p, (size_t)reserve_bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    rc = LBM_ERR_OOM;
+  } else if (cudaFreeAsync(p, st) != cudaSuccess) {
+    rc = LBM_ERR_CUDA;
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess && rc == LBM_OK) rc = LBM_ERR_CUDA;
+  cudaStreamDestroy(st);
+  cudaGetLastError();
+  return rc;
+}
+
+int lbm_trim_device_memory(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return LBM_ERR_ARG;
+  }
+  DeviceGuard g(device);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) {
+    cudaGetLastError();
+    return LBM_ERR_CUDA;
+  }
+  return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+}
+
 int lbm_host_alloc(size_t bytes, void **out) {
   if (!out || bytes == 0) return LBM_ERR_ARG;
   *out = nullptr;

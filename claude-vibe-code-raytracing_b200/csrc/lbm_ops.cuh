@@ -312,6 +312,21 @@ class Ops final : public OpsBase {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per) * std::max(1, sms);
   }
+  void warm(int device) override {
+    static const int shapes[] = {2, 4, 8, 4 | LBM_FUSED_COMPACT, 6 | LBM_FUSED_COMPACT, 4 | LBM_FUSED_ASYNC,
+                                 6 | LBM_FUSED_ASYNC, 4 | LBM_FUSED_STAGED, 6 | LBM_FUSED_STAGED};
+    for (int sh : shapes) {
+      if (!shape_ok(sh)) continue;
+      with_shape(sh, [&](auto T, auto S, auto W) {
+        constexpr int TY = decltype(T)::value, FORM = decltype(S)::value;
+        constexpr bool WIDE = decltype(W)::value;
+        batch_ctas<TY, FORM, WIDE>(device);
+        cudaFuncSetAttribute(step_kernel<TY, FORM, WIDE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_of<TY, FORM>());
+      });
+    }
+    cudaGetLastError();
+  }
   int fused_batch_ctas(int shape, int device) override {
     int r = 0;
     with_shape(shape, [&](auto T, auto S, auto W) {

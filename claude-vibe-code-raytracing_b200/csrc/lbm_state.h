@@ -83,6 +83,10 @@ class OpsBase {
   virtual cudaError_t read_fault(lbm_sim *h, unsigned long long out[4]) = 0;
   // a tile shape this storage form supports (rows 2, 4, 8; 4 | LBM_FUSED_STAGED for FP16/BF16)
   virtual bool shape_ok(int shape) const = 0;
+  // load every fused step and batch kernel instance of this storage form on
+  // the device (and set their shared-memory opt-in), so that no first launch
+  // waits for a module load
+  virtual void warm(int device) = 0;
 };
 
 OpsBase *make_ops_f32();

@@ -180,6 +180,16 @@ int lbm_absorb_dead_cells(lbm_sim *sim, const lbm_sphere *spheres, int nspheres,
 /* Sim.packVolume(out) (src/sim.js:586-600): 2*n bytes, R = (clamp01(phi)*255)|0,
  * G = 255 on SOLID cells. */
 int lbm_pack_volume(lbm_sim *sim, uint8_t *host_out);
+/* Server start-up, no counterpart in the reference: load every fused kernel
+ * of a storage form on the device (so no first launch waits for a module
+ * load) and, with reserve_bytes > 0, grow the device's memory pool by that
+ * much once (scene memory comes from the pool and stays there after a scene
+ * is destroyed, so later scenes allocate without mapping new memory).
+ * LBM_ERR_OOM when the reserve does not fit (the kernels are loaded
+ * anyway).  lbm_trim_device_memory returns the pool's unused memory to the
+ * device. */
+int lbm_prepare_device(int device, int storage, uint64_t reserve_bytes);
+int lbm_trim_device_memory(int device);
 /* Page-locked host memory for the buffers a host reads every frame (packed
  * volumes, rendered images): device-to-host copies into it run at full link
  * speed, while a pageable destination is copied through driver staging
