@@ -79,6 +79,7 @@ _SIGS = [
     ("lbm_download_field", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     ("lbm_download_field_f64", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_size_t]),
     ("lbm_init_flat", C.c_int, [C.c_void_p, C.c_double]),
+    ("lbm_init_profile", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int]),
     ("lbm_seed_hydrostatic", C.c_int, [C.c_void_p]),
     ("lbm_retag_cells", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int]),
     ("lbm_handle_fresh_cells", C.c_int, [C.c_void_p]),

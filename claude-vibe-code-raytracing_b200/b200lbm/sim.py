@@ -257,6 +257,19 @@ class Sim:
         check(self._h, lib().lbm_init_flat(self._h, float(waterlineY)))
         self._moved()
 
+    def initProfile(self, phi_col):
+        """initFlat with a column profile phi_col[y] (ny values) in place of
+        the waterline's tanh (lbm_init_profile): what writing phi, phiPrev and
+        h = w7 phi cell by cell after initFlat and then calling
+        seedHydrostatic gives, with the fields kept on the device."""
+        col = np.ascontiguousarray(phi_col, dtype=np.float64)
+        if col.shape != (self.ny,):
+            raise ValueError("phi_col needs ny values")
+        self.__dict__["_dirty"].clear()
+        self._sync()
+        check(self._h, lib().lbm_init_profile(self._h, col.ctypes.data_as(C.POINTER(C.c_double)), self.ny))
+        self._moved()
+
     def seedHydrostatic(self):
         """src/sim.js:144-173"""
         self._sync()

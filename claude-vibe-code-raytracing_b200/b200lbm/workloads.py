@@ -82,17 +82,28 @@ def big_spec(n=256):
                               vx=0.0, vy=0.0, vz=0.0)])
 
 
-def pool_below(sim, level, W=4.0):
-    """phi = 1/2 (1 + tanh(2 (level - y) / W)) on every cell, h = w7 phi, then
-    seedHydrostatic (the dam preset's pattern, src/worker.js:57-73)."""
-    nx, ny, nz = sim.nx, sim.ny, sim.nz
+def pool_column(ny, level, W=4.0):
+    """phi of a pool below `level`: 1/2 (1 + tanh(2 (level - y) / W)) per row."""
     ys = np.arange(ny, dtype=np.float64)
-    col = 0.5 * (1 + np.tanh(2 * (level - ys) / W))
+    return 0.5 * (1 + np.tanh(2 * (level - ys) / W))
+
+
+def pool_below_host(sim, level, W=4.0):
+    """phi = pool_column on every cell, h = w7 phi, then seedHydrostatic,
+    written from the host as the dam preset does (src/worker.js:57-73)."""
+    nx, ny, nz = sim.nx, sim.ny, sim.nz
+    col = pool_column(ny, level, W)
     phi = np.broadcast_to(col[None, :, None], (nz, ny, nx)).reshape(-1)
     sim.phi[:] = phi.astype(np.float32)
     sim.phiPrev[:] = phi.astype(np.float32)
     sim.h[:] = (phi[:, None] * W7[None, :]).astype(np.float32).reshape(-1)
     sim.seedHydrostatic()
+
+
+def pool_below(sim, level, W=4.0):
+    """The same state as pool_below_host, initialised on the device from the
+    column profile (Sim.initProfile): nothing crosses the host link."""
+    sim.initProfile(pool_column(sim.ny, level, W))
 
 
 def build(spec, storage="f16", device=0):
@@ -101,7 +112,6 @@ def build(spec, storage="f16", device=0):
     sim = Sim(nx, ny, nz, storage=storage, device=device)
     for k, v in PHYSICS.items():
         setattr(sim, k, v)
-    sim.initFlat(spec["level"])
     pool_below(sim, spec["level"], PHYSICS["W"])
     spheres = []
     for p in spec["spheres"]:

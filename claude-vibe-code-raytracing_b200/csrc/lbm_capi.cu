@@ -946,6 +946,21 @@ int lbm_init_flat(lbm_sim *h, double waterlineY) {
   return LBM_OK;
 }
 
+int lbm_init_profile(lbm_sim *h, const double *phi_col, int ny) {
+  if (!h || !phi_col || ny != h->ny) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  CK(copy_async(h, h->dPhiCol, phi_col, h->ny * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  h->ops->init_flat(h, h->dPhiCol);
+  CKL("init_profile");
+  h->ops->seed_hydrostatic(h);
+  CKL("seed_hydrostatic");
+  CK(cudaStreamSynchronize(h->stream));
+  h->boxLast = h->boxLastLast = Box{{1, 1, 1}, {0, 0, 0}};
+  h->fullRetagSteps = 0;
+  h->listsValid = false;
+  return LBM_OK;
+}
+
 int lbm_seed_hydrostatic(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);

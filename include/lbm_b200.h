@@ -125,6 +125,13 @@ int lbm_download_field_f64(lbm_sim *sim, int field, double *host, size_t count);
 /* ---- init (src/sim.js:112-173) --------------------------------------------- */
 int lbm_init_flat(lbm_sim *sim, double waterlineY);
 int lbm_seed_hydrostatic(lbm_sim *sim);
+/* initFlat with the caller's column profile instead of the waterline's tanh:
+ * phi = phiPrev = phi_col[y] (ny doubles) on every cell of row y, h = w7 phi,
+ * f = w27, rho 1, u 0, walls tagged, then seedHydrostatic -- what a host
+ * that writes phi and h cell by cell after initFlat (the dam preset,
+ * src/worker.js:57-73) gets for a profile that depends on y only, without
+ * moving the fields through the host. */
+int lbm_init_profile(lbm_sim *sim, const double *phi_col, int ny);
 
 /* ---- the seven phases, callable one by one (src/sim.js:176-582) ------------- */
 /* spheres may be NULL with nspheres 0 (the reference's solid === null). */
