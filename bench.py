@@ -701,8 +701,9 @@ def main():
 
     # ---------------- e2e through the public API (worker.js cadence)
     e2e_steps = min(args.e2e_steps, args.steps)
-    # two page-locked frame buffers, filled alternately by packVolumeAsync
-    # while the next steps run; every copy has landed before the clock stops
+    # two page-locked frame buffers, filled alternately: on a frame step the
+    # fused kernel packs the RG8 volume (stepFrame) and the copy runs while the
+    # next steps do; every copy has landed before the clock stops
     frames = [sim.frameBuffer(), sim.frameBuffer()]
     nframe = 0
     substeps = 2
@@ -712,14 +713,15 @@ def main():
     check(h, L.lbm_transfer_bytes(h, C.byref(x0[0]), C.byref(x0[1])))
     t0 = time.perf_counter()
     for s in range(e2e_steps):
-        sim.step(sol)
-        sol.absorbDeadCells(sim)
-        sol.step(1.0, sim.gravity)
         if (s + 1) % substeps == 0:
             if nframe >= 2:
                 sim.waitFrames()  # the consumer has taken frames[nframe % 2] by now
-            sim.packVolumeAsync(frames[nframe % 2])
+            sim.stepFrame(sol, frames[nframe % 2])
             nframe += 1
+        else:
+            sim.step(sol)
+        sol.absorbDeadCells(sim)
+        sol.step(1.0, sim.gravity)
     sim.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, ws, local)
@@ -760,7 +762,7 @@ def main():
                          "bytes_per_cell": bpc, "cells_per_launch": interior},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                    "path": "Sim.step + absorbDeadCells + RigidSphere.step, every 2 steps packVolumeAsync into alternating page-locked frame buffers (copy overlapped with the next steps; waitFrames before the clock stops)"},
+                    "path": "Sim.step + absorbDeadCells + RigidSphere.step; every 2nd step Sim.stepFrame (the step with packVolume fused into it) into alternating page-locked frame buffers (copy overlapped with the next steps; waitFrames before the clock stops)"},
             "gpu_launches": int(c1.value - c0.value),
             "clocks": clk,
             "cpu_baseline": cpu,

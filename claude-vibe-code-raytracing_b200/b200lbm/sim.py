@@ -379,6 +379,26 @@ class Sim:
         rc = lib().lbm_step(self._h, arr, len(sp), out)
         self._completed(rc, lambda: [b.add_impulse(out[i]) for i, b in enumerate(sp)])
 
+    def stepFrame(self, solid, out):
+        """step(solid) on a frame step: the fused kernel also writes the
+        step's RG8 volume (packVolume, src/sim.js:586-600), which is copied
+        into `out` (a frameBuffer) while the next steps run -- packVolumeAsync
+        after step without its separate pass over the grid.  `out` holds the
+        frame after waitFrames()."""
+        if is_generic(solid):
+            self.step(solid)
+            return self.packVolumeAsync(out)
+        buf = np.asarray(out).view(np.ndarray)
+        if buf.dtype != np.uint8 or buf.size < self.n * 2 or not buf.flags.c_contiguous:
+            raise ValueError("stepFrame needs a contiguous uint8 buffer of 2*n bytes")
+        sp = spheres_of(solid)
+        self._sync()
+        arr = to_c_array(sp)
+        res = impulse_array(len(sp))
+        rc = lib().lbm_step_frame(self._h, arr, len(sp), res, buf.ctypes.data_as(C.c_void_p))
+        self._completed(rc, lambda: [b.add_impulse(res[i]) for i, b in enumerate(sp)])
+        return out
+
     def step_begin(self, solid):
         """The first half of step (retagCells + handleFreshCells,
         src/sim.js:203-204); step_end(solid) with the same solid completes it."""

@@ -582,9 +582,11 @@ int coupled_post(lbm_sim *h, const CoupledCtx &c) {
   return LBM_OK;
 }
 
-// RG8 volume of the current state into host memory dst (pinned when captured)
-int coupled_frame(lbm_sim *h, uint8_t *dst) {
-  h->ops->pack(h, (uint8_t *)h->staging);
+// RG8 volume of the current state into host memory dst (pinned when captured);
+// fused: the fused step packed planes 1 .. nz-2 into the staging buffer already
+int coupled_frame(lbm_sim *h, uint8_t *dst, bool fused = false) {
+  if (fused) h->ops->pack_end_planes(h, (uint8_t *)h->staging);
+  else h->ops->pack(h, (uint8_t *)h->staging);
   CKL("packVolume");
   CK(copy_async(h, dst, h->staging, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->stream));
   return LBM_OK;
@@ -602,6 +604,18 @@ int coupled_finish(lbm_sim *h, lbm_sphere *sp, int ns) {
   h->lastRetagBox = h->hPlan.U;
   h->listsValid = true;
   if (h->hPlan.overflow) return fail(h, LBM_ERR_CAPACITY, "sphere moved beyond the planned retag box");
+  return LBM_OK;
+}
+
+// the copy stream, its two events and the device frame of the asynchronous
+// frame path, created on first use
+int ensure_frame_stream(lbm_sim *h) {
+  if (!h->copyStream) {
+    CK(cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->evPacked, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->evCopied, cudaEventDisableTiming));
+  }
+  if (!h->frameDev) DALLOC(h->frameDev, (size_t)h->n * 2);
   return LBM_OK;
 }
 
@@ -1200,6 +1214,34 @@ int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   return lbm_step_end(h, sp, ns, out);
 }
 
+int lbm_step_frame(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out, uint8_t *host_frame) {
+  if (!h || !host_frame) return LBM_ERR_ARG;
+  if (h->bfActive || !h->fusedOK) {
+    int rc = lbm_step(h, sp, ns, out);
+    return rc ? rc : lbm_pack_volume_async(h, host_frame);
+  }
+  DeviceGuard g(h->device);
+  int rc = ensure_frame_stream(h);
+  if (rc) return rc;
+  if ((rc = lbm_step_begin(h, sp, ns))) return rc;
+  // the device frame is reused: the previous copy out of it must be done
+  // before the fused kernel writes it
+  if (h->copyPending) CK(cudaStreamWaitEvent(h->stream, h->evCopied, 0));
+  h->fusePack = (uint8_t *)h->frameDev;
+  rc = lbm_step_end(h, sp, ns, out);
+  h->fusePack = nullptr;
+  if (rc && rc != LBM_ERR_NAN) return rc;
+  const int stepRc = rc;
+  h->ops->pack_end_planes(h, (uint8_t *)h->frameDev);
+  CKL("packVolume (end planes)");
+  CK(cudaEventRecord(h->evPacked, h->stream));
+  CK(cudaStreamWaitEvent(h->copyStream, h->evPacked, 0));
+  CK(copy_async(h, host_frame, h->frameDev, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->copyStream));
+  CK(cudaEventRecord(h->evCopied, h->copyStream));
+  h->copyPending = true;
+  return stepRc;
+}
+
 int lbm_absorb_dead_cells(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   if (!h) return LBM_ERR_ARG;
   int rc = check_spheres(h, sp, ns);
@@ -1283,12 +1325,8 @@ int lbm_host_free(void *p) {
 int lbm_pack_volume_async(lbm_sim *h, uint8_t *host_out) {
   if (!h || !host_out) return fail(h, LBM_ERR_ARG, "null");
   DeviceGuard g(h->device);
-  if (!h->copyStream) {
-    CK(cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&h->evPacked, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&h->evCopied, cudaEventDisableTiming));
-  }
-  if (!h->frameDev) DALLOC(h->frameDev, (size_t)h->n * 2);
+  int rc = ensure_frame_stream(h);
+  if (rc) return rc;
   // the device frame is reused: the previous copy out of it must be done
   if (h->copyPending) CK(cudaStreamWaitEvent(h->stream, h->evCopied, 0));
   h->ops->pack(h, (uint8_t *)h->frameDev);
@@ -1351,12 +1389,16 @@ int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_ev
   if (rc) return rc;
   long long frame = 0;
   for (int s = 0; s < nsteps; s++) {
+    const bool frameStep = frame_every > 0 && frames && (s + 1) % frame_every == 0;
     if ((rc = coupled_pre(h, c))) return rc;
+    // a frame step's fused kernel also writes the step's RG8 volume
+    h->fusePack = frameStep ? (uint8_t *)h->staging : nullptr;
     launch_fused(h);
+    h->fusePack = nullptr;
     if ((rc = coupled_post(h, c))) return rc;
     h->cur = 1 - h->cur;
-    if (frame_every > 0 && frames && (s + 1) % frame_every == 0) {
-      if ((rc = coupled_frame(h, frames + frame * 2 * h->n))) return rc;
+    if (frameStep) {
+      if ((rc = coupled_frame(h, frames + frame * 2 * h->n, true))) return rc;
       frame++;
     }
   }

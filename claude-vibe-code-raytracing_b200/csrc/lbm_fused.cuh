@@ -49,6 +49,7 @@ struct FusedArgs {
   const SolidSet *ss;
   int *status;   // set non-zero when a bounded wait of the step runs out
   int withhold;  // test hook: the staged form does not issue each tile's first copy
+  uint8_t *pack; // frame step: the RG8 volume of the step's result (planes 1 .. nz-2), else null
 };
 
 // slot of direction k within its e_z group (0..8 for D3Q27)
@@ -816,6 +817,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
       st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
       st_at(s.uz[nxt], i, nCell, 12, ldg_at(uzC, i, nCell, 12));
+      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
     } else if (tagI == TAG_FLUID) {
       // ring bases: group e_z sources come from plane z - e_z; the cell's own
       // (bounce-back) values are in plane z
@@ -952,6 +954,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       st_at(s.ux[nxt], i, nCell, 18, uxn);
       st_at(s.uy[nxt], i, nCell, 18, uyn);
       st_at(s.uz[nxt], i, nCell, 18, uzn);
+      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
+    } else if (a.pack && !haloWarp && x < nx && y < ny && z >= zb) {
+      // a wall cell of this tile: not updated, packed from the half that is
+      // current after the step
+      if (lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(s.phi[nxt], i, nCell, 12), false);
     }
     if constexpr (STAGE) __syncthreads();
     gxC = gxN;

@@ -603,6 +603,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
       st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
       st_at(s.uz[nxt], i, nCell, 12, ldg_at(uzC, i, nCell, 12));
+      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
     } else if (tagI == TAG_FLUID) {
       // ring copies: group e_z sources come from plane z - e_z; the cell's own
       // (bounce-back) values are in plane z
@@ -739,6 +740,11 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       st_at(s.ux[nxt], i, nCell, 18, uxn);
       st_at(s.uy[nxt], i, nCell, 18, uyn);
       st_at(s.uz[nxt], i, nCell, 18, uzn);
+      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
+    } else if (a.pack && cellWarp && x < nx && y < ny && z >= zb) {
+      // a wall cell of this tile: not updated, packed from the half that is
+      // current after the step
+      if (lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(s.phi[nxt], i, nCell, 12), false);
     }
     gxC = gxN;
     gyC = gyN;

@@ -899,20 +899,37 @@ static __global__ void k_plan(Plan *P, const lbm_sphere *sph, int nsph, int nx, 
   P->boxLast = now;
 }
 
+// packVolume's two bytes of cell i (src/sim.js:586-600): R = clamp01(phi) *
+// 255 truncated (a NaN gives 0), G = 255 for a SOLID cell, else 0
+template <class Real>
+__device__ __forceinline__ void pack_rg8(uint8_t *out, long long i, Real phi, bool solid) {
+  double p = (double)phi;
+  if (p < 0.0) p = 0.0;
+  else if (p > 1.0) p = 1.0;
+  const double v = p * 255.0;
+  uchar2 o;
+  o.x = (uint8_t)((v == v) ? (int)v : 0);
+  o.y = solid ? 255 : 0;
+  reinterpret_cast<uchar2 *>(out)[i] = o;
+}
+
 // packVolume (src/sim.js:586-600)
 template <class PopT>
 __global__ void k_pack(Scene<PopT, typename Prec<PopT>::Real> s, int cur, uint8_t *out) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= s.n) return;
-  double p = (double)s.phi[cur][i];
-  if (p < 0.0) p = 0.0;
-  else if (p > 1.0) p = 1.0;
-  double v = p * 255.0;
-  int r = (v == v) ? (int)v : 0;
-  uchar2 o;
-  o.x = (uint8_t)r;
-  o.y = s.tag[i] == TAG_SOLID ? 255 : 0;
-  reinterpret_cast<uchar2 *>(out)[i] = o;
+  pack_rg8(out, i, s.phi[cur][i], s.tag[i] == TAG_SOLID);
+}
+
+// packVolume of the planes z = 0 and z = nz - 1 only: the fused step packs
+// every other cell on a frame step
+template <class PopT>
+__global__ void k_pack_end_planes(Scene<PopT, typename Prec<PopT>::Real> s, int cur, uint8_t *out) {
+  const long long plane = (long long)s.nx * s.ny;
+  long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= 2 * plane) return;
+  const long long i = j < plane ? j : (long long)(s.nz - 1) * plane + (j - plane);
+  pack_rg8(out, i, s.phi[cur][i], s.tag[i] == TAG_SOLID);
 }
 
 // NaN/Inf watchdog: the lowest index of a cell whose phi, rho or u is not

@@ -290,6 +290,7 @@ class Ops final : public OpsBase {
     a.ss = &h->dPlan->ss;
     a.status = h->totals + 2;
     a.withhold = h->withholdStage ? 1 : 0;
+    a.pack = h->fusePack;
     return a;
   }
   size_t fused_args_bytes() const override { return sizeof(FusedArgs<PopT>); }
@@ -371,6 +372,11 @@ class Ops final : public OpsBase {
 
   void pack(lbm_sim *h, uint8_t *d_out) override {
     k_pack<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), h->cur, d_out);
+    h->launches++;
+  }
+  void pack_end_planes(lbm_sim *h, uint8_t *d_out) override {
+    const long long cells = 2LL * h->nx * h->ny;
+    k_pack_end_planes<PopT><<<nblocks(cells, 256), 256, 0, h->stream>>>(scene(h), h->cur, d_out);
     h->launches++;
   }
   void watch_finite(lbm_sim *h, unsigned long long *d_first) override {

@@ -56,6 +56,7 @@ class OpsBase {
   virtual void absorb_dead(lbm_sim *h, double *d_out) = 0;
   virtual void fused_step(lbm_sim *h, const FusedCfg &cfg) = 0;
   virtual void pack(lbm_sim *h, uint8_t *d_out) = 0;
+  virtual void pack_end_planes(lbm_sim *h, uint8_t *d_out) = 0;
   virtual void watch_finite(lbm_sim *h, unsigned long long *d_first) = 0;
   // Reference-layout float32 <-> device storage for population fields.
   // half: 0 = both halves (current state), 1 = [cur], 2 = [1-cur].
@@ -158,6 +159,9 @@ struct lbm_sim {
   // a step split by lbm_step_begin / lbm_step_end: the spheres' box of the
   // begun step, and how many spheres it was begun with (-1: none begun)
   lbm::Box stepNow{{1, 1, 1}, {0, 0, 0}};
+  // a frame step: the fused kernel writes the step's RG8 volume here
+  // (planes 1 .. nz-2; pack_end_planes adds the two end planes), else null
+  uint8_t *fusePack = nullptr;
   int stepBegunNs = -1;
   int fullRetagSteps = 0;
   int nsphLast = 0;

@@ -471,6 +471,35 @@ static napi_value js_pack_volume_async(napi_env env, napi_callback_info info) {
   return check_sim(env, h, lbm_pack_volume_async(h, d));
 }
 
+/* stepFrame(h, spheres, out, Uint8Array frame): step with packVolume fused
+ * into it; the frame is copied into `frame` asynchronously (waitFrames) */
+static napi_value js_step_frame(napi_env env, napi_callback_info info) {
+  Args a;
+  if (!args_get(env, info, &a, 4)) return NULL;
+  lbm_sim *h = arg_sim(&a, 0);
+  int n = 0;
+  lbm_sphere *sp = arg_spheres(&a, 1, &n);
+  lbm_impulse *out = arg_impulses(&a, 2, n);
+  size_t len = 0;
+  uint8_t *d = (uint8_t *)arg_typed(&a, 3, napi_uint8_array, &len);
+  if (a.failed) return NULL;
+  int nx = 0, ny = 0, nz = 0, st = 0;
+  lbm_get_dims(h, &nx, &ny, &nz, &st);
+  if (len < 2 * (size_t)nx * ny * nz) return throw_msg(env, LBM_ERR_ARG, "stepFrame needs 2 * nx * ny * nz bytes");
+  return check_sim(env, h, lbm_step_frame(h, sp, n, out, d));
+}
+
+/* initProfile(h, Float64Array phiCol[ny]): initFlat with a column profile */
+static napi_value js_init_profile(napi_env env, napi_callback_info info) {
+  Args a;
+  if (!args_get(env, info, &a, 2)) return NULL;
+  lbm_sim *h = arg_sim(&a, 0);
+  size_t len = 0;
+  double *col = (double *)arg_typed(&a, 1, napi_float64_array, &len);
+  if (a.failed) return NULL;
+  return check_sim(env, h, lbm_init_profile(h, col, (int)len));
+}
+
 /* runCoupled(h, spheres, nsteps, frameEvery, frames | null): the worker's tick
  * (src/worker.js:96-100) nsteps times on the device; spheres updated in place */
 static napi_value js_run_coupled(napi_env env, napi_callback_info info) {
@@ -820,6 +849,8 @@ static const napi_property_descriptor kExports[] = {
     FN("absorbDeadCells", js_absorb_dead_cells),
     FN("packVolume", js_pack_volume),
     FN("packVolumeAsync", js_pack_volume_async),
+    FN("stepFrame", js_step_frame),
+    FN("initProfile", js_init_profile),
     FN("waitFrames", js_wait_frames),
     FN("runCoupled", js_run_coupled),
     FN("sphereStep", js_sphere_step),

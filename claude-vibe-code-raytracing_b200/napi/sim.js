@@ -256,6 +256,15 @@ export class Sim {
     return frames;
   }
   packVolumeAsync(out) { this._sync(); addon.packVolumeAsync(this._h, out); return out; }
+  // step(solid) with packVolume fused into it; `out` holds the frame after waitFrames()
+  stepFrame(solid, out) {
+    if (spheresOf(solid) === null) {
+      this.step(solid);
+      return this.packVolumeAsync(out);
+    }
+    this._withImpulses((h, sp, imp) => addon.stepFrame(h, sp, imp, out), solid);
+    return out;
+  }
   waitFrames() { addon.waitFrames(this._h); }
   field64(name) {
     this._sync();

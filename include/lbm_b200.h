@@ -212,6 +212,13 @@ int lbm_host_free(void *p);
  * copy before packing again.  No counterpart in the reference, whose worker
  * packs synchronously and posts the buffer (src/worker.js:102-111). */
 int lbm_pack_volume_async(lbm_sim *sim, uint8_t *host_out);
+/* lbm_step + lbm_pack_volume_async on a frame step, with the pack fused into
+ * the step: the fused kernel writes the RG8 bytes of every cell it visits as
+ * it writes the macros, a small launch adds the planes z = 0 and nz - 1, and
+ * the volume is copied into host_frame on the copy stream (complete after
+ * lbm_wait_frames).  The same bytes as lbm_step then lbm_pack_volume. */
+int lbm_step_frame(lbm_sim *sim, const lbm_sphere *spheres, int nspheres, lbm_impulse *out,
+                   uint8_t *host_frame);
 int lbm_wait_frames(lbm_sim *sim);
 /* Same, into device memory, asynchronous on the handle's stream. */
 int lbm_pack_volume_device(lbm_sim *sim, void *device_out);

@@ -62,3 +62,69 @@ def test_async_frames_match_sync(gpu):
     sim2.waitFrames()
     for f in range(5):
         assert np.array_equal(bufs[f], want[f]), f
+
+
+SHAPES = ((4, 32), (0x406, 32), (0x806, 9), (0x104, 7), (2, 5))
+
+
+def _set_shape(sim, rows, zchunk):
+    from b200lbm import _capi
+    sim._sync()
+    _capi.check(sim.handle, _capi.lib().lbm_set_fused_config(sim.handle, rows, zchunk))
+
+
+def _odd_falling(SimC, SphC):
+    """35 x 21 x 26 (partial tiles, rows off the 8-cell blocks) with a sphere
+    moving down through the interface: SOLID cells, fresh and dead cells."""
+    sim = SimC(35, 21, 26)
+    scenes._params(sim, 0.7, 0.75, 0.01, 0.001)
+    sim.initFlat(8.5)
+    sol = SphC(35, 21, 26, cx=16.3, cy=12.2, cz=12.7, r=3.6, density=2.5)
+    sol.vy = -0.03
+    return sim, sol
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
+def test_fused_pack_equals_pack(gpu, storage):
+    """The RG8 volume written by the fused step on a frame step (stepFrame,
+    and run_coupled with frames) is byte for byte packVolume after the step,
+    for every launch form, with SOLID, wall and end-plane cells; the fields
+    are those of plain steps."""
+    import functools
+    SimS = functools.partial(gpu.Sim, storage=storage)
+    ref, rsol = _odd_falling(SimS, gpu.RigidSphere)
+    want = []
+    for t in range(6):
+        scenes.substep(ref, rsol)
+        want.append(ref.packVolume().copy())
+    assert any((w[1::2] == 255).any() for w in want)  # SOLID cells in the frames
+    dref, dsol = _odd_falling(SimS, gpu.RigidSphere)  # the device-resident loop, one step per call
+    want_dev = []
+    for t in range(6):
+        dref.run_coupled(dsol, 1)
+        want_dev.append(dref.packVolume().copy())
+    dref.close()
+    shapes = SHAPES if storage != "f64" else ((4, 32), (2, 5), (8, 16))
+    for rows, zchunk in shapes:
+        sim, sol = _odd_falling(SimS, gpu.RigidSphere)
+        _set_shape(sim, rows, zchunk)
+        bufs = [sim.frameBuffer(), sim.frameBuffer()]
+        for t in range(6):
+            out = bufs[t % 2]
+            sim.waitFrames()
+            sim.stepFrame(sol, out)
+            sol.absorbDeadCells(sim)
+            sol.step(1.0, sim.gravity)
+            sim.waitFrames()
+            assert np.array_equal(out, want[t]), (storage, hex(rows), zchunk, t)
+        for k in ("phi", "rho", "f", "h", "tag"):
+            assert np.array_equal(np.asarray(getattr(sim, k)), np.asarray(getattr(ref, k))), (storage, hex(rows), k)
+        sim.close()
+        # the device-resident loop with frames every 2 steps
+        sim, sol = _odd_falling(SimS, gpu.RigidSphere)
+        _set_shape(sim, rows, zchunk)
+        frames = sim.run_coupled(sol, 6, frame_every=2)
+        for j in range(3):
+            assert np.array_equal(frames[j], want_dev[2 * j + 1]), (storage, hex(rows), "run_coupled", j)
+        sim.close()
+    ref.close()
