@@ -470,7 +470,10 @@ void free_all(lbm_sim *h) {
   if (h->hOut) cudaFreeHost(h->hOut);
   if (h->hTotals) cudaFreeHost(h->hTotals);
   if (h->copyStream) cudaStreamSynchronize(h->copyStream);
-  if (h->frameDev) cudaFreeAsync(h->frameDev, h->stream);
+  for (int b = 0; b < 2; b++) {
+    if (h->frameDev[b]) cudaFreeAsync(h->frameDev[b], h->stream);
+    if (h->evFrame[b]) cudaEventDestroy(h->evFrame[b]);
+  }
   if (h->evPacked) cudaEventDestroy(h->evPacked);
   if (h->evCopied) cudaEventDestroy(h->evCopied);
   if (h->copyStream) cudaStreamDestroy(h->copyStream);
@@ -607,15 +610,37 @@ int coupled_finish(lbm_sim *h, lbm_sphere *sp, int ns) {
   return LBM_OK;
 }
 
-// the copy stream, its two events and the device frame of the asynchronous
-// frame path, created on first use
-int ensure_frame_stream(lbm_sim *h) {
+// the copy stream, its events and the two device frames of the asynchronous
+// frame path, created on first use; *buf receives the frame to pack into, and
+// the handle's stream waits until that frame's previous copy is done
+int next_frame(lbm_sim *h, uint8_t **buf, int *slot) {
   if (!h->copyStream) {
     CK(cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&h->evPacked, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->evCopied, cudaEventDisableTiming));
   }
-  if (!h->frameDev) DALLOC(h->frameDev, (size_t)h->n * 2);
+  const int b = h->frameNext;
+  if (!h->frameDev[b]) {
+    DALLOC(h->frameDev[b], (size_t)h->n * 2);
+    CK(cudaEventCreateWithFlags(&h->evFrame[b], cudaEventDisableTiming));
+  }
+  if (h->framePending[b]) CK(cudaStreamWaitEvent(h->stream, h->evFrame[b], 0));
+  *buf = (uint8_t *)h->frameDev[b];
+  *slot = b;
+  return LBM_OK;
+}
+
+// copy the frame packed into buffer `slot` (on the handle's stream) to host
+// memory on the copy stream
+int issue_frame_copy(lbm_sim *h, int slot, uint8_t *host) {
+  CK(cudaEventRecord(h->evPacked, h->stream));
+  CK(cudaStreamWaitEvent(h->copyStream, h->evPacked, 0));
+  CK(copy_async(h, host, h->frameDev[slot], (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->copyStream));
+  CK(cudaEventRecord(h->evFrame[slot], h->copyStream));
+  CK(cudaEventRecord(h->evCopied, h->copyStream));
+  h->framePending[slot] = true;
+  h->copyPending = true;
+  h->frameNext = 1 - slot;
   return LBM_OK;
 }
 
@@ -1221,24 +1246,22 @@ int lbm_step_frame(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out, u
     return rc ? rc : lbm_pack_volume_async(h, host_frame);
   }
   DeviceGuard g(h->device);
-  int rc = ensure_frame_stream(h);
+  int rc = lbm_step_begin(h, sp, ns);
   if (rc) return rc;
-  if ((rc = lbm_step_begin(h, sp, ns))) return rc;
-  // the device frame is reused: the previous copy out of it must be done
-  // before the fused kernel writes it
-  if (h->copyPending) CK(cudaStreamWaitEvent(h->stream, h->evCopied, 0));
-  h->fusePack = (uint8_t *)h->frameDev;
+  uint8_t *buf = nullptr;
+  int slot = 0;
+  if ((rc = next_frame(h, &buf, &slot))) {
+    h->stepBegunNs = -1;
+    return rc;
+  }
+  h->fusePack = buf;
   rc = lbm_step_end(h, sp, ns, out);
   h->fusePack = nullptr;
   if (rc && rc != LBM_ERR_NAN) return rc;
   const int stepRc = rc;
-  h->ops->pack_end_planes(h, (uint8_t *)h->frameDev);
+  h->ops->pack_end_planes(h, buf);
   CKL("packVolume (end planes)");
-  CK(cudaEventRecord(h->evPacked, h->stream));
-  CK(cudaStreamWaitEvent(h->copyStream, h->evPacked, 0));
-  CK(copy_async(h, host_frame, h->frameDev, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->copyStream));
-  CK(cudaEventRecord(h->evCopied, h->copyStream));
-  h->copyPending = true;
+  if ((rc = issue_frame_copy(h, slot, host_frame))) return rc;
   return stepRc;
 }
 
@@ -1325,18 +1348,13 @@ int lbm_host_free(void *p) {
 int lbm_pack_volume_async(lbm_sim *h, uint8_t *host_out) {
   if (!h || !host_out) return fail(h, LBM_ERR_ARG, "null");
   DeviceGuard g(h->device);
-  int rc = ensure_frame_stream(h);
+  uint8_t *buf = nullptr;
+  int slot = 0;
+  int rc = next_frame(h, &buf, &slot);
   if (rc) return rc;
-  // the device frame is reused: the previous copy out of it must be done
-  if (h->copyPending) CK(cudaStreamWaitEvent(h->stream, h->evCopied, 0));
-  h->ops->pack(h, (uint8_t *)h->frameDev);
+  h->ops->pack(h, buf);
   CKL("packVolume");
-  CK(cudaEventRecord(h->evPacked, h->stream));
-  CK(cudaStreamWaitEvent(h->copyStream, h->evPacked, 0));
-  CK(copy_async(h, host_out, h->frameDev, (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->copyStream));
-  CK(cudaEventRecord(h->evCopied, h->copyStream));
-  h->copyPending = true;
-  return LBM_OK;
+  return issue_frame_copy(h, slot, host_out);
 }
 
 int lbm_pack_volume(lbm_sim *h, uint8_t *host_out) {
@@ -1418,6 +1436,7 @@ int lbm_wait_frames(lbm_sim *h) {
   if (h->copyPending) {
     CK(cudaEventSynchronize(h->evCopied));
     h->copyPending = false;
+    h->framePending[0] = h->framePending[1] = false;
   }
   return LBM_OK;
 }

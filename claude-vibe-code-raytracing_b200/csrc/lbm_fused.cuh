@@ -452,7 +452,7 @@ __device__ __forceinline__ void collide_cell(const CollK<typename Prec<PopT>::Re
 // One tile (bx, by) of 32 x TY columns over z-chunk bz of one scene.
 // WIDE: 64-bit population offsets, for grids whose populations exceed 2^31
 // elements (more than ~76 M cells); 32-bit offsets otherwise.
-template <class PopT, int TY, bool STG, bool WIDE>
+template <class PopT, int TY, bool STG, bool WIDE, bool PACK = false>
 __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int by, int bz) {
   using POff = std::conditional_t<WIDE, long long, int>;
   using Real = typename Prec<PopT>::Real;
@@ -817,7 +817,7 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
       st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
       st_at(s.uz[nxt], i, nCell, 12, ldg_at(uzC, i, nCell, 12));
-      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
+      if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
     } else if (tagI == TAG_FLUID) {
       // ring bases: group e_z sources come from plane z - e_z; the cell's own
       // (bounce-back) values are in plane z
@@ -954,8 +954,8 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       st_at(s.ux[nxt], i, nCell, 18, uxn);
       st_at(s.uy[nxt], i, nCell, 18, uyn);
       st_at(s.uz[nxt], i, nCell, 18, uzn);
-      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
-    } else if (a.pack && !haloWarp && x < nx && y < ny && z >= zb) {
+      if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
+    } else if (PACK && !haloWarp && x < nx && y < ny && z >= zb) {
       // a wall cell of this tile: not updated, packed from the half that is
       // current after the step
       if (lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(s.phi[nxt], i, nCell, 12), false);
@@ -981,10 +981,12 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
 }
 
 // One scene: the grid is its tiles.
-template <class PopT, int TY, bool STG, bool WIDE>
+// PACK: the instance launched on frame steps, which also writes the RG8
+// volume; the other steps run an instance without that code
+template <class PopT, int TY, bool STG, bool WIDE, bool PACK = false>
 __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks)
     k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
-  fused_tile<PopT, TY, STG, WIDE>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fused_tile<PopT, TY, STG, WIDE, PACK>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many scenes in one persistent launch: tile w of the batch belongs to the

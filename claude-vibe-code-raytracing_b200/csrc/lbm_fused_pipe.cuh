@@ -124,7 +124,7 @@ struct PipeSmem {
 };
 
 // ---------------------------------------------------------------- the tile
-template <class PopT, int TY, int PF, bool WIDE>
+template <class PopT, int TY, int PF, bool WIDE, bool PACK = false>
 __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx, int by, int bz) {
   using POff = std::conditional_t<WIDE, long long, int>;
   using Real = typename Prec<PopT>::Real;
@@ -603,7 +603,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
       st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
       st_at(s.uz[nxt], i, nCell, 12, ldg_at(uzC, i, nCell, 12));
-      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
+      if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
     } else if (tagI == TAG_FLUID) {
       // ring copies: group e_z sources come from plane z - e_z; the cell's own
       // (bounce-back) values are in plane z
@@ -740,8 +740,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       st_at(s.ux[nxt], i, nCell, 18, uxn);
       st_at(s.uy[nxt], i, nCell, 18, uyn);
       st_at(s.uz[nxt], i, nCell, 18, uzn);
-      if (a.pack && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
-    } else if (a.pack && cellWarp && x < nx && y < ny && z >= zb) {
+      if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
+    } else if (PACK && cellWarp && x < nx && y < ny && z >= zb) {
       // a wall cell of this tile: not updated, packed from the half that is
       // current after the step
       if (lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(s.phi[nxt], i, nCell, 12), false);
@@ -773,10 +773,10 @@ struct PipeOcc {
   static constexpr int blocks = TY <= 4 ? 3 : 2;
 };
 
-template <class PopT, int TY, int PF, bool WIDE>
+template <class PopT, int TY, int PF, bool WIDE, bool PACK = false>
 __global__ void __launch_bounds__(32 * (TY + 2), PipeOcc<TY, PF>::blocks)
     k_fused_pipe(const __grid_constant__ FusedArgs<PopT> a) {
-  fused_tile_pipe<PopT, TY, PF, WIDE>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fused_tile_pipe<PopT, TY, PF, WIDE, PACK>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many scenes in one persistent launch (as k_fused_batch)

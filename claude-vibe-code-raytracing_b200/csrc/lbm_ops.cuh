@@ -244,10 +244,10 @@ class Ops final : public OpsBase {
     if constexpr (FORM == 0) return FusedSmem<PopT, TY, false>::warps;
     else return PipeSmem<PopT, TY, FORM>::warps;
   }
-  template <int TY, int FORM, bool WIDE>
+  template <int TY, int FORM, bool WIDE, bool PACK = false>
   static auto step_kernel() {
-    if constexpr (FORM == 0) return k_fused_step<PopT, TY, false, WIDE>;
-    else return k_fused_pipe<PopT, TY, FORM, WIDE>;
+    if constexpr (FORM == 0) return k_fused_step<PopT, TY, false, WIDE, PACK>;
+    else return k_fused_pipe<PopT, TY, FORM, WIDE, PACK>;
   }
   template <int TY, int FORM, bool WIDE>
   static auto batch_kernel() {
@@ -257,8 +257,13 @@ class Ops final : public OpsBase {
 
   template <int TY, int STG, bool WIDE>
   void launch_fused(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
+    if (a.pack) launch_fused_as<TY, STG, WIDE, true>(h, a, zchunk);
+    else launch_fused_as<TY, STG, WIDE, false>(h, a, zchunk);
+  }
+  template <int TY, int STG, bool WIDE, bool PACK>
+  void launch_fused_as(lbm_sim *h, const FusedArgs<PopT> &a, int zchunk) {
     constexpr size_t smem = smem_of<TY, STG>();
-    const auto kern = step_kernel<TY, STG, WIDE>();
+    const auto kern = step_kernel<TY, STG, WIDE, PACK>();
     // the shared-memory opt-in is per device
     static unsigned long long attrSet = 0;
     const unsigned long long bit = 1ull << (h->device & 63);
@@ -323,6 +328,8 @@ class Ops final : public OpsBase {
         constexpr bool WIDE = decltype(W)::value;
         batch_ctas<TY, FORM, WIDE>(device);
         cudaFuncSetAttribute(step_kernel<TY, FORM, WIDE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_of<TY, FORM>());
+        cudaFuncSetAttribute(step_kernel<TY, FORM, WIDE, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_of<TY, FORM>());
       });
     }

@@ -138,10 +138,14 @@ struct lbm_sim {
   void *staging = nullptr;
   size_t stagingBytes = 0;
   void *image = nullptr;  // rendered RGBA8 frame (lbm_render)
-  // lbm_pack_volume_async: packed frame on the device, copied to the host on
-  // copyStream; evPacked orders the copy after the pack, evCopied the next
-  // pack after the copy
-  void *frameDev = nullptr;
+  // lbm_pack_volume_async / lbm_step_frame: packed frames on the device, two
+  // used in turn, each copied to the host on copyStream; evPacked orders a
+  // copy after its pack, evFrame[b] the next pack into buffer b after b's
+  // copy, evCopied marks the last copy issued
+  void *frameDev[2] = {nullptr, nullptr};
+  cudaEvent_t evFrame[2] = {nullptr, nullptr};
+  bool framePending[2] = {false, false};
+  int frameNext = 0;
   cudaStream_t copyStream = nullptr;
   cudaEvent_t evPacked = nullptr, evCopied = nullptr;
   bool copyPending = false;
