@@ -249,9 +249,9 @@ int reduce_impulses(lbm_sim *h, double *d_out) {
   int ns = h->hPlan.ss.nsph;
   if (ns == 0) return LBM_OK;
   dim3 g1(h->partialsChunks, ns);
-  k_impulse_reduce1<<<g1, 256, 0, h->stream>>>(&h->dPlan->ss, h->partials, h->partialsChunks);
-  k_impulse_reduce2<<<ns, 32, 0, h->stream>>>(&h->dPlan->ss, h->partials, h->partialsChunks, d_out);
-  h->launches += 2;
+  k_impulse_reduce<<<g1, RED_THREADS, 0, h->stream>>>(&h->dPlan->ss, h->partials, h->partialsChunks, d_out,
+                                                      h->redTickets);
+  h->launches++;
   CKL("impulse reduction");
   return LBM_OK;
 }
@@ -459,7 +459,7 @@ void free_all(lbm_sim *h) {
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
                   h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
                   h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan, h->dWatch, h->linkChunks,
-                  h->linkBuf};
+                  h->linkBuf, h->redTickets};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, h->stream);
   for (int c = 0; c < 2; c++)
@@ -525,6 +525,8 @@ int coupled_prepare(lbm_sim *h, const lbm_sphere *sp, int ns, bool frames, Coupl
     DALLOC(h->impAcc, need * sizeof(double));
     h->impCap = need;
   }
+  // the slots start at zero; every step's reduction zeroes the slots it reads
+  CK(cudaMemsetAsync(h->impAcc, 0, need * sizeof(double), h->stream));
   long long pneed = (long long)std::max(ns, 1) * c.redChunks * 6;
   if (pneed > h->partialsCap) {
     if (h->partials) {
@@ -560,12 +562,6 @@ int coupled_pre(lbm_sim *h, const CoupledCtx &c) {
   int rc = launch_compaction(h, c.maxChunks);
   if (rc) return rc;
   h->ops->fresh_fill(h);
-  if (c.ns > 0) {
-    // sized for the most slots the plan can use (small spheres need few CTAs)
-    const unsigned zc = std::min(nblocks((long long)c.ns * c.slotCells * 6, 256), SWEEP_CTAS);
-    k_zero_targets<<<zc, 256, 0, h->stream>>>(h->dPlan, h->impAcc);
-    h->launches++;
-  }
   CKL("coupled step (before the fused kernel)");
   return LBM_OK;
 }
@@ -575,11 +571,11 @@ int coupled_post(lbm_sim *h, const CoupledCtx &c) {
   if (c.ns > 0) {
     double *dFluid = h->dOut, *dDead = h->dOut + LBM_MAX_SPHERES * 6;
     dim3 g1(c.redChunks, c.ns);
-    k_impulse_reduce1<<<g1, 256, 0, h->stream>>>(&h->dPlan->ss, h->partials, c.redChunks);
-    k_impulse_reduce2<<<c.ns, 32, 0, h->stream>>>(&h->dPlan->ss, h->partials, c.redChunks, dFluid);
+    k_impulse_reduce<<<g1, RED_THREADS, 0, h->stream>>>(&h->dPlan->ss, h->partials, c.redChunks, dFluid,
+                                                        h->redTickets);
     h->ops->absorb_dead(h, dDead);
     h->ops->sphere_step_device(h, h->dSph, c.ns, h->params.gravity, dFluid, dDead);
-    h->launches += 2;
+    h->launches++;
   }
   CKL("coupled step (after the fused kernel)");
   return LBM_OK;
@@ -715,6 +711,8 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
     DALLOC(h->totals, 3 * sizeof(int));
     CK(cudaMemsetAsync(h->totals, 0, 3 * sizeof(int), h->stream));
     DALLOC(h->dOut, 2 * LBM_MAX_SPHERES * 6 * sizeof(double));
+    DALLOC(h->redTickets, LBM_MAX_SPHERES * sizeof(unsigned));
+    CK(cudaMemsetAsync(h->redTickets, 0, LBM_MAX_SPHERES * sizeof(unsigned), h->stream));
     DALLOC(h->dSph, LBM_MAX_SPHERES * sizeof(lbm_sphere));
     DALLOC(h->dPlan, sizeof(Plan));
     CK(cudaMemsetAsync(h->dPlan, 0, sizeof(Plan), h->stream));

@@ -781,60 +781,60 @@ static __global__ void __launch_bounds__(DEAD_THREADS)
   if (threadIdx.x < 6) out[6 * b + threadIdx.x] = sh[threadIdx.x][0];
 }
 
-// Deterministic two-level reduction of the per-cell impulse arrays:
-// level 1 sums fixed chunks of 1024 cells, level 2 sums the chunk partials in
-// index order.  Independent of how the stream kernel was tiled.
+// Deterministic reduction of the per-cell impulse arrays in one launch.
+// Block (c, b) sums chunk c (1024 cells) of sphere b's slots -- the threads
+// stride the chunk, then a shared-memory tree -- zeroes the slots it read (so
+// the next step starts from zero without a clearing launch) and stores its
+// partial; the block that takes the last ticket of sphere b adds the partials
+// in chunk order and resets the ticket.  Which block finishes last does not
+// change the result, nor does how the stream kernel was tiled.
 constexpr int RED_CHUNK = 1024;
+constexpr int RED_THREADS = 256;
 
-static __global__ void k_impulse_reduce1(const SolidSet *__restrict__ ssp, double *partials, int maxChunks) {
+static __global__ void __launch_bounds__(RED_THREADS)
+    k_impulse_reduce(const SolidSet *__restrict__ ssp, double *partials, int maxChunks, double *out,
+                     unsigned *tickets) {
   const SolidSet &ss = *ssp;
-  int b = blockIdx.y;
+  const int b = blockIdx.y;
   if (b >= ss.nsph) return;
   const ImpulseTarget &t = ss.imp[b];
-  long long cells = (long long)t.dim[0] * t.dim[1] * t.dim[2];
-  long long c0 = (long long)blockIdx.x * RED_CHUNK;
-  __shared__ double sh[6][256];
+  const long long cells = (long long)t.dim[0] * t.dim[1] * t.dim[2];
+  int nch = (int)((cells + RED_CHUNK - 1) / RED_CHUNK);
+  if (nch < 1) nch = 1;  // an empty box still gives its zero
+  if (nch > maxChunks) nch = maxChunks;
+  if ((int)blockIdx.x >= nch) return;
+  const long long c0 = (long long)blockIdx.x * RED_CHUNK;
+  __shared__ double sh[6][RED_THREADS];
+  __shared__ bool last;
   double a[6] = {0, 0, 0, 0, 0, 0};
-  if (c0 < cells) {
-    for (int j = threadIdx.x; j < RED_CHUNK; j += blockDim.x) {
-      long long c = c0 + j;
-      if (c >= cells) break;
-      const double *p = t.acc + 6 * c;
-      for (int q = 0; q < 6; q++) a[q] = __dadd_rn(a[q], p[q]);
-    }
+  for (int j = threadIdx.x; j < RED_CHUNK; j += RED_THREADS) {
+    const long long c = c0 + j;
+    if (c >= cells) break;
+    double *p = t.acc + 6 * c;
+    for (int q = 0; q < 6; q++) a[q] = __dadd_rn(a[q], p[q]);
+    for (int q = 0; q < 6; q++) p[q] = 0.0;
   }
   for (int q = 0; q < 6; q++) sh[q][threadIdx.x] = a[q];
   __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+  for (int st = RED_THREADS / 2; st > 0; st >>= 1) {
     if ((int)threadIdx.x < st)
       for (int q = 0; q < 6; q++) sh[q][threadIdx.x] = __dadd_rn(sh[q][threadIdx.x], sh[q][threadIdx.x + st]);
     __syncthreads();
   }
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
     for (int q = 0; q < 6; q++) partials[((long long)b * maxChunks + blockIdx.x) * 6 + q] = sh[q][0];
-}
-
-static __global__ void k_impulse_reduce2(const SolidSet *__restrict__ ssp, const double *partials, int maxChunks,
-                                         double *out) {
-  const SolidSet &ss = *ssp;
-  int b = blockIdx.x;
-  if (b >= ss.nsph) return;
-  const ImpulseTarget &t = ss.imp[b];
-  long long cells = (long long)t.dim[0] * t.dim[1] * t.dim[2];
-  int nch = (int)((cells + RED_CHUNK - 1) / RED_CHUNK);
-  if (threadIdx.x < 6) {
-    double a = 0;
-    for (int c = 0; c < nch; c++) a = __dadd_rn(a, partials[((long long)b * maxChunks + c) * 6 + threadIdx.x]);
-    out[6 * b + threadIdx.x] = a;
+    __threadfence();
+    last = atomicAdd(&tickets[b], 1u) == (unsigned)nch - 1;
   }
-}
-
-// Clear the per-cell impulse slots the plan uses.
-static __global__ void k_zero_targets(const Plan *__restrict__ P, double *base) {
-  long long n = P->impDoubles;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    base[i] = 0.0;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < 6) {
+    double s = 0;
+    for (int c = 0; c < nch; c++) s = __dadd_rn(s, __ldcg(&partials[((long long)b * maxChunks + c) * 6 + threadIdx.x]));
+    out[6 * b + threadIdx.x] = s;
+  }
+  if (threadIdx.x == 0) tickets[b] = 0;
 }
 
 // Device-side plan for the device-resident loop: sphere descriptors from the

@@ -128,6 +128,7 @@ struct lbm_sim {
   double *impAcc = nullptr;  // per-cell impulse slots of every sphere
   long long impCap = 0;      // doubles
   double *partials = nullptr;
+  unsigned *redTickets = nullptr;  // [LBM_MAX_SPHERES] last-block tickets of the impulse reduction
   long long partialsCap = 0;  // doubles
   int partialsChunks = 0;
   double *dOut = nullptr;      // device [2][MAX][6]: fluid impulses, dead impulses
