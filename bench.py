@@ -715,7 +715,7 @@ def main():
     for s in range(e2e_steps):
         if (s + 1) % substeps == 0:
             if nframe >= 2:
-                sim.waitFrames()  # the consumer has taken frames[nframe % 2] by now
+                sim.waitFrameSlot()  # frames[nframe % 2] (two frames back) has landed: the consumer takes it
             sim.stepFrame(sol, frames[nframe % 2])
             nframe += 1
         else:

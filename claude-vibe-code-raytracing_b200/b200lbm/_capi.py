@@ -93,6 +93,7 @@ _SIGS = [
     ("lbm_step_begin", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int]),
     ("lbm_step_end", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
     ("lbm_step_frame", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse), C.c_void_p]),
+    ("lbm_wait_frame_slot", C.c_int, [C.c_void_p]),
     ("lbm_absorb_dead_cells", C.c_int,
      [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
     ("lbm_pack_volume", C.c_int, [C.c_void_p, C.c_void_p]),

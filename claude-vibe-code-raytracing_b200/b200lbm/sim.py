@@ -488,6 +488,12 @@ class Sim:
         """Wait until every packVolumeAsync copy has reached its buffer."""
         check(self._h, lib().lbm_wait_frames(self._h))
 
+    def waitFrameSlot(self):
+        """Wait only for the older of the two frames in flight: with two
+        frame buffers used in turn, the one the next stepFrame /
+        packVolumeAsync will fill holds its frame after this call."""
+        check(self._h, lib().lbm_wait_frame_slot(self._h))
+
     def frameBuffer(self):
         """A page-locked uint8 buffer of 2*n bytes for packVolume: the
         device-to-host copy of each frame then runs at full link speed (a

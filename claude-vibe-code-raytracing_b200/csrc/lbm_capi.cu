@@ -1439,6 +1439,17 @@ int lbm_wait_frames(lbm_sim *h) {
   return LBM_OK;
 }
 
+int lbm_wait_frame_slot(lbm_sim *h) {
+  if (!h) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  const int b = h->frameNext;
+  if (h->framePending[b]) {
+    CK(cudaEventSynchronize(h->evFrame[b]));
+    h->framePending[b] = false;
+  }
+  return LBM_OK;
+}
+
 int lbm_synchronize(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);
@@ -1630,6 +1641,8 @@ struct lbm_batch {
   std::vector<cudaEvent_t> joins;
   void *dArgs = nullptr;  // [2][n] descriptors (FusedArgs of the storage type)
   size_t argsCap = 0;
+  void *dSmall = nullptr;  // [2][n] arguments of the batched sparse kernels
+  size_t smallCap = 0;
   int *dTileStart = nullptr;  // [n + 1]
   int3 *dTileGrid = nullptr;  // [n]
   int tilesCap = 0;
@@ -1760,6 +1773,7 @@ int lbm_batch_destroy(lbm_batch *b) {
   DeviceGuard g(b->device);
   if (b->origin) cudaStreamSynchronize(b->origin);
   if (b->dArgs) cudaFreeAsync(b->dArgs, b->origin);
+  if (b->dSmall) cudaFreeAsync(b->dSmall, b->origin);
   if (b->dTileStart) cudaFreeAsync(b->dTileStart, b->origin);
   if (b->dTileGrid) cudaFreeAsync(b->dTileGrid, b->origin);
   if (b->origin) cudaStreamSynchronize(b->origin);
@@ -1828,6 +1842,30 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
                                      ctx[s]));
   int rc = batch_tables(b);
   if (rc) return rc;
+  // the sparse kernels' arguments of every scene for both parities, and the
+  // batched launches' grids (sized for the largest scene's plan bounds)
+  const size_t sb = ops->small_args_bytes();
+  std::vector<unsigned char> small(2 * (size_t)n * sb);
+  unsigned retagCtas = 1, compactCtas = 1;
+  int redX = 1, nsMax = 0;
+  for (int s = 0; s < n; s++) {
+    lbm_sim *h = b->sims[s];
+    for (int p = 0; p < 2; p++)
+      ops->small_args(h, h->cur ^ p, ctx[s].ns, ctx[s].slotCells, ctx[s].maxU, ctx[s].redChunks,
+                      &small[((size_t)p * n + s) * sb]);
+    retagCtas = std::max(retagCtas, std::min(nblocks(std::max(1LL, ctx[s].maxU), 256), SWEEP_CTAS));
+    compactCtas = std::max(compactCtas, (unsigned)std::min<long long>(std::max(1LL, ctx[s].maxChunks), SWEEP_CTAS));
+    redX = std::max(redX, ctx[s].redChunks);
+    nsMax = std::max(nsMax, ctx[s].ns);
+  }
+  if (small.size() > b->smallCap) {
+    if (b->dSmall) cudaFreeAsync(b->dSmall, b->origin);
+    b->dSmall = nullptr;
+    BCK(cudaMallocAsync(&b->dSmall, small.size(), b->origin));
+    b->smallCap = small.size();
+  }
+  BCK(cudaMemcpyAsync(b->dSmall, small.data(), small.size(), cudaMemcpyHostToDevice, b->origin));
+  BCK(cudaStreamSynchronize(b->origin));  // the host vector goes out of scope
   const int tiles = batch_tiles(b);
   const int ctas = std::min(tiles, ops->fused_batch_ctas(launch_shape(b, b->rows), b->device));
   const size_t ab = ops->fused_args_bytes();
@@ -1847,28 +1885,18 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
     b->pinnedCap = cap;
   }
 
-  // one coupled step of every scene: per-scene branches around the shared fused launch
+  // one coupled step of every scene: each kind of sparse kernel once for all
+  // scenes, around the shared fused launch, all on the batch's stream
   auto emit_step = [&](int parity) -> int {
-    BCK(cudaEventRecord(b->fork, b->origin));
-    for (int s = 0; s < n; s++) {
-      lbm_sim *h = b->sims[s];
-      BCK(cudaStreamWaitEvent(h->stream, b->fork, 0));
-      BSIM(h, coupled_pre(h, ctx[s]));
-      BCK(cudaEventRecord(b->joins[s], h->stream));
-      BCK(cudaStreamWaitEvent(b->origin, b->joins[s], 0));
-    }
+    const void *A = (const unsigned char *)b->dSmall + (size_t)parity * n * sb;
+    ops->batch_pre(A, n, retagCtas, compactCtas, b->origin);
+    BCK(cudaGetLastError());
     ops->fused_batch((const unsigned char *)b->dArgs + (size_t)parity * n * ab, b->dTileStart, b->dTileGrid,
                      n, launch_shape(b, b->rows), ctas, b->origin);
     BCK(cudaGetLastError());
-    BCK(cudaEventRecord(b->fork, b->origin));
-    for (int s = 0; s < n; s++) {
-      lbm_sim *h = b->sims[s];
-      BCK(cudaStreamWaitEvent(h->stream, b->fork, 0));
-      BSIM(h, coupled_post(h, ctx[s]));
-      h->cur = 1 - h->cur;
-      BCK(cudaEventRecord(b->joins[s], h->stream));
-      BCK(cudaStreamWaitEvent(b->origin, b->joins[s], 0));
-    }
+    ops->batch_post(A, n, redX, nsMax, b->origin);
+    BCK(cudaGetLastError());
+    for (int s = 0; s < n; s++) b->sims[s]->cur ^= 1;
     return LBM_OK;
   };
   // RG8 volume of every scene into frames[s][idx]
@@ -1892,7 +1920,8 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
   // the captured 2-step graph, reused while nothing it baked in has changed
   if (graph) {
     std::vector<long long> key = {b->rows, b->zchunk, (long long)(uintptr_t)b->dArgs,
-                                  (long long)(uintptr_t)b->dTileStart, ctas};
+                                  (long long)(uintptr_t)b->dTileStart, ctas, (long long)(uintptr_t)b->dSmall,
+                                  retagCtas, compactCtas, redX, nsMax};
     for (int s = 0; s < n; s++) {
       lbm_sim *h = b->sims[s];
       const long long v[] = {(long long)(uintptr_t)h,           h->cur,      ctx[s].ns,

@@ -368,16 +368,18 @@ __global__ void k_stream_hydro_macro(Scene<PopT, typename Prec<PopT>::Real> s, i
 
 // retag on a box (the union of the current and the two previous sphere boxes):
 // every cell outside it keeps tag == tagPrev, so only the box changes.
+// (the bodies of the sparse kernels take their block index and grid size, so
+// that a batched launch can run them for many scenes, one grid row each)
 template <class PopT>
-__global__ void k_retag_box(Scene<PopT, typename Prec<PopT>::Real> s, const Plan *__restrict__ P) {
+__device__ __forceinline__ void retag_box_body(const Scene<PopT, typename Prec<PopT>::Real> &s,
+                                               const Plan *__restrict__ P, unsigned bid, unsigned gdim) {
   const SolidSet &ss = P->ss;
   const Box bx = P->U;
   const int dx = bx.hi[0] - bx.lo[0] + 1, dy = bx.hi[1] - bx.lo[1] + 1, dz = bx.hi[2] - bx.lo[2] + 1;
   const long long total = (long long)dx * dy * dz;
   // grid-stride over the box the plan holds (launches are sized for the
   // largest box the step may plan, which can be far larger)
-  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < total;
-       l += (long long)gridDim.x * blockDim.x) {
+  for (long long l = bid * (long long)blockDim.x + threadIdx.x; l < total; l += (long long)gdim * blockDim.x) {
     const int x = bx.lo[0] + (int)(l % dx);
     const int y = bx.lo[1] + (int)((l / dx) % dy);
     const int z = bx.lo[2] + (int)(l / ((long long)dx * dy));
@@ -388,6 +390,10 @@ __global__ void k_retag_box(Scene<PopT, typename Prec<PopT>::Real> s, const Plan
     else
       s.tag[i] = owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) >= 0 ? TAG_SOLID : TAG_FLUID;
   }
+}
+template <class PopT>
+__global__ void k_retag_box(Scene<PopT, typename Prec<PopT>::Real> s, const Plan *__restrict__ P) {
+  retag_box_body<PopT>(s, P, blockIdx.x, gridDim.x);
 }
 
 // Count fresh (FLUID, was SOLID) and dead (SOLID, was FLUID) cells per chunk
@@ -406,14 +412,15 @@ __device__ __forceinline__ void box_cell(const Box &bx, long long l, int &x, int
   z = bx.lo[2] + (int)(l / ((long long)dx * dy));
 }
 
-static __global__ void k_compact_count(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
-                                       const Plan *__restrict__ P, int2 *counts) {
+__device__ __forceinline__ void compact_count_body(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
+                                                   const Plan *__restrict__ P, int2 *counts, unsigned bid,
+                                                   unsigned gdim) {
   __shared__ int sf[COMPACT_THREADS / 32], sd[COMPACT_THREADS / 32];
   const Box bx = P->U;
   const long long total = P->ucells;
   const int nchunks = P->nchunks;
   // CTAs stride over the chunks (block-uniform trip count)
-  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+  for (int c = bid; c < nchunks; c += gdim) {
     const long long base = (long long)c * COMPACT_CHUNK;
     int nf = 0, nd = 0;
     for (int j = threadIdx.x; j < COMPACT_CHUNK; j += blockDim.x) {
@@ -446,9 +453,13 @@ static __global__ void k_compact_count(const uint8_t *tag, const uint8_t *tagPre
     __syncthreads();  // sf / sd are rewritten for the next chunk
   }
 }
+static __global__ void k_compact_count(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
+                                       const Plan *__restrict__ P, int2 *counts) {
+  compact_count_body(tag, tagPrev, nx, ny, P, counts, blockIdx.x, gridDim.x);
+}
 
 // Exclusive scan of the per-chunk counts (single CTA, sequential per thread).
-static __global__ void k_compact_scan(int2 *counts, const Plan *__restrict__ P, int *totals) {
+__device__ __forceinline__ void compact_scan_body(int2 *counts, const Plan *__restrict__ P, int *totals) {
   __shared__ int2 part[1024];
   const int nchunks = P->nchunks;
   int per = (nchunks + blockDim.x - 1) / blockDim.x;
@@ -480,11 +491,14 @@ static __global__ void k_compact_scan(int2 *counts, const Plan *__restrict__ P, 
     run.y += v.y;
   }
 }
+static __global__ void k_compact_scan(int2 *counts, const Plan *__restrict__ P, int *totals) {
+  compact_scan_body(counts, P, totals);
+}
 
 // Emit the fresh / dead cell indices in scan order.
-static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
-                                      const Plan *__restrict__ P, const int2 *offsets, int *fresh,
-                                      int *dead, int cap) {
+__device__ __forceinline__ void compact_emit_body(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
+                                                  const Plan *__restrict__ P, const int2 *offsets, int *fresh,
+                                                  int *dead, int cap, unsigned bid, unsigned gdim) {
   __shared__ int wf[COMPACT_THREADS / 32], wd[COMPACT_THREADS / 32];
   __shared__ int runF, runD;
   const Box bx = P->U;
@@ -493,7 +507,7 @@ static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // CTAs stride over the chunks (block-uniform trip count); the inner loop
   // ends on a barrier, so runF / runD are free to be reset for the next chunk
-  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+  for (int c = bid; c < nchunks; c += gdim) {
     const long long base = (long long)c * COMPACT_CHUNK;
     if (threadIdx.x == 0) {
       runF = offsets[c].x;
@@ -546,15 +560,21 @@ static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev
     }
   }
 }
+static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev, int nx, int ny,
+                                      const Plan *__restrict__ P, const int2 *offsets, int *fresh,
+                                      int *dead, int cap) {
+  compact_emit_body(tag, tagPrev, nx, ny, P, offsets, fresh, dead, cap, blockIdx.x, gridDim.x);
+}
 
 // handleFreshCells (src/sim.js:257-310) over the scan-ordered fresh list, one
 // thread, FP64 arithmetic, in place -- later fresh cells see the values written
 // for earlier ones exactly as in the reference's single sweep.
 template <class PopT>
-__global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *fresh,
-                             const int *totals, int cap, double rhoL, double rhoG, int zlo, int zend) {
+__device__ __forceinline__ void fresh_fill_body(const Scene<PopT, typename Prec<PopT>::Real> &s, int cur,
+                                                const int *fresh, const int *totals, int cap, double rhoL,
+                                                double rhoG, int zlo, int zend) {
   using Real = typename Prec<PopT>::Real;
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (threadIdx.x != 0) return;
   int nf = totals[0];
   if (nf > cap) nf = cap;
   const int nx = s.nx, ny = s.ny;
@@ -608,6 +628,12 @@ __global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, 
       s.H[cur][pidx<7>(k, i)] = Codec<PopT>::enc((Real)hk, (Real)w7_of(k) * pR);
     }
   }
+}
+template <class PopT>
+__global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *fresh,
+                             const int *totals, int cap, double rhoL, double rhoG, int zlo, int zend) {
+  if (blockIdx.x != 0) return;
+  fresh_fill_body<PopT>(s, cur, fresh, totals, cap, rhoL, rhoG, zlo, zend);
 }
 
 // absorbDeadCells (src/solid.js:87-101): impulse rho(phi)*u of every cell on
@@ -744,14 +770,14 @@ constexpr int DEAD_THREADS = 256;
 
 // (static: Real = float is instantiated by several translation units)
 template <class Real>
-static __global__ void __launch_bounds__(DEAD_THREADS)
-    k_absorb_dead(const Real *__restrict__ phi, const Real *__restrict__ ux,
-                  const Real *__restrict__ uy, const Real *__restrict__ uz, int nx, int ny,
-                  const int *__restrict__ dead, const int *__restrict__ totals, int cap, double rhoL,
-                  double rhoG, const SolidSet *__restrict__ ssp, double *out) {
+__device__ __forceinline__ void absorb_dead_body(const Real *__restrict__ phi, const Real *__restrict__ ux,
+                                                 const Real *__restrict__ uy, const Real *__restrict__ uz,
+                                                 int nx, int ny, const int *__restrict__ dead,
+                                                 const int *__restrict__ totals, int cap, double rhoL,
+                                                 double rhoG, const SolidSet *__restrict__ ssp, double *out,
+                                                 int b) {
   __shared__ double sh[6][DEAD_THREADS];
   const SolidSet &ss = *ssp;
-  const int b = blockIdx.x;
   if (b >= ss.nsph) return;
   int nd = totals[1];
   if (nd > cap) nd = cap;
@@ -780,6 +806,14 @@ static __global__ void __launch_bounds__(DEAD_THREADS)
   }
   if (threadIdx.x < 6) out[6 * b + threadIdx.x] = sh[threadIdx.x][0];
 }
+template <class Real>
+static __global__ void __launch_bounds__(DEAD_THREADS)
+    k_absorb_dead(const Real *__restrict__ phi, const Real *__restrict__ ux,
+                  const Real *__restrict__ uy, const Real *__restrict__ uz, int nx, int ny,
+                  const int *__restrict__ dead, const int *__restrict__ totals, int cap, double rhoL,
+                  double rhoG, const SolidSet *__restrict__ ssp, double *out) {
+  absorb_dead_body(phi, ux, uy, uz, nx, ny, dead, totals, cap, rhoL, rhoG, ssp, out, blockIdx.x);
+}
 
 // Deterministic reduction of the per-cell impulse arrays in one launch.
 // Block (c, b) sums chunk c (1024 cells) of sphere b's slots -- the threads
@@ -791,19 +825,18 @@ static __global__ void __launch_bounds__(DEAD_THREADS)
 constexpr int RED_CHUNK = 1024;
 constexpr int RED_THREADS = 256;
 
-static __global__ void __launch_bounds__(RED_THREADS)
-    k_impulse_reduce(const SolidSet *__restrict__ ssp, double *partials, int maxChunks, double *out,
-                     unsigned *tickets) {
+__device__ __forceinline__ void impulse_reduce_body(const SolidSet *__restrict__ ssp, double *partials,
+                                                    int maxChunks, double *out, unsigned *tickets, int cx,
+                                                    int b) {
   const SolidSet &ss = *ssp;
-  const int b = blockIdx.y;
   if (b >= ss.nsph) return;
   const ImpulseTarget &t = ss.imp[b];
   const long long cells = (long long)t.dim[0] * t.dim[1] * t.dim[2];
   int nch = (int)((cells + RED_CHUNK - 1) / RED_CHUNK);
   if (nch < 1) nch = 1;  // an empty box still gives its zero
   if (nch > maxChunks) nch = maxChunks;
-  if ((int)blockIdx.x >= nch) return;
-  const long long c0 = (long long)blockIdx.x * RED_CHUNK;
+  if (cx >= nch) return;
+  const long long c0 = (long long)cx * RED_CHUNK;
   __shared__ double sh[6][RED_THREADS];
   __shared__ bool last;
   double a[6] = {0, 0, 0, 0, 0, 0};
@@ -822,7 +855,7 @@ static __global__ void __launch_bounds__(RED_THREADS)
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    for (int q = 0; q < 6; q++) partials[((long long)b * maxChunks + blockIdx.x) * 6 + q] = sh[q][0];
+    for (int q = 0; q < 6; q++) partials[((long long)b * maxChunks + cx) * 6 + q] = sh[q][0];
     __threadfence();
     last = atomicAdd(&tickets[b], 1u) == (unsigned)nch - 1;
   }
@@ -836,13 +869,18 @@ static __global__ void __launch_bounds__(RED_THREADS)
   }
   if (threadIdx.x == 0) tickets[b] = 0;
 }
+static __global__ void __launch_bounds__(RED_THREADS)
+    k_impulse_reduce(const SolidSet *__restrict__ ssp, double *partials, int maxChunks, double *out,
+                     unsigned *tickets) {
+  impulse_reduce_body(ssp, partials, maxChunks, out, tickets, blockIdx.x, blockIdx.y);
+}
 
 // Device-side plan for the device-resident loop: sphere descriptors from the
 // device sphere state, the retag box (current and two previous sphere boxes),
 // compaction chunking, and impulse slots of slotCells cells per sphere.
-static __global__ void k_plan(Plan *P, const lbm_sphere *sph, int nsph, int nx, int ny, int nz,
-                              double *impBase, long long slotCells, long long maxUCells) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+__device__ __forceinline__ void plan_body(Plan *P, const lbm_sphere *sph, int nsph, int nx, int ny, int nz,
+                                          double *impBase, long long slotCells, long long maxUCells) {
+  if (threadIdx.x != 0) return;
   SolidSet &ss = P->ss;
   ss.nsph = nsph;
   Box now{{1, 1, 1}, {0, 0, 0}};
@@ -897,6 +935,11 @@ static __global__ void k_plan(Plan *P, const lbm_sphere *sph, int nsph, int nx, 
   P->impDoubles = (long long)nsph * slotCells * 6;
   P->boxLastLast = P->boxLast;
   P->boxLast = now;
+}
+static __global__ void k_plan(Plan *P, const lbm_sphere *sph, int nsph, int nx, int ny, int nz,
+                              double *impBase, long long slotCells, long long maxUCells) {
+  if (blockIdx.x != 0) return;
+  plan_body(P, sph, nsph, nx, ny, nz, impBase, slotCells, maxUCells);
 }
 
 // packVolume's two bytes of cell i (src/sim.js:586-600): R = clamp01(phi) *

@@ -67,10 +67,10 @@ __global__ void k_reencode_h(Scene<PopT, typename Prec<PopT>::Real> s, int half,
 // The device-resident loop's RigidSphere.step(1.0, gravity), one thread per
 // sphere: the momentum-exchange and dead-cell impulses of the step are added
 // first, as RigidSphere.applyImpulseAtCell would have.
-static __global__ void k_sphere_step(lbm_sphere *sph, int nsph, double gravity, const double *fluid,
-                                     const double *dead, int nx, int ny, int nz) {
+__device__ __forceinline__ void sphere_step_body(lbm_sphere *sph, int nsph, double gravity, const double *fluid,
+                                                 const double *dead, int nx, int ny, int nz) {
   int b = threadIdx.x;
-  if (blockIdx.x != 0 || b >= nsph) return;
+  if (b >= nsph) return;
   lbm_sphere s = sph[b];
   double *F[6] = {&s.Fx, &s.Fy, &s.Fz, &s.Tx, &s.Ty, &s.Tz};
   for (int j = 0; j < 6; j++) {
@@ -79,6 +79,83 @@ static __global__ void k_sphere_step(lbm_sphere *sph, int nsph, double gravity, 
   }
   sphere_step_fp64(s, 1.0, gravity, nx, ny, nz);
   sph[b] = s;
+}
+static __global__ void k_sphere_step(lbm_sphere *sph, int nsph, double gravity, const double *fluid,
+                                     const double *dead, int nx, int ny, int nz) {
+  if (blockIdx.x != 0) return;
+  sphere_step_body(sph, nsph, gravity, fluid, dead, nx, ny, nz);
+}
+
+// ---------------------------------------------------------------- batched sparse kernels
+// A batch runs every scene's sparse kernels of a step (plan, retag, fresh /
+// dead compaction, fresh fill; after the shared fused launch the impulse
+// reduction, the dead-cell impulses and the sphere step) as one launch per
+// kind: grid row (or plane) s runs scene s's kernel body on scene s's
+// arguments, so a step of n scenes costs 9 launches instead of 9 n.
+template <class PopT>
+struct SmallArgs {
+  Scene<PopT, typename Prec<PopT>::Real> s;
+  int cur, ns, listCap, redChunks, zlo, zend;
+  Plan *plan;
+  lbm_sphere *sph;
+  double *impAcc;
+  long long slotCells, maxU;
+  int2 *counts;
+  int *fresh, *dead, *totals;
+  double *partials, *dFluid, *dDead;
+  unsigned *tickets;
+  double rhoL, rhoG, gravity;
+};
+
+template <class PopT>
+__global__ void kb_plan(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.x];
+  plan_body(a.plan, a.sph, a.ns, a.s.nx, a.s.ny, a.s.nz, a.impAcc, a.slotCells, a.maxU);
+}
+template <class PopT>
+__global__ void kb_retag_box(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.y];
+  retag_box_body<PopT>(a.s, a.plan, blockIdx.x, gridDim.x);
+}
+template <class PopT>
+__global__ void kb_compact_count(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.y];
+  compact_count_body(a.s.tag, a.s.tagPrev, a.s.nx, a.s.ny, a.plan, a.counts, blockIdx.x, gridDim.x);
+}
+template <class PopT>
+__global__ void kb_compact_scan(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.x];
+  compact_scan_body(a.counts, a.plan, a.totals);
+}
+template <class PopT>
+__global__ void kb_compact_emit(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.y];
+  compact_emit_body(a.s.tag, a.s.tagPrev, a.s.nx, a.s.ny, a.plan, a.counts, a.fresh, a.dead, a.listCap,
+                    blockIdx.x, gridDim.x);
+}
+template <class PopT>
+__global__ void kb_fresh_fill(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.x];
+  fresh_fill_body<PopT>(a.s, a.cur, a.fresh, a.totals, a.listCap, a.rhoL, a.rhoG, a.zlo, a.zend);
+}
+template <class PopT>
+__global__ void __launch_bounds__(RED_THREADS) kb_impulse_reduce(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.z];
+  if (a.ns == 0) return;
+  impulse_reduce_body(&a.plan->ss, a.partials, a.redChunks, a.dFluid, a.tickets, blockIdx.x, blockIdx.y);
+}
+template <class PopT>
+__global__ void __launch_bounds__(DEAD_THREADS) kb_absorb_dead(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.y];
+  if (a.ns == 0) return;
+  absorb_dead_body(a.s.phi[a.cur], a.s.ux[a.cur], a.s.uy[a.cur], a.s.uz[a.cur], a.s.nx, a.s.ny, a.dead, a.totals,
+                   a.listCap, a.rhoL, a.rhoG, &a.plan->ss, a.dDead, blockIdx.x);
+}
+template <class PopT>
+__global__ void kb_sphere_step(const SmallArgs<PopT> *__restrict__ A) {
+  const SmallArgs<PopT> &a = A[blockIdx.x];
+  if (a.ns == 0) return;
+  sphere_step_body(a.sph, a.ns, a.gravity, a.dFluid, a.dDead, a.s.nx, a.s.ny, a.s.nz);
 }
 
 // ---------------------------------------------------------------- launcher
@@ -317,6 +394,52 @@ class Ops final : public OpsBase {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * warps_of<TY, STG>(), smem);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per) * std::max(1, sms);
+  }
+  size_t small_args_bytes() const override { return sizeof(SmallArgs<PopT>); }
+  void small_args(lbm_sim *h, int cur, int ns, long long slotCells, long long maxU, int redChunks,
+                  void *out) override {
+    SmallArgs<PopT> a;
+    memset(&a, 0, sizeof(a));
+    a.s = scene(h);
+    a.cur = cur;
+    a.ns = ns;
+    a.listCap = (int)h->listCap;
+    a.redChunks = redChunks;
+    a.zlo = h->slab ? h->ownLo : 0;
+    a.zend = h->slab ? h->ownHi + 1 : 0;
+    a.plan = h->dPlan;
+    a.sph = h->dSph;
+    a.impAcc = h->impAcc;
+    a.slotCells = slotCells;
+    a.maxU = maxU;
+    a.counts = h->counts;
+    a.fresh = h->fresh;
+    a.dead = h->dead;
+    a.totals = h->totals;
+    a.partials = h->partials;
+    a.dFluid = h->dOut;
+    a.dDead = h->dOut + LBM_MAX_SPHERES * 6;
+    a.tickets = h->redTickets;
+    a.rhoL = h->params.rhoL;
+    a.rhoG = h->params.rhoG;
+    a.gravity = h->params.gravity;
+    memcpy(out, &a, sizeof(a));
+  }
+  void batch_pre(const void *d_small, int n, unsigned retagCtas, unsigned compactCtas, cudaStream_t st) override {
+    const auto *A = (const SmallArgs<PopT> *)d_small;
+    kb_plan<PopT><<<n, 32, 0, st>>>(A);
+    kb_retag_box<PopT><<<dim3(retagCtas, n), 256, 0, st>>>(A);
+    kb_compact_count<PopT><<<dim3(compactCtas, n), COMPACT_THREADS, 0, st>>>(A);
+    kb_compact_scan<PopT><<<n, 1024, 0, st>>>(A);
+    kb_compact_emit<PopT><<<dim3(compactCtas, n), COMPACT_THREADS, 0, st>>>(A);
+    kb_fresh_fill<PopT><<<n, 32, 0, st>>>(A);
+  }
+  void batch_post(const void *d_small, int n, int redChunks, int maxSpheres, cudaStream_t st) override {
+    if (maxSpheres <= 0) return;
+    const auto *A = (const SmallArgs<PopT> *)d_small;
+    kb_impulse_reduce<PopT><<<dim3(redChunks, maxSpheres, n), RED_THREADS, 0, st>>>(A);
+    kb_absorb_dead<PopT><<<dim3(maxSpheres, n), DEAD_THREADS, 0, st>>>(A);
+    kb_sphere_step<PopT><<<n, 32, 0, st>>>(A);
   }
   void warm(int device) override {
     static const int shapes[] = {2, 4, 8, 4 | LBM_FUSED_COMPACT, 6 | LBM_FUSED_COMPACT, 4 | LBM_FUSED_ASYNC,

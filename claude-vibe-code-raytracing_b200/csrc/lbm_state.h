@@ -88,6 +88,15 @@ class OpsBase {
   // the device (and set their shared-memory opt-in), so that no first launch
   // waits for a module load
   virtual void warm(int device) = 0;
+  // a batch's sparse kernels, one launch per kind for all scenes: the
+  // per-scene argument block, then the kernels before and after the fused
+  // launch over a device table of n such blocks
+  virtual size_t small_args_bytes() const = 0;
+  virtual void small_args(lbm_sim *h, int cur, int ns, long long slotCells, long long maxU, int redChunks,
+                          void *out) = 0;
+  virtual void batch_pre(const void *d_small, int n, unsigned retagCtas, unsigned compactCtas,
+                         cudaStream_t st) = 0;
+  virtual void batch_post(const void *d_small, int n, int redChunks, int maxSpheres, cudaStream_t st) = 0;
 };
 
 OpsBase *make_ops_f32();

@@ -372,6 +372,7 @@ SIM_ONLY(js_collide_phase, lbm_collide_phase)
 SIM_ONLY(js_stream_phase, lbm_stream_phase)
 SIM_ONLY(js_collide_hydro, lbm_collide_hydro)
 SIM_ONLY(js_wait_frames, lbm_wait_frames)
+SIM_ONLY(js_wait_frame_slot, lbm_wait_frame_slot)
 SIM_ONLY(js_synchronize, lbm_synchronize)
 
 static napi_value js_retag_cells(napi_env env, napi_callback_info info) {
@@ -852,6 +853,7 @@ static const napi_property_descriptor kExports[] = {
     FN("stepFrame", js_step_frame),
     FN("initProfile", js_init_profile),
     FN("waitFrames", js_wait_frames),
+    FN("waitFrameSlot", js_wait_frame_slot),
     FN("runCoupled", js_run_coupled),
     FN("sphereStep", js_sphere_step),
     FN("synchronize", js_synchronize),

@@ -266,6 +266,7 @@ export class Sim {
     return out;
   }
   waitFrames() { addon.waitFrames(this._h); }
+  waitFrameSlot() { addon.waitFrameSlot(this._h); }
   field64(name) {
     this._sync();
     const out = new Float64Array(this._count(name));

@@ -219,6 +219,12 @@ int lbm_pack_volume_async(lbm_sim *sim, uint8_t *host_out);
  * lbm_wait_frames).  The same bytes as lbm_step then lbm_pack_volume. */
 int lbm_step_frame(lbm_sim *sim, const lbm_sphere *spheres, int nspheres, lbm_impulse *out,
                    uint8_t *host_frame);
+/* The asynchronous frames use two device buffers in turn.  Wait until the copy
+ * out of the one the next lbm_step_frame / lbm_pack_volume_async will use has
+ * reached its host buffer: a host that alternates two host buffers in the
+ * same order thereby knows that the older one holds its frame (the worker's
+ * pool of posted frame buffers, src/worker.js:17-21, 158-163). */
+int lbm_wait_frame_slot(lbm_sim *sim);
 int lbm_wait_frames(lbm_sim *sim);
 /* Same, into device memory, asynchronous on the handle's stream. */
 int lbm_pack_volume_device(lbm_sim *sim, void *device_out);

@@ -18,7 +18,7 @@ HARNESS = os.path.join(ROOT, "tests", "napi", "build", "harness")
 EXPECTED = """create destroy lastError getDims deviceBytes footprintBytes setParams getParams uploadField retagCellsMask solidLinks
 downloadField downloadFieldF64 initFlat seedHydrostatic retagCells handleFreshCells computePhiGradients
 collidePhase streamPhase collideHydro streamHydroAndMacro step absorbDeadCells packVolume packVolumeAsync
-waitFrames stepFrame initProfile runCoupled sphereStep synchronize setNanWatchdog lastSets launchCount checkedBuild faultRecord
+waitFrames waitFrameSlot stepFrame initProfile runCoupled sphereStep synchronize setNanWatchdog lastSets launchCount checkedBuild faultRecord
 transferBytes fusedTiming fusedTimingQuery setFusedConfig getFusedConfig testWithholdStageCopy cameraDefault render
 batchCreate batchDestroy batchSetConfig batchRun batchTimeFused batchLaunchCount""".split()
 
