@@ -337,11 +337,19 @@ def serve_result(args, dev, ws=1, rank=0):
     from b200lbm import placement, serve, workloads
     torch.cuda.set_device(dev)
     reqs = workloads.request_stream(args.requests, seed=0)
-    reqs = placement.shard(reqs, ws, lambda r: workloads.cells(r["spec"]) * r["steps"])[rank]
     storage = "f16" if args.storage == "f32" else args.storage
     clocks = Clocks(dev)
     clocks.start()
-    rep = serve.Server(storage=storage, device=dev).run(reqs, realtime=True)
+    if ws > 1:
+        # one stream shared by every rank's server: each GPU claims the next
+        # request when it has room (placement.ClaimQueue over the group's store)
+        claims = placement.ClaimQueue(reqs, store=placement.default_store(), key="bench-serve")
+        barrier(ws)
+        rep = serve.Server(storage=storage, device=dev).run(None, realtime=True, claims=claims)
+        mine = set(rep["claimed"])
+        reqs = [r for r in reqs if r["rid"] in mine]
+    else:
+        rep = serve.Server(storage=storage, device=dev).run(reqs, realtime=True)
     clk = clocks.stop()
     seq = serve.sequential(reqs, storage="f32", device=dev)
     if ws > 1:

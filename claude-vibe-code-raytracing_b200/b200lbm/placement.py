@@ -9,6 +9,12 @@ rank, so every rank computes the same assignment without communicating.
 The only collectives are for reporting: the slowest rank's time
 (max_over_ranks) and the work summed over ranks (sum_over_ranks), on
 whatever process group is initialised (NCCL on GPUs, gloo in the CPU tests).
+
+A served request stream is not split up front: ClaimQueue hands the requests
+out in arrival order through one atomic counter in the process group's
+key-value store, and each serving process claims the next request when its
+GPU has room for it, so a GPU whose scenes finish early takes more of the
+stream (balance by live footprint, not by a static guess).
 """
 from __future__ import annotations
 
@@ -49,3 +55,41 @@ def max_over_ranks(v):
 def sum_over_ranks(v):
     import torch.distributed as dist
     return _reduce(v, dist.ReduceOp.SUM)
+
+
+class ClaimQueue:
+    """Requests shared by the serving processes of one job.  Every process
+    builds the same list (the same seeded trace); `claim` takes the next
+    unclaimed one in arrival order, atomically across processes (the store's
+    add), and `peek` shows it without taking it.  With store=None the queue
+    is local to one process."""
+
+    def __init__(self, requests, store=None, key="lbm-serve-next"):
+        self.requests = sorted(requests, key=lambda r: (r["arrival"], r["rid"]))
+        self.store = store
+        self.key = key
+        self._next = 0
+
+    def _counter(self, add):
+        if self.store is None:
+            self._next += add
+            return self._next
+        return int(self.store.add(self.key, add))
+
+    def peek(self):
+        i = self._counter(0)
+        return self.requests[i] if i < len(self.requests) else None
+
+    def claim(self):
+        i = self._counter(1) - 1
+        return self.requests[i] if i < len(self.requests) else None
+
+    def exhausted(self):
+        return self._counter(0) >= len(self.requests)
+
+
+def default_store():
+    """The key-value store of the initialised default process group (the
+    rendezvous store every rank already shares)."""
+    from torch.distributed import distributed_c10d
+    return distributed_c10d._get_default_store()

@@ -118,13 +118,18 @@ class Server:
         rc = lib().lbm_prepare_device(self.device, STORAGE[self.storage], want)
         self.prepared = want if rc == 0 else 0
 
-    def run(self, requests, realtime=True, on_frame=None, on_finish=None):
+    def run(self, requests, realtime=True, on_frame=None, on_finish=None, claims=None):
         """Serve `requests` (dicts with rid, arrival, spec, steps, frame_every;
         frame_every must be the same for all and divide every steps).
         realtime: a request becomes visible at its arrival time (seconds after
         the start); otherwise all are visible at once.  on_frame(rid, index,
         volume) gets every RG8 volume; on_finish(rid, sim, solid) runs before a
-        finished scene is released.  Returns the report dict."""
+        finished scene is released.  claims: a placement.ClaimQueue shared
+        with the other serving processes of the job (one per GPU); requests
+        are then claimed from it whenever this GPU has room for the next one
+        (`requests` is not used).  Returns the report dict."""
+        if claims is not None:
+            requests = claims.requests
         reqs = sorted(requests, key=lambda r: (r["arrival"], r["rid"]))
         every = {r["frame_every"] for r in reqs}
         if len(every) != 1:
@@ -134,7 +139,9 @@ class Server:
         if tick % every or any(r["steps"] % tick for r in reqs):
             raise ValueError("the tick must be a multiple of the frame cadence and divide every request")
         self.start()
-        queue = collections.deque(reqs)
+        queue = collections.deque(reqs if claims is None else ())
+        claimed = []
+        fpr = lambda r: footprint(r["spec"], self.storage)  # noqa: E731
         active = []  # dicts: req, sim, solid, done, fp, frames, last
         used = 0
         batch = None
@@ -155,11 +162,25 @@ class Server:
         pool = ThreadPoolExecutor(max_workers=2, thread_name_prefix="lbm-build")
         building = []  # (req, fp, future) admitted, not yet built
         try:
-            while queue or active or building:
+            while queue or active or building or (claims is not None and not claims.exhausted()):
                 tl0 = time.perf_counter()
                 now = clock()
-                for req in admit(list(queue), used, self.budget, now,
-                                 lambda r: footprint(r["spec"], self.storage)):
+                if claims is not None:
+                    # claim arrived requests while this GPU has room for them
+                    pending = used + sum(fpr(r) for r in queue)
+                    while True:
+                        nxt = claims.peek()
+                        if nxt is None or nxt["arrival"] > now:
+                            break
+                        if pending + fpr(nxt) > self.budget and (active or building or queue):
+                            break
+                        got = claims.claim()
+                        if got is None:
+                            break
+                        queue.append(got)
+                        claimed.append(got["rid"])
+                        pending += fpr(got)
+                for req in admit(list(queue), used, self.budget, now, fpr):
                     queue.remove(req)
                     fp = footprint(req["spec"], self.storage)
                     used += fp
@@ -177,10 +198,11 @@ class Server:
                 building = still_building
                 if not active:
                     # idle until the next arrival
-                    if queue:
-                        wait = queue[0]["arrival"] - (time.perf_counter() - t0)
+                    nxt = queue[0] if queue else (claims.peek() if claims is not None else None)
+                    if nxt is not None:
+                        wait = nxt["arrival"] - (time.perf_counter() - t0)
                         if wait > 0:
-                            time.sleep(wait)
+                            time.sleep(wait if queue else min(wait, 0.01))
                     continue
                 max_active = max(max_active, len(active))
                 ids = [a["req"]["rid"] for a in active]
@@ -251,7 +273,7 @@ class Server:
             pool.shutdown(wait=True)
         wall = time.perf_counter() - t0
         return {
-            "requests": len(reqs),
+            "requests": len(reqs) if claims is None else len(claimed),
             "wall_s": wall,
             "ticks": ticks,
             "scene_steps": scene_steps,
@@ -267,6 +289,7 @@ class Server:
             "slowest_ticks": [dict(run_s=r, membership_changed=c, active=a, building=b, cells=n)
                               for r, c, a, b, n in sorted(slow, key=lambda t: -t[0])[:5]],
             "reserved_bytes": self.prepared,
+            "claimed": claimed if claims is not None else None,
             **{f"{k}_s": percentiles(v, (50, 99, 100)) for k, v in seg.items()},
             "storage": self.storage,
             "budget_bytes": self.budget,

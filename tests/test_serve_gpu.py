@@ -37,7 +37,7 @@ def _trace():
             for i, s in enumerate(specs)]
 
 
-def _serve(gpu, reqs, **kw):
+def _serve(gpu, reqs, claims=None, **kw):
     from b200lbm.serve import Server
     from b200lbm.solid import spheres_of
     frames, final = {}, {}
@@ -49,7 +49,7 @@ def _serve(gpu, reqs, **kw):
         final[rid] = ({k: np.array(getattr(sim, k)) for k in ("phi", "rho", "ux", "f", "h")},
                       [b.state() for b in spheres_of(solid)])
 
-    rep = Server(**kw).run(reqs, realtime=False, on_frame=on_frame, on_finish=on_finish)
+    rep = Server(**kw).run(reqs, realtime=False, on_frame=on_frame, on_finish=on_finish, claims=claims)
     return rep, frames, final
 
 
@@ -84,4 +84,24 @@ def test_budget_serialises_without_changing_results(gpu):
         for a, b in zip(frames[rid], frames_all[rid]):
             assert np.array_equal(a, b)
         for k in final[rid][0]:
+            assert np.array_equal(final[rid][0][k], final_all[rid][0][k]), (rid, k)
+
+
+def test_claimed_stream_equals_listed(gpu):
+    """The same requests taken through a claim queue (as several serving
+    processes share one stream), here one process under a tight budget:
+    every request is claimed once and served bit for bit as from the list."""
+    from b200lbm import placement
+    from b200lbm.serve import footprint
+    reqs = _trace()
+    biggest = max(footprint(r["spec"], "f16") for r in reqs)
+    _, frames_all, final_all = _serve(gpu, reqs, storage="f16")
+    q = placement.ClaimQueue(reqs)
+    rep, frames, final = _serve(gpu, None, claims=q, storage="f16", budget_bytes=int(1.5 * biggest))
+    assert sorted(rep["claimed"]) == [r["rid"] for r in reqs]
+    for r in reqs:
+        rid = r["rid"]
+        for a, b in zip(frames[rid], frames_all[rid]):
+            assert np.array_equal(a, b), rid
+        for k in final_all[rid][0]:
             assert np.array_equal(final[rid][0][k], final_all[rid][0][k]), (rid, k)
