@@ -25,8 +25,8 @@ STAGED = 0x100
 COMPACT = 0x400
 ASYNC = 0x800
 CANDIDATES_F64 = [(4, 32), (4, 16), (8, 16), (8, 32), (2, 32), (4, 64)]
-CANDIDATES = [(6 | COMPACT, 32), (6 | ASYNC, 32), (6 | COMPACT, 16), (6 | ASYNC, 16), (6 | COMPACT, 64),
-              (4, 32), (4, 16), (8, 16), (4 | COMPACT, 32), (6 | STAGED, 32)]
+CANDIDATES = [(6 | COMPACT, 32), (6 | COMPACT, 64), (6 | COMPACT, 128), (6 | ASYNC, 32), (6 | COMPACT, 16),
+              (4, 32), (4, 64), (4, 128), (4, 16), (8, 16), (4 | COMPACT, 32), (6 | STAGED, 32)]
 
 
 def candidates_for(storage):

@@ -473,6 +473,7 @@ void free_all(lbm_sim *h) {
   for (int b = 0; b < 2; b++) {
     if (h->frameDev[b]) cudaFreeAsync(h->frameDev[b], h->stream);
     if (h->evFrame[b]) cudaEventDestroy(h->evFrame[b]);
+    if (h->evPackedSlot[b]) cudaEventDestroy(h->evPackedSlot[b]);
   }
   if (h->evPacked) cudaEventDestroy(h->evPacked);
   if (h->evCopied) cudaEventDestroy(h->evCopied);
@@ -606,6 +607,20 @@ int coupled_finish(lbm_sim *h, lbm_sphere *sp, int ns) {
   return LBM_OK;
 }
 
+// the deferred copy of lbm_step_frame's frame, if one is waiting
+int flush_frame_copy(lbm_sim *h) {
+  if (h->deferredSlot < 0) return LBM_OK;
+  const int slot = h->deferredSlot;
+  h->deferredSlot = -1;
+  CK(cudaStreamWaitEvent(h->copyStream, h->evPackedSlot[slot], 0));
+  CK(copy_async(h, h->deferredHost, h->frameDev[slot], (size_t)h->n * 2, cudaMemcpyDeviceToHost, h->copyStream));
+  CK(cudaEventRecord(h->evFrame[slot], h->copyStream));
+  CK(cudaEventRecord(h->evCopied, h->copyStream));
+  h->framePending[slot] = true;
+  h->copyPending = true;
+  return LBM_OK;
+}
+
 // the copy stream, its events and the two device frames of the asynchronous
 // frame path, created on first use; *buf receives the frame to pack into, and
 // the handle's stream waits until that frame's previous copy is done
@@ -615,10 +630,13 @@ int next_frame(lbm_sim *h, uint8_t **buf, int *slot) {
     CK(cudaEventCreateWithFlags(&h->evPacked, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->evCopied, cudaEventDisableTiming));
   }
+  int rc = flush_frame_copy(h);
+  if (rc) return rc;
   const int b = h->frameNext;
   if (!h->frameDev[b]) {
     DALLOC(h->frameDev[b], (size_t)h->n * 2);
     CK(cudaEventCreateWithFlags(&h->evFrame[b], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->evPackedSlot[b], cudaEventDisableTiming));
   }
   if (h->framePending[b]) CK(cudaStreamWaitEvent(h->stream, h->evFrame[b], 0));
   *buf = (uint8_t *)h->frameDev[b];
@@ -1224,6 +1242,7 @@ int lbm_step_end(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   }
   launch_fused(h);
   CKL("fused step");
+  if ((rc = flush_frame_copy(h))) return rc;
   if ((rc = reduce_impulses(h, h->dOut))) return rc;
   h->cur = 1 - h->cur;
   shift_boxes(h, h->stepNow);
@@ -1259,7 +1278,13 @@ int lbm_step_frame(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out, u
   const int stepRc = rc;
   h->ops->pack_end_planes(h, buf);
   CKL("packVolume (end planes)");
-  if ((rc = issue_frame_copy(h, slot, host_frame))) return rc;
+  // the copy to the host is issued with the next step's fused kernel (or by
+  // any wait for frames), so the step's own small read-backs do not queue
+  // behind it on the copy engine
+  CK(cudaEventRecord(h->evPackedSlot[slot], h->stream));
+  h->deferredSlot = slot;
+  h->deferredHost = host_frame;
+  h->frameNext = 1 - slot;
   return stepRc;
 }
 
@@ -1431,6 +1456,8 @@ int lbm_sphere_step_host(lbm_sphere *spheres, int n, double dt, double gravity, 
 int lbm_wait_frames(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);
+  int rc = flush_frame_copy(h);
+  if (rc) return rc;
   if (h->copyPending) {
     CK(cudaEventSynchronize(h->evCopied));
     h->copyPending = false;
@@ -1442,6 +1469,8 @@ int lbm_wait_frames(lbm_sim *h) {
 int lbm_wait_frame_slot(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
   DeviceGuard g(h->device);
+  int rc = flush_frame_copy(h);
+  if (rc) return rc;
   const int b = h->frameNext;
   if (h->framePending[b]) {
     CK(cudaEventSynchronize(h->evFrame[b]));

@@ -154,8 +154,14 @@ struct lbm_sim {
   // copy, evCopied marks the last copy issued
   void *frameDev[2] = {nullptr, nullptr};
   cudaEvent_t evFrame[2] = {nullptr, nullptr};
+  cudaEvent_t evPackedSlot[2] = {nullptr, nullptr};
   bool framePending[2] = {false, false};
   int frameNext = 0;
+  // lbm_step_frame's copy to the host, issued when the next step's fused
+  // kernel is queued (so it runs beside that kernel, not ahead of the step's
+  // small read-backs on the same copy engine); -1: none waiting
+  int deferredSlot = -1;
+  uint8_t *deferredHost = nullptr;
   cudaStream_t copyStream = nullptr;
   cudaEvent_t evPacked = nullptr, evCopied = nullptr;
   bool copyPending = false;

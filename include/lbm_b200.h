@@ -215,8 +215,11 @@ int lbm_pack_volume_async(lbm_sim *sim, uint8_t *host_out);
 /* lbm_step + lbm_pack_volume_async on a frame step, with the pack fused into
  * the step: the fused kernel writes the RG8 bytes of every cell it visits as
  * it writes the macros, a small launch adds the planes z = 0 and nz - 1, and
- * the volume is copied into host_frame on the copy stream (complete after
- * lbm_wait_frames).  The same bytes as lbm_step then lbm_pack_volume. */
+ * the volume is copied into host_frame on the copy stream.  The copy starts
+ * when the next step's fused kernel is queued (it then runs beside that
+ * kernel) or at the next lbm_wait_frames / lbm_wait_frame_slot, and is
+ * complete after lbm_wait_frames.  The same bytes as lbm_step then
+ * lbm_pack_volume. */
 int lbm_step_frame(lbm_sim *sim, const lbm_sphere *spheres, int nspheres, lbm_impulse *out,
                    uint8_t *host_frame);
 /* The asynchronous frames use two device buffers in turn.  Wait until the copy
