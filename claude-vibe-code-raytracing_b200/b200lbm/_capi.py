@@ -120,6 +120,7 @@ _SIGS = [
     ("lbm_checked_build", C.c_int, []),
     ("lbm_fault_record", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("lbm_test_withhold_stage_copy", C.c_int, [C.c_void_p, C.c_int]),
+    ("lbm_test_sequential_fill", C.c_int, [C.c_void_p, C.c_int]),
     ("lbm_set_nan_watchdog", C.c_int, [C.c_void_p, C.c_int]),
     ("lbm_transfer_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("lbm_fused_timing", C.c_int, [C.c_void_p, C.c_int]),

@@ -1495,6 +1495,12 @@ int lbm_set_nan_watchdog(lbm_sim *h, int every) {
   return LBM_OK;
 }
 
+int lbm_test_sequential_fill(lbm_sim *h, int on) {
+  if (!h) return LBM_ERR_ARG;
+  h->sequentialFill = on != 0;
+  return LBM_OK;
+}
+
 int lbm_test_withhold_stage_copy(lbm_sim *h, int on) {
   if (!h) return LBM_ERR_ARG;
   h->withholdStage = on != 0;

@@ -566,74 +566,174 @@ static __global__ void k_compact_emit(const uint8_t *tag, const uint8_t *tagPrev
   compact_emit_body(tag, tagPrev, nx, ny, P, offsets, fresh, dead, cap, blockIdx.x, gridDim.x);
 }
 
-// handleFreshCells (src/sim.js:257-310) over the scan-ordered fresh list, one
-// thread, FP64 arithmetic, in place -- later fresh cells see the values written
-// for earlier ones exactly as in the reference's single sweep.
+// One fresh cell (src/sim.js:264-308): the FLUID neighbours' phi, rho and u
+// averaged in the reference's neighbour order (dz, dy, dx ascending), then phi,
+// phiPrev, rho, u and the equilibrium populations written.  nb(j, p, r, x, y,
+// z) gives neighbour j's five values.
+template <class PopT, class NB>
+__device__ __forceinline__ void fill_cell(const Scene<PopT, typename Prec<PopT>::Real> &s, int cur, long long i,
+                                          double rhoL, double rhoG, NB &&nb) {
+  using Real = typename Prec<PopT>::Real;
+  const int nx = s.nx, ny = s.ny;
+  double psum = 0, rsum = 0, vxs = 0, vys = 0, vzs = 0;
+  int pcnt = 0;
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        if (!dx && !dy && !dz) continue;
+        long long j = i + ((long long)dz * ny + dy) * nx + dx;
+        if (s.tag[j] == TAG_FLUID) {
+          Real vp, vr, vx_, vy_, vz_;
+          nb(j, vp, vr, vx_, vy_, vz_);
+          psum += (double)vp;
+          rsum += (double)vr;
+          vxs += (double)vx_;
+          vys += (double)vy_;
+          vzs += (double)vz_;
+          pcnt++;
+        }
+      }
+  double p = pcnt > 0 ? psum / pcnt : (double)s.phi[cur][i];
+  double r = pcnt > 0 ? rsum / pcnt : 1.0;
+  double vx = pcnt > 0 ? vxs / pcnt : 0;
+  double vy = pcnt > 0 ? vys / pcnt : 0;
+  double vz = pcnt > 0 ? vzs / pcnt : 0;
+  Real pR = (Real)p;
+  s.phi[cur][i] = pR;
+  s.phi[1 - cur][i] = pR;  // phiPrev[i] = p
+  s.rho[cur][i] = (Real)r;
+  s.ux[cur][i] = (Real)vx;
+  s.uy[cur][i] = (Real)vy;
+  s.uz[cur][i] = (Real)vz;
+  double rhoPhase = rhoG + p * (rhoL - rhoG);
+  double u2 = vx * vx + vy * vy + vz * vz;
+  for (int k = 0; k < Q27; k++) {
+    double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
+    double Qi = eu * (3.0 + 4.5 * eu) - 1.5 * u2;
+    double fk = (double)w27_of(k) * (r + rhoPhase * Qi);
+    s.F[cur][pidx<27>(k, i)] = Codec<PopT>::enc((Real)fk, (Real)w27_of(k));
+  }
+  for (int k = 0; k < Q7; k++) {
+    double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
+    double hk = (double)w7_of(k) * p * (1 + 4.0 * eu);
+    s.H[cur][pidx<7>(k, i)] = Codec<PopT>::enc((Real)hk, (Real)w7_of(k) * pR);
+  }
+}
+
+// Fresh cells a block fills in parallel; a longer list is filled by one
+// thread in list order.
+constexpr int FILL_PAR_MAX = 512;
+constexpr int FILL_THREADS = 256;
+
+// handleFreshCells over the scan-ordered fresh list (src/sim.js:257-310).  The
+// reference fills in scan order, in place: a fresh cell sees the filled values
+// of fresh neighbours before it in scan order and the old values of those
+// after it.  In parallel that order is kept by rounds: the old phi, rho and u
+// of every listed cell are saved first; in each round a cell whose fresh
+// neighbours before it in scan order were all filled in earlier rounds is
+// filled, reading the saved old values for fresh neighbours after it.  The
+// arithmetic of each cell is the sequential one (fill_cell), so the results
+// are the same bit for bit.  A z slab fills its own planes only (its copied
+// planes receive the neighbouring slab's filled values).  sequential != 0: one
+// thread in list order (also used for lists longer than FILL_PAR_MAX).
 template <class PopT>
 __device__ __forceinline__ void fresh_fill_body(const Scene<PopT, typename Prec<PopT>::Real> &s, int cur,
                                                 const int *fresh, const int *totals, int cap, double rhoL,
-                                                double rhoG, int zlo, int zend) {
+                                                double rhoG, int zlo, int zend, int sequential) {
   using Real = typename Prec<PopT>::Real;
-  if (threadIdx.x != 0) return;
   int nf = totals[0];
   if (nf > cap) nf = cap;
-  const int nx = s.nx, ny = s.ny;
-  for (int q = 0; q < nf; q++) {
-    long long i = fresh[q];
-    // a z slab fills the cells of its own planes only: its copied planes
-    // receive the neighbouring slab's filled values
-    if (zend > 0) {
-      const long long z = i / ((long long)nx * ny);
-      if (z < zlo || z >= zend) continue;
+  const long long nxny = (long long)s.nx * s.ny;
+  auto skip = [&](long long i) -> bool {
+    if (zend <= 0) return false;
+    const long long z = i / nxny;
+    return z < zlo || z >= zend;
+  };
+  auto current = [&](long long j, Real &p, Real &r, Real &x, Real &y, Real &z) {
+    p = s.phi[cur][j];
+    r = s.rho[cur][j];
+    x = s.ux[cur][j];
+    y = s.uy[cur][j];
+    z = s.uz[cur][j];
+  };
+  if (sequential || nf > FILL_PAR_MAX) {
+    if (threadIdx.x != 0) return;
+    for (int q = 0; q < nf; q++) {
+      const long long i = fresh[q];
+      if (!skip(i)) fill_cell<PopT>(s, cur, i, rhoL, rhoG, current);
     }
-    double psum = 0, rsum = 0, vxs = 0, vys = 0, vzs = 0;
-    int pcnt = 0;
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) {
-          if (!dx && !dy && !dz) continue;
-          long long j = i + ((long long)dz * ny + dy) * nx + dx;
-          if (s.tag[j] == TAG_FLUID) {
-            psum += (double)s.phi[cur][j];
-            rsum += (double)s.rho[cur][j];
-            vxs += (double)s.ux[cur][j];
-            vys += (double)s.uy[cur][j];
-            vzs += (double)s.uz[cur][j];
-            pcnt++;
+    return;
+  }
+  __shared__ int sIdx[FILL_PAR_MAX];
+  __shared__ int sDone[FILL_PAR_MAX];  // round in which the cell was filled (or skipped), 0: not yet
+  __shared__ Real sOld[5][FILL_PAR_MAX];
+  for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+    const long long i = fresh[q];
+    sIdx[q] = (int)i;
+    sDone[q] = 0;
+    current(i, sOld[0][q], sOld[1][q], sOld[2][q], sOld[3][q], sOld[4][q]);
+  }
+  __syncthreads();
+  // list position of cell j, or -1 (the list is sorted by cell index)
+  auto find = [&](long long j) -> int {
+    int lo = 0, hi = nf - 1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const int v = sIdx[mid];
+      if (v == j) return mid;
+      if (v < j) lo = mid + 1;
+      else hi = mid - 1;
+    }
+    return -1;
+  };
+  for (int round = 1;; round++) {
+    int waiting = 0;
+    for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+      if (sDone[q]) continue;
+      const long long i = sIdx[q];
+      if (skip(i)) {
+        sDone[q] = round;
+        continue;
+      }
+      bool ready = true;
+      for (int dz = -1; dz <= 0 && ready; dz++)
+        for (int dy = -1; dy <= 1 && ready; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            if (dz == 0 && (dy > 0 || (dy == 0 && dx >= 0))) break;  // only neighbours before i
+            const long long j = i + ((long long)dz * s.ny + dy) * s.nx + dx;
+            const int pos = find(j);
+            if (pos >= 0 && (sDone[pos] == 0 || sDone[pos] >= round)) {
+              ready = false;
+              break;
+            }
           }
+      if (!ready) {
+        waiting = 1;
+        continue;
+      }
+      fill_cell<PopT>(s, cur, i, rhoL, rhoG, [&](long long j, Real &p, Real &r, Real &x, Real &y, Real &z) {
+        const int pos = j > i ? find(j) : -1;
+        if (pos >= 0) {
+          p = sOld[0][pos];
+          r = sOld[1][pos];
+          x = sOld[2][pos];
+          y = sOld[3][pos];
+          z = sOld[4][pos];
+        } else {
+          current(j, p, r, x, y, z);
         }
-    double p = pcnt > 0 ? psum / pcnt : (double)s.phi[cur][i];
-    double r = pcnt > 0 ? rsum / pcnt : 1.0;
-    double vx = pcnt > 0 ? vxs / pcnt : 0;
-    double vy = pcnt > 0 ? vys / pcnt : 0;
-    double vz = pcnt > 0 ? vzs / pcnt : 0;
-    Real pR = (Real)p;
-    s.phi[cur][i] = pR;
-    s.phi[1 - cur][i] = pR;  // phiPrev[i] = p
-    s.rho[cur][i] = (Real)r;
-    s.ux[cur][i] = (Real)vx;
-    s.uy[cur][i] = (Real)vy;
-    s.uz[cur][i] = (Real)vz;
-    double rhoPhase = rhoG + p * (rhoL - rhoG);
-    double u2 = vx * vx + vy * vy + vz * vz;
-    for (int k = 0; k < Q27; k++) {
-      double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
-      double Qi = eu * (3.0 + 4.5 * eu) - 1.5 * u2;
-      double fk = (double)w27_of(k) * (r + rhoPhase * Qi);
-      s.F[cur][pidx<27>(k, i)] = Codec<PopT>::enc((Real)fk, (Real)w27_of(k));
+      });
+      sDone[q] = round;
     }
-    for (int k = 0; k < Q7; k++) {
-      double eu = dcomp(k, 0) * vx + dcomp(k, 1) * vy + dcomp(k, 2) * vz;
-      double hk = (double)w7_of(k) * p * (1 + 4.0 * eu);
-      s.H[cur][pidx<7>(k, i)] = Codec<PopT>::enc((Real)hk, (Real)w7_of(k) * pR);
-    }
+    if (!__syncthreads_or(waiting)) break;
   }
 }
 template <class PopT>
-__global__ void k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *fresh,
-                             const int *totals, int cap, double rhoL, double rhoG, int zlo, int zend) {
+__global__ void __launch_bounds__(FILL_THREADS)
+    k_fresh_fill(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *fresh, const int *totals, int cap,
+                 double rhoL, double rhoG, int zlo, int zend, int sequential) {
   if (blockIdx.x != 0) return;
-  fresh_fill_body<PopT>(s, cur, fresh, totals, cap, rhoL, rhoG, zlo, zend);
+  fresh_fill_body<PopT>(s, cur, fresh, totals, cap, rhoL, rhoG, zlo, zend, sequential);
 }
 
 // absorbDeadCells (src/solid.js:87-101): impulse rho(phi)*u of every cell on

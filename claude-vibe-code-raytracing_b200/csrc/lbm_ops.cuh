@@ -95,7 +95,7 @@ static __global__ void k_sphere_step(lbm_sphere *sph, int nsph, double gravity, 
 template <class PopT>
 struct SmallArgs {
   Scene<PopT, typename Prec<PopT>::Real> s;
-  int cur, ns, listCap, redChunks, zlo, zend;
+  int cur, ns, listCap, redChunks, zlo, zend, seqFill;
   Plan *plan;
   lbm_sphere *sph;
   double *impAcc;
@@ -134,9 +134,9 @@ __global__ void kb_compact_emit(const SmallArgs<PopT> *__restrict__ A) {
                     blockIdx.x, gridDim.x);
 }
 template <class PopT>
-__global__ void kb_fresh_fill(const SmallArgs<PopT> *__restrict__ A) {
+__global__ void __launch_bounds__(FILL_THREADS) kb_fresh_fill(const SmallArgs<PopT> *__restrict__ A) {
   const SmallArgs<PopT> &a = A[blockIdx.x];
-  fresh_fill_body<PopT>(a.s, a.cur, a.fresh, a.totals, a.listCap, a.rhoL, a.rhoG, a.zlo, a.zend);
+  fresh_fill_body<PopT>(a.s, a.cur, a.fresh, a.totals, a.listCap, a.rhoL, a.rhoG, a.zlo, a.zend, a.seqFill);
 }
 template <class PopT>
 __global__ void __launch_bounds__(RED_THREADS) kb_impulse_reduce(const SmallArgs<PopT> *__restrict__ A) {
@@ -259,9 +259,10 @@ class Ops final : public OpsBase {
     h->launches++;
   }
   void fresh_fill(lbm_sim *h) override {
-    k_fresh_fill<PopT><<<1, 32, 0, h->stream>>>(scene(h), h->cur, h->fresh, h->totals,
-                                                 (int)h->listCap, h->params.rhoL, h->params.rhoG,
-                                                 h->slab ? h->ownLo : 0, h->slab ? h->ownHi + 1 : 0);
+    k_fresh_fill<PopT><<<1, FILL_THREADS, 0, h->stream>>>(scene(h), h->cur, h->fresh, h->totals,
+                                                           (int)h->listCap, h->params.rhoL, h->params.rhoG,
+                                                           h->slab ? h->ownLo : 0, h->slab ? h->ownHi + 1 : 0,
+                                                           h->sequentialFill ? 1 : 0);
     h->launches++;
   }
   void absorb_dead(lbm_sim *h, double *d_out) override {
@@ -407,6 +408,7 @@ class Ops final : public OpsBase {
     a.redChunks = redChunks;
     a.zlo = h->slab ? h->ownLo : 0;
     a.zend = h->slab ? h->ownHi + 1 : 0;
+    a.seqFill = h->sequentialFill ? 1 : 0;
     a.plan = h->dPlan;
     a.sph = h->dSph;
     a.impAcc = h->impAcc;
@@ -432,7 +434,7 @@ class Ops final : public OpsBase {
     kb_compact_count<PopT><<<dim3(compactCtas, n), COMPACT_THREADS, 0, st>>>(A);
     kb_compact_scan<PopT><<<n, 1024, 0, st>>>(A);
     kb_compact_emit<PopT><<<dim3(compactCtas, n), COMPACT_THREADS, 0, st>>>(A);
-    kb_fresh_fill<PopT><<<n, 32, 0, st>>>(A);
+    kb_fresh_fill<PopT><<<n, FILL_THREADS, 0, st>>>(A);
   }
   void batch_post(const void *d_small, int n, int redChunks, int maxSpheres, cudaStream_t st) override {
     if (maxSpheres <= 0) return;

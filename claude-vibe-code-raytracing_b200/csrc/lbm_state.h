@@ -182,6 +182,8 @@ struct lbm_sim {
   // a frame step: the fused kernel writes the step's RG8 volume here
   // (planes 1 .. nz-2; pack_end_planes adds the two end planes), else null
   uint8_t *fusePack = nullptr;
+  // test hook: fill fresh cells with one thread in list order
+  bool sequentialFill = false;
   int stepBegunNs = -1;
   int fullRetagSteps = 0;
   int nsphLast = 0;

@@ -290,6 +290,10 @@ int lbm_fault_record(lbm_sim *sim, int64_t out[4]);
  * abandoned and LBM_ERR_TIMEOUT is reported; the fault record then holds
  * location code 90.  No effect on the other forms. */
 int lbm_test_withhold_stage_copy(lbm_sim *sim, int on);
+/* Test hook for the fresh-cell fill: while on, the handle's fresh cells are
+ * filled by one thread in scan order (the reference's loop) instead of in
+ * parallel rounds; the results are the same bit for bit either way. */
+int lbm_test_sequential_fill(lbm_sim *sim, int on);
 /* Host->device and device->host bytes this handle has copied since creation. */
 int lbm_transfer_bytes(const lbm_sim *sim, uint64_t *h2d, uint64_t *d2h);
 /* Time the fused step kernel with CUDA events on the handle's stream.
