@@ -939,10 +939,21 @@ __device__ __forceinline__ void impulse_reduce_body(const SolidSet *__restrict__
   const long long c0 = (long long)cx * RED_CHUNK;
   __shared__ double sh[6][RED_THREADS];
   __shared__ bool last;
+  // Only cells within sqrt(3) outside the sphere hold links (a FLUID cell next
+  // to one the sphere contains); the rest of the box stays zero and is
+  // neither read nor cleared.  Skipping a +0 term does not change a sum.
+  const SphereDesc &sp = ss.sph[b];
+  const double rIn = sp.r > 1.0 ? sp.r - 1.0 : 0.0, rOut = sp.r + 2.0;
+  const double in2 = rIn * rIn, out2 = rOut * rOut;
+  const int dxb = t.dim[0], dyb = t.dim[1];
   double a[6] = {0, 0, 0, 0, 0, 0};
   for (int j = threadIdx.x; j < RED_CHUNK; j += RED_THREADS) {
     const long long c = c0 + j;
     if (c >= cells) break;
+    const int lx = (int)(c % dxb), ly = (int)((c / dxb) % dyb), lz = (int)(c / ((long long)dxb * dyb));
+    const double ex = t.lo[0] + lx + 0.5 - sp.cx, ey = t.lo[1] + ly + 0.5 - sp.cy, ez = t.lo[2] + lz + 0.5 - sp.cz;
+    const double d2 = ex * ex + ey * ey + ez * ez;
+    if (d2 < in2 || d2 > out2) continue;
     double *p = t.acc + 6 * c;
     for (int q = 0; q < 6; q++) a[q] = __dadd_rn(a[q], p[q]);
     for (int q = 0; q < 6; q++) p[q] = 0.0;
