@@ -52,6 +52,10 @@ class LbmImpulse(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("Fx", "Fy", "Fz", "Tx", "Ty", "Tz")]
 
 
+class LbmRigidMotion(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("cx", "cy", "cz", "vx", "vy", "vz", "wx", "wy", "wz")]
+
+
 class LbmCamera(C.Structure):
     _fields_ = [("azimuth", C.c_double), ("elev", C.c_double), ("dist", C.c_double),
                 ("light", C.c_double * 3)]
@@ -92,6 +96,9 @@ _SIGS = [
     ("lbm_step", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
     ("lbm_step_begin", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int]),
     ("lbm_step_end", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse)]),
+    ("lbm_voxelize_mesh", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LbmRigidMotion), C.c_void_p,
+                                     C.c_void_p]),
+    ("lbm_retag_cells_mesh", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LbmRigidMotion)]),
     ("lbm_step_frame", C.c_int, [C.c_void_p, C.POINTER(LbmSphere), C.c_int, C.POINTER(LbmImpulse), C.c_void_p]),
     ("lbm_wait_frame_slot", C.c_int, [C.c_void_p]),
     ("lbm_absorb_dead_cells", C.c_int,

@@ -297,6 +297,15 @@ class Sim:
     # momentum exchange comes back as a scan-ordered list of links that is
     # replayed through its applyImpulseAtCell (src/sim.js:517-536).
     def _retag_generic(self, solid):
+        if getattr(solid, "use_device", False) and hasattr(solid, "world_triangles"):
+            # a mesh body (b200lbm.MeshSolid): voxelised on the device
+            tri = np.ascontiguousarray(solid.world_triangles(), dtype=np.float64)
+            m = solid.motion()
+            self._sync()
+            check(self._h, lib().lbm_retag_cells_mesh(self._h, tri.ctypes.data_as(C.c_void_p), len(tri),
+                                                      C.byref(m)))
+            self._moved()
+            return
         mask, us = evaluate_generic(solid, self.nx, self.ny, self.nz)
         self._sync()
         check(self._h, lib().lbm_retag_cells_mask(self._h, mask.ctypes.data_as(C.c_void_p),

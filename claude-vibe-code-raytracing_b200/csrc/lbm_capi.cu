@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "lbm_kernels.cuh"
+#include "lbm_mesh.cuh"
 #include "lbm_render.h"
 #include "lbm_sphere.cuh"
 #include "lbm_state.h"
@@ -459,7 +460,7 @@ void free_all(lbm_sim *h) {
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
                   h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
                   h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan, h->dWatch, h->linkChunks,
-                  h->linkBuf, h->redTickets};
+                  h->linkBuf, h->redTickets, h->meshTri};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, h->stream);
   for (int c = 0; c < 2; c++)
@@ -1065,6 +1066,86 @@ int lbm_retag_cells_mask(lbm_sim *h, const uint8_t *solid_mask, const float *sur
   CKL("retag (mask)");
   CK(cudaStreamSynchronize(h->stream));  // the staging buffer is reused by the next call
   // solid cells may be anywhere: a following fused step retags the whole grid
+  h->fullRetagSteps = 2;
+  h->lastRetagBox = interior(h);
+  h->listsValid = false;
+  return LBM_OK;
+}
+
+// a mesh's cells and surface velocity into the staging buffer (mask at 0, the
+// velocities at *usOff): the whole grid cleared, the mesh's bounding box
+// grown by one cell voxelised
+static int voxelize_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigid_motion *m, size_t *usOff) {
+  const size_t n = (size_t)h->n;
+  *usOff = (n + 255) / 256 * 256;
+  int rc = ensure_staging(h, *usOff + 12 * n);
+  if (rc) return rc;
+  uint8_t *dMask = (uint8_t *)h->staging;
+  float *dUs = (float *)((uint8_t *)h->staging + *usOff);
+  CK(cudaMemsetAsync(dMask, 0, n, h->stream));
+  CK(cudaMemsetAsync(dUs, 0, 12 * n, h->stream));
+  if (ntri == 0) return LBM_OK;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (long long j = 0; j < 3LL * ntri; j++)
+    for (int a = 0; a < 3; a++) {
+      const double v = tri[3 * j + a];
+      if (!(v == v)) return fail(h, LBM_ERR_ARG, "mesh vertex is NaN");
+      lo[a] = std::min(lo[a], v);
+      hi[a] = std::max(hi[a], v);
+    }
+  const int dimsN[3] = {h->nx, h->ny, h->nz};
+  int b0[3], b1[3];
+  for (int a = 0; a < 3; a++) {
+    b0[a] = (int)std::max(0.0, std::floor(lo[a]) - 1.0);
+    b1[a] = (int)std::min((double)dimsN[a] - 1, std::ceil(hi[a]) + 1.0);
+    if (b1[a] < b0[a]) return LBM_OK;  // the mesh lies outside the grid
+  }
+  const size_t tb = (size_t)ntri * 9 * sizeof(double);
+  if (tb > h->meshCap) {
+    if (h->meshTri) {
+      cudaFreeAsync(h->meshTri, h->stream);
+      h->deviceBytes -= h->meshCap;
+      h->meshTri = nullptr;
+    }
+    DALLOC(h->meshTri, tb);
+    h->meshCap = tb;
+  }
+  CK(copy_async(h, h->meshTri, tri, tb, cudaMemcpyHostToDevice, h->stream));
+  const int3 lo3 = make_int3(b0[0], b0[1], b0[2]);
+  const int3 dim3_ = make_int3(b1[0] - b0[0] + 1, b1[1] - b0[1] + 1, b1[2] - b0[2] + 1);
+  const long long cells = (long long)dim3_.x * dim3_.y * dim3_.z;
+  MeshMotion mm{m->cx, m->cy, m->cz, m->vx, m->vy, m->vz, m->wx, m->wy, m->wz};
+  k_voxelize_mesh<<<nblocks(cells, MESH_THREADS), MESH_THREADS, 0, h->stream>>>(
+      (const double *)h->meshTri, ntri, h->nx, h->ny, lo3, dim3_, mm, dMask, dUs);
+  h->launches++;
+  CKL("voxelize mesh");
+  return LBM_OK;
+}
+
+int lbm_voxelize_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigid_motion *m, uint8_t *mask_out,
+                      float *us_out) {
+  if (!h || ntri < 0 || (ntri > 0 && !tri) || !m || !mask_out) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  size_t usOff = 0;
+  int rc = voxelize_mesh(h, tri, ntri, m, &usOff);
+  if (rc) return rc;
+  CK(copy_async(h, mask_out, h->staging, (size_t)h->n, cudaMemcpyDeviceToHost, h->stream));
+  if (us_out)
+    CK(copy_async(h, us_out, (uint8_t *)h->staging + usOff, 12 * (size_t)h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return LBM_OK;
+}
+
+int lbm_retag_cells_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigid_motion *m) {
+  if (!h || ntri < 0 || (ntri > 0 && !tri) || !m) return LBM_ERR_ARG;
+  DeviceGuard g(h->device);
+  int rc = need_phases(h);
+  if (rc) return rc;
+  size_t usOff = 0;
+  if ((rc = voxelize_mesh(h, tri, ntri, m, &usOff))) return rc;
+  h->ops->retag_mask(h, (const uint8_t *)h->staging, (const float *)((uint8_t *)h->staging + usOff));
+  CKL("retag (mesh)");
+  CK(cudaStreamSynchronize(h->stream));  // the staging buffer is reused by the next call
   h->fullRetagSteps = 2;
   h->lastRetagBox = interior(h);
   h->listsValid = false;

@@ -137,6 +137,8 @@ struct lbm_sim {
   double *impAcc = nullptr;  // per-cell impulse slots of every sphere
   long long impCap = 0;      // doubles
   double *partials = nullptr;
+  void *meshTri = nullptr;  // a mesh's triangles for lbm_voxelize_mesh / lbm_retag_cells_mesh
+  size_t meshCap = 0;
   unsigned *redTickets = nullptr;  // [LBM_MAX_SPHERES] last-block tickets of the impulse reduction
   long long partialsCap = 0;  // doubles
   int partialsChunks = 0;

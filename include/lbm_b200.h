@@ -145,6 +145,24 @@ int lbm_handle_fresh_cells(lbm_sim *sim);
  * solid at rest).  Boundary cells become WALL whatever the mask says.  The
  * next fused lbm_step retags the whole grid. */
 int lbm_retag_cells_mask(lbm_sim *sim, const uint8_t *solid_mask, const float *surface_velocity);
+/* A rigid body given as a closed triangle mesh (README.md:65-73: the solid
+ * interface is mesh-agnostic), voxelised on the device.  tri: 9 doubles per
+ * triangle (three vertices, world coordinates in cells); a cell is inside
+ * when the ray from its centre towards +x crosses the mesh an odd number of
+ * times (edge functions with a top-left rule, every operation rounded
+ * explicitly).  Inside cells get the rigid-body surface velocity
+ * v + w x (centre - c) of src/solid.js:57-66 as float. */
+typedef struct {
+  double cx, cy, cz; /* the point the angular velocity turns about */
+  double vx, vy, vz; /* linear velocity */
+  double wx, wy, wz; /* angular velocity */
+} lbm_rigid_motion;
+/* the mask (n bytes) and, with us_out, the surface velocities (3n floats) */
+int lbm_voxelize_mesh(lbm_sim *sim, const double *tri, int ntri, const lbm_rigid_motion *motion,
+                      uint8_t *mask_out, float *us_out);
+/* retagCells for the mesh body: lbm_retag_cells_mask with the mask and
+ * velocities made on the device */
+int lbm_retag_cells_mesh(lbm_sim *sim, const double *tri, int ntri, const lbm_rigid_motion *motion);
 int lbm_compute_phi_gradients(lbm_sim *sim);
 int lbm_collide_phase(lbm_sim *sim);
 int lbm_stream_phase(lbm_sim *sim);
