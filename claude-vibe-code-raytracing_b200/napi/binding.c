@@ -36,6 +36,7 @@ _Static_assert(sizeof(lbm_sphere) == LBM_SPHERE_F64 * sizeof(double), "lbm_spher
 _Static_assert(sizeof(lbm_impulse) == 6 * sizeof(double), "lbm_impulse is 6 doubles");
 _Static_assert(sizeof(lbm_params) == 8 * sizeof(double), "lbm_params is 8 doubles");
 _Static_assert(sizeof(lbm_camera) == 6 * sizeof(double), "lbm_camera is 6 doubles");
+_Static_assert(sizeof(lbm_rigid_motion) == 9 * sizeof(double), "lbm_rigid_motion is 9 doubles");
 
 #define MAX_ARGS 8
 
@@ -417,6 +418,44 @@ static napi_value js_retag_cells_mask(napi_env env, napi_callback_info info) {
   const size_t n = (size_t)nx * ny * nz;
   if (mlen < n || (us && ulen < 3 * n)) return throw_msg(env, LBM_ERR_ARG, "retagCellsMask: n mask bytes, 3n velocities");
   return check_sim(env, h, lbm_retag_cells_mask(h, mask, us));
+}
+
+/* retagCellsMesh(h, Float64Array tri[9 * ntri], Float64Array motion[9]):
+ * retagCells for a rigid triangle mesh, voxelised on the device */
+static napi_value js_retag_cells_mesh(napi_env env, napi_callback_info info) {
+  Args a;
+  if (!args_get(env, info, &a, 3)) return NULL;
+  lbm_sim *h = arg_sim(&a, 0);
+  size_t tlen = 0, mlen = 0;
+  double *tri = (double *)arg_typed(&a, 1, napi_float64_array, &tlen);
+  double *mo = (double *)arg_typed(&a, 2, napi_float64_array, &mlen);
+  if (a.failed) return NULL;
+  if (tlen % 9 != 0 || mlen < 9) return throw_msg(env, LBM_ERR_ARG, "retagCellsMesh: 9 numbers per triangle, 9 of motion");
+  lbm_rigid_motion m;
+  memcpy(&m, mo, sizeof m);
+  return check_sim(env, h, lbm_retag_cells_mesh(h, tri, (int)(tlen / 9), &m));
+}
+
+/* voxelizeMesh(h, tri, motion, Uint8Array mask[n], Float32Array us[3n] | null) */
+static napi_value js_voxelize_mesh(napi_env env, napi_callback_info info) {
+  Args a;
+  if (!args_get(env, info, &a, 4)) return NULL;
+  lbm_sim *h = arg_sim(&a, 0);
+  size_t tlen = 0, mlen = 0, klen = 0, ulen = 0;
+  double *tri = (double *)arg_typed(&a, 1, napi_float64_array, &tlen);
+  double *mo = (double *)arg_typed(&a, 2, napi_float64_array, &mlen);
+  uint8_t *mask = (uint8_t *)arg_typed(&a, 3, napi_uint8_array, &klen);
+  float *us = NULL;
+  if (a.argc > 4 && !is_nullish(&a, 4)) us = (float *)arg_typed(&a, 4, napi_float32_array, &ulen);
+  if (a.failed) return NULL;
+  int nx = 0, ny = 0, nz = 0, st = 0;
+  lbm_get_dims(h, &nx, &ny, &nz, &st);
+  const size_t n = (size_t)nx * ny * nz;
+  if (tlen % 9 != 0 || mlen < 9 || klen < n || (us && ulen < 3 * n))
+    return throw_msg(env, LBM_ERR_ARG, "voxelizeMesh: 9 numbers per triangle, 9 of motion, n mask bytes, 3n velocities");
+  lbm_rigid_motion m;
+  memcpy(&m, mo, sizeof m);
+  return check_sim(env, h, lbm_voxelize_mesh(h, tri, (int)(tlen / 9), &m, mask, us));
 }
 
 /* solidLinks(h, Int32Array cells | null, Int8Array dirs | null, Float64Array mom | null)
@@ -839,6 +878,8 @@ static const napi_property_descriptor kExports[] = {
     FN("seedHydrostatic", js_seed_hydrostatic),
     FN("retagCells", js_retag_cells),
     FN("retagCellsMask", js_retag_cells_mask),
+    FN("retagCellsMesh", js_retag_cells_mesh),
+    FN("voxelizeMesh", js_voxelize_mesh),
     FN("solidLinks", js_solid_links),
     FN("handleFreshCells", js_handle_fresh_cells),
     FN("computePhiGradients", js_compute_phi_gradients),

@@ -154,6 +154,16 @@ export class Sim {
   // hydro stream the device returns the momentum-exchange links in scan order
   // and each is applied through solid.applyImpulseAtCell (src/sim.js:517-536).
   _retagGeneric(solid) {
+    if (solid.useDevice && typeof solid.worldTriangles === 'function') {
+      // a mesh body: voxelised on the device (triangles as 9 numbers each;
+      // motion = cx cy cz vx vy vz wx wy wz)
+      this._sync();
+      addon.retagCellsMesh(this._h, Float64Array.from(solid.worldTriangles()),
+        Float64Array.of(solid.cx, solid.cy, solid.cz, solid.vx, solid.vy, solid.vz,
+                        solid.wx, solid.wy, solid.wz));
+      this._moved();
+      return;
+    }
     const { nx, ny, nz } = this;
     const mask = this._mask ?? (this._mask = new Uint8Array(this.n));
     const us = this._us ?? (this._us = new Float32Array(3 * this.n));

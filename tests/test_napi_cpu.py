@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ADDON = os.path.join(ROOT, "claude-vibe-code-raytracing_b200", "napi", "build", "lbm_b200.node")
 HARNESS = os.path.join(ROOT, "tests", "napi", "build", "harness")
 
-EXPECTED = """create destroy lastError getDims deviceBytes footprintBytes setParams getParams uploadField retagCellsMask solidLinks
+EXPECTED = """create destroy lastError getDims deviceBytes footprintBytes setParams getParams uploadField retagCellsMask retagCellsMesh voxelizeMesh solidLinks
 downloadField downloadFieldF64 initFlat seedHydrostatic retagCells handleFreshCells computePhiGradients
 collidePhase streamPhase collideHydro streamHydroAndMacro step absorbDeadCells packVolume packVolumeAsync
 waitFrames waitFrameSlot stepFrame initProfile runCoupled sphereStep synchronize setNanWatchdog lastSets launchCount checkedBuild faultRecord
