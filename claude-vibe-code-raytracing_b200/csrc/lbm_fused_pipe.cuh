@@ -41,7 +41,6 @@ namespace lbm {
 constexpr int PIPE_STAGED = 1;
 constexpr int PIPE_COMPACT = 2;
 constexpr int PIPE_ASYNC = 3;
-constexpr int PIPE_DIRECT = 4;
 
 // ---------------------------------------------------------------- compact ring
 // Direction k's slot array in one ring copy covers the local columns
@@ -131,7 +130,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
   using SM = PipeSmem<PopT, TY, PF>;
-  constexpr bool STG = SM::STG, ASY = SM::ASY, DIR = PF == PIPE_DIRECT;
+  constexpr bool STG = SM::STG, ASY = SM::ASY;
   using R = PipeRing<TY>;
   using LD = CellLoad<PopT>;
   using CO = CellOut<PopT>;
@@ -514,32 +513,6 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
 
   int q = zb - 1;
   for (; q <= ze; q++) {
-    if constexpr (DIR) {
-      // the direct form: loads, the barrier after which plane q's ring slots
-      // are free, then each cell collided straight into the ring
-      LD L, L2;
-      if (cellWarp) load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
-      else halo_load(q, L, L2);
-      __syncthreads();
-      CO o;
-      Real d0, d1, d2, d3, d4;
-      if (cellWarp) {
-        collide_cell<PopT, 0, 0, 0>(K, L, o, gxN, gyN, gzN, lapN, phN);
-        emit(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, tx, ty, o);
-      } else if (haloRows) {
-        collide_cell<PopT, 1, 0, 1>(K, L, o, d0, d1, d2, d3, d4);
-        emit(IC<1>{}, IC<0>{}, IC<1>{}, 0, 0, true, q, tx, -1, o);
-        collide_cell<PopT, 1, 0, -1>(K, L2, o, d0, d1, d2, d3, d4);
-        emit(IC<1>{}, IC<0>{}, IC<-1>{}, 0, 0, true, q, tx, TY, o);
-      } else if (!sideRight) {
-        collide_cell<PopT, 1, 1, 0>(K, L, o, d0, d1, d2, d3, d4);
-        emit(IC<2>{}, IC<1>{}, IC<0>{}, 1, sideSy, sideAct, q, sideLx - 1, sideLy - 1, o);
-      } else {
-        collide_cell<PopT, 1, -1, 0>(K, L, o, d0, d1, d2, d3, d4);
-        emit(IC<2>{}, IC<-1>{}, IC<0>{}, -1, sideSy, sideAct, q, sideLx - 1, sideLy - 1, o);
-      }
-      __syncthreads();
-    } else {
     CO o;
     if (cellWarp) {
       LD L;
@@ -601,7 +574,6 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     __syncthreads();
     if constexpr (STG) {
       if (*abortF) break;
-    }
     }
 
     // pull plane z = q - 1 (nothing while z < zb)
@@ -798,7 +770,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
 // in shared memory, 6 rows two
 template <int TY, int PF>
 struct PipeOcc {
-  static constexpr int blocks = TY <= 4 || PF == PIPE_DIRECT ? 3 : 2;
+  static constexpr int blocks = TY <= 4 ? 3 : 2;
 };
 
 template <class PopT, int TY, int PF, bool WIDE, bool PACK = false>

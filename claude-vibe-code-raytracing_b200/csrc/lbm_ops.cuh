@@ -280,7 +280,7 @@ class Ops final : public OpsBase {
   // BF16 storage); SHAPE_WIDE marks a launch over a grid whose populations
   // need 64-bit offsets.  f(IC<rows>, IC<form>, wide) is called with the
   // shape's compile-time launch form: 0 plain, PIPE_STAGED, PIPE_COMPACT,
-  // PIPE_ASYNC, PIPE_DIRECT.
+  // PIPE_ASYNC.
   template <class F>
   static void with_shape(int shape, F &&f) {
     const bool wide = (shape & SHAPE_WIDE) != 0;
@@ -299,8 +299,6 @@ class Ops final : public OpsBase {
       case 6 | LBM_FUSED_COMPACT: pipe(IC<6>{}, IC<PIPE_COMPACT>{}); break;
       case 4 | LBM_FUSED_ASYNC: pipe(IC<4>{}, IC<PIPE_ASYNC>{}); break;
       case 6 | LBM_FUSED_ASYNC: pipe(IC<6>{}, IC<PIPE_ASYNC>{}); break;
-      case 4 | LBM_FUSED_DIRECT: pipe(IC<4>{}, IC<PIPE_DIRECT>{}); break;
-      case 6 | LBM_FUSED_DIRECT: pipe(IC<6>{}, IC<PIPE_DIRECT>{}); break;
       case 4 | LBM_FUSED_STAGED: pipe(IC<4>{}, IC<PIPE_STAGED>{}); break;
       case 6 | LBM_FUSED_STAGED: pipe(IC<6>{}, IC<PIPE_STAGED>{}); break;
       default: go(IC<8>{}, IC<0>{}); break;
@@ -311,8 +309,7 @@ class Ops final : public OpsBase {
     if (shape == 2 || shape == 4 || shape == 8) return true;
     const int rows = shape & 0xff, form = shape & ~0xff;
     return kPipe && (rows == 4 || rows == 6) &&
-           (form == LBM_FUSED_COMPACT || form == LBM_FUSED_ASYNC || form == LBM_FUSED_STAGED ||
-            form == LBM_FUSED_DIRECT);
+           (form == LBM_FUSED_COMPACT || form == LBM_FUSED_ASYNC || form == LBM_FUSED_STAGED);
   }
   // shared memory, warps and kernels of a launch form
   template <int TY, int FORM>
@@ -448,8 +445,7 @@ class Ops final : public OpsBase {
   }
   void warm(int device) override {
     static const int shapes[] = {2, 4, 8, 4 | LBM_FUSED_COMPACT, 6 | LBM_FUSED_COMPACT, 4 | LBM_FUSED_ASYNC,
-                                 6 | LBM_FUSED_ASYNC, 4 | LBM_FUSED_STAGED, 6 | LBM_FUSED_STAGED,
-                                 4 | LBM_FUSED_DIRECT, 6 | LBM_FUSED_DIRECT};
+                                 6 | LBM_FUSED_ASYNC, 4 | LBM_FUSED_STAGED, 6 | LBM_FUSED_STAGED};
     for (int sh : shapes) {
       if (!shape_ok(sh)) continue;
       with_shape(sh, [&](auto T, auto S, auto W) {

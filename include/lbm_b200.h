@@ -328,9 +328,6 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
  *   rows = 4 or 6 | LBM_FUSED_ASYNC: the compact ring, each thread's loads of
  *     the next plane issued one plane ahead as per-thread asynchronous copies
  *     into shared memory (FP32/FP16/BF16);
- *   rows = 4 or 6 | LBM_FUSED_DIRECT: the compact ring, each plane collided
- *     after the barrier that frees its ring slots and written straight into
- *     the ring (fewer registers: three CTAs per SM at 6 rows);
  *   rows = 4 or 6 | LBM_FUSED_STAGED: the compact ring, the tile rows of the
  *     next plane staged by bulk asynchronous copies waited on with bounded
  *     mbarrier waits (FP32/FP16/BF16).
@@ -338,7 +335,6 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
 #define LBM_FUSED_STAGED 0x100
 #define LBM_FUSED_COMPACT 0x400
 #define LBM_FUSED_ASYNC 0x800
-#define LBM_FUSED_DIRECT 0x1000
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
 /* ---- one scene in z slabs (several handles, one or more GPUs) -------------- */
 /* Declares the handle a z slab of a larger scene: its local plane k is the

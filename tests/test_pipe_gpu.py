@@ -18,10 +18,8 @@ pytestmark = pytest.mark.gpu
 STAGED = 0x100
 COMPACT = 0x400
 ASYNC = 0x800
-DIRECT = 0x1000
 PIPE_SHAPES = ((4 | STAGED, 32), (6 | STAGED, 32), (4 | STAGED, 5), (6 | STAGED, 9), (4 | COMPACT, 32),
-               (6 | COMPACT, 7), (6 | ASYNC, 32), (4 | ASYNC, 6), (6 | ASYNC, 5), (6 | DIRECT, 32),
-               (4 | DIRECT, 7))
+               (6 | COMPACT, 7), (6 | ASYNC, 32), (4 | ASYNC, 6), (6 | ASYNC, 5))
 
 
 @pytest.fixture(scope="module")
