@@ -48,7 +48,7 @@ struct FusedArgs {
   double om, omP, A, beta4, kappa, rhoG, dRho, gravity, sharpC4;
   const SolidSet *ss;
   int *status;   // set non-zero when a bounded wait of the step runs out
-  int withhold;  // test hook: the staged form does not issue each tile's first copy
+  int withhold;  // test hook: the bulk-staged form does not issue each tile's first copy
   uint8_t *pack; // frame step: the RG8 volume of the step's result (planes 1 .. nz-2), else null
 };
 
@@ -67,35 +67,20 @@ constexpr int RING_F_M = 0, RING_F_Z = 18, RING_F_P = 36;  // 2x9, 2x9, 3x9
 constexpr int RING_H_M = 63, RING_H_Z = 65, RING_H_P = 75;  // 2x1, 2x5, 3x1
 constexpr int RING_PLANES = 78;
 
-// Shared memory of one CTA: the post-collision ring, the tags of three planes
-// and, in the staged form (STG: FP16/BF16 storage, 4 rows), a staging buffer
-// that receives the tile rows' raw populations of a plane by bulk
-// asynchronous copy, plus its mbarrier and an abort flag.  A
-// 32-cell row starts anywhere inside an 8-cell block, so it spans at most
-// SB = 5 whole blocks.  The staged form is a tile shape of its own
-// (LBM_FUSED_STAGED), chosen where it measures faster.
-template <class PopT, int TY, bool STG = false>
+// Shared memory of one CTA: the post-collision ring (78 planes of the
+// halo-padded tile) and the tags of three planes.
+template <class PopT, int TY>
 struct FusedSmem {
   using Real = typename Prec<PopT>::Real;
   static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;
-  static constexpr bool STAGE = STG && TY == 4 && sizeof(PopT) == 2;
-  static constexpr int NBUF = 1;  // the buffer of plane q + 1 is filled while plane q is pulled
-  static constexpr int SB = 5;
-  static constexpr int ROWF = SB * PopGroups<Q27>::BLOCK, ROWH = SB * PopGroups<Q7>::BLOCK;  // per staged row
   static constexpr size_t ringBytes = (size_t)RING_PLANES * NC * sizeof(Real);
-  static constexpr size_t stageOff = (ringBytes + 3 * NC + 15) / 16 * 16;
-  static constexpr size_t bufBytes = STAGE ? (size_t)TY * (ROWF + ROWH) * sizeof(PopT) : 0;
-  static constexpr size_t barOff = stageOff + NBUF * bufBytes;
-  static constexpr size_t bytes = STAGE ? barOff + 32 : ringBytes + 3 * NC;
+  static constexpr size_t bytes = ringBytes + 3 * NC;
   static constexpr int warps = TY + 2;  // TY cell warps, 2 halo warps
   static constexpr int threads = 32 * warps;
-  static_assert((ROWF * sizeof(PopT)) % 16 == 0 && (ROWH * sizeof(PopT)) % 16 == 0,
-                "bulk copies move whole 16-byte units");
 };
 
-// CTAs per SM the register budget is sized for (the staged 4-row form, with
-// its staging buffer beside the ring, still fits 3 per SM)
-template <class PopT, int TY, bool STG = false>
+// CTAs per SM the register budget is sized for
+template <class PopT, int TY>
 struct FusedOcc {
   static constexpr int blocks = TY >= 8 ? 2 : (TY >= 4 ? 3 : 5);
 };
@@ -452,23 +437,18 @@ __device__ __forceinline__ void collide_cell(const CollK<typename Prec<PopT>::Re
 // One tile (bx, by) of 32 x TY columns over z-chunk bz of one scene.
 // WIDE: 64-bit population offsets, for grids whose populations exceed 2^31
 // elements (more than ~76 M cells); 32-bit offsets otherwise.
-template <class PopT, int TY, bool STG, bool WIDE, bool PACK = false>
+template <class PopT, int TY, bool WIDE, bool PACK = false>
 __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int by, int bz) {
   using POff = std::conditional_t<WIDE, long long, int>;
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
-  using SM = FusedSmem<PopT, TY, STG>;
+  using SM = FusedSmem<PopT, TY>;
   using LD = CellLoad<PopT>;
   using CO = CellOut<PopT>;
   constexpr int RX = SM::RX, NC = SM::NC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real *ring = reinterpret_cast<Real *>(smem_raw);                        // [78][NC]
   uint8_t *stag = smem_raw + SM::ringBytes;                               // [3][NC]
-  constexpr bool STAGE = SM::STAGE;
-  constexpr int ROWF = SM::ROWF, ROWH = SM::ROWH, BUF = TY * (ROWF + ROWH), NBUF = SM::NBUF;
-  PopT *stage = reinterpret_cast<PopT *>(smem_raw + SM::stageOff);        // [2][TY rows F, TY rows H]
-  int *abortF = reinterpret_cast<int *>(smem_raw + SM::barOff + 16);
-  const uint32_t bar0 = smem_u32(smem_raw + SM::barOff);  // mbarrier of buffer b at bar0 + 8b
 
   const auto &s = a.s;
   const SolidSet &ss = *a.ss;
@@ -584,72 +564,6 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     load_small(q, gx_, gy_, L);
   };
 
-  // ---- staging of the tile rows' populations (staged form)
-  // Row r of plane q covers cells row0 .. row0 + min(31, nx - 1 - x0) of the
-  // flat order, i.e. whole blocks (row0 >> 3) .. (last >> 3): one bulk copy
-  // for f and one for h, into buffer q & 1.  Rows past the grid are skipped.
-  const bool producer = STAGE && ty == TY + 1 && tx == 31;  // an idle lane of halo warp B
-  auto issue = [&](int q) __attribute__((always_inline)) {
-    const int buf = q % NBUF;
-    const uint32_t bar = bar0 + 8 * buf;
-    const int span = min(31, nx - 1 - x0);
-    uint32_t total = 0;
-    for (int r = 0; r < TY; r++) {
-      if (y0 + r >= ny) break;
-      const int row0 = (q * ny + y0 + r) * nx + x0;
-      total += (uint32_t)(((row0 + span) >> 3) - (row0 >> 3) + 1) * (BLK27 + BLK7) * sizeof(PopT);
-    }
-    mbar_expect(bar, total);
-    for (int r = 0; r < TY; r++) {
-      if (y0 + r >= ny) break;
-      const int row0 = (q * ny + y0 + r) * nx + x0;
-      const int b0 = row0 >> 3, nb = ((row0 + span) >> 3) - b0 + 1;
-      const bool ok = lbm_ok(nb <= SM::SB, 20, nb) &&
-                      lbm_ok((long long)(b0 + nb) * BLK27 <= nF, 21, b0);
-      if (!ok) continue;
-      bulk_g2s(smem_u32(stage + buf * BUF + r * ROWF), Fc + (long long)b0 * BLK27,
-               (uint32_t)(nb * BLK27 * sizeof(PopT)), bar);
-      bulk_g2s(smem_u32(stage + buf * BUF + TY * ROWF + r * ROWH), Hc + (long long)b0 * BLK7,
-               (uint32_t)(nb * BLK7 * sizeof(PopT)), bar);
-    }
-  };
-  uint32_t phase = 0;  // parity of the next wait, one bit per buffer
-  auto stage_wait = [&](int q) __attribute__((always_inline)) {
-    const int buf = q % NBUF;
-    const uint32_t par = (phase >> buf) & 1u;
-    phase ^= 1u << buf;
-    if (!haloWarp && !mbar_wait(bar0 + 8 * buf, par)) {
-      record_stage_timeout(q);
-      if (a.status) atomicOr(a.status, 1);
-      *abortF = 1;
-    }
-  };
-  // a cell thread's populations of plane q from the staging buffer
-  auto stage_pops = [&](int q, LD &L) __attribute__((always_inline)) {
-    const PopT *sF = stage + (q % NBUF) * BUF + ty * ROWF;
-    const PopT *sH = stage + (q % NBUF) * BUF + TY * ROWF + ty * ROWH;
-    const int row0 = (q * ny + y) * nx + x0;
-    const bool inside = x < nx && y < ny;
-    const int off = inside ? ((row0 + tx) >> 3) - (row0 >> 3) : 0;
-    const int e = inside ? ((row0 + tx) & 7) : 0;
-    static_for<0, G27>([&](auto GG) {
-      constexpr int g = decltype(GG)::value;
-      PopT t[4];
-      ld4_shared(sF + sm_at((off * G27 + g) * 32 + e * 4, ROWF - 3, 22), t);
-      static_for<4 * g, (4 * g + 4 < Q27 ? 4 * g + 4 : Q27)>([&](auto KK) {
-        constexpr int k = decltype(KK)::value;
-        L.fv[k] = t[k & 3];
-      });
-      if constexpr (g < G7) {
-        ld4_shared(sH + sm_at((off * G7 + g) * 32 + e * 4, ROWH - 3, 23), t);
-        static_for<4 * g, (4 * g + 4 < Q7 ? 4 * g + 4 : Q7)>([&](auto KK) {
-          constexpr int k = decltype(KK)::value;
-          L.hv[k] = t[k & 3];
-        });
-      }
-    });
-  };
-
   // Emit phase: the collided values and the tag of a cell into ring cell lc of
   // plane q.  Values computed for non-fluid cells land in ring slots that are
   // never read as sources.
@@ -689,13 +603,6 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   // and below the tile (both rows loaded before either is computed); halo
   // warp B the side columns and corners.
   // (lambdas are forced inline: an outlined closure would live in local memory)
-  // Staged form: the cell warps' phi stencil, rho, u and tag of plane q are
-  // loaded one plane early (prefetch) into Lc; their populations arrive in
-  // the staging buffer; the halo warps load as in the plain form.
-  LD Lc;
-  auto prefetch = [&](int q) __attribute__((always_inline)) {
-    if (!haloWarp) load_small(q, x, y, Lc);
-  };
   auto halo_plane = [&](int q, CO &o) __attribute__((always_inline)) {
     Real d0, d1, d2, d3, d4;
     if (haloA) {
@@ -710,23 +617,11 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       compute(IC<2>{}, IC<0>{}, IC<0>{}, L, o, d0, d1, d2, d3, d4);
     }
   };
-  auto collide_staged = [&](int q, CO &o, Real &ogx, Real &ogy, Real &ogz, Real &olap,
-                            Real &ophi) __attribute__((always_inline)) {
-    stage_wait(q);
-    if (!haloWarp) {
-      stage_pops(q, Lc);
-      compute(IC<0>{}, IC<0>{}, IC<0>{}, Lc, o, ogx, ogy, ogz, olap, ophi);
-    } else {
-      halo_plane(q, o);
-    }
-  };
   // collide plane q into registers (o: a cell warp's cell, halo warp A's two
   // rows, halo warp B's side cell) ...
   auto collide_plane = [&](int q, CO &o, Real &ogx, Real &ogy, Real &ogz, Real &olap,
                            Real &ophi) __attribute__((always_inline)) {
-    if constexpr (STAGE) {
-      collide_staged(q, o, ogx, ogy, ogz, olap, ophi);
-    } else if (!haloWarp) {
+    if (!haloWarp) {
       LD L;
       load(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, x, y, L);
       compute(IC<0>{}, IC<0>{}, IC<0>{}, L, o, ogx, ogy, ogz, olap, ophi);
@@ -750,46 +645,19 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   Real gxN = 0, gyN = 0, gzN = 0, lapN = 0, phN = 0;
   const bool colActive = !haloWarp && x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
 
-  if constexpr (STAGE) {
-    if (producer) {
-      for (int b = 0; b < NBUF; b++) mbar_init(bar0 + 8 * b);
-      mbar_init_fence();
-      *abortF = 0;
-    }
-    __syncthreads();
-    if (producer)
-      for (int b = 0; b < NBUF; b++)
-        if (!(a.withhold && b == 0)) issue(zb - 1 + b);
-    prefetch(zb - 1);
-  }
-
   // Iteration q collides plane q and pulls plane q - 1 (planes zb-1 .. ze are
-  // collided, zb .. ze-1 pulled).  Plain form: load and collide plane q into
-  // registers, barrier (every warp has pulled plane q - 2), write the ring,
-  // barrier, pull plane q - 1.  Staged form: collide into the ring, barrier,
-  // pull, barrier.  In the staged form the copy of plane q + 1
-  // goes out as soon as plane q's buffer is read (after the first barrier),
-  // and the cell warps' register loads of plane q + 1 right after plane q's
-  // collision.
-  int q = zb - 1;
-  for (; q <= ze; q++) {
+  // collided, zb .. ze-1 pulled): load and collide plane q into registers,
+  // barrier (every warp has pulled plane q - 2), write the ring, barrier, pull
+  // plane q - 1.
+  for (int q = zb - 1; q <= ze; q++) {
     CO o;
     collide_plane(q, o, gxN, gyN, gzN, lapN, phN);
-    if constexpr (STAGE) {
-      emit_plane(q, o);
-      if (q < ze) prefetch(q + 1);
-    } else {
-      // plane q's slots of the ring are free once every warp has pulled
-      // plane q - 2; a warp that gets here early has its loads and collision
-      // of plane q behind it
-      __syncthreads();
-      emit_plane(q, o);
-    }
+    // plane q's slots of the ring are free once every warp has pulled plane
+    // q - 2; a warp that gets here early has its loads and collision of plane
+    // q behind it
     __syncthreads();
-    if constexpr (STAGE) {
-      if (*abortF) break;
-      if (producer && q + NBUF <= ze) issue(q + NBUF);
-    }
+    emit_plane(q, o);
+    __syncthreads();
     // pull plane z = q - 1 (nothing while z < zb)
     const int z = q - 1;
     const int sC = (z + 3) % 3;
@@ -960,41 +828,29 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       // current after the step
       if (lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(s.phi[nxt], i, nCell, 12), false);
     }
-    if constexpr (STAGE) __syncthreads();
     gxC = gxN;
     gyC = gyN;
     gzC = gzN;
     lapC = lapN;
     phC = phN;
   }
-
-  if constexpr (STAGE) {
-    if (q <= ze && producer) {
-      // stopped at plane q: let the copy of plane q land (bounded) before the
-      // buffer is released (the copy of plane q + 1 was not issued)
-      if (!(a.withhold && q == zb - 1)) mbar_wait(bar0 + 8 * (q % NBUF), ((phase >> (q % NBUF)) & 1u) ^ 1u);
-    }
-    __syncthreads();
-    if (producer)
-      for (int b = 0; b < NBUF; b++) mbar_inval(bar0 + 8 * b);
-  }
 }
 
 // One scene: the grid is its tiles.
 // PACK: the instance launched on frame steps, which also writes the RG8
 // volume; the other steps run an instance without that code
-template <class PopT, int TY, bool STG, bool WIDE, bool PACK = false>
-__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks)
+template <class PopT, int TY, bool WIDE, bool PACK = false>
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY>::blocks)
     k_fused_step(const __grid_constant__ FusedArgs<PopT> a) {
-  fused_tile<PopT, TY, STG, WIDE, PACK>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fused_tile<PopT, TY, WIDE, PACK>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Many scenes in one persistent launch: tile w of the batch belongs to the
 // scene s with tileStart[s] <= w < tileStart[s+1]; each scene's descriptor
 // gives its own grid, physics constants and state.  CTAs stride over the
 // tiles, so one launch of about one wave advances every scene by a step.
-template <class PopT, int TY, bool STG, bool WIDE>
-__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks)
+template <class PopT, int TY, bool WIDE>
+__global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY>::blocks)
     k_fused_batch(const FusedArgs<PopT> *__restrict__ args, const int *__restrict__ tileStart,
                   const int3 *__restrict__ tileGrid, int nscenes) {
   const int total = tileStart[nscenes];
@@ -1017,7 +873,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), FusedOcc<PopT, TY, STG>::blocks
     if (lin < WORDS)
       reinterpret_cast<uint32_t *>(&sa)[lin] = reinterpret_cast<const uint32_t *>(args + lo)[lin];
     __syncthreads();
-    fused_tile<PopT, TY, STG, WIDE>(sa, bx, by, bz);
+    fused_tile<PopT, TY, WIDE>(sa, bx, by, bz);
     __syncthreads();  // the next tile reuses shared memory
   }
 }

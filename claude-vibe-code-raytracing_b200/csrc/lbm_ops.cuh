@@ -314,22 +314,22 @@ class Ops final : public OpsBase {
   // shared memory, warps and kernels of a launch form
   template <int TY, int FORM>
   static constexpr size_t smem_of() {
-    if constexpr (FORM == 0) return FusedSmem<PopT, TY, false>::bytes;
+    if constexpr (FORM == 0) return FusedSmem<PopT, TY>::bytes;
     else return PipeSmem<PopT, TY, FORM>::bytes;
   }
   template <int TY, int FORM>
   static constexpr int warps_of() {
-    if constexpr (FORM == 0) return FusedSmem<PopT, TY, false>::warps;
+    if constexpr (FORM == 0) return FusedSmem<PopT, TY>::warps;
     else return PipeSmem<PopT, TY, FORM>::warps;
   }
   template <int TY, int FORM, bool WIDE, bool PACK = false>
   static auto step_kernel() {
-    if constexpr (FORM == 0) return k_fused_step<PopT, TY, false, WIDE, PACK>;
+    if constexpr (FORM == 0) return k_fused_step<PopT, TY, WIDE, PACK>;
     else return k_fused_pipe<PopT, TY, FORM, WIDE, PACK>;
   }
   template <int TY, int FORM, bool WIDE>
   static auto batch_kernel() {
-    if constexpr (FORM == 0) return k_fused_batch<PopT, TY, false, WIDE>;
+    if constexpr (FORM == 0) return k_fused_batch<PopT, TY, WIDE>;
     else return k_fused_pipe_batch<PopT, TY, FORM, WIDE>;
   }
 
