@@ -875,10 +875,13 @@ int lbm_upload_field(lbm_sim *h, int field, const void *host, size_t count) {
     case LBM_FIELD_UY:
     case LBM_FIELD_UZ: {
       int a = field - LBM_FIELD_RHO + 1;
+      const bool pad = (field == LBM_FIELD_UX || field == LBM_FIELD_UY) && h->ops->u_in_pads();
       for (int c = 0; c < 2; c++) {
         int rc = put_scalar(h, h->mac[c][a], src);
         if (rc) return rc;
+        if (pad) h->ops->u_array(h, field - LBM_FIELD_UX, c, h->mac[c][a], true);
       }
+      CKL("upload u");
       CK(cudaStreamSynchronize(h->stream));
       return LBM_OK;
     }
@@ -930,7 +933,12 @@ int lbm_download_field(lbm_sim *h, int field, void *host, size_t count) {
     case LBM_FIELD_UX:
     case LBM_FIELD_UY:
     case LBM_FIELD_UZ:
-      // macro slots: 0 phi, 1 rho, 2 ux, 3 uy, 4 uz
+      // macro slots: 0 phi, 1 rho, 2 ux, 3 uy, 4 uz (ux, uy gathered first
+      // from the population pads where the storage form keeps them there)
+      if ((field == LBM_FIELD_UX || field == LBM_FIELD_UY) && h->ops->u_in_pads()) {
+        h->ops->u_array(h, field - LBM_FIELD_UX, h->cur, h->mac[h->cur][field - LBM_FIELD_RHO + 1], false);
+        CKL("download u");
+      }
       return get_scalar(h, h->mac[h->cur][field == LBM_FIELD_PHI ? 0 : field - LBM_FIELD_RHO + 1], dst);
     default: {
       void *arr = nullptr;
@@ -972,6 +980,10 @@ int lbm_download_field_f64(lbm_sim *h, int field, double *host, size_t count) {
     return LBM_OK;
   }
   const void *arr = nullptr;
+  if ((field == LBM_FIELD_UX || field == LBM_FIELD_UY) && h->ops->u_in_pads()) {
+    h->ops->u_array(h, field - LBM_FIELD_UX, h->cur, h->mac[h->cur][field - LBM_FIELD_RHO + 1], false);
+    CKL("download u");
+  }
   if (field == LBM_FIELD_PHI_PREV) arr = h->mac[1 - h->cur][0];
   else if (field >= LBM_FIELD_RHO && field <= LBM_FIELD_PHI)
     arr = h->mac[h->cur][field == LBM_FIELD_PHI ? 0 : field - LBM_FIELD_RHO + 1];

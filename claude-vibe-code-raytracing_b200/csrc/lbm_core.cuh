@@ -193,6 +193,30 @@ struct Scene {
   Real *gx, *gy, *gz, *lap;
   Real *usx, *usy, *usz;
   Real *bfx, *bfy, *bfz;  // body force; null when never set
+
+  // Where ux and uy live.  When a population is as wide as a macro (FP32 and
+  // FP64 storage) they take the pad slots of the last direction group of f
+  // (element 27) and of h (element 7), which every step reads and writes with
+  // their groups anyway, so the step moves 16 B (FP32) less per cell than
+  // with separate arrays; the 16-bit forms keep the ux, uy arrays.  Every
+  // access goes through these four functions.
+  static constexpr bool UPAD = sizeof(PopT) == sizeof(Real);
+  __device__ __forceinline__ Real ux_at(int c, long long i) const {
+    if constexpr (UPAD) return (Real)F[c][pidx<27>(27, i)];
+    else return ux[c][i];
+  }
+  __device__ __forceinline__ Real uy_at(int c, long long i) const {
+    if constexpr (UPAD) return (Real)H[c][pidx<7>(7, i)];
+    else return uy[c][i];
+  }
+  __device__ __forceinline__ void set_ux(int c, long long i, Real v) const {
+    if constexpr (UPAD) F[c][pidx<27>(27, i)] = (PopT)v;
+    else ux[c][i] = v;
+  }
+  __device__ __forceinline__ void set_uy(int c, long long i, Real v) const {
+    if constexpr (UPAD) H[c][pidx<7>(7, i)] = (PopT)v;
+    else uy[c][i] = v;
+  }
 };
 
 // Scalar physics parameters, precomputed on the host in double

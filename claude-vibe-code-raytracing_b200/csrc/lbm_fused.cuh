@@ -461,6 +461,8 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
   const Real *__restrict__ rhoC = s.rho[cur];
   const Real *__restrict__ uxC = s.ux[cur];
   const Real *__restrict__ uyC = s.uy[cur];
+  // ux, uy in the pad slots of f's and h's last groups (FP32 / FP64 storage)
+  constexpr bool UPAD = Scene<PopT, Real>::UPAD;
   const Real *__restrict__ uzC = s.uz[cur];
   const uint8_t *__restrict__ tagA = s.tag;
   const int nx = s.nx, ny = s.ny, nz = s.nz, nxny = nx * ny;
@@ -524,8 +526,13 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
     L.pzp = ldg_at(phiC, min(ci + nxny, last), nCell, 5);
     L.pzm = ldg_at(phiC, max(ci - nxny, 0), nCell, 5);
     L.sumF = ldg_at(rhoC, ci, nCell, 6);
-    L.ux = ldg_at(uxC, ci, nCell, 6);
-    L.uy = ldg_at(uyC, ci, nCell, 6);
+    if constexpr (UPAD) {
+      L.ux = (Real)ldg_at(Fc, (long long)(ci >> 3) * BLK27 + (ci & 7) * 4 + pofs(27), nF, 6);
+      L.uy = (Real)ldg_at(Hc, (long long)(ci >> 3) * BLK7 + (ci & 7) * 4 + pofs(7), nH, 6);
+    } else {
+      L.ux = ldg_at(uxC, ci, nCell, 6);
+      L.uy = ldg_at(uyC, ci, nCell, 6);
+    }
     L.uz = ldg_at(uzC, ci, nCell, 6);
     // boundary cells never act as fluid (they are walls after any retag)
     const bool inner = gx_ >= 1 && gx_ <= nx - 2 && gy_ >= 1 && gy_ <= ny - 2 && q >= 1 && q <= nz - 2;
@@ -682,8 +689,10 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       }
       st_at(s.phi[nxt], i, nCell, 12, ldg_at(phiC, i, nCell, 12));
       st_at(s.rho[nxt], i, nCell, 12, ldg_at(rhoC, i, nCell, 12));
-      st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
-      st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
+      if constexpr (!UPAD) {  // (in the pads, copied with the groups above)
+        st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
+        st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
+      }
       st_at(s.uz[nxt], i, nCell, 12, ldg_at(uzC, i, nCell, 12));
       if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
     } else if (tagI == TAG_FLUID) {
@@ -819,8 +828,14 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
       }
       st_at(s.rho[nxt], i, nCell, 18, rhoN);
       st_at(s.phi[nxt], i, nCell, 18, p);
-      st_at(s.ux[nxt], i, nCell, 18, uxn);
-      st_at(s.uy[nxt], i, nCell, 18, uyn);
+      if constexpr (UPAD) {
+        // into the pads of the groups stored above (the same sectors)
+        st_at(Fn, bF + pofs(27), nF, 18, (PopT)uxn);
+        st_at(Hn, bH + pofs(7), nH, 18, (PopT)uyn);
+      } else {
+        st_at(s.ux[nxt], i, nCell, 18, uxn);
+        st_at(s.uy[nxt], i, nCell, 18, uyn);
+      }
       st_at(s.uz[nxt], i, nCell, 18, uzn);
       if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
     } else if (PACK && !haloWarp && x < nx && y < ny && z >= zb) {

@@ -161,6 +161,8 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   const Real *__restrict__ rhoC = s.rho[cur];
   const Real *__restrict__ uxC = s.ux[cur];
   const Real *__restrict__ uyC = s.uy[cur];
+  // ux, uy in the pad slots of f's and h's last groups (FP32 / FP64 storage)
+  constexpr bool UPAD = Scene<PopT, Real>::UPAD;
   const Real *__restrict__ uzC = s.uz[cur];
   const uint8_t *__restrict__ tagA = s.tag;
   const int nx = s.nx, ny = s.ny, nz = s.nz, nxny = nx * ny;
@@ -241,8 +243,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     L.pzp = ldg_at(phiC, min(ci + nxny, last), nCell, 5);
     L.pzm = ldg_at(phiC, max(ci - nxny, 0), nCell, 5);
     L.sumF = ldg_at(rhoC, ci, nCell, 6);
-    L.ux = ldg_at(uxC, ci, nCell, 6);
-    L.uy = ldg_at(uyC, ci, nCell, 6);
+    if constexpr (UPAD) {
+      L.ux = (Real)ldg_at(Fc, (long long)(ci >> 3) * BLK27 + (ci & 7) * 4 + pofs(27), nF, 6);
+      L.uy = (Real)ldg_at(Hc, (long long)(ci >> 3) * BLK7 + (ci & 7) * 4 + pofs(7), nH, 6);
+    } else {
+      L.ux = ldg_at(uxC, ci, nCell, 6);
+      L.uy = ldg_at(uyC, ci, nCell, 6);
+    }
     L.uz = ldg_at(uzC, ci, nCell, 6);
     const bool inner = gx_ >= 1 && gx_ <= nx - 2 && gy_ >= 1 && gy_ <= ny - 2 && q >= 1 && q <= nz - 2;
     if (!inside || (!inner && tg == TAG_FLUID)) tg = TAG_WALL;
@@ -360,8 +367,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     });
     const int mi = sm_at((int)(rowlo & 3u) + t, MROW, 37);
     L.sumF = sM[(0 * TY + ty) * MROW + mi];
-    L.ux = sM[(1 * TY + ty) * MROW + mi];
-    L.uy = sM[(2 * TY + ty) * MROW + mi];
+    if constexpr (UPAD) {  // in the pads of the staged rows' last groups
+      L.ux = (Real)f[sm_at((off * G27 + 6) * 32 + e * 4 + 3, ROWF, 35)];
+      L.uy = (Real)h[sm_at((off * G7 + 1) * 32 + e * 4 + 3, ROWH, 36)];
+    } else {
+      L.ux = sM[(1 * TY + ty) * MROW + mi];
+      L.uy = sM[(2 * TY + ty) * MROW + mi];
+    }
     L.uz = sM[(3 * TY + ty) * MROW + mi];
     uint8_t tg = sT[ty * TROW + sm_at((int)(rowlo & 15u) + t, TROW, 38)];
     // phi stencil: staged rows ty (y - 1), ty + 1 (y), ty + 2 (y + 1) of plane
@@ -451,9 +463,11 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
                              min(ci + nxny, last), max(ci - nxny, 0), ci, ci, ci, ci};
     const Real *arr[SM::NS] = {phiC, phiC, phiC, phiC, phiC, phiC, phiC, rhoC, uxC, uyC, uzC};
 #pragma unroll
-    for (int j = 0; j < SM::NS; j++)
+    for (int j = 0; j < SM::NS; j++) {
+      if (UPAD && (j == 8 || j == 9)) continue;  // ux, uy arrive in the pads of the group slots
       if (lbm_ok(src[j] >= 0 && src[j] < nCell, j < 7 ? 5 : 6, src[j]))
         cp_async<4>(smem_u32(aS + j * NT + lin), arr[j] + src[j]);
+    }
     cp_async_commit();
     tgq = ldg_at(tagA, ci, nCell, 1);
   };
@@ -483,8 +497,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     L.pzp = aS[5 * NT + lin];
     L.pzm = aS[6 * NT + lin];
     L.sumF = aS[7 * NT + lin];
-    L.ux = aS[8 * NT + lin];
-    L.uy = aS[9 * NT + lin];
+    if constexpr (UPAD) {
+      L.ux = (Real)aF[(6 * NT + lin) * 4 + 3];
+      L.uy = (Real)aH[(1 * NT + lin) * 4 + 3];
+    } else {
+      L.ux = aS[8 * NT + lin];
+      L.uy = aS[9 * NT + lin];
+    }
     L.uz = aS[10 * NT + lin];
     uint8_t tg = tgq;
     const bool inside = x < nx && y < ny;
@@ -600,8 +619,10 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       }
       st_at(s.phi[nxt], i, nCell, 12, ldg_at(phiC, i, nCell, 12));
       st_at(s.rho[nxt], i, nCell, 12, ldg_at(rhoC, i, nCell, 12));
-      st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
-      st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
+      if constexpr (!UPAD) {  // (in the pads, copied with the groups above)
+        st_at(s.ux[nxt], i, nCell, 12, ldg_at(uxC, i, nCell, 12));
+        st_at(s.uy[nxt], i, nCell, 12, ldg_at(uyC, i, nCell, 12));
+      }
       st_at(s.uz[nxt], i, nCell, 12, ldg_at(uzC, i, nCell, 12));
       if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, ldg_at(phiC, i, nCell, 12), true);
     } else if (tagI == TAG_FLUID) {
@@ -737,8 +758,14 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       }
       st_at(s.rho[nxt], i, nCell, 18, rhoN);
       st_at(s.phi[nxt], i, nCell, 18, p);
-      st_at(s.ux[nxt], i, nCell, 18, uxn);
-      st_at(s.uy[nxt], i, nCell, 18, uyn);
+      if constexpr (UPAD) {
+        // into the pads of the groups stored above (the same sectors)
+        st_at(Fn, bF + pofs(27), nF, 18, (PopT)uxn);
+        st_at(Hn, bH + pofs(7), nH, 18, (PopT)uyn);
+      } else {
+        st_at(s.ux[nxt], i, nCell, 18, uxn);
+        st_at(s.uy[nxt], i, nCell, 18, uyn);
+      }
       st_at(s.uz[nxt], i, nCell, 18, uzn);
       if (PACK && lbm_ok(i < nCell, 50, i)) pack_rg8(a.pack, i, p, false);
     } else if (PACK && cellWarp && x < nx && y < ny && z >= zb) {

@@ -83,7 +83,9 @@ __global__ void k_init_flat(Scene<PopT, typename Prec<PopT>::Real> s, const doub
   for (int c = 0; c < 2; c++) {
     s.phi[c][i] = phiR;
     s.rho[c][i] = (Real)1.0;
-    s.ux[c][i] = s.uy[c][i] = s.uz[c][i] = (Real)0;
+    s.set_ux(c, i, (Real)0);
+    s.set_uy(c, i, (Real)0);
+    s.uz[c][i] = (Real)0;
     for (int k = 0; k < Q27; k++) {
       Real w = (Real)w27_of(k);
       s.F[c][pidx<27>(k, i)] = Codec<PopT>::enc(w, w);
@@ -209,7 +211,7 @@ __global__ void k_collide_phase(Scene<PopT, typename Prec<PopT>::Real> s, int cu
   const Real sharpC = (Real)k.sharpC;
   const Real sharpFac = (Real)4.0;
   Real p = s.phi[cur][i];
-  Real uxi = s.ux[cur][i], uyi = s.uy[cur][i], uzi = s.uz[cur][i];
+  Real uxi = s.ux_at(cur, i), uyi = s.uy_at(cur, i), uzi = s.uz[cur][i];
   Real ggx = s.gx[i], ggy = s.gy[i], ggz = s.gz[i];
   Real gmag = sqrt(ggx * ggx + ggy * ggy + ggz * ggz) + (Real)1e-12;
   Real sharpen = sharpC * p * ((Real)1 - p);
@@ -260,7 +262,7 @@ __global__ void k_collide_hydro(Scene<PopT, typename Prec<PopT>::Real> s, int cu
   Real fx = bx + mu * s.gx[i];
   Real fy = by + mu * s.gy[i] + rhoPhase * gravity;
   Real fz = bz + mu * s.gz[i];
-  Real uxe = s.ux[cur][i], uye = s.uy[cur][i], uze = s.uz[cur][i];
+  Real uxe = s.ux_at(cur, i), uye = s.uy_at(cur, i), uze = s.uz[cur][i];
   Real u2 = uxe * uxe + uye * uye + uze * uze;
   Real negU2half = (Real)-1.5 * u2;
   Real uF = uxe * fx + uye * fy + uze * fz;
@@ -358,8 +360,8 @@ __global__ void k_stream_hydro_macro(Scene<PopT, typename Prec<PopT>::Real> s, i
     uyn *= sc;
     uzn *= sc;
   }
-  s.ux[cur][i] = uxn;
-  s.uy[cur][i] = uyn;
+  s.set_ux(cur, i, uxn);
+  s.set_uy(cur, i, uyn);
   s.uz[cur][i] = uzn;
 }
 
@@ -602,8 +604,8 @@ __device__ __forceinline__ void fill_cell(const Scene<PopT, typename Prec<PopT>:
   s.phi[cur][i] = pR;
   s.phi[1 - cur][i] = pR;  // phiPrev[i] = p
   s.rho[cur][i] = (Real)r;
-  s.ux[cur][i] = (Real)vx;
-  s.uy[cur][i] = (Real)vy;
+  s.set_ux(cur, i, (Real)vx);
+  s.set_uy(cur, i, (Real)vy);
   s.uz[cur][i] = (Real)vz;
   double rhoPhase = rhoG + p * (rhoL - rhoG);
   double u2 = vx * vx + vy * vy + vz * vz;
@@ -652,8 +654,8 @@ __device__ __forceinline__ void fresh_fill_body(const Scene<PopT, typename Prec<
   auto current = [&](long long j, Real &p, Real &r, Real &x, Real &y, Real &z) {
     p = s.phi[cur][j];
     r = s.rho[cur][j];
-    x = s.ux[cur][j];
-    y = s.uy[cur][j];
+    x = s.ux_at(cur, j);
+    y = s.uy_at(cur, j);
     z = s.uz[cur][j];
   };
   if (sequential || nf > FILL_PAR_MAX) {
@@ -869,10 +871,28 @@ __global__ void __launch_bounds__(LINK_CHUNK) k_link_emit(Scene<PopT, typename P
 constexpr int DEAD_THREADS = 256;
 
 // (static: Real = float is instantiated by several translation units)
+// the dead-cell sweep reads phi and u through one of these: plain arrays
+// (the allocation-free entry's caller arrays) or a scene's current half
 template <class Real>
-__device__ __forceinline__ void absorb_dead_body(const Real *__restrict__ phi, const Real *__restrict__ ux,
-                                                 const Real *__restrict__ uy, const Real *__restrict__ uz,
-                                                 int nx, int ny, const int *__restrict__ dead,
+struct ArrayFields {
+  const Real *phi, *ux, *uy, *uz;
+  __device__ __forceinline__ double p(long long i) const { return (double)phi[i]; }
+  __device__ __forceinline__ double vx(long long i) const { return (double)ux[i]; }
+  __device__ __forceinline__ double vy(long long i) const { return (double)uy[i]; }
+  __device__ __forceinline__ double vz(long long i) const { return (double)uz[i]; }
+};
+template <class PopT>
+struct SceneFields {
+  const Scene<PopT, typename Prec<PopT>::Real> &s;
+  int cur;
+  __device__ __forceinline__ double p(long long i) const { return (double)s.phi[cur][i]; }
+  __device__ __forceinline__ double vx(long long i) const { return (double)s.ux_at(cur, i); }
+  __device__ __forceinline__ double vy(long long i) const { return (double)s.uy_at(cur, i); }
+  __device__ __forceinline__ double vz(long long i) const { return (double)s.uz[cur][i]; }
+};
+
+template <class Fields>
+__device__ __forceinline__ void absorb_dead_body(const Fields &fd, int nx, int ny, const int *__restrict__ dead,
                                                  const int *__restrict__ totals, int cap, double rhoL,
                                                  double rhoG, const SolidSet *__restrict__ ssp, double *out,
                                                  int b) {
@@ -893,9 +913,9 @@ __device__ __forceinline__ void absorb_dead_body(const Real *__restrict__ phi, c
     const int z = (int)(t / ny);
     if (ss.zend > 0 && (z < ss.zlo || z >= ss.zend)) continue;
     if (owner_of<LBM_MAX_SPHERES>(ss.sph, ss.nsph, x, y, z) != b) continue;
-    const double rhoPhase = __dadd_rn(rhoG, __dmul_rn((double)phi[i], dRho));
-    impulse_terms(ss.sph[b], x, y, z, __dmul_rn(rhoPhase, (double)ux[i]),
-                  __dmul_rn(rhoPhase, (double)uy[i]), __dmul_rn(rhoPhase, (double)uz[i]), acc);
+    const double rhoPhase = __dadd_rn(rhoG, __dmul_rn(fd.p(i), dRho));
+    impulse_terms(ss.sph[b], x, y, z, __dmul_rn(rhoPhase, fd.vx(i)), __dmul_rn(rhoPhase, fd.vy(i)),
+                  __dmul_rn(rhoPhase, fd.vz(i)), acc);
   }
   for (int j = 0; j < 6; j++) sh[j][threadIdx.x] = acc[j];
   __syncthreads();
@@ -912,7 +932,16 @@ static __global__ void __launch_bounds__(DEAD_THREADS)
                   const Real *__restrict__ uy, const Real *__restrict__ uz, int nx, int ny,
                   const int *__restrict__ dead, const int *__restrict__ totals, int cap, double rhoL,
                   double rhoG, const SolidSet *__restrict__ ssp, double *out) {
-  absorb_dead_body(phi, ux, uy, uz, nx, ny, dead, totals, cap, rhoL, rhoG, ssp, out, blockIdx.x);
+  absorb_dead_body(ArrayFields<Real>{phi, ux, uy, uz}, nx, ny, dead, totals, cap, rhoL, rhoG, ssp, out,
+                   blockIdx.x);
+}
+// the same over a scene's current half
+template <class PopT>
+static __global__ void __launch_bounds__(DEAD_THREADS)
+    k_absorb_dead_scene(Scene<PopT, typename Prec<PopT>::Real> s, int cur, const int *__restrict__ dead,
+                        const int *__restrict__ totals, int cap, double rhoL, double rhoG,
+                        const SolidSet *__restrict__ ssp, double *out) {
+  absorb_dead_body(SceneFields<PopT>{s, cur}, s.nx, s.ny, dead, totals, cap, rhoL, rhoG, ssp, out, blockIdx.x);
 }
 
 // Deterministic reduction of the per-cell impulse arrays in one launch.
@@ -1100,7 +1129,7 @@ __global__ void k_watch_finite(Scene<PopT, typename Prec<PopT>::Real> s, int cur
     bool bad = false;
     if (i < s.n)
       bad = !isfinite((double)s.phi[cur][i]) || !isfinite((double)s.rho[cur][i]) ||
-            !isfinite((double)s.ux[cur][i]) || !isfinite((double)s.uy[cur][i]) ||
+            !isfinite((double)s.ux_at(cur, i)) || !isfinite((double)s.uy_at(cur, i)) ||
             !isfinite((double)s.uz[cur][i]);
     const unsigned m = __ballot_sync(0xffffffffu, bad);
     if (m && (int)(threadIdx.x & 31) == __ffs(m) - 1) atomicMin(first, (unsigned long long)i);

@@ -92,6 +92,21 @@ static __global__ void k_sphere_step(lbm_sphere *sph, int nsph, double gravity, 
 // reduction, the dead-cell impulses and the sphere step) as one launch per
 // kind: grid row (or plane) s runs scene s's kernel body on scene s's
 // arguments, so a step of n scenes costs 9 launches instead of 9 n.
+// ux (comp 0) or uy (comp 1) of one half between a plain array and the
+// place the scene keeps it (Scene::ux_at / set_ux), for the field transfers
+template <class PopT>
+__global__ void k_u_array(Scene<PopT, typename Prec<PopT>::Real> s, int comp, int half,
+                          typename Prec<PopT>::Real *arr, int toScene) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= s.n) return;
+  if (toScene) {
+    if (comp == 0) s.set_ux(half, i, arr[i]);
+    else s.set_uy(half, i, arr[i]);
+  } else {
+    arr[i] = comp == 0 ? s.ux_at(half, i) : s.uy_at(half, i);
+  }
+}
+
 template <class PopT>
 struct SmallArgs {
   Scene<PopT, typename Prec<PopT>::Real> s;
@@ -148,8 +163,8 @@ template <class PopT>
 __global__ void __launch_bounds__(DEAD_THREADS) kb_absorb_dead(const SmallArgs<PopT> *__restrict__ A) {
   const SmallArgs<PopT> &a = A[blockIdx.y];
   if (a.ns == 0) return;
-  absorb_dead_body(a.s.phi[a.cur], a.s.ux[a.cur], a.s.uy[a.cur], a.s.uz[a.cur], a.s.nx, a.s.ny, a.dead, a.totals,
-                   a.listCap, a.rhoL, a.rhoG, &a.plan->ss, a.dDead, blockIdx.x);
+  absorb_dead_body(SceneFields<PopT>{a.s, a.cur}, a.s.nx, a.s.ny, a.dead, a.totals, a.listCap, a.rhoL, a.rhoG,
+                   &a.plan->ss, a.dDead, blockIdx.x);
 }
 template <class PopT>
 __global__ void kb_sphere_step(const SmallArgs<PopT> *__restrict__ A) {
@@ -267,10 +282,9 @@ class Ops final : public OpsBase {
   }
   void absorb_dead(lbm_sim *h, double *d_out) override {
     const int ns = h->hPlan.ss.nsph > 0 ? h->hPlan.ss.nsph : 1;
-    k_absorb_dead<Real><<<ns, DEAD_THREADS, 0, h->stream>>>(
-        (const Real *)h->mac[h->cur][0], (const Real *)h->mac[h->cur][2], (const Real *)h->mac[h->cur][3],
-        (const Real *)h->mac[h->cur][4], h->nx, h->ny, h->dead, h->totals, (int)h->listCap,
-        h->params.rhoL, h->params.rhoG, &h->dPlan->ss, d_out);
+    k_absorb_dead_scene<PopT><<<ns, DEAD_THREADS, 0, h->stream>>>(scene(h), h->cur, h->dead, h->totals,
+                                                                  (int)h->listCap, h->params.rhoL,
+                                                                  h->params.rhoG, &h->dPlan->ss, d_out);
     h->launches++;
   }
 
@@ -395,6 +409,11 @@ class Ops final : public OpsBase {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * warps_of<TY, STG>(), smem);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per) * std::max(1, sms);
+  }
+  bool u_in_pads() const override { return Scene<PopT, Real>::UPAD; }
+  void u_array(lbm_sim *h, int comp, int half, void *arr, bool toScene) override {
+    k_u_array<PopT><<<nblocks(h->n, 256), 256, 0, h->stream>>>(scene(h), comp, half, (Real *)arr, toScene ? 1 : 0);
+    h->launches++;
   }
   size_t small_args_bytes() const override { return sizeof(SmallArgs<PopT>); }
   void small_args(lbm_sim *h, int cur, int ns, long long slotCells, long long maxU, int redChunks,

@@ -88,6 +88,10 @@ class OpsBase {
   // the device (and set their shared-memory opt-in), so that no first launch
   // waits for a module load
   virtual void warm(int device) = 0;
+  // ux and uy held in the population pad slots (FP32 / FP64 storage), and
+  // their copy to or from a plain array of one half (the field transfers)
+  virtual bool u_in_pads() const = 0;
+  virtual void u_array(lbm_sim *h, int comp, int half, void *arr, bool toScene) = 0;
   // a batch's sparse kernels, one launch per kind for all scenes: the
   // per-scene argument block, then the kernels before and after the fused
   // launch over a device table of n such blocks
