@@ -134,6 +134,7 @@ _SIGS = [
     ("lbm_fused_timing_query", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("lbm_set_fused_config", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("lbm_get_fused_config", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("lbm_get_launch_shape", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("lbm_set_slab", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     ("lbm_slab_copy_planes", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int]),
     ("lbm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),

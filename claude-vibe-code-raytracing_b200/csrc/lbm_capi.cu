@@ -460,7 +460,7 @@ void free_all(lbm_sim *h) {
                   h->grad[2], h->grad[3], h->us[0], h->us[1], h->us[2], h->bf[0], h->bf[1],
                   h->bf[2], h->fresh, h->dead, h->counts, h->totals, h->impAcc, h->partials,
                   h->dOut, h->dSph, h->staging, h->dPhiCol, h->dPlan, h->dWatch, h->linkChunks,
-                  h->linkBuf, h->redTickets, h->meshTri};
+                  h->linkBuf, h->redTickets, h->meshTri, h->dMaps};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, h->stream);
   for (int c = 0; c < 2; c++)
@@ -742,6 +742,7 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
     return LBM_OK;
   };
   rc = body();
+  if (rc == LBM_OK) rc = ops->build_stage_maps(h);
   if (rc != LBM_OK) {
     free_all(h);
     delete h;
@@ -1682,7 +1683,7 @@ int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
   if (!h) return LBM_ERR_ARG;
   if (!h->ops->shape_ok(rows) || zchunk < 1)
     return fail(h, LBM_ERR_ARG,
-                "rows must be 2, 4 or 8, or 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED (FP32/FP16/BF16 storage), and zchunk >= 1");
+                "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA (FP32/FP16/BF16 storage), and zchunk >= 1");
   if (h->ops->fused_smem(rows) > 227 * 1024)
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;
@@ -1744,6 +1745,12 @@ int lbm_slab_copy_planes(lbm_sim *dst, int dst_plane, const lbm_sim *src, int sr
   CK(copy(dst->tag + dc, src->tag + sc, (size_t)cells));
   CK(cudaStreamSynchronize(dst->stream));
   dst->listsValid = false;
+  return LBM_OK;
+}
+
+int lbm_get_launch_shape(const lbm_sim *h, int *shape) {
+  if (!h || !shape) return LBM_ERR_ARG;
+  *shape = resolve_shape(h, h->cfg.ty);
   return LBM_OK;
 }
 
@@ -1850,6 +1857,13 @@ int batch_tables(lbm_batch *b) {
 // the batch's shape for a launch: SHAPE_WIDE when any scene needs 64-bit
 // population offsets
 int launch_shape(const lbm_batch *b, int rows) {
+  // the TMA-staged form needs every scene's tensor maps (nx a multiple of
+  // 16); otherwise the batch runs the compact form of the same rows
+  for (lbm_sim *h : b->sims)
+    if (resolve_shape(h, rows) != rows) {
+      rows = resolve_shape(h, rows);
+      break;
+    }
   for (lbm_sim *h : b->sims)
     if (needs_wide(h->n)) return rows | SHAPE_WIDE;
   return rows;
@@ -1945,7 +1959,7 @@ int lbm_batch_set_config(lbm_batch *b, int rows, int zchunk) {
   if (!b) return LBM_ERR_ARG;
   if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
     return bfail(b, LBM_ERR_ARG,
-                 "rows must be 2, 4 or 8, or 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED (FP32/FP16/BF16 storage), and zchunk >= 1");
+                 "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA (FP32/FP16/BF16 storage), and zchunk >= 1");
   b->rows = rows;
   b->zchunk = zchunk;
   return LBM_OK;
@@ -2125,7 +2139,7 @@ int lbm_batch_time_fused(lbm_batch *b, int rows, int zchunk, int reps, double *m
   if (!b || !ms || reps < 1) return LBM_ERR_ARG;
   if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
     return bfail(b, LBM_ERR_ARG,
-                 "rows must be 2, 4 or 8, or 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED (FP32/FP16/BF16 storage), and zchunk >= 1");
+                 "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA (FP32/FP16/BF16 storage), and zchunk >= 1");
   DeviceGuard g(b->device);
   const int keepRows = b->rows, keepZ = b->zchunk;
   b->rows = rows;

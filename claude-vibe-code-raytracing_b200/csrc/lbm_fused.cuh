@@ -40,6 +40,21 @@
 
 namespace lbm {
 
+// An encoded tensor map (the driver's 128-byte, 64-byte aligned descriptor).
+struct alignas(64) TensorMap {
+  unsigned long long w[16];
+};
+// Tensor maps of one scene for the TMA-staged form (tiles of TMA_ROWS rows):
+// per half, the f and h populations as 4-D arrays (elements of an 8-cell
+// block, blocks of a row, y, z; box: 4 blocks x TMA_ROWS rows) and phi, rho,
+// ux, uy, uz as 3-D arrays (x, y, z; box 32 x TMA_ROWS, phi 40 x
+// TMA_ROWS + 2); the tags (x, y, z; box 32 x TMA_ROWS).  Built on the host
+// when the scene is created, for nx a multiple of 16.
+constexpr int TMA_ROWS = 6;
+struct StageMaps {
+  TensorMap f[2], h[2], phi[2], rho[2], ux[2], uy[2], uz[2], tag;
+};
+
 template <class PopT>
 struct FusedArgs {
   Scene<PopT, typename Prec<PopT>::Real> s;
@@ -50,6 +65,7 @@ struct FusedArgs {
   int *status;   // set non-zero when a bounded wait of the step runs out
   int withhold;  // test hook: the bulk-staged form does not issue each tile's first copy
   uint8_t *pack; // frame step: the RG8 volume of the step's result (planes 1 .. nz-2), else null
+  const StageMaps *maps;  // tensor maps of the TMA-staged form (device memory), else null
 };
 
 // slot of direction k within its e_z group (0..8 for D3Q27)
@@ -125,6 +141,29 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
 }
+// One box of a tensor map (a 3-D or 4-D array in global memory) into shared
+// memory, completion counted in bytes on an mbarrier.  Coordinates are
+// innermost first; the innermost one times the element size is a multiple of
+// 16 bytes, the destination is 128-byte aligned, and cells of the box outside
+// the array arrive as zeros (the whole box is counted).  No multicast.
+__device__ __forceinline__ void tma_g2s_3d(uint32_t dst, const void *map, int c0, int c1, int c2, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_g2s_4d(uint32_t dst, const void *map, int c0, int c1, int c2, int c3,
+                                           uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+// orders this CTA's earlier shared-memory reads before later copies of the
+// asynchronous proxy into the same bytes
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 // Per-thread asynchronous copies global -> shared (cp.async, 4 / 8 / 16
 // bytes, both addresses aligned to the size).  A thread's copies complete, and
 // become visible to that thread, at its next cp_async_wait_all; the 16-byte

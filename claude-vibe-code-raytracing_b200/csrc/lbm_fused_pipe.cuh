@@ -1,5 +1,6 @@
 // The compact-ring forms of the fused LBM step (tile shapes 4 or 6 rows |
-// LBM_FUSED_COMPACT, LBM_FUSED_ASYNC or LBM_FUSED_STAGED).
+// LBM_FUSED_COMPACT, LBM_FUSED_ASYNC or LBM_FUSED_STAGED; 6 rows |
+// LBM_FUSED_TMA).
 //
 // Same algorithm and arithmetic as fused_tile (lbm_fused.cuh): a CTA owns a
 // 32 x TY column of cells and marches it up a z-chunk; each plane is collided
@@ -25,7 +26,16 @@
 //       - STAGED: the tile rows of plane q + 1 arrive by bulk asynchronous
 //         copies (cp.async.bulk, completion counted in bytes on an mbarrier)
 //         issued by one producer lane as soon as every cell warp has read the
-//         current stage (a second mbarrier).
+//         current stage (a second mbarrier);
+//       - TMA: the same stage (rows of plane q + 1, phi of plane q + 2) as
+//         six to eight tensor-map box copies (the tile's 4 population blocks
+//         x 6 rows of f and of h, the rho / u / tag rows, the phi rows with
+//         their halo), issued by one lane of the halo-row warp right after
+//         the barrier that follows the cell warps' reads of the stage, so the
+//         copies land while plane q is emitted and plane q - 1 pulled and no
+//         cell warp waits on a load it issued.
+//         Needs nx a multiple of 16 (whole blocks per tile row, 16-byte row
+//         strides of the tags).
 //
 // Results are bit-identical to fused_tile in every form (the collision is the
 // same collide_cell, the pull sums in the same order).  FP32, FP16 and BF16
@@ -41,6 +51,7 @@ namespace lbm {
 constexpr int PIPE_STAGED = 1;
 constexpr int PIPE_COMPACT = 2;
 constexpr int PIPE_ASYNC = 3;
+constexpr int PIPE_TMA = 4;
 
 // ---------------------------------------------------------------- compact ring
 // Direction k's slot array in one ring copy covers the local columns
@@ -89,22 +100,36 @@ struct PipeRing {
 template <class PopT, int TY, int PF>
 struct PipeSmem {
   using Real = typename Prec<PopT>::Real;
-  static constexpr bool STG = PF == PIPE_STAGED, ASY = PF == PIPE_ASYNC;
+  static constexpr bool STG = PF == PIPE_STAGED, ASY = PF == PIPE_ASYNC, TMA = PF == PIPE_TMA;
   using R = PipeRing<TY>;
   static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;  // tag planes keep the full halo frame
-  static constexpr int SB = 5;                              // blocks a 32-cell row can span
+  // blocks a 32-cell row can span (4 when rows start on a block: TMA)
+  static constexpr int SB = TMA ? 4 : 5;
   static constexpr int ROWF = SB * PopGroups<Q27>::BLOCK, ROWH = SB * PopGroups<Q7>::BLOCK;
-  static constexpr int MROW = 36;  // floats of one staged rho / u row (16-byte aligned copy)
-  static constexpr int TROW = 48;  // bytes of one staged tag row
-  static constexpr int PROW = 40;  // floats of one staged phi row (x0 - 1 .. x0 + 32)
+  static constexpr int MROW = TMA ? 32 : 36;  // floats of one staged rho / u row (16-byte aligned copy)
+  static constexpr int TROW = TMA ? 32 : 48;  // bytes of one staged tag row
+  static constexpr int PROW = 40;             // floats of one staged phi row (x0 - 4 .. x0 + 35)
+  // floats of one staged phi plane (a 128-byte multiple for the tensor copies)
+  static constexpr int PSL = TMA ? ((TY + 2) * PROW + 31) / 32 * 32 : (TY + 2) * PROW;
+  // alignment of the stage buffers: tensor-copy destinations are 128-byte
+  // aligned (the base itself is aligned up by the tile, see `lead`)
+  static constexpr size_t AL = TMA ? 128 : 16;
+  static constexpr size_t lead = TMA ? 128 : 0;  // room to align the base up
   static constexpr size_t ringBytes = (size_t)R::TOTAL * sizeof(Real);
   static constexpr size_t tagOff = ringBytes;
-  static constexpr size_t stF = (tagOff + 3 * NC + 15) / 16 * 16;
+  static constexpr size_t stF = (tagOff + 3 * NC + AL - 1) / AL * AL;
   static constexpr size_t stH = stF + (size_t)TY * ROWF * sizeof(PopT);
   static constexpr size_t stM = stH + (size_t)TY * ROWH * sizeof(PopT);
   static constexpr size_t stT = stM + (size_t)4 * TY * MROW * sizeof(Real);
-  static constexpr size_t phiOff = stT + (size_t)TY * TROW;
-  static constexpr size_t barOff = (phiOff + (size_t)3 * (TY + 2) * PROW * sizeof(Real) + 15) / 16 * 16;
+  static constexpr size_t phiOff = (stT + (size_t)TY * TROW + AL - 1) / AL * AL;
+  static constexpr size_t barOff = (phiOff + (size_t)3 * PSL * sizeof(Real) + 15) / 16 * 16;
+  // bytes of one TMA stage: the rows of f, h, rho, uz, the tags (and ux, uy
+  // unless they sit in the pad slots), one phi plane; the prologue adds two
+  // phi planes
+  static constexpr bool UPAD = sizeof(PopT) == sizeof(Real);
+  static constexpr uint32_t tmaRows = (uint32_t)(TY * (ROWF + ROWH) * sizeof(PopT) +
+                                                 (UPAD ? 2 : 4) * TY * MROW * sizeof(Real) + TY * TROW);
+  static constexpr uint32_t tmaPhi = (uint32_t)((TY + 2) * PROW * sizeof(Real));
   // the async form's per-thread slots after the tag planes: [G27][32 TY]
   // groups of f, [G7][32 TY] groups of h, [11][32 TY] words (phi and its six
   // neighbours, rho, ux, uy, uz)
@@ -112,15 +137,19 @@ struct PipeSmem {
   static constexpr size_t aF = (tagOff + 3 * NC + 15) / 16 * 16;
   static constexpr size_t aH = aF + (size_t)PopGroups<Q27>::G * NT * GB;
   static constexpr size_t aS = aH + (size_t)PopGroups<Q7>::G * NT * GB;
-  // staged: two mbarriers (stage full, stage read) and the abort flag;
-  // compact: ring and tags only
-  static constexpr size_t bytes = STG ? barOff + 32 : ASY ? aS + (size_t)NS * NT * 4 : aF;
+  // staged: two mbarriers (stage full, stage read) and the abort flag (TMA:
+  // the first mbarrier only); compact: ring and tags only
+  static constexpr size_t bytes = (STG || TMA) ? lead + barOff + 32 : ASY ? aS + (size_t)NS * NT * 4 : aF;
   static constexpr int warps = TY + 2;  // TY cell warps, the halo rows above and below, the sides
   static constexpr int threads = 32 * warps;
   static_assert(sizeof(Real) == 4, "the pipelined form holds FP32 arithmetic values in its ring");
   static_assert((ROWF * sizeof(PopT)) % 16 == 0 && (ROWH * sizeof(PopT)) % 16 == 0, "whole 16-byte units");
   static_assert(stF % 16 == 0 && stH % 16 == 0 && stM % 16 == 0 && stT % 16 == 0 && phiOff % 16 == 0,
                 "bulk copy destinations are 16-byte aligned");
+  static_assert(!TMA || (TY == TMA_ROWS && stF % 128 == 0 && stH % 128 == 0 && stM % 128 == 0 &&
+                         (TY * MROW * sizeof(Real)) % 128 == 0 && stT % 128 == 0 && phiOff % 128 == 0 &&
+                         (PSL * sizeof(Real)) % 128 == 0),
+                "tensor copy destinations are 128-byte aligned; the maps' boxes are TMA_ROWS rows");
 };
 
 // ---------------------------------------------------------------- the tile
@@ -130,7 +159,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
   using SM = PipeSmem<PopT, TY, PF>;
-  constexpr bool STG = SM::STG, ASY = SM::ASY;
+  constexpr bool STG = SM::STG, ASY = SM::ASY, TMA = SM::TMA;
   using R = PipeRing<TY>;
   using LD = CellLoad<PopT>;
   using CO = CellOut<PopT>;
@@ -139,16 +168,19 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   constexpr int BLK27 = PopGroups<Q27>::BLOCK, BLK7 = PopGroups<Q7>::BLOCK;
   constexpr int ROWF = SM::ROWF, ROWH = SM::ROWH, MROW = SM::MROW, TROW = SM::TROW, PROW = SM::PROW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Real *ring = reinterpret_cast<Real *>(smem_raw);
-  uint8_t *stag = smem_raw + SM::tagOff;                            // [3][NC]
-  PopT *sF = reinterpret_cast<PopT *>(smem_raw + SM::stF);          // [TY][ROWF]
-  PopT *sH = reinterpret_cast<PopT *>(smem_raw + SM::stH);          // [TY][ROWH]
-  Real *sM = reinterpret_cast<Real *>(smem_raw + SM::stM);          // [4][TY][MROW] rho ux uy uz
-  uint8_t *sT = smem_raw + SM::stT;                                 // [TY][TROW]
-  Real *sP = reinterpret_cast<Real *>(smem_raw + SM::phiOff);       // [3][TY + 2][PROW]
-  const uint32_t bar = smem_u32(smem_raw + SM::barOff);       // stage q landed (1 arrival + bytes)
-  const uint32_t barE = smem_u32(smem_raw + SM::barOff + 8);  // stage q read (one arrival per cell warp)
-  int *abortF = reinterpret_cast<int *>(smem_raw + SM::barOff + 16);
+  // the TMA form aligns its base up to 128 bytes (room for it is in SM::bytes)
+  unsigned char *smem = smem_raw;
+  if constexpr (SM::lead > 0) smem += (SM::lead - (smem_u32(smem_raw) & (SM::lead - 1))) & (SM::lead - 1);
+  Real *ring = reinterpret_cast<Real *>(smem);
+  uint8_t *stag = smem + SM::tagOff;                           // [3][NC]
+  PopT *sF = reinterpret_cast<PopT *>(smem + SM::stF);         // [TY][ROWF]
+  PopT *sH = reinterpret_cast<PopT *>(smem + SM::stH);         // [TY][ROWH]
+  Real *sM = reinterpret_cast<Real *>(smem + SM::stM);         // [4][TY][MROW] rho ux uy uz
+  uint8_t *sT = smem + SM::stT;                                // [TY][TROW]
+  Real *sP = reinterpret_cast<Real *>(smem + SM::phiOff);      // [3][PSL]: TY + 2 rows of PROW
+  const uint32_t bar = smem_u32(smem + SM::barOff);       // stage q landed (1 arrival + bytes)
+  const uint32_t barE = smem_u32(smem + SM::barOff + 8);  // stage q read (one arrival per cell warp)
+  int *abortF = reinterpret_cast<int *>(smem + SM::barOff + 16);
 
   const auto &s = a.s;
   const SolidSet &ss = *a.ss;
@@ -193,8 +225,9 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   const int sideLy = sideLane < TY ? sideLane + 1 : (sideLane == TY ? 0 : TY + 1);   // frame row
   const int sideSy = sideLane < TY ? 0 : (sideLane == TY ? 1 : -1);
   // the producer: lane 0 of cell warp 0 issues each stage as soon as every
-  // cell warp has read the previous one
-  const bool producer = STG && ty == 0 && tx == 0;
+  // cell warp has read the previous one (TMA: lane 0 of the halo-row warp,
+  // after the barrier that follows those reads)
+  const bool producer = (STG && ty == 0 && tx == 0) || (TMA && haloRows && tx == 0);
 
   // ---- halo loads (plain, into registers), as in fused_tile
   auto needs = [&](auto MODEc, auto SXc, auto SYc, auto KK, int sx, int sy,
@@ -288,7 +321,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       const uint32_t cnt = (uint32_t)((c1 | 3) - a0 + 1);
       if (!lbm_ok(cnt <= PROW, 30, cnt) || !lbm_ok(a0 + cnt <= nCell + ARRAY_PAD, 40, a0)) continue;
       if (go)
-        bulk_g2s(smem_u32(sP + ((P % 3) * (TY + 2) + (r + 1)) * PROW), phiC + a0, cnt * sizeof(Real), bar);
+        bulk_g2s(smem_u32(sP + (P % 3) * SM::PSL + (r + 1) * PROW), phiC + a0, cnt * sizeof(Real), bar);
       else
         bytes += cnt * sizeof(Real);
     }
@@ -339,6 +372,34 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     }
   };
 
+  // TMA stage(q): rows of plane q and phi of plane q + 1 (prologue: also phi
+  // of planes q - 1 and q), one box per array.  Boxes reaching outside the
+  // grid (the right-hand tile's last blocks, rows past ny, planes -1 and nz,
+  // columns x0 - 4 .. x0 - 1 of the first tile) bring zeros, which only cells
+  // outside the grid and boundary cells (walls) read.
+  auto issue_tma = [&](int q, bool prologue) __attribute__((always_inline)) {
+    const StageMaps *m = a.maps;
+    mbar_expect(bar, SM::tmaRows + (prologue ? 3u : 1u) * SM::tmaPhi);
+    tma_g2s_4d(smem_u32(sF), &m->f[cur], 0, x0 >> 3, y0, q, bar);
+    tma_g2s_4d(smem_u32(sH), &m->h[cur], 0, x0 >> 3, y0, q, bar);
+    tma_g2s_3d(smem_u32(sM), &m->rho[cur], x0, y0, q, bar);
+    if constexpr (!UPAD) {
+      tma_g2s_3d(smem_u32(sM + 1 * TY * MROW), &m->ux[cur], x0, y0, q, bar);
+      tma_g2s_3d(smem_u32(sM + 2 * TY * MROW), &m->uy[cur], x0, y0, q, bar);
+    }
+    tma_g2s_3d(smem_u32(sM + 3 * TY * MROW), &m->uz[cur], x0, y0, q, bar);
+    tma_g2s_3d(smem_u32(sT), &m->tag, x0, y0, q, bar);
+    auto phi = [&](int P) __attribute__((always_inline)) {
+      const int slot = P - 3 * (int)((unsigned)(P + 3) / 3u) + 3;  // P mod 3 for P >= -1
+      tma_g2s_3d(smem_u32(sP + slot * SM::PSL), &m->phi[cur], x0 - 4, y0 - 1, P, bar);
+    };
+    phi(q + 1);
+    if (prologue) {
+      phi(q - 1);
+      phi(q);
+    }
+  };
+
   // a cell warp's cell of plane q from the stage.  Positions inside the staged
   // rows follow from the rows' first flat indices modulo 16, computed in
   // 32-bit arithmetic (2^32 is a multiple of 16).
@@ -385,7 +446,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       int i = t + 1 + dx + (int)(c0 & 3u);
       i = i < 0 ? 0 : (i >= PROW ? PROW - 1 : i);
       const int slot = P - 3 * (int)((unsigned)(P + 3) / 3u) + 3;  // P mod 3 for P >= -1
-      return sP[(slot * (TY + 2) + rr) * PROW + sm_at(i, PROW, 39)];
+      return sP[slot * SM::PSL + rr * PROW + sm_at(i, PROW, 39)];
     };
     L.p = pat(q, ty + 1, 0);
     L.pxp = pat(q, ty + 1, 1);
@@ -439,9 +500,9 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   // load uses; the tag (one byte, no copy size that small) by a plain load
   // into a register that is held until plane q is collided
   constexpr int NT = SM::NT, GB = SM::GB;
-  PopT *aF = reinterpret_cast<PopT *>(smem_raw + SM::aF);  // [G27][NT] groups
-  PopT *aH = reinterpret_cast<PopT *>(smem_raw + SM::aH);  // [G7][NT] groups
-  Real *aS = reinterpret_cast<Real *>(smem_raw + SM::aS);  // [11][NT] words
+  PopT *aF = reinterpret_cast<PopT *>(smem + SM::aF);  // [G27][NT] groups
+  PopT *aH = reinterpret_cast<PopT *>(smem + SM::aH);  // [G7][NT] groups
+  Real *aS = reinterpret_cast<Real *>(smem + SM::aS);  // [11][NT] words
   const int lin = ty * 32 + tx;
   auto async_issue = [&](int q, uint8_t &tgq) __attribute__((always_inline)) {
     const bool inside = x < nx && y < ny && q >= 0 && q < nz;
@@ -518,12 +579,16 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
 
   if (producer) {
     mbar_init(bar);
-    mbar_init_count(barE, TY);
+    if constexpr (STG) mbar_init_count(barE, TY);
     mbar_init_fence();
+    if constexpr (TMA) fence_proxy_async();  // the initialised mbarrier, seen by the tensor copies
   }
-  if (STG && threadIdx.x == 0 && threadIdx.y == 0) *abortF = 0;
+  if ((STG || TMA) && threadIdx.x == 0 && threadIdx.y == 0) *abortF = 0;
   __syncthreads();
-  if (producer && !a.withhold) issue(zb - 1, true);
+  if (producer && !a.withhold) {
+    if constexpr (TMA) issue_tma(zb - 1, true);
+    else issue(zb - 1, true);
+  }
   uint32_t parity = 0;
   uint8_t tgNext = 0;
   if constexpr (ASY) {
@@ -551,6 +616,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
           // that ran out (set before the arrivals) stops the issuing.
           if (mbar_wait(barE, parity) && q < ze && !*abortF) issue(q + 1, false);
         }
+      } else if constexpr (TMA) {
+        if (!mbar_wait(bar, parity)) {
+          record_stage_timeout(q);
+          if (a.status) atomicOr(a.status, 1);
+          *abortF = 1;
+        }
+        stage_load(q, L);
       } else if constexpr (ASY) {
         async_load(q, tgNext, L);
       } else {
@@ -575,6 +647,15 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     parity ^= 1u;
     // every warp has pulled plane q - 2 and the cell warps have read the stage
     __syncthreads();
+    if constexpr (TMA) {
+      // stage q + 1 into the buffers of stage q, which every cell warp read
+      // before the barrier above; it lands while plane q is emitted and plane
+      // q - 1 pulled.  A wait that ran out (set before the barrier) stops it.
+      if (producer && q < ze && !*abortF) {
+        fence_proxy_async();
+        issue_tma(q + 1, false);
+      }
+    }
     if (cellWarp) {
       emit(IC<0>{}, IC<0>{}, IC<0>{}, 0, 0, true, q, tx, ty, o);
       // the slots of plane q were read before the barrier above: plane q + 1
@@ -591,7 +672,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       emit(IC<2>{}, IC<-1>{}, IC<0>{}, -1, sideSy, sideAct, q, sideLx - 1, sideLy - 1, o);
     }
     __syncthreads();
-    if constexpr (STG) {
+    if constexpr (STG || TMA) {
       if (*abortF) break;
     }
 
@@ -783,12 +864,12 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   // Stopped early (a wait ran out): the copy of stage q was issued (unless
   // withheld) and may still be in flight; let it land (bounded) before the
   // shared memory is released.  Normal exit: every issued copy was waited for.
-  if constexpr (STG) {
+  if constexpr (STG || TMA) {
     if (q <= ze && producer && !(a.withhold && q == zb - 1)) mbar_wait(bar, parity ^ 1u);
     __syncthreads();
     if (producer) {
       mbar_inval(bar);
-      mbar_inval(barE);
+      if constexpr (STG) mbar_inval(barE);
     }
   }
 }

@@ -2,6 +2,7 @@
 // storage type.  Included once per storage type by lbm_inst_*.cu.
 #pragma once
 
+#include <cudaTypedefs.h>  // the driver's tensor-map encoder type
 #include <string.h>
 
 #include <algorithm>
@@ -12,6 +13,26 @@
 #include "lbm_state.h"
 
 namespace lbm {
+
+static_assert(sizeof(TensorMap) == sizeof(CUtensorMap) && alignof(TensorMap) == alignof(CUtensorMap),
+              "TensorMap holds one CUtensorMap");
+
+// The driver's tensor-map encoder, looked up once through the runtime (no
+// link against the driver library); null where the driver lacks it.
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
 
 // ---------------------------------------------------------------- transfers
 template <class PopT>
@@ -315,6 +336,7 @@ class Ops final : public OpsBase {
       case 6 | LBM_FUSED_ASYNC: pipe(IC<6>{}, IC<PIPE_ASYNC>{}); break;
       case 4 | LBM_FUSED_STAGED: pipe(IC<4>{}, IC<PIPE_STAGED>{}); break;
       case 6 | LBM_FUSED_STAGED: pipe(IC<6>{}, IC<PIPE_STAGED>{}); break;
+      case TMA_ROWS | LBM_FUSED_TMA: pipe(IC<TMA_ROWS>{}, IC<PIPE_TMA>{}); break;
       default: go(IC<8>{}, IC<0>{}); break;
     }
   }
@@ -322,6 +344,7 @@ class Ops final : public OpsBase {
   bool shape_ok(int shape) const override {
     if (shape == 2 || shape == 4 || shape == 8) return true;
     const int rows = shape & 0xff, form = shape & ~0xff;
+    if (form == LBM_FUSED_TMA) return kPipe && rows == TMA_ROWS;
     return kPipe && (rows == 4 || rows == 6) &&
            (form == LBM_FUSED_COMPACT || form == LBM_FUSED_ASYNC || form == LBM_FUSED_STAGED);
   }
@@ -388,6 +411,7 @@ class Ops final : public OpsBase {
     a.status = h->totals + 2;
     a.withhold = h->withholdStage ? 1 : 0;
     a.pack = h->fusePack;
+    a.maps = (const StageMaps *)h->dMaps;
     return a;
   }
   size_t fused_args_bytes() const override { return sizeof(FusedArgs<PopT>); }
@@ -409,6 +433,56 @@ class Ops final : public OpsBase {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * warps_of<TY, STG>(), smem);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     return std::max(1, per) * std::max(1, sms);
+  }
+  int build_stage_maps(lbm_sim *h) override {
+    if (!kPipe || h->nx % 16 != 0) return LBM_OK;
+    const auto enc = tensor_map_encoder();
+    if (!enc) return LBM_OK;
+    StageMaps m;
+    memset(&m, 0, sizeof(m));
+    const cuuint64_t nx = h->nx, ny = h->ny, nz = h->nz, pb = sizeof(PopT), rb = sizeof(float);
+    const CUtensorMapDataType popType =
+        sizeof(PopT) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+    bool ok = true;
+    auto map = [&](TensorMap *out, CUtensorMapDataType type, int rank, void *base, const cuuint64_t *dims,
+                   const cuuint64_t *strides, const cuuint32_t *box) {
+      const cuuint32_t unit[5] = {1, 1, 1, 1, 1};
+      ok = ok && enc(reinterpret_cast<CUtensorMap *>(out), type, (cuuint32_t)rank, base, dims, strides, box,
+                     unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    constexpr cuuint32_t TY = TMA_ROWS;
+    // populations: (elements of a block, blocks of a row, y, z); box 4 blocks x TY rows
+    const cuuint64_t b27 = PopGroups<Q27>::BLOCK, b7 = PopGroups<Q7>::BLOCK;
+    const cuuint64_t dF[4] = {b27, nx / 8, ny, nz}, sF[3] = {b27 * pb, nx / 8 * b27 * pb, ny * nx / 8 * b27 * pb};
+    const cuuint64_t dH[4] = {b7, nx / 8, ny, nz}, sH[3] = {b7 * pb, nx / 8 * b7 * pb, ny * nx / 8 * b7 * pb};
+    const cuuint32_t bF[4] = {(cuuint32_t)b27, 4, TY, 1}, bH[4] = {(cuuint32_t)b7, 4, TY, 1};
+    // cell arrays: (x, y, z); box 32 x TY, phi 40 x (TY + 2)
+    const cuuint64_t d3[3] = {nx, ny, nz}, sR[2] = {nx * rb, nx * ny * rb}, sT[2] = {nx, nx * ny};
+    const cuuint32_t bRow[3] = {32, TY, 1}, bPhi[3] = {40, TY + 2, 1};
+    for (int c = 0; c < 2; c++) {
+      map(&m.f[c], popType, 4, h->F[c], dF, sF, bF);
+      map(&m.h[c], popType, 4, h->H[c], dH, sH, bH);
+      map(&m.phi[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, h->mac[c][0], d3, sR, bPhi);
+      map(&m.rho[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, h->mac[c][1], d3, sR, bRow);
+      map(&m.ux[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, h->mac[c][2], d3, sR, bRow);
+      map(&m.uy[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, h->mac[c][3], d3, sR, bRow);
+      map(&m.uz[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, h->mac[c][4], d3, sR, bRow);
+    }
+    map(&m.tag, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->tag, d3, sT, bRow);
+    if (!ok) return LBM_OK;  // no maps: the form runs as the compact one
+    void *d = nullptr;
+    if (cudaMallocAsync(&d, sizeof(StageMaps), h->stream) != cudaSuccess) {
+      cudaGetLastError();
+      return LBM_ERR_OOM;
+    }
+    if (cudaMemcpyAsync(d, &m, sizeof(StageMaps), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+      cudaFreeAsync(d, h->stream);
+      return LBM_ERR_CUDA;
+    }
+    h->dMaps = d;
+    return LBM_OK;
   }
   bool u_in_pads() const override { return Scene<PopT, Real>::UPAD; }
   void u_array(lbm_sim *h, int comp, int half, void *arr, bool toScene) override {
@@ -464,7 +538,8 @@ class Ops final : public OpsBase {
   }
   void warm(int device) override {
     static const int shapes[] = {2, 4, 8, 4 | LBM_FUSED_COMPACT, 6 | LBM_FUSED_COMPACT, 4 | LBM_FUSED_ASYNC,
-                                 6 | LBM_FUSED_ASYNC, 4 | LBM_FUSED_STAGED, 6 | LBM_FUSED_STAGED};
+                                 6 | LBM_FUSED_ASYNC, 4 | LBM_FUSED_STAGED, 6 | LBM_FUSED_STAGED,
+                                 TMA_ROWS | LBM_FUSED_TMA};
     for (int sh : shapes) {
       if (!shape_ok(sh)) continue;
       with_shape(sh, [&](auto T, auto S, auto W) {
@@ -499,7 +574,7 @@ class Ops final : public OpsBase {
 
   void fused_step(lbm_sim *h, const FusedCfg &cfg) override {
     FusedArgs<PopT> a = make_args(h, h->cur, cfg.zchunk);
-    const int shape = cfg.ty | (needs_wide(h->n) ? SHAPE_WIDE : 0);
+    const int shape = resolve_shape(h, cfg.ty) | (needs_wide(h->n) ? SHAPE_WIDE : 0);
     with_shape(shape, [&](auto T, auto S, auto W) {
       launch_fused<decltype(T)::value, decltype(S)::value, decltype(W)::value>(h, a, cfg.zchunk);
     });

@@ -19,7 +19,7 @@ namespace lbm {
 // Launch configuration of the fused step kernel.
 struct FusedCfg {
   int ty = 4;       // tile shape: cell rows per CTA (CTA = 32 x (rows + 2) threads),
-                    // | LBM_FUSED_STAGED for the staged form
+                    // | LBM_FUSED_COMPACT / _ASYNC / _STAGED / _TMA for the compact-ring forms
   int zchunk = 32;  // z planes marched per CTA
 };
 
@@ -101,6 +101,9 @@ class OpsBase {
   virtual void batch_pre(const void *d_small, int n, unsigned retagCtas, unsigned compactCtas,
                          cudaStream_t st) = 0;
   virtual void batch_post(const void *d_small, int n, int redChunks, int maxSpheres, cudaStream_t st) = 0;
+  // the tensor maps of the TMA-staged form (h->dMaps), where the storage
+  // form and the grid allow them (nx a multiple of 16); none otherwise
+  virtual int build_stage_maps(lbm_sim *) { return 0; }
 };
 
 OpsBase *make_ops_f32();
@@ -141,6 +144,7 @@ struct lbm_sim {
   double *impAcc = nullptr;  // per-cell impulse slots of every sphere
   long long impCap = 0;      // doubles
   double *partials = nullptr;
+  void *dMaps = nullptr;    // tensor maps of the TMA-staged form (device memory), or null
   void *meshTri = nullptr;  // a mesh's triangles for lbm_voxelize_mesh / lbm_retag_cells_mesh
   size_t meshCap = 0;
   unsigned *redTickets = nullptr;  // [LBM_MAX_SPHERES] last-block tickets of the impulse reduction
@@ -215,3 +219,13 @@ struct lbm_sim {
   std::vector<cudaEvent_t> evStart, evStop;
   size_t evUsed = 0;
 };
+
+namespace lbm {
+// the tile shape a fused launch of `shape` on this handle uses: the
+// TMA-staged form needs the scene's tensor maps (nx a multiple of 16),
+// otherwise the compact form of the same rows
+inline int resolve_shape(const lbm_sim *h, int shape) {
+  if ((shape & LBM_FUSED_TMA) && !h->dMaps) return shape_rows(shape) | LBM_FUSED_COMPACT | (shape & SHAPE_WIDE);
+  return shape;
+}
+}  // namespace lbm

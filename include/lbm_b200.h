@@ -302,9 +302,9 @@ int lbm_launch_count(const lbm_sim *sim, int64_t *count);
  * (x | y<<8)}, all zero when none. */
 int lbm_checked_build(void);
 int lbm_fault_record(lbm_sim *sim, int64_t out[4]);
-/* Test hook for the bounded waits: while on, the fused kernel's staged form
- * (rows 4 | LBM_FUSED_STAGED) does not issue the first plane copy of
- * each tile, so that plane's wait runs out (about a second), the step is
+/* Test hook for the bounded waits: while on, the fused kernel's staged forms
+ * (rows 4 or 6 | LBM_FUSED_STAGED, 6 | LBM_FUSED_TMA) do not issue the first
+ * plane copy of each tile, so that plane's wait runs out (about a second), the step is
  * abandoned and LBM_ERR_TIMEOUT is reported; the fault record then holds
  * location code 90.  No effect on the other forms. */
 int lbm_test_withhold_stage_copy(lbm_sim *sim, int on);
@@ -330,12 +330,23 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
  *     into shared memory (FP32/FP16/BF16);
  *   rows = 4 or 6 | LBM_FUSED_STAGED: the compact ring, the tile rows of the
  *     next plane staged by bulk asynchronous copies waited on with bounded
- *     mbarrier waits (FP32/FP16/BF16).
+ *     mbarrier waits (FP32/FP16/BF16);
+ *   rows = 6 | LBM_FUSED_TMA: the compact ring, the tile rows of the next
+ *     plane staged by tensor-map (TMA) box copies, one per array, issued by a
+ *     halo warp and waited on with bounded mbarrier waits (FP32/FP16/BF16);
+ *     needs nx a multiple of 16, and a scene without it runs
+ *     6 | LBM_FUSED_COMPACT instead (lbm_get_fused_config reports the shape
+ *     that was set, lbm_get_launch_shape the one that runs).
  * Every shape gives the same results bit for bit. */
 #define LBM_FUSED_STAGED 0x100
 #define LBM_FUSED_COMPACT 0x400
 #define LBM_FUSED_ASYNC 0x800
+#define LBM_FUSED_TMA 0x1000
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
+/* The tile shape the handle's fused launches use: the shape that was set,
+ * or 6 | LBM_FUSED_COMPACT where 6 | LBM_FUSED_TMA was set on a scene whose
+ * nx is not a multiple of 16. */
+int lbm_get_launch_shape(const lbm_sim *sim, int *shape);
 /* ---- one scene in z slabs (several handles, one or more GPUs) -------------- */
 /* Declares the handle a z slab of a larger scene: its local plane k is the
  * scene's plane k + zoff; local planes own_lo .. own_hi (within 1 .. nz - 2)

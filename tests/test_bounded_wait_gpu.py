@@ -1,7 +1,7 @@
 """Bounded device waits of the fused step.
 
-The staged form of the fused kernel (FP16/BF16 storage, tile shape
-4 | LBM_FUSED_STAGED) waits on an mbarrier for each plane's bulk copy.  Every
+The staged forms of the fused kernel (tile shapes 4 | LBM_FUSED_STAGED and
+6 | LBM_FUSED_TMA) wait on an mbarrier for each plane's bulk or tensor copy.  Every
 such wait is bounded: when it runs out the tile stops, the step is abandoned,
 the library returns LBM_ERR_TIMEOUT and the fault record holds location code
 90.  The test makes the wait run out by withholding the copy it waits for
@@ -20,6 +20,7 @@ pytestmark = pytest.mark.gpu
 
 FAULT_STAGE_WAIT = 90
 STAGED = 0x100
+TMA = 0x1000
 
 
 @pytest.fixture(scope="module")
@@ -37,14 +38,16 @@ def _scene(gpu, storage):
     return sim
 
 
-@pytest.mark.parametrize("storage", ["f16", "bf16"])
-def test_withheld_copy_times_out_and_handle_recovers(gpu, storage):
+@pytest.mark.parametrize("storage,shape", [("f16", 4 | STAGED), ("bf16", 4 | STAGED), ("f32", 6 | TMA),
+                                           ("f16", 6 | TMA)])
+def test_withheld_copy_times_out_and_handle_recovers(gpu, storage, shape):
     from b200lbm import _capi
     L = _capi.lib()
     sim = _scene(gpu, storage)
     sim._sync()
     h = sim.handle
-    _capi.check(h, L.lbm_set_fused_config(h, 4 | STAGED, 32))
+    _capi.check(h, L.lbm_set_fused_config(h, shape, 32))
+    assert sim.launch_shape() == shape
     rec = (C.c_int64 * 4)()
     _capi.check(h, L.lbm_fault_record(h, rec))  # clear any earlier record
 
@@ -61,7 +64,7 @@ def test_withheld_copy_times_out_and_handle_recovers(gpu, storage):
     sim.run_coupled(None, 6)
     fresh = _scene(gpu, storage)
     fresh._sync()
-    _capi.check(fresh.handle, L.lbm_set_fused_config(fresh.handle, 4 | STAGED, 32))
+    _capi.check(fresh.handle, L.lbm_set_fused_config(fresh.handle, shape, 32))
     fresh.run_coupled(None, 6)
     for k in ("phi", "rho", "ux", "f", "h"):
         a, b = np.array(getattr(sim, k)), np.array(getattr(fresh, k))

@@ -119,3 +119,95 @@ def test_pipelined_batch_equals_alone(gpu, storage):
         for k in a:
             assert np.array_equal(a[k], b[k]), f"scene {i}: {k} differs"
         assert sa == sb, f"scene {i}: sphere state differs"
+
+
+TMA = 0x1000
+TMA_SHAPES = ((6 | TMA, 32), (6 | TMA, 5), (6 | TMA, 9), (6 | TMA, 1))
+
+
+def _tma16(SimC, SphC):
+    """16 x 22 x 19: one x tile half outside the grid (its last two blocks
+    arrive as zeros), y tiles that do not divide ny, a sphere."""
+    sim = SimC(16, 22, 19)
+    scenes._params(sim, 0.7, 0.75, 0.01, 0.001)
+    sim.initFlat(7.5)
+    return sim, SphC(16, 22, 19, cx=8.2, cy=12.5, cz=9.4, r=3.0, density=2.0)
+
+
+def _tma48(SimC, SphC):
+    """48 x 40 x 36, a falling sphere: two x tiles, the second partial."""
+    sim = SimC(48, 40, 36)
+    scenes._params(sim, 0.8, 0.7, 0.008, 0.0015)
+    sim.initFlat(12)
+    sol = SphC(48, 40, 36, cx=30.5, cy=24.0, cz=17.2, r=5.0, density=2.5)
+    sol.vy = -0.03
+    return sim, sol
+
+
+def _tma64(SimC, SphC):
+    from b200lbm import CompositeSolid
+    sim = SimC(64, 26, 30)
+    scenes._params(sim, 0.8, 0.7, 0.008, 0.0015)
+    sim.initFlat(9)
+    a = SphC(64, 26, 30, cx=20, cy=15, cz=14, r=3.5, density=2.5)
+    b = SphC(64, 26, 30, cx=41, cy=17, cz=16, r=3.0, density=1.8)
+    return sim, CompositeSolid([a, b])
+
+
+TMA_BUILDERS = [_tma16, _tma48, _tma64]
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_tma_equals_plain_alone(gpu, storage):
+    """6 | LBM_FUSED_TMA (tensor-map copies of each plane's tile rows) gives
+    what the plain 4-row form gives, bit for bit, on grids with nx a multiple
+    of 16; on others it runs the compact form (and still agrees)."""
+    SimS = functools.partial(gpu.Sim, storage=storage)
+    for bi, bld in enumerate(TMA_BUILDERS + [_odd]):
+        ref_sim, ref_sol = bld(SimS, gpu.RigidSphere)
+        _set_shape(ref_sim, 4, 32)
+        ref_sim.run_coupled(ref_sol, 9)
+        for _ in range(3):
+            scenes.substep(ref_sim, ref_sol)
+        want = _state(ref_sim, ref_sol)
+        for rows, zchunk in TMA_SHAPES:
+            sim, sol = bld(SimS, gpu.RigidSphere)
+            _set_shape(sim, rows, zchunk)
+            staged = sim.nx % 16 == 0
+            assert sim.launch_shape() == (rows if staged else 6 | COMPACT), (storage, bi)
+            sim.run_coupled(sol, 9)
+            for _ in range(3):
+                scenes.substep(sim, sol)
+            got = _state(sim, sol)
+            for k in want[0]:
+                assert np.array_equal(got[0][k], want[0][k]), (storage, bi, rows, zchunk, k)
+            assert got[1] == want[1], (storage, bi, rows, zchunk)
+            sim.close()
+        ref_sim.close()
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_tma_batch_equals_alone(gpu, storage):
+    """A batch of TMA-capable scenes runs the TMA form; a batch with one scene
+    whose nx is not a multiple of 16 runs the compact form; both equal the
+    scenes run alone."""
+    SimS = functools.partial(gpu.Sim, storage=storage)
+    for builders in (TMA_BUILDERS, TMA_BUILDERS + [_odd]):
+        ref = [bld(SimS, gpu.RigidSphere) for bld in builders]
+        for sim, solid in ref:
+            sim.run_coupled(solid, 8)
+        mixed = [bld(SimS, gpu.RigidSphere) for bld in builders]
+        with gpu.Batch(mixed) as batch:
+            batch.set_config(6 | TMA, 32)
+            batch.run(4)
+            batch.set_config(6 | TMA, 7)
+            batch.run(2, use_graph=False)
+            batch.run(2)
+        for i, ((sim, solid), (rsim, rsolid)) in enumerate(zip(mixed, ref)):
+            a, sa = _state(sim, solid)
+            b, sb = _state(rsim, rsolid)
+            for k in a:
+                assert np.array_equal(a[k], b[k]), f"scene {i}: {k} differs"
+            assert sa == sb, f"scene {i}: sphere state differs"
+        for sim, _ in ref + mixed:
+            sim.close()
