@@ -239,9 +239,10 @@ def run_reference(args, ws, rank):
 def _shape_name(rows, zchunk):
     """'4x32' for the plain form; a suffix names the compact-ring forms:
     'c' register loads, 'a' per-thread async copies, 's' bulk-staged rows,
-    't' tensor-map (TMA) staged rows."""
+    't' tensor-map (TMA) staged rows, 'p' register loads behind tensor
+    prefetches into L2."""
     form = "s" if rows & 0x100 else "c" if rows & 0x400 else "a" if rows & 0x800 else \
-        "t" if rows & 0x1000 else ""
+        "t" if rows & 0x1000 else "p" if rows & 0x2000 else ""
     return f"{rows & 0xff}{form}x{zchunk}"
 
 
@@ -578,7 +579,7 @@ def run_phases(args, dev):
 
 def kernel_name(rows, batch=False):
     """The fused kernel a tile shape launches."""
-    pipe = bool(rows & (0x100 | 0x400 | 0x800 | 0x1000))
+    pipe = bool(rows & (0x100 | 0x400 | 0x800 | 0x1000 | 0x2000))
     return ("k_fused_pipe" if pipe else "k_fused_step" if not batch else "k_fused_batch") + \
         ("_batch" if batch and pipe else "")
 

@@ -20,12 +20,16 @@ import os
 
 # Compact-ring forms (FP32, FP16 and BF16 storage): rows | COMPACT register
 # loads, rows | ASYNC per-thread async copies one plane ahead, rows | STAGED
-# tile rows staged by bulk asynchronous copies.  Plain forms: rows 2, 4, 8.
+# tile rows staged by bulk asynchronous copies, 6 | L2PF register loads behind
+# tensor prefetches into L2 (the compact form where a scene has no tensor
+# maps).  Plain forms: rows 2, 4, 8.
 STAGED = 0x100
 COMPACT = 0x400
 ASYNC = 0x800
+L2PF = 0x2000
 CANDIDATES_F64 = [(4, 32), (4, 16), (8, 16), (8, 32), (2, 32), (4, 64)]
-CANDIDATES = [(6 | COMPACT, 32), (6 | COMPACT, 64), (6 | COMPACT, 128), (6 | ASYNC, 32), (6 | COMPACT, 16),
+CANDIDATES = [(6 | L2PF, 24), (6 | COMPACT, 32), (6 | COMPACT, 64), (6 | COMPACT, 128), (6 | ASYNC, 32),
+              (6 | COMPACT, 16),
               (4, 32), (4, 64), (4, 128), (4, 16), (8, 16), (4 | COMPACT, 32), (6 | STAGED, 32)]
 
 

@@ -547,16 +547,17 @@ class Sim:
 
     def launch_shape(self):
         """The tile shape the fused launches use: the shape set, or
-        6 | LBM_FUSED_COMPACT where 6 | LBM_FUSED_TMA was set on a scene whose
-        nx is not a multiple of 16."""
+        6 | LBM_FUSED_COMPACT where 6 | LBM_FUSED_TMA or 6 | LBM_FUSED_L2PF
+        was set on a scene whose nx is not a multiple of 16."""
         r = C.c_int()
         check(self._h, lib().lbm_get_launch_shape(self._h, C.byref(r)))
         return r.value
 
     def set_fused_config(self, rows, zchunk=32):
         """Fused step launch shape: rows per CTA (2, 4, 8; 4 or 6 | 0x400
-        compact, | 0x800 async, | 0x100 staged; 6 | 0x1000 TMA-staged) and z
-        planes per CTA.  Every shape gives the same bits."""
+        compact, | 0x800 async, | 0x100 staged; 6 | 0x1000 TMA-staged,
+        6 | 0x2000 compact with tensor prefetches into L2) and z planes per
+        CTA.  Every shape gives the same bits."""
         self._sync()
         check(self._h, lib().lbm_set_fused_config(self._h, int(rows), int(zchunk)))
 

@@ -698,10 +698,14 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
   h->ops = ops;
   h->n = (long long)nx * ny * nz;
   h->fusedOK = h->n < (1LL << 31) - 64;  // cell indices are 32-bit in the fused kernel
-  // default launch shape: the compact-ring 6-row form where the storage form
-  // has it (FP32 values in the ring: FP32, FP16, BF16), the plain 4-row form
-  // for FP64
-  if (ops->shape_ok(6 | LBM_FUSED_COMPACT)) h->cfg.ty = 6 | LBM_FUSED_COMPACT;
+  // default launch shape: the compact-ring 6-row form with tensor prefetches
+  // into L2 (the plain compact form where nx is not a multiple of 16) in
+  // z-chunks of 24 planes, where the storage form has it (FP32 values in the
+  // ring: FP32, FP16, BF16); the plain 4-row form for FP64
+  if (ops->shape_ok(6 | LBM_FUSED_L2PF)) {
+    h->cfg.ty = 6 | LBM_FUSED_L2PF;
+    h->cfg.zchunk = 24;
+  }
   h->params = lbm_params{0.6, 0.7, 0.012, 0.0010, 1.0, 0.05, 4.0, 0.02};  // src/sim.js:88-95
   int rc = LBM_OK;
   auto body = [&]() -> int {
@@ -1683,7 +1687,7 @@ int lbm_set_fused_config(lbm_sim *h, int rows, int zchunk) {
   if (!h) return LBM_ERR_ARG;
   if (!h->ops->shape_ok(rows) || zchunk < 1)
     return fail(h, LBM_ERR_ARG,
-                "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA (FP32/FP16/BF16 storage), and zchunk >= 1");
+                "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA or _L2PF (FP32/FP16/BF16 storage), and zchunk >= 1");
   if (h->ops->fused_smem(rows) > 227 * 1024)
     return fail(h, LBM_ERR_ARG, "that row count needs more than 227 KB of shared memory");
   h->cfg.ty = rows;
@@ -1857,8 +1861,9 @@ int batch_tables(lbm_batch *b) {
 // the batch's shape for a launch: SHAPE_WIDE when any scene needs 64-bit
 // population offsets
 int launch_shape(const lbm_batch *b, int rows) {
-  // the TMA-staged form needs every scene's tensor maps (nx a multiple of
-  // 16); otherwise the batch runs the compact form of the same rows
+  // the TMA-staged and L2-prefetch forms need every scene's tensor maps (nx
+  // a multiple of 16); otherwise the batch runs the compact form of the same
+  // rows
   for (lbm_sim *h : b->sims)
     if (resolve_shape(h, rows) != rows) {
       rows = resolve_shape(h, rows);
@@ -1959,7 +1964,7 @@ int lbm_batch_set_config(lbm_batch *b, int rows, int zchunk) {
   if (!b) return LBM_ERR_ARG;
   if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
     return bfail(b, LBM_ERR_ARG,
-                 "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA (FP32/FP16/BF16 storage), and zchunk >= 1");
+                 "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA or _L2PF (FP32/FP16/BF16 storage), and zchunk >= 1");
   b->rows = rows;
   b->zchunk = zchunk;
   return LBM_OK;
@@ -2139,7 +2144,7 @@ int lbm_batch_time_fused(lbm_batch *b, int rows, int zchunk, int reps, double *m
   if (!b || !ms || reps < 1) return LBM_ERR_ARG;
   if (!b->sims[0]->ops->shape_ok(rows) || zchunk < 1)
     return bfail(b, LBM_ERR_ARG,
-                 "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA (FP32/FP16/BF16 storage), and zchunk >= 1");
+                 "rows must be 2, 4 or 8, 4 or 6 | LBM_FUSED_COMPACT, _ASYNC or _STAGED, or 6 | LBM_FUSED_TMA or _L2PF (FP32/FP16/BF16 storage), and zchunk >= 1");
   DeviceGuard g(b->device);
   const int keepRows = b->rows, keepZ = b->zchunk;
   b->rows = rows;

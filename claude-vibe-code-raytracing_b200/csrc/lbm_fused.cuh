@@ -161,6 +161,19 @@ __device__ __forceinline__ void tma_g2s_4d(uint32_t dst, const void *map, int c0
       "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
       : "memory");
 }
+// One box of a tensor map brought into L2 only (no shared memory, no
+// completion to wait for); the same coordinate rules as the copies above,
+// and the parts of the box outside the array are skipped.  No multicast.
+__device__ __forceinline__ void tma_l2_3d(const void *map, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(map), "r"(c0),
+               "r"(c1), "r"(c2)
+               : "memory");
+}
+__device__ __forceinline__ void tma_l2_4d(const void *map, int c0, int c1, int c2, int c3) {
+  asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(map), "r"(c0),
+               "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
 // orders this CTA's earlier shared-memory reads before later copies of the
 // asynchronous proxy into the same bytes
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

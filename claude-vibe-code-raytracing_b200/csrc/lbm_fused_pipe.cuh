@@ -36,6 +36,14 @@
 //         cell warp waits on a load it issued.
 //         Needs nx a multiple of 16 (whole blocks per tile row, 16-byte row
 //         strides of the tags).
+//       - L2PF: the COMPACT loads; in addition, one lane of the halo-row warp
+//         asks the tensor-copy unit, right after the first barrier of plane
+//         q, to bring the tile's rows of plane q + 2 (FP16/BF16: q + 3):
+//         f, h, rho, u, tags, and phi with its halo rows one plane further,
+//         into L2.  Nothing
+//         is staged in shared memory and nothing is waited on: the cell and
+//         halo warps' own loads then find their lines in L2.  Same tensor
+//         maps and coordinates as TMA.
 //
 // Results are bit-identical to fused_tile in every form (the collision is the
 // same collide_cell, the pull sums in the same order).  FP32, FP16 and BF16
@@ -52,6 +60,13 @@ constexpr int PIPE_STAGED = 1;
 constexpr int PIPE_COMPACT = 2;
 constexpr int PIPE_ASYNC = 3;
 constexpr int PIPE_TMA = 4;
+constexpr int PIPE_L2PF = 5;
+// planes ahead of the one being collided that the L2-prefetch form asks for
+// (measured at 256^3: FP32 2 of 1-4, FP16 3)
+template <class PopT>
+constexpr int l2pf_ahead() {
+  return sizeof(PopT) == 4 ? 2 : 3;
+}
 
 // ---------------------------------------------------------------- compact ring
 // Direction k's slot array in one ring copy covers the local columns
@@ -82,19 +97,32 @@ struct PipeRing {
       if (kDir[j][2] == ez) o += S(j);
     return o;
   }
-  // f: e_z = -1 group in 2 copies, e_z = 0 in 2, e_z = +1 in 3; h likewise
+  // Copies of each e_z group, one per plane whose slots may still be read
+  // while the next plane is written.  A plane's e_z = -1 slots are read by
+  // the pulls of the plane below and of itself, its e_z = 0 slots by its own
+  // pull, its e_z = +1 slots by its own pull and the plane above's, its tags
+  // by the pulls of the planes below, at and above it; a barrier separates
+  // the pull of plane q - 2 from the writes of plane q, so 2 / 2 / 3 copies
+  // and 3 tag planes suffice.
+  static constexpr int CM = 2, CZ = 2, CP = 3, CT = 3;
+  // f: e_z = -1 group in CM copies, e_z = 0 in CZ, e_z = +1 in CP; h likewise
   static constexpr int FM = 0;
-  static constexpr int FZ = FM + 2 * grp(27, -1);
-  static constexpr int FP = FZ + 2 * grp(27, 0);
-  static constexpr int HM = FP + 3 * grp(27, 1);
-  static constexpr int HZ = HM + 2 * grp(7, -1);
-  static constexpr int HP = HZ + 2 * grp(7, 0);
-  static constexpr int TOTAL = HP + 3 * grp(7, 1);
+  static constexpr int FZ = FM + CM * grp(27, -1);
+  static constexpr int FP = FZ + CZ * grp(27, 0);
+  static constexpr int HM = FP + CP * grp(27, 1);
+  static constexpr int HZ = HM + CM * grp(7, -1);
+  static constexpr int HP = HZ + CZ * grp(7, 0);
+  static constexpr int TOTAL = HP + CP * grp(7, 1);
   // index of local cell (lx, ly) in direction k's array, without the copy base
   static constexpr int at(int Q, int k, int lx, int ly) {
     return off(Q, k) + (ly - RY0(k)) * W(k) + (lx - CX0(k));
   }
 };
+// copy of plane p in a ring of C copies (p >= -C)
+template <int C>
+__device__ __forceinline__ int ring_copy(int p) {
+  return (int)((unsigned)(p + C) % (unsigned)C);
+}
 
 // ---------------------------------------------------------------- shared memory
 template <class PopT, int TY, int PF>
@@ -102,6 +130,7 @@ struct PipeSmem {
   using Real = typename Prec<PopT>::Real;
   static constexpr bool STG = PF == PIPE_STAGED, ASY = PF == PIPE_ASYNC, TMA = PF == PIPE_TMA;
   using R = PipeRing<TY>;
+  static constexpr int CT = R::CT;  // tag planes
   static constexpr int RX = 34, RY = TY + 2, NC = RX * RY;  // tag planes keep the full halo frame
   // blocks a 32-cell row can span (4 when rows start on a block: TMA)
   static constexpr int SB = TMA ? 4 : 5;
@@ -117,7 +146,7 @@ struct PipeSmem {
   static constexpr size_t lead = TMA ? 128 : 0;  // room to align the base up
   static constexpr size_t ringBytes = (size_t)R::TOTAL * sizeof(Real);
   static constexpr size_t tagOff = ringBytes;
-  static constexpr size_t stF = (tagOff + 3 * NC + AL - 1) / AL * AL;
+  static constexpr size_t stF = (tagOff + CT * NC + AL - 1) / AL * AL;
   static constexpr size_t stH = stF + (size_t)TY * ROWF * sizeof(PopT);
   static constexpr size_t stM = stH + (size_t)TY * ROWH * sizeof(PopT);
   static constexpr size_t stT = stM + (size_t)4 * TY * MROW * sizeof(Real);
@@ -134,7 +163,7 @@ struct PipeSmem {
   // groups of f, [G7][32 TY] groups of h, [11][32 TY] words (phi and its six
   // neighbours, rho, ux, uy, uz)
   static constexpr int NT = 32 * TY, GB = 4 * (int)sizeof(PopT), NS = 11;
-  static constexpr size_t aF = (tagOff + 3 * NC + 15) / 16 * 16;
+  static constexpr size_t aF = (tagOff + CT * NC + 15) / 16 * 16;
   static constexpr size_t aH = aF + (size_t)PopGroups<Q27>::G * NT * GB;
   static constexpr size_t aS = aH + (size_t)PopGroups<Q7>::G * NT * GB;
   // staged: two mbarriers (stage full, stage read) and the abort flag (TMA:
@@ -159,11 +188,12 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   using Real = typename Prec<PopT>::Real;
   using C = Codec<PopT>;
   using SM = PipeSmem<PopT, TY, PF>;
-  constexpr bool STG = SM::STG, ASY = SM::ASY, TMA = SM::TMA;
+  constexpr bool STG = SM::STG, ASY = SM::ASY, TMA = SM::TMA, L2P = PF == PIPE_L2PF;
   using R = PipeRing<TY>;
+  constexpr int CM = R::CM, CZ = R::CZ, CP = R::CP, CT = R::CT;
   using LD = CellLoad<PopT>;
   using CO = CellOut<PopT>;
-  constexpr int RX = SM::RX, NC = SM::NC, TAGS = 3 * NC, RING = R::TOTAL;
+  constexpr int RX = SM::RX, NC = SM::NC, TAGS = CT * NC, RING = R::TOTAL;
   constexpr int G27 = PopGroups<Q27>::G, G7 = PopGroups<Q7>::G;
   constexpr int BLK27 = PopGroups<Q27>::BLOCK, BLK7 = PopGroups<Q7>::BLOCK;
   constexpr int ROWF = SM::ROWF, ROWH = SM::ROWH, MROW = SM::MROW, TROW = SM::TROW, PROW = SM::PROW;
@@ -400,6 +430,22 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     }
   };
 
+  // L2 prefetch of plane P's tile rows (and phi of plane P + 1, rows y0 - 1 ..
+  // y0 + TY), the boxes and coordinates of issue_tma
+  auto prefetch_l2 = [&](int P) __attribute__((always_inline)) {
+    const StageMaps *m = a.maps;
+    tma_l2_4d(&m->f[cur], 0, x0 >> 3, y0, P);
+    tma_l2_4d(&m->h[cur], 0, x0 >> 3, y0, P);
+    tma_l2_3d(&m->rho[cur], x0, y0, P);
+    if constexpr (!UPAD) {
+      tma_l2_3d(&m->ux[cur], x0, y0, P);
+      tma_l2_3d(&m->uy[cur], x0, y0, P);
+    }
+    tma_l2_3d(&m->uz[cur], x0, y0, P);
+    tma_l2_3d(&m->tag, x0, y0, P);
+    tma_l2_3d(&m->phi[cur], x0 - 4, y0 - 1, P + 1);
+  };
+
   // a cell warp's cell of plane q from the stage.  Positions inside the staged
   // rows follow from the rows' first flat indices modulo 16, computed in
   // 32-bit arithmetic (2^32 is a multiple of 16).
@@ -464,12 +510,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
   auto emit = [&](auto MODEc, auto SXc, auto SYc, int sx, int sy, bool active, int q, int lx, int ly,
                   const CO &o) __attribute__((always_inline)) {
     constexpr int MODE = decltype(MODEc)::value, SX = decltype(SXc)::value, SY = decltype(SYc)::value;
-    const int cM = R::FM + (q & 1) * R::grp(27, -1), cZ = R::FZ + (q & 1) * R::grp(27, 0);
-    const int cP = R::FP + (q % 3) * R::grp(27, 1);
-    const int hM = R::HM + (q & 1) * R::grp(7, -1), hZ = R::HZ + (q & 1) * R::grp(7, 0);
-    const int hP = R::HP + (q % 3) * R::grp(7, 1);
+    const int qM = ring_copy<CM>(q), qZ = ring_copy<CZ>(q), qP = ring_copy<CP>(q);
+    const int cM = R::FM + qM * R::grp(27, -1), cZ = R::FZ + qZ * R::grp(27, 0);
+    const int cP = R::FP + qP * R::grp(27, 1);
+    const int hM = R::HM + qM * R::grp(7, -1), hZ = R::HZ + qZ * R::grp(7, 0);
+    const int hP = R::HP + qP * R::grp(7, 1);
     const int lc = (ly + 1) * RX + (lx + 1);
-    if (MODE != 2 || active) stag[sm_at((q % 3) * NC + lc, TAGS, 2)] = (MODE == 1 && SY < 0) ? o.tg2 : o.tg;
+    if (MODE != 2 || active) stag[sm_at(ring_copy<CT>(q) * NC + lc, TAGS, 2)] = (MODE == 1 && SY < 0) ? o.tg2 : o.tg;
     static_for<0, Q27>([&](auto KK) {
       constexpr int k = decltype(KK)::value;
       constexpr int ez = kDir[k][2];
@@ -647,6 +694,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     parity ^= 1u;
     // every warp has pulled plane q - 2 and the cell warps have read the stage
     __syncthreads();
+    if constexpr (L2P) {
+      // plane q + 2 (q + 3) into L2 (the cell warps load plane q + 1 next,
+      // so this has at least a plane and a half to land); planes past the
+      // chunk's last are not needed
+      constexpr int AH = l2pf_ahead<PopT>();
+      if (haloRows && tx == 0 && a.maps && q + AH <= ze) prefetch_l2(q + AH);
+    }
     if constexpr (TMA) {
       // stage q + 1 into the buffers of stage q, which every cell warp read
       // before the barrier above; it lands while plane q is emitted and plane
@@ -678,7 +732,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
 
     // pull plane z = q - 1 (nothing while z < zb)
     const int z = q - 1;
-    const int sC = (z + 3) % 3;
+    const int sC = ring_copy<CT>(z);
     const uint8_t tagI = colActive && z >= zb ? stag[sm_at(sC * NC + own, TAGS, 9)] : TAG_WALL;
     const int i = z * nxny + y * nx + x;
     const POff bF = (POff)(i >> 3) * BLK27 + (i & 7) * 4;
@@ -709,13 +763,15 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     } else if (tagI == TAG_FLUID) {
       // ring copies: group e_z sources come from plane z - e_z; the cell's own
       // (bounce-back) values are in plane z
-      const int sFM = R::FM + ((z + 1) & 1) * R::grp(27, -1), sFZ = R::FZ + (z & 1) * R::grp(27, 0);
-      const int sFP = R::FP + ((z + 2) % 3) * R::grp(27, 1);
-      const int oFM = R::FM + (z & 1) * R::grp(27, -1), oFP = R::FP + (z % 3) * R::grp(27, 1);
-      const int sHM = R::HM + ((z + 1) & 1) * R::grp(7, -1), sHZ = R::HZ + (z & 1) * R::grp(7, 0);
-      const int sHP = R::HP + ((z + 2) % 3) * R::grp(7, 1);
-      const int oHM = R::HM + (z & 1) * R::grp(7, -1), oHP = R::HP + (z % 3) * R::grp(7, 1);
-      const int tbM = ((z + 1) % 3) * NC + own, tbZ = sC * NC + own, tbP = ((z + 2) % 3) * NC + own;
+      const int zMs = ring_copy<CM>(z + 1), zMo = ring_copy<CM>(z), zZ = ring_copy<CZ>(z);
+      const int zPs = ring_copy<CP>(z - 1), zPo = ring_copy<CP>(z);
+      const int sFM = R::FM + zMs * R::grp(27, -1), sFZ = R::FZ + zZ * R::grp(27, 0);
+      const int sFP = R::FP + zPs * R::grp(27, 1);
+      const int oFM = R::FM + zMo * R::grp(27, -1), oFP = R::FP + zPo * R::grp(27, 1);
+      const int sHM = R::HM + zMs * R::grp(7, -1), sHZ = R::HZ + zZ * R::grp(7, 0);
+      const int sHP = R::HP + zPs * R::grp(7, 1);
+      const int oHM = R::HM + zMo * R::grp(7, -1), oHP = R::HP + zPo * R::grp(7, 1);
+      const int tbM = ring_copy<CT>(z + 1) * NC + own, tbZ = sC * NC + own, tbP = ring_copy<CT>(z - 1) * NC + own;
       const Real rhoPhOld = rfma(phC, dRho, rhoG);
       Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
       Real hn[Q7];

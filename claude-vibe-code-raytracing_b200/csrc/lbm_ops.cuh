@@ -337,6 +337,7 @@ class Ops final : public OpsBase {
       case 4 | LBM_FUSED_STAGED: pipe(IC<4>{}, IC<PIPE_STAGED>{}); break;
       case 6 | LBM_FUSED_STAGED: pipe(IC<6>{}, IC<PIPE_STAGED>{}); break;
       case TMA_ROWS | LBM_FUSED_TMA: pipe(IC<TMA_ROWS>{}, IC<PIPE_TMA>{}); break;
+      case TMA_ROWS | LBM_FUSED_L2PF: pipe(IC<TMA_ROWS>{}, IC<PIPE_L2PF>{}); break;
       default: go(IC<8>{}, IC<0>{}); break;
     }
   }
@@ -344,7 +345,7 @@ class Ops final : public OpsBase {
   bool shape_ok(int shape) const override {
     if (shape == 2 || shape == 4 || shape == 8) return true;
     const int rows = shape & 0xff, form = shape & ~0xff;
-    if (form == LBM_FUSED_TMA) return kPipe && rows == TMA_ROWS;
+    if (form == LBM_FUSED_TMA || form == LBM_FUSED_L2PF) return kPipe && rows == TMA_ROWS;
     return kPipe && (rows == 4 || rows == 6) &&
            (form == LBM_FUSED_COMPACT || form == LBM_FUSED_ASYNC || form == LBM_FUSED_STAGED);
   }
@@ -539,7 +540,7 @@ class Ops final : public OpsBase {
   void warm(int device) override {
     static const int shapes[] = {2, 4, 8, 4 | LBM_FUSED_COMPACT, 6 | LBM_FUSED_COMPACT, 4 | LBM_FUSED_ASYNC,
                                  6 | LBM_FUSED_ASYNC, 4 | LBM_FUSED_STAGED, 6 | LBM_FUSED_STAGED,
-                                 TMA_ROWS | LBM_FUSED_TMA};
+                                 TMA_ROWS | LBM_FUSED_TMA, TMA_ROWS | LBM_FUSED_L2PF};
     for (int sh : shapes) {
       if (!shape_ok(sh)) continue;
       with_shape(sh, [&](auto T, auto S, auto W) {

@@ -222,10 +222,11 @@ struct lbm_sim {
 
 namespace lbm {
 // the tile shape a fused launch of `shape` on this handle uses: the
-// TMA-staged form needs the scene's tensor maps (nx a multiple of 16),
-// otherwise the compact form of the same rows
+// TMA-staged and L2-prefetch forms need the scene's tensor maps (nx a
+// multiple of 16), otherwise the compact form of the same rows
 inline int resolve_shape(const lbm_sim *h, int shape) {
-  if ((shape & LBM_FUSED_TMA) && !h->dMaps) return shape_rows(shape) | LBM_FUSED_COMPACT | (shape & SHAPE_WIDE);
+  if ((shape & (LBM_FUSED_TMA | LBM_FUSED_L2PF)) && !h->dMaps)
+    return shape_rows(shape) | LBM_FUSED_COMPACT | (shape & SHAPE_WIDE);
   return shape;
 }
 }  // namespace lbm

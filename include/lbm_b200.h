@@ -323,8 +323,7 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
  *   rows = 2, 4 or 8: the plain form (every storage form);
  *   rows = 4 or 6 | LBM_FUSED_COMPACT: the compact shared-memory ring (each
  *     direction keeps only the cells that can source it) with register loads
- *     of each plane (FP32/FP16/BF16 storage); 6 | LBM_FUSED_COMPACT is the
- *     default for those storage forms;
+ *     of each plane (FP32/FP16/BF16 storage);
  *   rows = 4 or 6 | LBM_FUSED_ASYNC: the compact ring, each thread's loads of
  *     the next plane issued one plane ahead as per-thread asynchronous copies
  *     into shared memory (FP32/FP16/BF16);
@@ -336,16 +335,25 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
  *     halo warp and waited on with bounded mbarrier waits (FP32/FP16/BF16);
  *     needs nx a multiple of 16, and a scene without it runs
  *     6 | LBM_FUSED_COMPACT instead (lbm_get_fused_config reports the shape
- *     that was set, lbm_get_launch_shape the one that runs).
+ *     that was set, lbm_get_launch_shape the one that runs);
+ *   rows = 6 | LBM_FUSED_L2PF: the compact form with register loads, plus
+ *     one lane per CTA that asks the tensor-copy unit, once per plane, to
+ *     bring the tile's rows two planes ahead (three for FP16/BF16) into L2
+ *     (tensor-map prefetches, nothing staged in shared memory, nothing
+ *     waited on), so the cells' loads hit L2; needs nx a multiple of 16, otherwise it runs as
+ *     6 | LBM_FUSED_COMPACT.  6 | LBM_FUSED_L2PF with z-chunks of 24 planes
+ *     is the default for FP32, FP16 and BF16 storage; rows 4, z-chunks of
+ *     32 for FP64.
  * Every shape gives the same results bit for bit. */
 #define LBM_FUSED_STAGED 0x100
 #define LBM_FUSED_COMPACT 0x400
 #define LBM_FUSED_ASYNC 0x800
 #define LBM_FUSED_TMA 0x1000
+#define LBM_FUSED_L2PF 0x2000
 int lbm_set_fused_config(lbm_sim *sim, int rows, int zchunk);
 /* The tile shape the handle's fused launches use: the shape that was set,
- * or 6 | LBM_FUSED_COMPACT where 6 | LBM_FUSED_TMA was set on a scene whose
- * nx is not a multiple of 16. */
+ * or 6 | LBM_FUSED_COMPACT where 6 | LBM_FUSED_TMA or 6 | LBM_FUSED_L2PF was
+ * set on a scene whose nx is not a multiple of 16. */
 int lbm_get_launch_shape(const lbm_sim *sim, int *shape);
 /* ---- one scene in z slabs (several handles, one or more GPUs) -------------- */
 /* Declares the handle a z slab of a larger scene: its local plane k is the

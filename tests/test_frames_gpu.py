@@ -128,3 +128,46 @@ def test_fused_pack_equals_pack(gpu, storage):
             assert np.array_equal(frames[j], want_dev[2 * j + 1]), (storage, hex(rows), "run_coupled", j)
         sim.close()
     ref.close()
+
+
+def _falling48(SimC, SphC):
+    """48 x 21 x 26: nx a multiple of 16 (the tensor-map forms run), the last
+    x tile partial, a sphere moving down through the interface."""
+    sim = SimC(48, 21, 26)
+    scenes._params(sim, 0.7, 0.75, 0.01, 0.001)
+    sim.initFlat(8.5)
+    sol = SphC(48, 21, 26, cx=20.3, cy=12.2, cz=12.7, r=3.6, density=2.5)
+    sol.vy = -0.03
+    return sim, sol
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_fused_pack_tensor_map_forms(gpu, storage):
+    """On a scene with tensor maps, the frame-step instances of the TMA-staged
+    form (6 | 0x1000) and of the L2-prefetch form (6 | 0x2000) write, byte
+    for byte, packVolume after the step, and the fields of plain steps."""
+    import functools
+    SimS = functools.partial(gpu.Sim, storage=storage)
+    ref, rsol = _falling48(SimS, gpu.RigidSphere)
+    _set_shape(ref, 4, 32)
+    want = []
+    for t in range(6):
+        scenes.substep(ref, rsol)
+        want.append(ref.packVolume().copy())
+    for rows, zchunk in ((0x1006, 32), (0x2006, 24), (0x2006, 5), (0x2006, 3)):
+        sim, sol = _falling48(SimS, gpu.RigidSphere)
+        _set_shape(sim, rows, zchunk)
+        assert sim.launch_shape() == rows
+        bufs = [sim.frameBuffer(), sim.frameBuffer()]
+        for t in range(6):
+            out = bufs[t % 2]
+            sim.waitFrames()
+            sim.stepFrame(sol, out)
+            sol.absorbDeadCells(sim)
+            sol.step(1.0, sim.gravity)
+            sim.waitFrames()
+            assert np.array_equal(out, want[t]), (storage, hex(rows), zchunk, t)
+        for k in ("phi", "rho", "f", "h", "tag"):
+            assert np.array_equal(np.asarray(getattr(sim, k)), np.asarray(getattr(ref, k))), (storage, hex(rows), k)
+        sim.close()
+    ref.close()

@@ -122,7 +122,11 @@ def test_pipelined_batch_equals_alone(gpu, storage):
 
 
 TMA = 0x1000
-TMA_SHAPES = ((6 | TMA, 32), (6 | TMA, 5), (6 | TMA, 9), (6 | TMA, 1))
+L2PF = 0x2000
+# the two forms that use the scene's tensor maps: rows staged by tensor copies
+# (TMA) and register loads behind tensor prefetches into L2 (L2PF)
+TMA_SHAPES = ((6 | TMA, 32), (6 | TMA, 5), (6 | TMA, 9), (6 | TMA, 1), (6 | L2PF, 24), (6 | L2PF, 5),
+              (6 | L2PF, 2), (6 | L2PF, 1))
 
 
 def _tma16(SimC, SphC):
@@ -159,9 +163,10 @@ TMA_BUILDERS = [_tma16, _tma48, _tma64]
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
 def test_tma_equals_plain_alone(gpu, storage):
-    """6 | LBM_FUSED_TMA (tensor-map copies of each plane's tile rows) gives
-    what the plain 4-row form gives, bit for bit, on grids with nx a multiple
-    of 16; on others it runs the compact form (and still agrees)."""
+    """6 | LBM_FUSED_TMA (tensor-map copies of each plane's tile rows) and 6 |
+    LBM_FUSED_L2PF (tensor prefetches of the rows two planes ahead into L2)
+    give what the plain 4-row form gives, bit for bit, on grids with nx a
+    multiple of 16; on others they run the compact form (and still agree)."""
     SimS = functools.partial(gpu.Sim, storage=storage)
     for bi, bld in enumerate(TMA_BUILDERS + [_odd]):
         ref_sim, ref_sol = bld(SimS, gpu.RigidSphere)
@@ -186,11 +191,11 @@ def test_tma_equals_plain_alone(gpu, storage):
         ref_sim.close()
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16"])
-def test_tma_batch_equals_alone(gpu, storage):
-    """A batch of TMA-capable scenes runs the TMA form; a batch with one scene
-    whose nx is not a multiple of 16 runs the compact form; both equal the
-    scenes run alone."""
+@pytest.mark.parametrize("storage,form", [("f32", TMA), ("f16", TMA), ("f32", L2PF), ("bf16", L2PF)])
+def test_tma_batch_equals_alone(gpu, storage, form):
+    """A batch of scenes with tensor maps runs the TMA (or L2PF) form; a batch
+    with one scene whose nx is not a multiple of 16 runs the compact form;
+    both equal the scenes run alone."""
     SimS = functools.partial(gpu.Sim, storage=storage)
     for builders in (TMA_BUILDERS, TMA_BUILDERS + [_odd]):
         ref = [bld(SimS, gpu.RigidSphere) for bld in builders]
@@ -198,9 +203,9 @@ def test_tma_batch_equals_alone(gpu, storage):
             sim.run_coupled(solid, 8)
         mixed = [bld(SimS, gpu.RigidSphere) for bld in builders]
         with gpu.Batch(mixed) as batch:
-            batch.set_config(6 | TMA, 32)
+            batch.set_config(6 | form, 32)
             batch.run(4)
-            batch.set_config(6 | TMA, 7)
+            batch.set_config(6 | form, 7)
             batch.run(2, use_graph=False)
             batch.run(2)
         for i, ((sim, solid), (rsim, rsolid)) in enumerate(zip(mixed, ref)):
