@@ -700,11 +700,12 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
   h->fusedOK = h->n < (1LL << 31) - 64;  // cell indices are 32-bit in the fused kernel
   // default launch shape: the compact-ring 6-row form with tensor prefetches
   // into L2 (the plain compact form where nx is not a multiple of 16) in
-  // z-chunks of 24 planes, where the storage form has it (FP32 values in the
-  // ring: FP32, FP16, BF16); the plain 4-row form for FP64
+  // z-chunks of 22 planes (FP32) or 24 (FP16, BF16), the fastest measured at
+  // 256^3, where the storage form has it (FP32 values in the ring); the
+  // plain 4-row form for FP64
   if (ops->shape_ok(6 | LBM_FUSED_L2PF)) {
     h->cfg.ty = 6 | LBM_FUSED_L2PF;
-    h->cfg.zchunk = 24;
+    h->cfg.zchunk = ops->pop_bytes() == 4 ? 22 : 24;
   }
   h->params = lbm_params{0.6, 0.7, 0.012, 0.0010, 1.0, 0.05, 4.0, 0.02};  // src/sim.js:88-95
   int rc = LBM_OK;

@@ -275,8 +275,10 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     const int ci = inside ? q * nxny + gy_ * nx + gx_ : 0;
     const POff bF = (POff)(ci >> 3) * BLK27 + (ci & 7) * 4;
     const POff bH = (POff)(ci >> 3) * BLK7 + (ci & 7) * 4;
-    auto groups = [&](auto QQ, auto NG, const PopT *src, POff base, long long lim, int code,
-                      PopT *dst) __attribute__((always_inline)) {
+    // pad: element Q of the last group (ux for f, uy for h where they sit in
+    // the pads), taken from that group's load where it is made
+    auto groups = [&](auto QQ, auto NG, const PopT *src, POff base, long long lim, int code, PopT *dst,
+                      PopT &pad) __attribute__((always_inline)) {
       constexpr int Q = decltype(QQ)::value;
       static_for<0, decltype(NG)::value>([&](auto GG) {
         constexpr int g = decltype(GG)::value;
@@ -291,11 +293,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
             constexpr int k = decltype(KK)::value;
             dst[k] = t[k & 3];
           });
+          if constexpr (4 * g + 3 == Q) pad = t[3];
         }
       });
     };
-    groups(IC<Q27>{}, IC<G27>{}, Fc, bF, nF, 3, L.fv);
-    groups(IC<Q7>{}, IC<G7>{}, Hc, bH, nH, 4, L.hv);
+    PopT padF = PopT(), padH = PopT();
+    groups(IC<Q27>{}, IC<G27>{}, Fc, bF, nF, 3, L.fv, padF);
+    groups(IC<Q7>{}, IC<G7>{}, Hc, bH, nH, 4, L.hv, padH);
     uint8_t tg = ldg_at(tagA, ci, nCell, 1);
     const int last = (int)nCell - 1;
     L.p = ldg_at(phiC, ci, nCell, 5);
@@ -306,7 +310,11 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
     L.pzp = ldg_at(phiC, min(ci + nxny, last), nCell, 5);
     L.pzm = ldg_at(phiC, max(ci - nxny, 0), nCell, 5);
     L.sumF = ldg_at(rhoC, ci, nCell, 6);
-    if constexpr (UPAD) {
+    if constexpr (UPAD && MODE == 0) {
+      // a tile cell loads every group, the pads included
+      L.ux = (Real)padF;
+      L.uy = (Real)padH;
+    } else if constexpr (UPAD) {
       L.ux = (Real)ldg_at(Fc, (long long)(ci >> 3) * BLK27 + (ci & 7) * 4 + pofs(27), nF, 6);
       L.uy = (Real)ldg_at(Hc, (long long)(ci >> 3) * BLK7 + (ci & 7) * 4 + pofs(7), nH, 6);
     } else {
@@ -868,16 +876,6 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       // macros (src/sim.js:545-576)
       const Real rhoN = rhoA > (Real)0.01 ? rhoA : (Real)0.01;
       const Real p = hsum < (Real)0 ? (Real)0 : hsum > (Real)1 ? (Real)1 : hsum;
-      static_for<0, Q7>([&](auto KK) {
-        constexpr int k = decltype(KK)::value;
-        val4[k & 3] = hn[k];
-        ref4[k & 3] = (Real)D7<k>::w * p;
-        if constexpr ((k & 3) == 3 || k == Q7 - 1) {
-          if constexpr (k == Q7 - 1) val4[3] = ref4[3] = 0;
-          C::enc4(val4, ref4, enc4);
-          st4_at(Hn, bH + pofs(k & ~3), nH, 17, enc4);
-        }
-      });
       const Real one = (Real)1, half = (Real)0.5;
       const Real rhoPhN = rfma(p, dRho, rhoG);
       const Real mu = rfma(-kappa, lapC, rmul(rmul(rmul(beta4, p), rsub(p, one)), rfma((Real)2, p, -one)));
@@ -893,12 +891,26 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         uyn = rmul(uyn, sc);
         uzn = rmul(uzn, sc);
       }
+      // h, the last group's pad holding uy where u sits in the pads (the
+      // FP32 / FP64 codec stores it unchanged), +0 otherwise
+      static_for<0, Q7>([&](auto KK) {
+        constexpr int k = decltype(KK)::value;
+        val4[k & 3] = hn[k];
+        ref4[k & 3] = (Real)D7<k>::w * p;
+        if constexpr ((k & 3) == 3 || k == Q7 - 1) {
+          if constexpr (k == Q7 - 1) {
+            val4[3] = UPAD ? uyn : (Real)0;
+            ref4[3] = 0;
+          }
+          C::enc4(val4, ref4, enc4);
+          st4_at(Hn, bH + pofs(k & ~3), nH, 17, enc4);
+        }
+      });
       st_at(s.rho[nxt], i, nCell, 18, rhoN);
       st_at(s.phi[nxt], i, nCell, 18, p);
       if constexpr (UPAD) {
-        // into the pads of the groups stored above (the same sectors)
+        // into the pad of f's last group, stored above (the same sectors)
         st_at(Fn, bF + pofs(27), nF, 18, (PopT)uxn);
-        st_at(Hn, bH + pofs(7), nH, 18, (PopT)uyn);
       } else {
         st_at(s.ux[nxt], i, nCell, 18, uxn);
         st_at(s.uy[nxt], i, nCell, 18, uyn);

@@ -341,9 +341,9 @@ int lbm_fused_timing_query(lbm_sim *sim, double *total_ms, int64_t *launches);
  *     bring the tile's rows two planes ahead (three for FP16/BF16) into L2
  *     (tensor-map prefetches, nothing staged in shared memory, nothing
  *     waited on), so the cells' loads hit L2; needs nx a multiple of 16, otherwise it runs as
- *     6 | LBM_FUSED_COMPACT.  6 | LBM_FUSED_L2PF with z-chunks of 24 planes
- *     is the default for FP32, FP16 and BF16 storage; rows 4, z-chunks of
- *     32 for FP64.
+ *     6 | LBM_FUSED_COMPACT.  6 | LBM_FUSED_L2PF is the default for FP32
+ *     (z-chunks of 22 planes), FP16 and BF16 (24); rows 4, z-chunks of 32
+ *     for FP64.
  * Every shape gives the same results bit for bit. */
 #define LBM_FUSED_STAGED 0x100
 #define LBM_FUSED_COMPACT 0x400
