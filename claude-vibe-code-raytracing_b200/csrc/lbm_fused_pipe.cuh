@@ -40,10 +40,9 @@
 //         asks the tensor-copy unit, right after the first barrier of plane
 //         q, to bring the tile's rows of plane q + 2 (FP16/BF16: q + 3):
 //         f, h, rho, u, tags, and phi with its halo rows one plane further,
-//         into L2.  Nothing
-//         is staged in shared memory and nothing is waited on: the cell and
-//         halo warps' own loads then find their lines in L2.  Same tensor
-//         maps and coordinates as TMA.
+//         into L2.  Nothing is staged in shared memory and nothing is waited
+//         on: the cell and halo warps' own loads then find their lines in
+//         L2.  Same tensor maps and coordinates as TMA.
 //
 // Results are bit-identical to fused_tile in every form (the collision is the
 // same collide_cell, the pull sums in the same order).  FP32, FP16 and BF16
@@ -784,7 +783,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       Real rhoA = 0, mx = 0, my = 0, mz = 0, hsum = 0;
       Real hn[Q7];
       Real val4[4], ref4[4];
-      PopT enc4[4];
+      PopT enc4[4], lastF[4];
       uint32_t orTags = 0;
       static_for<0, Q27>([&](auto KK) {
         constexpr int k = decltype(KK)::value;
@@ -807,7 +806,13 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         if constexpr ((k & 3) == 3 || k == Q27 - 1) {
           if constexpr (k == Q27 - 1) val4[3] = ref4[3] = 0;  // pad of the last group: encodes to +0
           C::enc4(val4, ref4, enc4);
-          st4_at(Fn, bF + pofs(k & ~3), nF, 15, enc4);
+          if constexpr (UPAD && k == Q27 - 1) {
+            // the last group waits for ux, its pad (stored at once below
+            // where SOLID links rewrite its elements)
+            lastF[0] = enc4[0], lastF[1] = enc4[1], lastF[2] = enc4[2], lastF[3] = enc4[3];
+          } else {
+            st4_at(Fn, bF + pofs(k & ~3), nF, 15, enc4);
+          }
         }
         rhoA += fk;
         if constexpr (ex != 0) mx += (Real)ex * fk;
@@ -827,6 +832,7 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       // momentum exchange (src/sim.js:517-536), directions from a bit mask.
       static_assert(TAG_FLUID == 0 && (TAG_SOLID & TAG_WALL) == 0, "tag bits");
       if (orTags & TAG_SOLID) {
+        if constexpr (UPAD) st4_at(Fn, bF + pofs(Q27 - 3), nF, 15, lastF);  // before the links rewrite it
         uint32_t solidM = 0;
 #pragma unroll 1
         for (int k = 1; k < Q27; k++) {
@@ -909,8 +915,14 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
       st_at(s.rho[nxt], i, nCell, 18, rhoN);
       st_at(s.phi[nxt], i, nCell, 18, p);
       if constexpr (UPAD) {
-        // into the pad of f's last group, stored above (the same sectors)
-        st_at(Fn, bF + pofs(27), nF, 18, (PopT)uxn);
+        // f's last group with ux in its pad (where SOLID links were written,
+        // the group went out above and only the pad remains)
+        if (orTags & TAG_SOLID) {
+          st_at(Fn, bF + pofs(27), nF, 18, (PopT)uxn);
+        } else {
+          lastF[3] = (PopT)uxn;
+          st4_at(Fn, bF + pofs(Q27 - 3), nF, 15, lastF);
+        }
       } else {
         st_at(s.ux[nxt], i, nCell, 18, uxn);
         st_at(s.uy[nxt], i, nCell, 18, uyn);
