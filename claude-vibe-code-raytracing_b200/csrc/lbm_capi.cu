@@ -383,6 +383,39 @@ int fetch_out(lbm_sim *h, const double *d_src, int ns, lbm_impulse *out) {
   return LBM_OK;
 }
 
+// the sphere fields the dead-cell impulses depend on (set_solids copies
+// these; F, T and the mass properties do not enter)
+bool same_sphere_geometry(const lbm_sphere &a, const lbm_sphere &b) {
+  return a.cx == b.cx && a.cy == b.cy && a.cz == b.cz && a.r == b.r && a.vx == b.vx && a.vy == b.vy &&
+         a.vz == b.vz && a.wx == b.wx && a.wy == b.wy && a.wz == b.wz;
+}
+// record the handle's state with a dead-cell result computed ahead
+void dead_ahead_stamp(lbm_sim *h) {
+  auto &A = h->deadAhead;
+  A.launches = h->launches;
+  A.h2d = h->h2dBytes;
+  A.d2h = h->d2hBytes;
+  A.params = h->params;
+  A.cur = h->cur;
+}
+// the result computed ahead, if nothing has moved since and the spheres are
+// the ones it was computed for; consumed either way
+bool dead_ahead_take(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
+  auto &A = h->deadAhead;
+  if (!A.valid) return false;
+  A.valid = false;
+  if (A.ns != ns || A.launches != h->launches || A.h2d != h->h2dBytes || A.d2h != h->d2hBytes ||
+      A.cur != h->cur || memcmp(&A.params, &h->params, sizeof(lbm_params)) != 0)
+    return false;
+  for (int b = 0; b < ns; b++)
+    if (!same_sphere_geometry(A.sp[b], sp[b])) return false;
+  if (out)
+    for (int b = 0; b < ns; b++)
+      out[b] = lbm_impulse{A.out[6 * b + 0], A.out[6 * b + 1], A.out[6 * b + 2],
+                           A.out[6 * b + 3], A.out[6 * b + 4], A.out[6 * b + 5]};
+  return true;
+}
+
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
@@ -394,6 +427,12 @@ struct DeviceGuard {
     cudaGetDevice(&now);
     if (prev >= 0 && now != prev) cudaSetDevice(prev);
   }
+};
+// An entry point's guard on one handle: its device, and any dead-cell result
+// computed ahead is dropped (the call may move the state it was computed on;
+// lbm_step_end computes a new one at its end).
+struct EntryGuard : DeviceGuard {
+  explicit EntryGuard(lbm_sim *h) : DeviceGuard(h->device) { h->deadAhead.valid = false; }
 };
 
 __global__ void k_f32_to_real_d(double *dst, const float *src, long long n) {
@@ -762,7 +801,7 @@ int lbm_create(int nx, int ny, int nz, int storage, int device, lbm_sim **out) {
 
 int lbm_destroy(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_all(h);
   delete h;
@@ -834,7 +873,7 @@ int lbm_upload_field(lbm_sim *h, int field, const void *host, size_t count) {
   if (!h || !host) return fail(h, LBM_ERR_ARG, "null");
   if (field < 0 || field >= LBM_FIELD_COUNT) return fail(h, LBM_ERR_ARG, "unknown field");
   if (count != field_count(h, field)) return fail(h, LBM_ERR_ARG, "element count mismatch");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   const float *src = (const float *)host;
   size_t n = (size_t)h->n;
   switch (field) {
@@ -917,7 +956,7 @@ int lbm_download_field(lbm_sim *h, int field, void *host, size_t count) {
   if (!h || !host) return fail(h, LBM_ERR_ARG, "null");
   if (field < 0 || field >= LBM_FIELD_COUNT) return fail(h, LBM_ERR_ARG, "unknown field");
   if (count != field_count(h, field)) return fail(h, LBM_ERR_ARG, "element count mismatch");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   float *dst = (float *)host;
   size_t n = (size_t)h->n;
   switch (field) {
@@ -966,7 +1005,7 @@ int lbm_download_field_f64(lbm_sim *h, int field, double *host, size_t count) {
   if (field == LBM_FIELD_TAG || field == LBM_FIELD_TAG_PREV)
     return fail(h, LBM_ERR_ARG, "tags are uint8; use lbm_download_field");
   if (count != field_count(h, field)) return fail(h, LBM_ERR_ARG, "element count mismatch");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   size_t n = (size_t)h->n;
   if (field <= LBM_FIELD_H2) {
     bool isH = field == LBM_FIELD_H || field == LBM_FIELD_H2;
@@ -1005,7 +1044,7 @@ int lbm_download_field_f64(lbm_sim *h, int field, double *host, size_t count) {
 
 int lbm_init_flat(lbm_sim *h, double waterlineY) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   std::vector<double> col(h->ny);
   for (int y = 0; y < h->ny; y++) col[y] = 0.5 * (1 + tanh(2 * ((double)y - waterlineY) / h->params.W));
   CK(copy_async(h, h->dPhiCol, col.data(), h->ny * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -1022,7 +1061,7 @@ int lbm_init_flat(lbm_sim *h, double waterlineY) {
 
 int lbm_init_profile(lbm_sim *h, const double *phi_col, int ny) {
   if (!h || !phi_col || ny != h->ny) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   CK(copy_async(h, h->dPhiCol, phi_col, h->ny * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   h->ops->init_flat(h, h->dPhiCol);
   CKL("init_profile");
@@ -1037,7 +1076,7 @@ int lbm_init_profile(lbm_sim *h, const double *phi_col, int ny) {
 
 int lbm_seed_hydrostatic(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   h->ops->seed_hydrostatic(h);
   CKL("seed_hydrostatic");
   CK(cudaStreamSynchronize(h->stream));
@@ -1055,7 +1094,7 @@ int lbm_retag_cells(lbm_sim *h, const lbm_sphere *sp, int ns) {
   if (!h) return LBM_ERR_ARG;
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   if ((rc = need_phases(h))) return rc;
   if ((rc = set_solids(h, sp, ns, false))) return rc;
   if ((rc = upload_plan(h))) return rc;
@@ -1070,7 +1109,7 @@ int lbm_retag_cells(lbm_sim *h, const lbm_sphere *sp, int ns) {
 
 int lbm_retag_cells_mask(lbm_sim *h, const uint8_t *solid_mask, const float *surface_velocity) {
   if (!h || !solid_mask) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   const size_t n = (size_t)h->n;
@@ -1143,7 +1182,7 @@ static int voxelize_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigi
 int lbm_voxelize_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigid_motion *m, uint8_t *mask_out,
                       float *us_out) {
   if (!h || ntri < 0 || (ntri > 0 && !tri) || !m || !mask_out) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   size_t usOff = 0;
   int rc = voxelize_mesh(h, tri, ntri, m, &usOff);
   if (rc) return rc;
@@ -1156,7 +1195,7 @@ int lbm_voxelize_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigid_m
 
 int lbm_retag_cells_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigid_motion *m) {
   if (!h || ntri < 0 || (ntri > 0 && !tri) || !m) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   size_t usOff = 0;
@@ -1172,7 +1211,7 @@ int lbm_retag_cells_mesh(lbm_sim *h, const double *tri, int ntri, const lbm_rigi
 
 int lbm_solid_links(lbm_sim *h, int32_t *cells, int8_t *dirs, double *mom, int cap, int *count) {
   if (!h || !count || cap < 0 || (cap > 0 && (!cells || !dirs || !mom))) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   const long long chunks = (h->n + LINK_CHUNK - 1) / LINK_CHUNK;
@@ -1217,7 +1256,7 @@ int lbm_solid_links(lbm_sim *h, int32_t *cells, int8_t *dirs, double *mom, int c
 
 int lbm_handle_fresh_cells(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   if ((rc = compact_sets(h, h->lastRetagBox))) return rc;
@@ -1228,7 +1267,7 @@ int lbm_handle_fresh_cells(lbm_sim *h) {
 
 int lbm_compute_phi_gradients(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   h->ops->gradients(h);
@@ -1238,7 +1277,7 @@ int lbm_compute_phi_gradients(lbm_sim *h) {
 
 int lbm_collide_phase(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   h->ops->collide_phase(h);
@@ -1248,7 +1287,7 @@ int lbm_collide_phase(lbm_sim *h) {
 
 int lbm_stream_phase(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   h->ops->stream_phase(h);
@@ -1258,7 +1297,7 @@ int lbm_stream_phase(lbm_sim *h) {
 
 int lbm_collide_hydro(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = need_phases(h);
   if (rc) return rc;
   h->ops->collide_hydro(h);
@@ -1270,7 +1309,7 @@ int lbm_stream_hydro_and_macro(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_imp
   if (!h) return LBM_ERR_ARG;
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   if ((rc = need_phases(h))) return rc;
   if ((rc = set_solids(h, sp, ns, true))) return rc;
   if ((rc = upload_plan(h))) return rc;
@@ -1290,7 +1329,7 @@ int lbm_step_begin(lbm_sim *h, const lbm_sphere *sp, int ns) {
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
   if (h->stepBegunNs >= 0) return fail(h, LBM_ERR_STATE, "a step was begun and not ended");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   if (h->bfActive || !h->fusedOK) {
     // A pending external body force is consumed by the phase-by-phase path,
     // which reads it (src/sim.js:434-436, 558-560); grids too large for the
@@ -1331,7 +1370,7 @@ int lbm_step_end(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   if (h->stepBegunNs < 0) return fail(h, LBM_ERR_STATE, "lbm_step_end without lbm_step_begin");
   if (ns != h->stepBegunNs) return fail(h, LBM_ERR_ARG, "lbm_step_end with another sphere count than its begin");
   h->stepBegunNs = -1;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   if (h->bfActive || !h->fusedOK) {
     if ((rc = lbm_compute_phi_gradients(h))) return rc;
     if ((rc = lbm_collide_phase(h))) return rc;
@@ -1345,8 +1384,29 @@ int lbm_step_end(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
   if ((rc = reduce_impulses(h, h->dOut))) return rc;
   h->cur = 1 - h->cur;
   shift_boxes(h, h->stepNow);
-  if ((rc = fetch_out(h, h->dOut, ns, out))) return rc;
-  return watch_after(h, 1);
+  h->deadAhead.valid = false;
+  if (ns > 0 && out && h->listsValid) {
+    // absorbDeadCells follows every step (src/worker.js:96-100) and reads
+    // only the new half and this step's dead list with the same spheres:
+    // run it now on the step's plan and fetch it with the step's impulses,
+    // so lbm_absorb_dead_cells needs no launch and no wait of its own
+    double *d = h->dOut + LBM_MAX_SPHERES * 6;
+    h->ops->absorb_dead(h, d);
+    CKL("absorbDeadCells");
+    CK(copy_async(h, h->hOut + LBM_MAX_SPHERES * 6, d, (size_t)ns * 6 * sizeof(double), cudaMemcpyDeviceToHost,
+                  h->stream));
+    if ((rc = fetch_out(h, h->dOut, ns, out))) return rc;
+    auto &A = h->deadAhead;
+    A.ns = ns;
+    memcpy(A.sp, sp, (size_t)ns * sizeof(lbm_sphere));
+    memcpy(A.out, h->hOut + LBM_MAX_SPHERES * 6, (size_t)ns * 6 * sizeof(double));
+    A.valid = true;
+  } else if ((rc = fetch_out(h, h->dOut, ns, out))) {
+    return rc;
+  }
+  rc = watch_after(h, 1);
+  if (h->deadAhead.valid) dead_ahead_stamp(h);  // the watchdog's scan moves nothing
+  return rc;
 }
 
 int lbm_step(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out) {
@@ -1361,7 +1421,7 @@ int lbm_step_frame(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out, u
     int rc = lbm_step(h, sp, ns, out);
     return rc ? rc : lbm_pack_volume_async(h, host_frame);
   }
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = lbm_step_begin(h, sp, ns);
   if (rc) return rc;
   uint8_t *buf = nullptr;
@@ -1377,6 +1437,7 @@ int lbm_step_frame(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse *out, u
   const int stepRc = rc;
   h->ops->pack_end_planes(h, buf);
   CKL("packVolume (end planes)");
+  if (h->deadAhead.valid) dead_ahead_stamp(h);  // the pack writes the frame only
   // the copy to the host is issued with the next step's fused kernel (or by
   // any wait for frames), so the step's own small read-backs do not queue
   // behind it on the copy engine
@@ -1392,7 +1453,8 @@ int lbm_absorb_dead_cells(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse 
   int rc = check_spheres(h, sp, ns);
   if (rc) return rc;
   if (ns == 0) return LBM_OK;
-  DeviceGuard g(h->device);
+  if (dead_ahead_take(h, sp, ns, out)) return LBM_OK;
+  EntryGuard g(h);
   if (!h->listsValid && (rc = compact_sets(h, h->lastRetagBox))) return rc;
   if ((rc = set_solids(h, sp, ns, false))) return rc;
   if ((rc = upload_plan(h))) return rc;
@@ -1404,7 +1466,7 @@ int lbm_absorb_dead_cells(lbm_sim *h, const lbm_sphere *sp, int ns, lbm_impulse 
 
 int lbm_pack_volume_device(lbm_sim *h, void *dev_out) {
   if (!h || !dev_out) return fail(h, LBM_ERR_ARG, "null");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   h->ops->pack(h, (uint8_t *)dev_out);
   CKL("packVolume");
   return LBM_OK;
@@ -1469,7 +1531,7 @@ int lbm_host_free(void *p) {
 
 int lbm_pack_volume_async(lbm_sim *h, uint8_t *host_out) {
   if (!h || !host_out) return fail(h, LBM_ERR_ARG, "null");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   uint8_t *buf = nullptr;
   int slot = 0;
   int rc = next_frame(h, &buf, &slot);
@@ -1481,7 +1543,7 @@ int lbm_pack_volume_async(lbm_sim *h, uint8_t *host_out) {
 
 int lbm_pack_volume(lbm_sim *h, uint8_t *host_out) {
   if (!h || !host_out) return fail(h, LBM_ERR_ARG, "null");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = ensure_staging(h, (size_t)h->n * 2);
   if (rc) return rc;
   h->ops->pack(h, (uint8_t *)h->staging);
@@ -1495,7 +1557,7 @@ int lbm_render(lbm_sim *h, const lbm_sphere *sphere, const lbm_camera *cam, int 
                uint8_t *host_out) {
   if (!h || !cam || !host_out || width < 1 || height < 1 || (long long)width * height > (1LL << 28))
     return fail(h, LBM_ERR_ARG, "bad render arguments");
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = ensure_staging(h, (size_t)h->n * 2);
   if (rc) return rc;
   const size_t bytes = (size_t)width * height * 4;
@@ -1523,7 +1585,7 @@ int lbm_render(lbm_sim *h, const lbm_sphere *sphere, const lbm_camera *cam, int 
 
 int lbm_run_coupled(lbm_sim *h, lbm_sphere *sp, int ns, int nsteps, int frame_every, uint8_t *frames) {
   if (!h || nsteps < 0) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   CoupledCtx c;
   int rc = coupled_prepare(h, sp, ns, frame_every > 0 && frames, c);
   if (rc) return rc;
@@ -1554,7 +1616,7 @@ int lbm_sphere_step_host(lbm_sphere *spheres, int n, double dt, double gravity, 
 
 int lbm_wait_frames(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = flush_frame_copy(h);
   if (rc) return rc;
   if (h->copyPending) {
@@ -1567,7 +1629,7 @@ int lbm_wait_frames(lbm_sim *h) {
 
 int lbm_wait_frame_slot(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = flush_frame_copy(h);
   if (rc) return rc;
   const int b = h->frameNext;
@@ -1580,7 +1642,7 @@ int lbm_wait_frame_slot(lbm_sim *h) {
 
 int lbm_synchronize(lbm_sim *h) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   int rc = lbm_wait_frames(h);
   if (rc) return rc;
   return sync_status(h);
@@ -1610,7 +1672,7 @@ void *lbm_stream(lbm_sim *h) { return h ? (void *)h->stream : nullptr; }
 
 int lbm_last_sets(lbm_sim *h, int *n_fresh, int *n_dead) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   CK(copy_async(h, h->hTotals, h->totals, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (n_fresh) *n_fresh = h->hTotals[0];
@@ -1623,7 +1685,7 @@ int lbm_download_sets(lbm_sim *h, int32_t *fresh, int cap_fresh, int32_t *dead, 
   int nf = 0, nd = 0;
   int rc = lbm_last_sets(h, &nf, &nd);
   if (rc) return rc;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   if (fresh && cap_fresh > 0 && nf > 0)
     CK(copy_async(h, fresh, h->fresh, std::min(nf, cap_fresh) * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (dead && cap_dead > 0 && nd > 0)
@@ -1648,7 +1710,7 @@ int lbm_checked_build(void) {
 
 int lbm_fault_record(lbm_sim *h, int64_t out[4]) {
   if (!h || !out) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   unsigned long long r[4] = {0, 0, 0, 0};
   CK(h->ops->read_fault(h, r));
   for (int j = 0; j < 4; j++) out[j] = (int64_t)r[j];
@@ -1671,7 +1733,7 @@ int lbm_fused_timing(lbm_sim *h, int enable) {
 
 int lbm_fused_timing_query(lbm_sim *h, double *total_ms, int64_t *launches) {
   if (!h) return LBM_ERR_ARG;
-  DeviceGuard g(h->device);
+  EntryGuard g(h);
   CK(cudaStreamSynchronize(h->stream));
   double tot = 0;
   for (size_t i = 0; i < h->evUsed; i++) {
@@ -1721,6 +1783,7 @@ int lbm_slab_copy_planes(lbm_sim *dst, int dst_plane, const lbm_sim *src, int sr
   if (nplanes == 0) return LBM_OK;
   lbm_sim *h = dst;  // errors are reported on the destination handle
   DeviceGuard g(dst->device);
+  dst->deadAhead.valid = false;
   if (dst->device != src->device) {
     // NVLink peer copies; an already-enabled peer is fine
     cudaError_t pe = cudaDeviceEnablePeerAccess(src->device, 0);
@@ -1983,6 +2046,7 @@ int lbm_batch_run(lbm_batch *b, lbm_sphere *const *spheres, const int *nspheres,
     for (int s = 0; s < n; s++)
       if (!frames[s]) return bfail(b, LBM_ERR_ARG, "frames[" + std::to_string(s) + "] is NULL");
   DeviceGuard g(b->device);
+  for (lbm_sim *sim : b->sims) sim->deadAhead.valid = false;
   OpsBase *ops = b->sims[0]->ops;
   std::vector<CoupledCtx> ctx(n);
   for (int s = 0; s < n; s++)

@@ -214,6 +214,23 @@ struct lbm_sim {
   unsigned long long h2dBytes = 0, d2hBytes = 0;
   std::string err;
 
+  // absorbDeadCells computed by the step that precedes it (lbm_step_end)
+  // and fetched with the step's impulses: the result, the spheres it was
+  // computed for, and the handle's launch and transfer counts, parameters and
+  // current half when it was taken.  lbm_absorb_dead_cells returns it while
+  // all of these still match; anything that moves device state in between
+  // either changes them or clears `valid` itself.
+  struct DeadAhead {
+    bool valid = false;
+    int ns = 0;
+    lbm_sphere sp[LBM_MAX_SPHERES];
+    double out[LBM_MAX_SPHERES * 6];
+    long long launches = 0;
+    unsigned long long h2d = 0, d2h = 0;
+    lbm_params params;
+    int cur = 0;
+  } deadAhead;
+
   // CUDA-event timing of the fused kernel (lbm_fused_timing)
   bool timing = false;
   std::vector<cudaEvent_t> evStart, evStop;

@@ -198,7 +198,12 @@ int lbm_step_end(lbm_sim *sim, const lbm_sphere *spheres, int nspheres, lbm_impu
 
 /* RigidSphere.absorbDeadCells(sim) (src/solid.js:87-101): impulse rho(phi)*u
  * of every cell that turned FLUID -> SOLID at the last retag, summed in scan
- * order in FP64 per owning sphere. */
+ * order in FP64 per owning sphere.  lbm_step / lbm_step_end (fused path)
+ * already compute this sum for the spheres they were given and fetch it with
+ * their own impulses; called next with spheres of the same position, radius
+ * and velocities, this returns that result without a launch or a wait.  Any
+ * other call on the handle in between (or other spheres) makes it compute
+ * anew; the bits are the same either way. */
 int lbm_absorb_dead_cells(lbm_sim *sim, const lbm_sphere *spheres, int nspheres,
                           lbm_impulse *out);
 
