@@ -797,9 +797,15 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         const uint8_t ts = stag[sm_at(tb + so, TAGS, 13)];
         const bool fl = ts == TAG_FLUID;
         // source (tx - ex, ty - ey) in direction k's array; own cell in o's
+#ifdef LBM_CHECKED
         const int si = sbF + r33 + R::at(27, k, -ex, -ey);
         const int oi = obF + r33 + R::at(27, o, 0, 0);
         const Real fk = ring[sm_at(fl ? si : oi, RING, 14)];
+#else
+        const Real fS = ring[sbF + r33 + R::at(27, k, -ex, -ey)];
+        const Real fO = ring[obF + r33 + R::at(27, o, 0, 0)];
+        const Real fk = fl ? fS : fO;
+#endif
         orTags |= ts;
         val4[k & 3] = fk;
         ref4[k & 3] = (Real)D::w;
@@ -821,9 +827,15 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         if constexpr (k < Q7) {
           const int sbH = ez < 0 ? sHM : (ez == 0 ? sHZ : sHP);
           const int obH = oz < 0 ? oHM : (oz == 0 ? sHZ : oHP);
+#ifdef LBM_CHECKED
           const int shi = sbH + r33 + R::at(7, k, -ex, -ey);
           const int ohi = obH + r33 + R::at(7, o, 0, 0);
           const Real hk = ring[sm_at(fl ? shi : ohi, RING, 16)];
+#else
+          const Real hS = ring[sbH + r33 + R::at(7, k, -ex, -ey)];
+          const Real hO = ring[obH + r33 + R::at(7, o, 0, 0)];
+          const Real hk = fl ? hS : hO;
+#endif
           hn[k] = hk;
           hsum += hk;
         }
