@@ -779,8 +779,16 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
         const uint8_t ts = stag[sm_at(tb + so, TAGS, 13)];
         const bool fl = ts == TAG_FLUID;
         // fluid source: its post-collision value; otherwise halfway bounce-back
-        // of the cell's own opposite value (moving-wall term added below)
+        // of the cell's own opposite value (moving-wall term added below).
+        // Both slots are read and the value selected, so each load keeps its
+        // compile-time offset and no address is selected per direction.
+#ifdef LBM_CHECKED
         const Real fk = ring[sm_at(fl ? sbF + slot27(k) * NC + so : obF + slot27(o) * NC, RING, 14)];
+#else
+        const Real fS = ring[sbF + slot27(k) * NC + so];
+        const Real fO = ring[obF + slot27(o) * NC];
+        const Real fk = fl ? fS : fO;
+#endif
         orTags |= ts;
         val4[k & 3] = fk;
         ref4[k & 3] = (Real)D::w;
@@ -797,7 +805,13 @@ __device__ __forceinline__ void fused_tile(const FusedArgs<PopT> &a, int bx, int
           constexpr int hs = (ez == 0 ? k : 0), hso = (oz == 0 ? o : 0);
           const int sbH = ez < 0 ? sbHM : (ez == 0 ? sbHZ : sbHP);
           const int obH = oz < 0 ? obHM : (oz == 0 ? sbHZ : obHP);
+#ifdef LBM_CHECKED
           const Real hk = ring[sm_at(fl ? sbH + hs * NC + so : obH + hso * NC, RING, 16)];
+#else
+          const Real hS = ring[sbH + hs * NC + so];
+          const Real hO = ring[obH + hso * NC];
+          const Real hk = fl ? hS : hO;
+#endif
           hn[k] = hk;
           hsum += hk;
         }

@@ -796,7 +796,9 @@ __device__ __forceinline__ void fused_tile_pipe(const FusedArgs<PopT> &a, int bx
         const int obF = oz < 0 ? oFM : (oz == 0 ? sFZ : oFP);
         const uint8_t ts = stag[sm_at(tb + so, TAGS, 13)];
         const bool fl = ts == TAG_FLUID;
-        // source (tx - ex, ty - ey) in direction k's array; own cell in o's
+        // source (tx - ex, ty - ey) in direction k's array; own cell in o's.
+        // Both are read and the value selected, so each load keeps its
+        // compile-time offset and no address is selected per direction.
 #ifdef LBM_CHECKED
         const int si = sbF + r33 + R::at(27, k, -ex, -ey);
         const int oi = obF + r33 + R::at(27, o, 0, 0);
